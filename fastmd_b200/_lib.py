@@ -1,0 +1,462 @@
+"""ctypes layer over libfastmd_b200.so (include/fastmd.h)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+FMD_FORM_PLAIN_FP64 = 0
+FMD_FORM_MIXED = 1
+FMD_LANGEVIN, FMD_NVT_NH, FMD_NPT_NH = 0, 1, 2
+
+STATUS_NAMES = {
+    0: "OK", 1: "ERR_ARG", 2: "ERR_CONFIG", 3: "ERR_IO", 4: "ERR_CUDA", 5: "ERR_OVERFLOW",
+    6: "ERR_TIMEOUT", 7: "ERR_FAULT", 8: "ERR_CAPACITY", 9: "ERR_NO_DEVICE", 10: "ERR_STATE",
+}
+
+
+class FastMDError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib_path():
+    return os.path.join(_HERE, "lib", "libfastmd_b200.so")
+
+
+class MeltSpec(C.Structure):
+    _fields_ = [
+        ("nchains", C.c_int32), ("chain_length", C.c_int32), ("density", C.c_double), ("seed", C.c_uint64),
+        ("type_block", C.c_int32), ("bond_length", C.c_double), ("min_dist", C.c_double),
+        ("pushoff_steps", C.c_int32), ("pushoff_fcap", C.c_double), ("pushoff_dt", C.c_double),
+    ]
+
+
+class SystemDescC(C.Structure):
+    _fields_ = [
+        ("natoms", C.c_int32), ("ntypes", C.c_int32), ("box_L", C.c_double),
+        ("xyz", C.c_void_p), ("vel", C.c_void_p), ("image", C.c_void_p), ("type", C.c_void_p),
+        ("mol", C.c_void_p), ("mass", C.c_void_p),
+        ("nbonds", C.c_int32), ("bonds", C.c_void_p), ("bond_type", C.c_void_p),
+        ("nangles", C.c_int32), ("angles", C.c_void_p), ("angle_type", C.c_void_p),
+    ]
+
+
+class ThermoRow(C.Structure):
+    _fields_ = [
+        ("step", C.c_int64), ("ke", C.c_double), ("pe", C.c_double), ("temp", C.c_double),
+        ("stress", C.c_double * 6), ("box_L", C.c_double), ("conserved", C.c_double),
+    ]
+
+    def as_array(self):
+        return np.array([self.ke, self.pe, self.temp] + list(self.stress))
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32), ("max_replicas", C.c_int32), ("max_atoms", C.c_int64),
+        ("hbm_budget_gb", C.c_double), ("graph_steps", C.c_int32),
+    ]
+
+
+class ReplicaInfo(C.Structure):
+    _fields_ = [
+        ("slot", C.c_int32), ("natoms", C.c_int32), ("step", C.c_int64), ("nsteps", C.c_int64),
+        ("status_word", C.c_int32), ("active", C.c_int32), ("box_L", C.c_double), ("rebuilds", C.c_int64),
+    ]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("batch", BatchOpts), ("steps_per_round", C.c_int32)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [
+        ("request_id", C.c_int64), ("status", C.c_int32), ("natoms", C.c_int32), ("steps", C.c_int64),
+        ("submit_time", C.c_double), ("start_time", C.c_double), ("finish_time", C.c_double),
+        ("thermo", ThermoRow), ("rg", C.c_double),
+    ]
+
+
+def lib():
+    """Load the shared library; raises if it was not built."""
+    global _LIB
+    if _LIB is None:
+        p = lib_path()
+        if not os.path.exists(p):
+            raise ImportError(f"{p} is missing: build it with `make -C fastmd_b200/csrc` "
+                              "(there is no CPU fallback)")
+        L = C.CDLL(p)
+        L.fmd_version.restype = C.c_char_p
+        L.fmd_last_error.restype = C.c_int32
+        L.fmd_last_error.argtypes = [C.c_char_p, C.c_size_t]
+        _LIB = L
+    return _LIB
+
+
+def _err():
+    buf = C.create_string_buffer(1024)
+    lib().fmd_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def _call(name, *args):
+    fn = getattr(lib(), name)
+    fn.restype = C.c_int32
+    st = fn(*args)
+    if st != 0:
+        raise FastMDError(st, _err())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _c(a, dt):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+@dataclass
+class SystemDesc:
+    """An in-memory system (what a LAMMPS data file carries)."""
+    xyz: np.ndarray
+    box_L: float
+    type: np.ndarray
+    mol: np.ndarray | None = None
+    vel: np.ndarray | None = None
+    image: np.ndarray | None = None
+    mass: np.ndarray | None = None
+    bonds: np.ndarray | None = None
+    bond_type: np.ndarray | None = None
+    angles: np.ndarray | None = None
+    angle_type: np.ndarray | None = None
+    ntypes: int = 0
+
+    def to_c(self):
+        keep = []
+
+        def arr(a, dt):
+            a = _c(a, dt)
+            keep.append(a)
+            return _ptr(a)
+
+        n = len(self.type)
+        d = SystemDescC()
+        d.natoms = n
+        d.ntypes = self.ntypes or (int(np.max(self.type)) + 1 if n else 1)
+        d.box_L = float(self.box_L)
+        d.xyz = arr(np.asarray(self.xyz).reshape(-1), np.float64)
+        d.vel = arr(None if self.vel is None else np.asarray(self.vel).reshape(-1), np.float64)
+        d.image = arr(None if self.image is None else np.asarray(self.image).reshape(-1), np.int32)
+        d.type = arr(self.type, np.int32)
+        d.mol = arr(self.mol, np.int32)
+        d.mass = arr(self.mass, np.float64)
+        nb = 0 if self.bonds is None else len(self.bonds)
+        d.nbonds = nb
+        d.bonds = arr(None if nb == 0 else np.asarray(self.bonds).reshape(-1), np.int32)
+        d.bond_type = arr(None if nb == 0 else (self.bond_type if self.bond_type is not None else np.zeros(nb)),
+                          np.int32)
+        na = 0 if self.angles is None else len(self.angles)
+        d.nangles = na
+        d.angles = arr(None if na == 0 else np.asarray(self.angles).reshape(-1), np.int32)
+        d.angle_type = arr(None if na == 0 else (self.angle_type if self.angle_type is not None else np.zeros(na)),
+                           np.int32)
+        return d, keep
+
+
+def generate_melt(nchains, chain_length, density=0.85, seed=42, type_block=0, bond_length=0.0, min_dist=0.0):
+    """Host-side seeded random-walk melt (no push-off).  Returns a SystemDesc."""
+    spec = MeltSpec(nchains=nchains, chain_length=chain_length, density=density, seed=seed,
+                    type_block=type_block, bond_length=bond_length, min_dist=min_dist)
+    counts = np.zeros(3, np.int32)
+    L = C.c_double()
+    _call("fmd_generate_melt", C.byref(spec), _ptr(counts), C.byref(L), None, None, None, None, None, None)
+    n, nb, na = (int(x) for x in counts)
+    xyz = np.zeros((n, 3))
+    img = np.zeros((n, 3), np.int32)
+    typ = np.zeros(n, np.int32)
+    mol = np.zeros(n, np.int32)
+    bonds = np.zeros((nb, 2), np.int32)
+    angles = np.zeros((na, 3), np.int32)
+    _call("fmd_generate_melt", C.byref(spec), _ptr(counts), C.byref(L), _ptr(xyz), _ptr(img), _ptr(typ), _ptr(mol),
+          _ptr(bonds), _ptr(angles))
+    nt = 2 if type_block > 0 else 1
+    return SystemDesc(xyz=xyz, box_L=L.value, type=typ, mol=mol, image=img, mass=np.ones(nt), bonds=bonds,
+                      bond_type=np.zeros(nb, np.int32), angles=angles, angle_type=np.zeros(na, np.int32), ntypes=nt)
+
+
+def parse_run_conf(text):
+    """Parse run.conf text; returns a dict of the reference's keys."""
+    iout = np.zeros(11, np.int32)
+    fout = np.zeros(9)
+    lj = np.zeros(16 * 16 * 2)
+    bond = np.zeros(4 * 64)
+    angle = np.zeros(2 * 64)
+    seed = C.c_uint64()
+    _call("fmd_parse_run_conf", text.encode(), _ptr(iout), _ptr(fout), _ptr(lj), C.c_int32(len(lj)), _ptr(bond),
+          C.c_int32(len(bond)), _ptr(angle), C.c_int32(len(angle)), C.byref(seed))
+    nt = int(iout[1])
+    return dict(natoms=int(iout[0]), ntypes=nt, nsteps=int(iout[2]), ensemble=int(iout[3]),
+                chain_length=int(iout[4]), thermo_on=int(iout[5]), thermo_freq=int(iout[6]), rg_on=int(iout[7]),
+                rg_freq=int(iout[8]), rc=fout[0], skin=fout[1], dt=fout[2], T_start=fout[3], T_stop=fout[4],
+                Tdamp=fout[5], P_start=fout[6], P_stop=fout[7], Pdamp=fout[8],
+                lj=lj[: nt * nt * 2].reshape(nt, nt, 2).copy(), bond=bond[: 4 * iout[9]].reshape(-1, 4).copy(),
+                angle=angle[: 2 * iout[10]].reshape(-1, 2).copy(), seed=int(seed.value))
+
+
+def read_lammps_data(path):
+    counts = np.zeros(4, np.int32)
+    L = C.c_double()
+    _call("fmd_read_lammps_data", str(path).encode(), _ptr(counts), C.byref(L), *([None] * 10))
+    n, nb, na, nt = (int(x) for x in counts)
+    xyz = np.zeros((n, 3))
+    img = np.zeros((n, 3), np.int32)
+    typ = np.zeros(n, np.int32)
+    mol = np.zeros(n, np.int32)
+    vel = np.zeros((n, 3))
+    bonds = np.zeros((nb, 2), np.int32)
+    btype = np.zeros(nb, np.int32)
+    angles = np.zeros((na, 3), np.int32)
+    atype = np.zeros(na, np.int32)
+    mass = np.zeros(nt)
+    _call("fmd_read_lammps_data", str(path).encode(), _ptr(counts), C.byref(L), _ptr(xyz), _ptr(img), _ptr(typ),
+          _ptr(mol), _ptr(vel), _ptr(bonds), _ptr(btype), _ptr(angles), _ptr(atype), _ptr(mass))
+    return SystemDesc(xyz=xyz, box_L=L.value, type=typ, mol=mol, vel=vel, image=img, mass=mass, bonds=bonds,
+                      bond_type=btype, angles=angles, angle_type=atype, ntypes=nt)
+
+
+def format_thermo_row(row: ThermoRow) -> str:
+    buf = C.create_string_buffer(512)
+    _call("fmd_format_thermo_row", C.byref(row), buf, C.c_size_t(512))
+    return buf.value.decode()
+
+
+def format_rg_row(step: int, rg: float) -> str:
+    buf = C.create_string_buffer(128)
+    _call("fmd_format_rg_row", C.c_int64(step), C.c_double(rg), buf, C.c_size_t(128))
+    return buf.value.decode()
+
+
+def _melt_spec(gen):
+    if gen is None:
+        return None
+    if isinstance(gen, MeltSpec):
+        return gen
+    return MeltSpec(**gen)
+
+
+class Simulation:
+    """One system: ``Simulation(run_conf_text, data_path=... | desc=... | gen=..., form=...)``."""
+
+    def __init__(self, run_conf, data_path=None, desc: SystemDesc | None = None, gen=None,
+                 form=FMD_FORM_MIXED):
+        self._h = C.c_void_p()
+        spec = _melt_spec(gen)
+        dc, self._keep = (desc.to_c() if desc is not None else (None, None))
+        _call("fmd_sim_create", run_conf.encode(), None if data_path is None else str(data_path).encode(),
+              None if dc is None else C.byref(dc), None if spec is None else C.byref(spec), C.c_int32(form),
+              C.byref(self._h))
+        self.form = form
+        n = C.c_int32()
+        nb = C.c_int32()
+        na = C.c_int32()
+        _call("fmd_sim_info", self._h, C.byref(n), C.byref(nb), C.byref(na), None, None)
+        self.natoms, self.nbonds, self.nangles = n.value, nb.value, na.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fmd_sim_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        _call("fmd_step", self._h, C.c_int64(n))
+
+    @property
+    def step_count(self):
+        s = C.c_int64()
+        _call("fmd_sim_info", self._h, None, None, None, C.byref(s), None)
+        return s.value
+
+    @property
+    def box_L(self):
+        L = C.c_double()
+        _call("fmd_sim_info", self._h, None, None, None, None, C.byref(L))
+        return L.value
+
+    def forces(self):
+        f = np.zeros((self.natoms, 3))
+        pe = np.zeros(self.natoms)
+        vir = np.zeros(6)
+        _call("fmd_compute_forces", self._h, _ptr(f), _ptr(pe), _ptr(vir))
+        return f, pe, vir
+
+    def state(self):
+        x = np.zeros((self.natoms, 3))
+        v = np.zeros((self.natoms, 3))
+        img = np.zeros((self.natoms, 3), np.int32)
+        _call("fmd_get_state", self._h, _ptr(x), _ptr(v), _ptr(img))
+        return x, v, img
+
+    def set_state(self, xyz=None, vel=None, image=None):
+        x = _c(None if xyz is None else np.asarray(xyz).reshape(-1), np.float64)
+        v = _c(None if vel is None else np.asarray(vel).reshape(-1), np.float64)
+        i = _c(None if image is None else np.asarray(image).reshape(-1), np.int32)
+        _call("fmd_set_state", self._h, _ptr(x), _ptr(v), _ptr(i))
+
+    def thermo(self) -> ThermoRow:
+        r = ThermoRow()
+        _call("fmd_thermo", self._h, C.byref(r))
+        return r
+
+    def rg(self):
+        r = C.c_double()
+        _call("fmd_rg", self._h, C.byref(r))
+        return r.value
+
+    def pairs(self):
+        n = C.c_int64()
+        _call("fmd_pairs", self._h, None, None, C.c_int64(0), C.byref(n))
+        i = np.zeros(n.value, np.int32)
+        j = np.zeros(n.value, np.int32)
+        _call("fmd_pairs", self._h, _ptr(i), _ptr(j), C.c_int64(n.value), C.byref(n))
+        return i, j
+
+    def counters(self):
+        r = C.c_int64()
+        s = C.c_int32()
+        m = C.c_int32()
+        _call("fmd_sim_counters", self._h, C.byref(r), C.byref(s), C.byref(m))
+        return dict(rebuilds=r.value, status_word=s.value, max_neighbors=m.value)
+
+
+class Batch:
+    """Many replicas advanced together (the mixed form)."""
+
+    def __init__(self, max_replicas=256, max_atoms=0, hbm_budget_gb=150.0, graph_steps=0, device=0):
+        self._h = C.c_void_p()
+        o = BatchOpts(device=device, max_replicas=max_replicas, max_atoms=max_atoms, hbm_budget_gb=hbm_budget_gb,
+                      graph_steps=graph_steps)
+        _call("fmd_batch_create", C.byref(o), C.byref(self._h))
+        self._natoms = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fmd_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, run_conf, data_path=None, desc: SystemDesc | None = None, gen=None):
+        slot = C.c_int32()
+        spec = _melt_spec(gen)
+        dc, keep = (desc.to_c() if desc is not None else (None, None))
+        _call("fmd_batch_add_replica", self._h, run_conf.encode(),
+              None if data_path is None else str(data_path).encode(), None if dc is None else C.byref(dc),
+              None if spec is None else C.byref(spec), C.byref(slot))
+        info = self.info(slot.value)
+        self._natoms[slot.value] = info.natoms
+        return slot.value
+
+    def run(self, nsteps):
+        _call("fmd_batch_run", self._h, C.c_int64(nsteps))
+
+    def retire(self, slot):
+        _call("fmd_batch_retire", self._h, C.c_int32(slot))
+        self._natoms.pop(slot, None)
+
+    def info(self, slot) -> ReplicaInfo:
+        r = ReplicaInfo()
+        _call("fmd_batch_replica_info", self._h, C.c_int32(slot), C.byref(r))
+        return r
+
+    def state(self, slot):
+        n = self._natoms[slot]
+        x = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        img = np.zeros((n, 3), np.int32)
+        _call("fmd_batch_get_state", self._h, C.c_int32(slot), _ptr(x), _ptr(v), _ptr(img))
+        return x, v, img
+
+    def thermo(self, slot) -> ThermoRow:
+        r = ThermoRow()
+        _call("fmd_batch_thermo", self._h, C.c_int32(slot), C.byref(r))
+        return r
+
+    def rg(self, slot):
+        r = C.c_double()
+        _call("fmd_batch_rg", self._h, C.c_int32(slot), C.byref(r))
+        return r.value
+
+    def forces(self, slot):
+        n = self._natoms[slot]
+        f = np.zeros((n, 3))
+        pe = np.zeros(n)
+        vir = np.zeros(6)
+        _call("fmd_batch_compute_forces", self._h, C.c_int32(slot), _ptr(f), _ptr(pe), _ptr(vir))
+        return f, pe, vir
+
+    def totals(self):
+        a = C.c_int32()
+        n = C.c_int64()
+        b = C.c_int64()
+        _call("fmd_batch_totals", self._h, C.byref(a), C.byref(n), C.byref(b))
+        return dict(active=a.value, atoms=n.value, bytes=b.value)
+
+
+class Server:
+    """Continuous-batching request loop on its own host thread."""
+
+    def __init__(self, max_replicas=256, hbm_budget_gb=150.0, steps_per_round=0, graph_steps=0, device=0):
+        self._h = C.c_void_p()
+        o = ServerOpts(batch=BatchOpts(device=device, max_replicas=max_replicas, max_atoms=0,
+                                       hbm_budget_gb=hbm_budget_gb, graph_steps=graph_steps),
+                       steps_per_round=steps_per_round)
+        _call("fmd_server_create", C.byref(o), C.byref(self._h))
+
+    def submit(self, run_conf, gen):
+        rid = C.c_int64()
+        spec = _melt_spec(gen)
+        _call("fmd_server_submit", self._h, run_conf.encode(), C.byref(spec), C.byref(rid))
+        return rid.value
+
+    def poll(self, cap=256):
+        out = (RequestResult * cap)()
+        n = C.c_int32()
+        _call("fmd_server_poll", self._h, out, C.c_int32(cap), C.byref(n))
+        return [out[k] for k in range(n.value)]
+
+    def stats(self):
+        q, r, f, a = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        s = C.c_double()
+        _call("fmd_server_stats", self._h, C.byref(q), C.byref(r), C.byref(f), C.byref(a), C.byref(s))
+        return dict(queued=q.value, running=r.value, finished=f.value, atoms_resident=a.value, atom_steps=s.value)
+
+    def drain(self, timeout_s=600.0):
+        _call("fmd_server_drain", self._h, C.c_double(timeout_s))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fmd_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,269 @@
+// extern "C" entry points of include/fastmd.h for the host helpers and the
+// one-system API.  Every call converts exceptions into a status code.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "engine.h"
+#include "host.h"
+
+namespace fmd {
+const std::string& last_error();
+}
+
+struct fmd_sim {
+  std::unique_ptr<fmd::SimEngine> eng;
+  int32_t form = 0;
+};
+
+namespace {
+
+template <typename F>
+fmd_status guarded(F&& f) {
+  try {
+    f();
+    fmd::set_last_error("");
+    return FMD_OK;
+  } catch (const fmd::Error& e) {
+    fmd::set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    fmd::set_last_error("host out of memory");
+    return FMD_ERR_CAPACITY;
+  } catch (const std::exception& e) {
+    fmd::set_last_error(e.what());
+    return FMD_ERR_ARG;
+  }
+}
+
+void require_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    throw fmd::Error(FMD_ERR_NO_DEVICE, "no CUDA device available");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+FMD_API const char* fmd_version(void) { return "fastmd_b200 0.1.0 (sm_100a)"; }
+
+FMD_API int32_t fmd_last_error(char* buf, size_t len) {
+  const std::string& s = fmd::last_error();
+  if (buf && len > 0) {
+    std::strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int32_t)s.size();
+}
+
+FMD_API fmd_status fmd_device_count(int32_t* n) {
+  return guarded([&] {
+    if (!n) throw fmd::Error(FMD_ERR_ARG, "null");
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+      cudaGetLastError();
+      c = 0;
+    }
+    *n = c;
+  });
+}
+
+FMD_API fmd_status fmd_generate_melt(const fmd_melt_spec* spec, int32_t* counts, double* box_L, double* xyz,
+                                     int32_t* image, int32_t* type, int32_t* mol, int32_t* bonds, int32_t* angles) {
+  return guarded([&] {
+    if (!spec || !counts || !box_L) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    if (!xyz) {
+      const int64_t n = (int64_t)spec->nchains * spec->chain_length;
+      counts[0] = (int32_t)n;
+      counts[1] = spec->nchains * std::max(0, spec->chain_length - 1);
+      counts[2] = spec->nchains * std::max(0, spec->chain_length - 2);
+      *box_L = std::cbrt((double)n / spec->density);
+      return;
+    }
+    fmd::Topology t = fmd::generate_melt(*spec);
+    counts[0] = t.natoms;
+    counts[1] = t.nbonds();
+    counts[2] = t.nangles();
+    *box_L = t.box_L;
+    std::memcpy(xyz, t.xyz.data(), t.xyz.size() * sizeof(double));
+    if (image) std::memcpy(image, t.image.data(), t.image.size() * sizeof(int32_t));
+    if (type) std::memcpy(type, t.type.data(), t.type.size() * sizeof(int32_t));
+    if (mol) std::memcpy(mol, t.mol.data(), t.mol.size() * sizeof(int32_t));
+    if (bonds) std::memcpy(bonds, t.bonds.data(), t.bonds.size() * sizeof(int32_t));
+    if (angles) std::memcpy(angles, t.angles.data(), t.angles.size() * sizeof(int32_t));
+  });
+}
+
+FMD_API fmd_status fmd_parse_run_conf(const char* text, int32_t* iout, double* fout, double* lj, int32_t lj_cap,
+                                      double* bond, int32_t bond_cap, double* angle, int32_t angle_cap,
+                                      uint64_t* seed) {
+  return guarded([&] {
+    if (!text || !iout || !fout) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    fmd::RunConfig c = fmd::parse_run_conf(text);
+    const int32_t iv[11] = {c.natoms,  c.ntypes, (int32_t)c.nsteps, c.ensemble, c.chain_length, c.thermo_on,
+                            c.thermo_freq, c.rg_on, c.rg_freq, (int32_t)c.bond.size(), (int32_t)c.angle.size()};
+    std::memcpy(iout, iv, sizeof(iv));
+    const double fv[9] = {c.rc, c.skin, c.dt, c.T_start, c.T_stop, c.Tdamp, c.P_start, c.P_stop, c.Pdamp};
+    std::memcpy(fout, fv, sizeof(fv));
+    if (lj)
+      for (int k = 0; k < (int)c.lj.size() && k < lj_cap; ++k) lj[k] = c.lj[k];
+    if (bond)
+      for (int k = 0; k < (int)c.bond.size() && 4 * k + 3 < bond_cap; ++k)
+        for (int e = 0; e < 4; ++e) bond[4 * k + e] = c.bond[k][e];
+    if (angle)
+      for (int k = 0; k < (int)c.angle.size() && 2 * k + 1 < angle_cap; ++k)
+        for (int e = 0; e < 2; ++e) angle[2 * k + e] = c.angle[k][e];
+    if (seed) *seed = c.seed;
+  });
+}
+
+FMD_API fmd_status fmd_read_lammps_data(const char* path, int32_t* counts, double* box_L, double* xyz,
+                                        int32_t* image, int32_t* type, int32_t* mol, double* vel, int32_t* bonds,
+                                        int32_t* bond_type, int32_t* angles, int32_t* angle_type, double* masses) {
+  return guarded([&] {
+    if (!path || !counts || !box_L) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    fmd::Topology t = fmd::read_lammps_data(path);
+    counts[0] = t.natoms;
+    counts[1] = t.nbonds();
+    counts[2] = t.nangles();
+    counts[3] = t.ntypes;
+    *box_L = t.box_L;
+    if (!xyz) return;
+    std::memcpy(xyz, t.xyz.data(), t.xyz.size() * sizeof(double));
+    if (image) std::memcpy(image, t.image.data(), t.image.size() * sizeof(int32_t));
+    if (type) std::memcpy(type, t.type.data(), t.type.size() * sizeof(int32_t));
+    if (mol) std::memcpy(mol, t.mol.data(), t.mol.size() * sizeof(int32_t));
+    if (vel) std::memcpy(vel, t.vel.data(), t.vel.size() * sizeof(double));
+    if (bonds) std::memcpy(bonds, t.bonds.data(), t.bonds.size() * sizeof(int32_t));
+    if (bond_type) std::memcpy(bond_type, t.bond_type.data(), t.bond_type.size() * sizeof(int32_t));
+    if (angles) std::memcpy(angles, t.angles.data(), t.angles.size() * sizeof(int32_t));
+    if (angle_type) std::memcpy(angle_type, t.angle_type.data(), t.angle_type.size() * sizeof(int32_t));
+    if (masses) std::memcpy(masses, t.mass.data(), t.mass.size() * sizeof(double));
+  });
+}
+
+FMD_API fmd_status fmd_format_thermo_row(const fmd_thermo_row* r, char* buf, size_t len) {
+  return guarded([&] {
+    if (!r || !buf) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    std::snprintf(buf, len, "%d  %.4f  %.4f  %.4f  %.4f  %.4f  %.4f  %.4f  %.4f  %.4f", (int)r->step, r->ke, r->pe,
+                  r->temp, r->stress[0], r->stress[1], r->stress[2], r->stress[3], r->stress[4], r->stress[5]);
+  });
+}
+
+FMD_API fmd_status fmd_format_rg_row(int64_t step, double rg, char* buf, size_t len) {
+  return guarded([&] {
+    if (!buf) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    std::snprintf(buf, len, "%d  %.4f", (int)step, rg);
+  });
+}
+
+FMD_API fmd_status fmd_sim_create(const char* conf, const char* data_path, const fmd_system_desc* desc,
+                                  const fmd_melt_spec* gen, int32_t form, fmd_sim** out) {
+  return guarded([&] {
+    if (!conf || !out) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    *out = nullptr;
+    fmd::RunConfig cfg = fmd::parse_run_conf(conf);
+    fmd::Topology t = fmd::load_atoms(cfg, data_path, desc, gen);
+    require_device();
+    std::unique_ptr<fmd_sim> s(new fmd_sim());
+    s->form = form;
+    if (form == FMD_FORM_PLAIN_FP64)
+      s->eng = fmd::make_plain_engine(cfg, std::move(t), gen);
+    else if (form == FMD_FORM_MIXED)
+      s->eng = fmd::make_mixed_engine(cfg, std::move(t), gen);
+    else
+      throw fmd::Error(FMD_ERR_ARG, "unknown form");
+    *out = s.release();
+  });
+}
+
+FMD_API fmd_status fmd_sim_destroy(fmd_sim* sim) {
+  return guarded([&] { delete sim; });
+}
+
+#define SIM_CHECK() \
+  if (!sim || !sim->eng) throw fmd::Error(FMD_ERR_ARG, "null simulation handle")
+
+FMD_API fmd_status fmd_sim_info(const fmd_sim* sim, int32_t* natoms, int32_t* nbonds, int32_t* nangles, int64_t* step,
+                                double* box_L) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (natoms) *natoms = sim->eng->natoms();
+    if (nbonds) *nbonds = sim->eng->nbonds();
+    if (nangles) *nangles = sim->eng->nangles();
+    if (step) *step = sim->eng->step_count();
+    if (box_L) *box_L = sim->eng->box_L();
+  });
+}
+
+FMD_API fmd_status fmd_step(fmd_sim* sim, int64_t nsteps) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (nsteps < 0) throw fmd::Error(FMD_ERR_ARG, "nsteps < 0");
+    sim->eng->step(nsteps);
+  });
+}
+
+FMD_API fmd_status fmd_compute_forces(fmd_sim* sim, double* f, double* pe, double* virial) {
+  return guarded([&] {
+    SIM_CHECK();
+    sim->eng->compute_forces(f, pe, virial);
+  });
+}
+
+FMD_API fmd_status fmd_get_state(fmd_sim* sim, double* xyz, double* vel, int32_t* image) {
+  return guarded([&] {
+    SIM_CHECK();
+    sim->eng->get_state(xyz, vel, image);
+  });
+}
+
+FMD_API fmd_status fmd_set_state(fmd_sim* sim, const double* xyz, const double* vel, const int32_t* image) {
+  return guarded([&] {
+    SIM_CHECK();
+    sim->eng->set_state(xyz, vel, image);
+  });
+}
+
+FMD_API fmd_status fmd_thermo(fmd_sim* sim, fmd_thermo_row* row) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (!row) throw fmd::Error(FMD_ERR_ARG, "null row");
+    sim->eng->thermo(row);
+  });
+}
+
+FMD_API fmd_status fmd_rg(fmd_sim* sim, double* rg) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (!rg) throw fmd::Error(FMD_ERR_ARG, "null rg");
+    *rg = sim->eng->rg();
+  });
+}
+
+FMD_API fmd_status fmd_pairs(fmd_sim* sim, int32_t* i, int32_t* j, int64_t cap, int64_t* n) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (!n || (cap > 0 && (!i || !j))) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    *n = sim->eng->pairs(i, j, cap);
+  });
+}
+
+FMD_API fmd_status fmd_sim_counters(const fmd_sim* sim, int64_t* rebuilds, int32_t* status_word, int32_t* max_neighbors) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (rebuilds) *rebuilds = sim->eng->rebuilds();
+    if (status_word) *status_word = sim->eng->status_word();
+    if (max_neighbors) *max_neighbors = sim->eng->max_neighbors();
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,34 @@
+// Engine interface shared by the FP64 plain form and the mixed batched form.
+#pragma once
+#include <memory>
+
+#include "host.h"
+
+namespace fmd {
+
+class SimEngine {
+ public:
+  virtual ~SimEngine() = default;
+  virtual void step(int64_t nsteps) = 0;
+  virtual void compute_forces(double* f, double* pe, double* vir) = 0;
+  virtual void get_state(double* xyz, double* vel, int32_t* image) = 0;
+  virtual void set_state(const double* xyz, const double* vel, const int32_t* image) = 0;
+  virtual void thermo(fmd_thermo_row* row) = 0;
+  virtual double rg() = 0;
+  virtual int64_t pairs(int32_t* pi, int32_t* pj, int64_t cap) = 0;
+  virtual int32_t natoms() const = 0;
+  virtual int32_t nbonds() const = 0;
+  virtual int32_t nangles() const = 0;
+  virtual int64_t step_count() const = 0;
+  virtual double box_L() = 0;
+  virtual int64_t rebuilds() const = 0;
+  virtual int32_t status_word() = 0;
+  virtual int32_t max_neighbors() const = 0;
+};
+
+// FP64 mirror of the reference step loop (one system, host-driven rebuild test).
+std::unique_ptr<SimEngine> make_plain_engine(const RunConfig& cfg, Topology topo, const fmd_melt_spec* pushoff);
+// Mixed-precision engine over a one-replica batch.
+std::unique_ptr<SimEngine> make_mixed_engine(const RunConfig& cfg, Topology topo, const fmd_melt_spec* pushoff);
+
+}  // namespace fmd

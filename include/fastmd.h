@@ -1,0 +1,285 @@
+/*
+ * fastmd_b200 — C ABI for the bead-spring MD per-step path on NVIDIA B200.
+ *
+ * The reference fastMD has two boundaries around this path, and this header
+ * replaces both:
+ *
+ *  1. The process boundary `fastMD <run.conf>` (src/main.cu:24-36): run.conf
+ *     keys (src/io/config.cpp:32-127), LAMMPS data input
+ *     (src/io/lammps_data.cpp:18-229), thermo rows (src/analysis/thermo.cu:80,192)
+ *     and rg rows (src/analysis/rg.cu:95,127-129).  fmd_sim_create() takes the
+ *     same run.conf text and data file; fmd_thermo()/fmd_rg() return the values
+ *     behind the same columns; fmd_format_thermo_row()/fmd_format_rg_row()
+ *     produce the reference's text rows.
+ *
+ *  2. The in-process launchers that take raw device pointers and a stream
+ *     (force/lj.cuh:4-12, force/fene.cuh:11-19, force/angle.cuh:9-15,
+ *     neighbor/verlet_list.cuh:28-30, core/morton.cuh:17-18).  The fmd_launch_*
+ *     entry points below accept the reference's own buffer layouts (float4 with
+ *     the type id bit-cast into .w, int2 bonds, int4 angles, transposed Verlet
+ *     list) so a caller of those launchers can switch one call at a time.
+ *
+ * Conventions (all functions):
+ *  - Every function returns fmd_status; nothing calls exit().  On failure
+ *    fmd_last_error() gives a message (thread-local).
+ *  - Host buffers are caller-owned.  Device memory behind a handle is owned by
+ *    the handle.  fmd_launch_* calls touch only caller-provided device memory
+ *    plus the scratch the call names.
+ *  - A handle is used by one host thread at a time; a server owns its thread.
+ *  - Atom arrays in and out of fmd_sim/fmd_batch are in data-file order
+ *    (the order atoms were given), regardless of the device storage order.
+ */
+#ifndef FASTMD_B200_H
+#define FASTMD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FMD_API __attribute__((visibility("default")))
+#else
+#define FMD_API
+#endif
+
+typedef int32_t fmd_status;
+enum {
+  FMD_OK = 0,
+  FMD_ERR_ARG = 1,       /* bad argument or handle */
+  FMD_ERR_CONFIG = 2,    /* run.conf problem (reference: std::runtime_error, config.cpp:195-210) */
+  FMD_ERR_IO = 3,        /* file or data-file problem (reference: lammps_data.cpp:21-49) */
+  FMD_ERR_CUDA = 4,      /* CUDA runtime error (reference: CUDA_CHECK -> exit, types.cuh:7-15) */
+  FMD_ERR_OVERFLOW = 5,  /* neighbor-list or cell capacity exceeded (reference truncates, verlet_list.cu:215) */
+  FMD_ERR_TIMEOUT = 6,   /* a bounded device-side wait expired */
+  FMD_ERR_FAULT = 7,     /* replica fault: non-finite state or FENE bond past R0 (reference clamps, fene.cu:33) */
+  FMD_ERR_CAPACITY = 8,  /* batch slots or device-memory budget exhausted */
+  FMD_ERR_NO_DEVICE = 9, /* no usable CUDA device */
+  FMD_ERR_STATE = 10     /* call not valid in the current state */
+};
+
+/* Numerical form of a simulation. */
+enum {
+  FMD_FORM_PLAIN_FP64 = 0, /* mirrors the reference kernels and step loop in FP64, one system at a time */
+  FMD_FORM_MIXED = 1       /* FP32 forces on cell-relative positions, FP64 reductions and thermostat
+                              scalars; batched, device-side rebuilds, CUDA-graph step loop */
+};
+
+/* Ensembles (run.conf nvt_langevin / nvt_nh / npt_nh; config.cpp:76-97). */
+enum { FMD_LANGEVIN = 0, FMD_NVT_NH = 1, FMD_NPT_NH = 2 };
+
+/* Seeded Kremer-Grest melt: random-walk chains, then an optional capped-force
+ * Langevin push-off.  All draws come from the library's Philox stream. */
+typedef struct fmd_melt_spec {
+  int32_t nchains;
+  int32_t chain_length;
+  double density;        /* beads per sigma^3; L = cbrt(N / density) */
+  uint64_t seed;
+  int32_t type_block;    /* > 0: types alternate 0,1 in blocks of this many beads along each chain */
+  double bond_length;    /* random-walk step (0 -> 0.97) */
+  double min_dist;       /* reject non-bonded beads closer than this (0 -> 0.8) */
+  int32_t pushoff_steps; /* capped-force Langevin steps run on the device at creation (0 -> none) */
+  double pushoff_fcap;   /* |F| cap per atom during push-off (0 -> 50) */
+  double pushoff_dt;     /* push-off time step (0 -> run.conf dt) */
+} fmd_melt_spec;
+
+/* An in-memory system (what a LAMMPS data file carries). */
+typedef struct fmd_system_desc {
+  int32_t natoms;
+  int32_t ntypes;        /* number of atom types (masses length) */
+  double box_L;          /* cubic box edge; positions wrapped into [0, L) or unwrapped with images */
+  const double* xyz;     /* [3N] */
+  const double* vel;     /* [3N] or NULL (zero) */
+  const int32_t* image;  /* [3N] or NULL (zero) */
+  const int32_t* type;   /* [N] 0-based */
+  const int32_t* mol;    /* [N] molecule ids or NULL (all 1) */
+  const double* mass;    /* [ntypes] or NULL (all 1) */
+  int32_t nbonds;
+  const int32_t* bonds;  /* [2*nbonds] 0-based atom indices */
+  const int32_t* bond_type;  /* [nbonds] 0-based */
+  int32_t nangles;
+  const int32_t* angles;     /* [3*nangles] i, j (vertex), k */
+  const int32_t* angle_type; /* [nangles] */
+} fmd_system_desc;
+
+/* Values behind one thermo row (analysis/thermo.cu:140-195), in FP64.
+ * stress[] is in the reference's emission order xx, xy, xz, yy, yz, zz (the
+ * reference's header labels them Pxx Pyy Pzz Pxy Pxz Pyz). */
+typedef struct fmd_thermo_row {
+  int64_t step;
+  double ke;        /* kinetic energy per atom */
+  double pe;        /* potential energy per atom */
+  double temp;      /* 2/3 KE per atom (no COM correction, thermo.cu:178) */
+  double stress[6];
+  double box_L;
+  double conserved; /* extended energy per atom (thermostat / barostat terms included) */
+} fmd_thermo_row;
+
+typedef struct fmd_sim fmd_sim;
+typedef struct fmd_batch fmd_batch;
+typedef struct fmd_server fmd_server;
+
+/* ---------------------------------------------------------------- library */
+FMD_API const char* fmd_version(void);
+FMD_API int32_t fmd_last_error(char* buf, size_t len);
+FMD_API fmd_status fmd_device_count(int32_t* n);
+
+/* ------------------------------------------------------- host-only helpers */
+/* Generate a melt on the host (no push-off; no GPU needed).  First call with
+ * out arrays NULL to get counts[0..2] = natoms, nbonds, nangles and *box_L. */
+FMD_API fmd_status fmd_generate_melt(const fmd_melt_spec* spec, int32_t* counts, double* box_L,
+                                     double* xyz, int32_t* image, int32_t* type, int32_t* mol,
+                                     int32_t* bonds, int32_t* angles);
+/* Parse run.conf text the way src/io/config.cpp:10-213 does.
+ * iout: natoms, ntypes, nsteps, ensemble, chain_length, thermo_on, thermo_freq,
+ *       rg_on, rg_freq, n_bond_types, n_angle_types
+ * fout: rc, skin, dt, T_start, T_stop, Tdamp, P_start, P_stop, Pdamp
+ * lj[ntypes*ntypes*2], bond[4*n_bond_types], angle[2*n_angle_types] (theta0 in radians). */
+FMD_API fmd_status fmd_parse_run_conf(const char* text, int32_t* iout, double* fout, double* lj,
+                                      int32_t lj_cap, double* bond, int32_t bond_cap, double* angle,
+                                      int32_t angle_cap, uint64_t* seed);
+/* Read a LAMMPS data file (src/io/lammps_data.cpp:18-229).  First call with
+ * xyz == NULL to get counts[0..3] = natoms, nbonds, nangles, ntypes. */
+FMD_API fmd_status fmd_read_lammps_data(const char* path, int32_t* counts, double* box_L, double* xyz,
+                                        int32_t* image, int32_t* type, int32_t* mol, double* vel,
+                                        int32_t* bonds, int32_t* bond_type, int32_t* angles,
+                                        int32_t* angle_type, double* masses);
+/* Reference text rows: "%d  %.4f ..." (thermo.cu:192) and "%d  %.4f" (rg.cu:127). */
+FMD_API fmd_status fmd_format_thermo_row(const fmd_thermo_row* row, char* buf, size_t len);
+FMD_API fmd_status fmd_format_rg_row(int64_t step, double rg, char* buf, size_t len);
+
+/* ---------------------------------------------------------- one simulation */
+/* Exactly one of data_path / desc / gen supplies the atoms.  data_path NULL and
+ * desc NULL and gen NULL: use run.conf's lammps_data_file key. */
+FMD_API fmd_status fmd_sim_create(const char* run_conf_text, const char* data_path,
+                                  const fmd_system_desc* desc, const fmd_melt_spec* gen,
+                                  int32_t form, fmd_sim** out);
+FMD_API fmd_status fmd_sim_destroy(fmd_sim* sim);
+FMD_API fmd_status fmd_sim_info(const fmd_sim* sim, int32_t* natoms, int32_t* nbonds,
+                                int32_t* nangles, int64_t* step, double* box_L);
+/* Advance nsteps (main.cu:403-736 semantics). */
+FMD_API fmd_status fmd_step(fmd_sim* sim, int64_t nsteps);
+/* Forces at the current positions: f[3N], pe[N] (per-atom share, as force.w),
+ * virial[6] (xx,xy,xz,yy,yz,zz).  Any of the outputs may be NULL. */
+FMD_API fmd_status fmd_compute_forces(fmd_sim* sim, double* f, double* pe, double* virial);
+/* Wrapped positions in [0, L), velocities, image flags, in data-file order. */
+FMD_API fmd_status fmd_get_state(fmd_sim* sim, double* xyz, double* vel, int32_t* image);
+FMD_API fmd_status fmd_set_state(fmd_sim* sim, const double* xyz, const double* vel, const int32_t* image);
+FMD_API fmd_status fmd_thermo(fmd_sim* sim, fmd_thermo_row* row);
+FMD_API fmd_status fmd_rg(fmd_sim* sim, double* rg);
+/* Current Verlet pair set (unordered pairs i < j within rc + skin at the last
+ * rebuild, 1-2 bonded pairs excluded), in data-file indices. */
+FMD_API fmd_status fmd_pairs(fmd_sim* sim, int32_t* i, int32_t* j, int64_t cap, int64_t* n);
+/* Counters: rebuilds, device status word, neighbor-list capacity per atom. */
+FMD_API fmd_status fmd_sim_counters(const fmd_sim* sim, int64_t* rebuilds, int32_t* status_word,
+                                    int32_t* max_neighbors);
+
+/* ------------------------------------------------------ batched replicas */
+typedef struct fmd_batch_opts {
+  int32_t device;          /* CUDA device ordinal */
+  int32_t max_replicas;    /* slot count */
+  int64_t max_atoms;       /* total atom capacity (padded); 0 -> sized from budget */
+  double hbm_budget_gb;    /* device-memory budget for the batch (0 -> 150) */
+  int32_t graph_steps;     /* steps captured per CUDA graph launch (0 -> 50) */
+} fmd_batch_opts;
+
+typedef struct fmd_replica_info {
+  int32_t slot;
+  int32_t natoms;
+  int64_t step;
+  int64_t nsteps;          /* run.conf nsteps (target) */
+  int32_t status_word;     /* 0 healthy; bits: 1 overflow, 2 non-finite, 4 FENE overstretch, 8 cell capacity */
+  int32_t active;
+  double box_L;
+  int64_t rebuilds;
+} fmd_replica_info;
+
+FMD_API fmd_status fmd_batch_create(const fmd_batch_opts* opts, fmd_batch** out);
+FMD_API fmd_status fmd_batch_destroy(fmd_batch* b);
+/* Admit a replica (run.conf text plus one atom source); returns its slot.
+ * FMD_ERR_CAPACITY when no slot or memory is free. */
+FMD_API fmd_status fmd_batch_add_replica(fmd_batch* b, const char* run_conf_text, const char* data_path,
+                                         const fmd_system_desc* desc, const fmd_melt_spec* gen,
+                                         int32_t* slot);
+/* Bytes of device memory a replica would take (admission control). */
+FMD_API fmd_status fmd_batch_estimate_bytes(const char* run_conf_text, int32_t natoms, double box_L,
+                                            int64_t* bytes);
+/* Advance every active replica by up to nsteps (a replica stops at its own
+ * run.conf nsteps). */
+FMD_API fmd_status fmd_batch_run(fmd_batch* b, int64_t nsteps);
+FMD_API fmd_status fmd_batch_retire(fmd_batch* b, int32_t slot);
+FMD_API fmd_status fmd_batch_replica_info(fmd_batch* b, int32_t slot, fmd_replica_info* info);
+FMD_API fmd_status fmd_batch_get_state(fmd_batch* b, int32_t slot, double* xyz, double* vel, int32_t* image);
+FMD_API fmd_status fmd_batch_thermo(fmd_batch* b, int32_t slot, fmd_thermo_row* row);
+FMD_API fmd_status fmd_batch_rg(fmd_batch* b, int32_t slot, double* rg);
+FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* f, double* pe, double* virial);
+FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n);
+/* Totals: active replicas, atoms, device bytes in use. */
+FMD_API fmd_status fmd_batch_totals(fmd_batch* b, int32_t* active, int64_t* atoms, int64_t* bytes);
+
+/* ------------------------------------------------------------- serving */
+/* A request loop on its own host thread: submitted requests are admitted as
+ * slots and the device-memory budget allow, advanced together in the batch,
+ * retired when their run.conf nsteps is reached, and their slots back-filled. */
+typedef struct fmd_server_opts {
+  fmd_batch_opts batch;
+  int32_t steps_per_round; /* steps between admission / retirement decisions (0 -> 200) */
+} fmd_server_opts;
+
+typedef struct fmd_request_result {
+  int64_t request_id;
+  fmd_status status;
+  int32_t natoms;
+  int64_t steps;
+  double submit_time;      /* seconds, server clock */
+  double start_time;
+  double finish_time;
+  fmd_thermo_row thermo;   /* final thermo values */
+  double rg;               /* final mean chain Rg */
+} fmd_request_result;
+
+FMD_API fmd_status fmd_server_create(const fmd_server_opts* opts, fmd_server** out);
+FMD_API fmd_status fmd_server_submit(fmd_server* s, const char* run_conf_text, const fmd_melt_spec* gen,
+                                     int64_t* request_id);
+/* Collect up to cap finished results; *n receives the count. */
+FMD_API fmd_status fmd_server_poll(fmd_server* s, fmd_request_result* out, int32_t cap, int32_t* n);
+/* queued, running, finished, atoms resident, atom-steps done. */
+FMD_API fmd_status fmd_server_stats(fmd_server* s, int64_t* queued, int64_t* running, int64_t* finished,
+                                    int64_t* atoms_resident, double* atom_steps);
+FMD_API fmd_status fmd_server_drain(fmd_server* s, double timeout_s);
+FMD_API fmd_status fmd_server_destroy(fmd_server* s);
+
+/* ------------------------------------------- reference-layout launchers */
+/* Cell list + full Verlet list, replacing VerletList::build
+ * (neighbor/verlet_list.cuh:28-30, verlet_list.cu:337-376).  pos is float4
+ * [natoms] with the type id bit-cast into .w; neighbors is the transposed
+ * layout neighbors[k * natoms + i] with max_neighbors rows; exclusions are the
+ * CSR of build_exclusions (lammps_data.cpp:231-253), or NULL.  Unlike the
+ * reference, an overflow is reported (FMD_ERR_OVERFLOW after the stream is
+ * synchronized when sync != 0) instead of truncated silently.
+ * scratch: device memory of fmd_verlet_scratch_bytes() bytes. */
+FMD_API fmd_status fmd_verlet_scratch_bytes(int32_t natoms, float rc_skin, float box_L, size_t* bytes);
+FMD_API fmd_status fmd_launch_verlet_build(const void* pos, int32_t natoms, float box_L,
+                                           const int32_t* exclusion_offsets, const int32_t* exclusion_list,
+                                           float rc_skin, int32_t max_neighbors, int32_t* neighbors,
+                                           int32_t* num_neighbors, void* scratch, size_t scratch_bytes,
+                                           int32_t* overflow_flag, void* stream);
+/* LJ over the transposed list, replacing launch_lj_kernel (force/lj.cuh:4-12;
+ * lj.cu:4-122): force[i] = (F, pe_i) overwritten, virial[6] accumulated. */
+FMD_API fmd_status fmd_launch_lj(const void* pos, void* force, float* virial, const void* lj_params,
+                                 const int32_t* neighbors, const int32_t* num_neighbors, int32_t natoms,
+                                 int32_t ntypes, float rc2, float box_L, float inv_L, void* stream);
+/* 30-bit Morton sort of pos and vel, replacing MortonSorter::sort_and_permute
+ * (core/morton.cuh:17-18; morton.cu:65-85); the permutation is bit-exact with
+ * a stable sort of (key, index).  perm (device, [padded natoms]) receives the
+ * order.  scratch: fmd_morton_scratch_bytes() bytes. */
+FMD_API fmd_status fmd_morton_scratch_bytes(int32_t natoms, size_t* bytes);
+FMD_API fmd_status fmd_launch_morton_sort(void* pos, void* vel, int32_t natoms, float inv_L, int32_t* perm,
+                                          void* scratch, size_t scratch_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTMD_B200_H */
