@@ -1,0 +1,366 @@
+"""Benchmark: aggregate atom-steps/s of the bead-spring MD step on B200.
+
+Workload (one GPU): 64 independent Kremer-Grest melts of 300 chains x 100
+beads (30,000 beads each, density 0.85, L = 32.80), LJ eps = sig = 1,
+rc = 2.5, skin = 0.3, FENE k = 30, R0 = 1.5 with WCA, harmonic angle k = 5,
+theta0 = 180 deg; nvt_langevin T = 1, Tdamp = 1, seed = replica index (+ 1000
+* rank), dt = 0.001.  Each replica is a seeded random-walk melt pushed off for
+2,000 capped-force (|F| <= 50) Langevin steps on the device.  One bench step
+advances every replica by one MD step in the mixed form (FP32 forces on
+cell-relative positions, FP64 reductions), batched in CUDA graphs.  The device
+working set (~1.5 GB) is far larger than L2, so no flush is needed.
+
+Timing: W untimed warm-up steps, then K timed steps on the library's own
+stream with CUDA events, barrier + synchronize on both sides, max over ranks.
+Multi-GPU: one process per GPU, each with its own 64 replicas (weak scaling,
+no data-path collective; the barrier and the max reduction use
+torch.distributed).
+
+Also reported (rank 0, N = 1): the force kernel's roofline from a live
+CUDA-event timing of the kernel alone, the end-to-end rate through the public
+C API (fmd_batch_run in thermo-sized chunks + thermo readout), the FP64 plain
+form on one 30K replica, and the CPU baseline (the FP64 oracle port on the
+host cores, a bounded sample).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s (aggregate over replicas), Kremer-Grest melt, 30K beads per replica"
+NCHAINS, CHAIN_LEN, DENSITY = 300, 100, 0.85
+PUSHOFF = 2000
+
+
+def run_conf(seed, nsteps=10_000_000):
+    return (f"ntypes 1\nrc 2.5\nskin 0.3\ndt 0.001\nnsteps {nsteps}\nnvt_langevin 1.0 1.0 1.0 {seed}\n"
+            "lj 0 0 1.0 1.0\nbond_type 0 30.0 1.5 1.0 1.0\nangle_type 0 5.0 180.0\n")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                line = out.stdout.strip().splitlines()[0]
+                self.samples.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, n in enumerate(names):
+                if len(s) > 5 + k and "Active" in s[5 + k] and "Not" not in s[5 + k]:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        return rank, world, local, dist
+    return 0, 1, 0, None
+
+
+def allmax(dist, value, local):
+    if dist is None:
+        return value
+    import torch
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, local):
+    if dist is None:
+        return
+    import torch
+    if torch.cuda.is_available():
+        dist.barrier(device_ids=[local])
+    else:
+        dist.barrier()
+
+
+# --------------------------------------------------------------------- CPU
+def cpu_oracle_rate(desc, seconds=12.0, threads=None):
+    """FP64 oracle port (OpenMP over the host cores) stepping one 30K replica."""
+    from oracle import pyoracle as po
+    threads = threads or os.cpu_count() or 1
+    s = po.System(xyz=desc["xyz"], L=desc["L"], type=desc["type"], mass=np.ones(1), lj=np.ones((1, 1, 2)),
+                  bonds=desc["bonds"], bond_type=np.zeros(len(desc["bonds"]), np.int32),
+                  fene=np.array([[30.0, 1.5, 1.0, 1.0]]), angles=desc["angles"],
+                  angle_type=np.zeros(len(desc["angles"]), np.int32), angle_p=np.array([[5.0, np.pi]]),
+                  mol=desc["mol"], vel=desc["vel"], image=desc["image"])
+    sim = po.Sim(s, ensemble="langevin", T=(1.0, 1.0, 1.0), seed=1, nsteps=10**7, nthreads=threads)
+    sim.step(2)
+    t0 = time.perf_counter()
+    sim.step(5)
+    per = (time.perf_counter() - t0) / 5
+    nsteps = max(5, int(seconds / max(per, 1e-6)))
+    t0 = time.perf_counter()
+    sim.step(nsteps)
+    dt = time.perf_counter() - t0
+    n = len(desc["type"])
+    return n * nsteps / dt, threads, f"one {n}-bead replica of the workload, {nsteps} steps, FP64 oracle port, " \
+                                    f"{threads} OpenMP threads, {dt:.1f} s"
+
+
+def cpu_state_from_generator(seed):
+    import fastmd_b200 as fm
+    d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=seed)
+    return dict(xyz=d.xyz, L=d.box_L, type=d.type, bonds=d.bonds, angles=d.angles, mol=d.mol,
+                vel=np.zeros_like(d.xyz), image=d.image)
+
+
+def run_reference(args, rank, world, local, dist):
+    """--impl reference: the FP64 CPU oracle port stepping the workload's
+    replica on the host cores (the reference has no CPU stepping path)."""
+    if rank != 0:
+        return
+    from oracle import pyoracle as po
+    desc = cpu_state_from_generator(0)
+    threads = os.cpu_count() or 1
+    s = po.System(xyz=desc["xyz"], L=desc["L"], type=desc["type"], mass=np.ones(1), lj=np.ones((1, 1, 2)),
+                  bonds=desc["bonds"], bond_type=np.zeros(len(desc["bonds"]), np.int32),
+                  fene=np.array([[30.0, 1.5, 1.0, 1.0]]), angles=desc["angles"],
+                  angle_type=np.zeros(len(desc["angles"]), np.int32), angle_p=np.array([[5.0, np.pi]]),
+                  mol=desc["mol"], vel=desc["vel"], image=desc["image"])
+    sim = po.Sim(s, ensemble="langevin", T=(1.0, 1.0, 1.0), seed=1, nsteps=10**7, nthreads=threads,
+                 force_cap=50.0)
+    sim.step(args.warmup)
+    t0 = time.perf_counter()
+    sim.step(args.steps)
+    dt = time.perf_counter() - t0
+    n = len(desc["type"])
+    v = n * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "atom-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random-walk melt)",
+        "config": {"workload": "kg_melt_30k_langevin (one replica of the 64x30K workload per step)",
+                   "beads_per_replica": n, "density": DENSITY, "rc": 2.5, "skin": 0.3, "dt": 0.001},
+        "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"one {n}-bead replica, {args.steps} steps (+{args.warmup} warm-up), "
+                                   "FP64 oracle port (the reference has no CPU stepping path)"},
+        "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------- GPU
+def force_profile_traffic():
+    """Per-launch DRAM bytes of the force kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_force_kg30k_langevin.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch_full_workload:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--replicas", type=int, default=64)
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e / plain / CPU legs")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, world, local, dist = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank, world, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import fastmd_b200 as fm
+
+    R = args.replicas
+    b = fm.Batch(max_replicas=R, max_atoms=R * 30080 + 4096, hbm_budget_gb=150.0, graph_steps=50, device=local)
+    t_setup = time.perf_counter()
+    slots = []
+    for r in range(R):
+        seed = r + 1000 * rank
+        slots.append(b.add(run_conf(seed), gen=dict(nchains=NCHAINS, chain_length=CHAIN_LEN, density=DENSITY,
+                                                    seed=seed, pushoff_steps=PUSHOFF)))
+    t_setup = time.perf_counter() - t_setup
+    natoms = sum(b.info(s).natoms for s in slots)
+    lib = fm.lib()
+
+    # warm-up
+    b.run(args.warmup)
+    barrier(dist, local)
+    with ClockSampler(local) as clk:
+        lib.fmd_batch_mark(b._h, 0)
+        b.run(args.steps)
+        lib.fmd_batch_mark(b._h, 1)
+        import ctypes as C
+        ms = C.c_double()
+        lib.fmd_batch_elapsed_ms(b._h, C.byref(ms))
+    barrier(dist, local)
+    dev_ms = allmax(dist, ms.value, local)
+    total_atoms = allmax(dist, float(natoms), local) * world  # equal per rank
+    value = total_atoms * args.steps / (dev_ms * 1e-3)
+    for s in slots:
+        st = b.info(s).status_word
+        if st != 0:
+            raise SystemExit(f"replica {s} faulted with status {st}")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 forces / f64 reductions",
+        "data": "synthetic (seeded random-walk melts, 2,000-step capped push-off)",
+        "config": {"workload": "kg_melt_64x30k_langevin_batched", "replicas_per_gpu": R,
+                   "beads_per_replica": NCHAINS * CHAIN_LEN, "chains": NCHAINS, "chain_length": CHAIN_LEN,
+                   "density": DENSITY, "rc": 2.5, "skin": 0.3, "dt": 0.001, "ensemble": "nvt_langevin T=1 Tdamp=1",
+                   "form": "mixed (FP32 cell-offset forces, FP64 reductions)", "graph_steps": 50,
+                   "l2": "working set > L2 (no flush needed)", "parallelism": f"replicas x{world} (no collective)"},
+    }
+
+    if rank == 0:
+        line["clocks"] = clk.summary()
+        kps = C.c_int32()
+        lib.fmd_batch_kernels_per_step(b._h, C.byref(kps))
+        line["gpu_launches"] = int(kps.value) * args.steps
+        # ---- roofline of the force kernel
+        entries = C.c_int64()
+        mx = C.c_int32()
+        lib.fmd_batch_list_stats(b._h, C.byref(entries), C.byref(mx))
+        fms = C.c_double()
+        lib.fmd_batch_time_force(b._h, 50, C.byref(fms))
+        per_atom_fixed = 180  # see DESIGN.md: pos_i, pos_j set, force, count, id, bonded topology
+        alg_bytes = natoms * per_atom_fixed + 4 * entries.value
+        achieved = alg_bytes / (fms.value * 1e-3) / 1e9
+        peak, kind = measured_peaks()
+        traffic = force_profile_traffic()
+        line["roofline"] = {"kernel": "k_force (LJ + FENE + angle, gathered)", "bound": "hbm", "achieved": achieved,
+                            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
+                            "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                            "ms_per_launch": fms.value, "mean_neighbors": entries.value / natoms,
+                            "max_neighbors": mx.value}
+        if not args.no_extras:
+            # ---- end to end through the public C API: run in thermo-sized
+            # chunks (100 steps) and read every replica's thermo row.
+            chunk = 100
+            nchunks = max(1, args.steps // chunk)
+            t0 = time.perf_counter()
+            lib.fmd_batch_mark(b._h, 0)
+            rows = 0
+            for _ in range(nchunks):
+                b.run(chunk)
+                for s in slots:
+                    b.thermo(s)
+                    rows += 1
+            lib.fmd_batch_mark(b._h, 1)
+            wall = time.perf_counter() - t0
+            e2e_ms = C.c_double()
+            lib.fmd_batch_elapsed_ms(b._h, C.byref(e2e_ms))
+            e2e_s = max(wall, e2e_ms.value * 1e-3)
+            rep_bytes = 3072 * R  # replica table up + down per run() call
+            line["e2e"] = {"value": natoms * chunk * nchunks / e2e_s, "unit": "atom-steps/s",
+                           "h2d_bytes_per_step": rep_bytes / chunk, "d2h_bytes_per_step": rep_bytes / chunk,
+                           "how": "fmd_batch_run(100) + fmd_batch_thermo for every replica per chunk, wall clock"}
+            # ---- plain FP64 form, one 30K replica at a time (host-driven like the reference)
+            try:
+                x, v, img = b.state(slots[0])
+                d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0)
+                d.xyz, d.vel, d.image = x, v, img
+                ps = fm.Simulation(run_conf(0), desc=d, form=fm.FMD_FORM_PLAIN_FP64)
+                ps.step(20)
+                k = 200
+                t0 = time.perf_counter()
+                ps.step(k)
+                pt = time.perf_counter() - t0
+                line["plain_fp64_one_replica"] = {"value": len(d.type) * k / pt, "unit": "atom-steps/s",
+                                                  "steps": k, "note": "one 30K replica, host wall clock"}
+                line["speedup_vs_plain_fp64"] = value / line["plain_fp64_one_replica"]["value"]
+                ps.close()
+            except Exception as e:  # reported, not fatal
+                line["plain_fp64_one_replica"] = {"error": str(e)}
+            # ---- CPU baseline (FP64 oracle port on the host cores)
+            try:
+                x, v, img = b.state(slots[0])
+                d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0)
+                desc = dict(xyz=x, L=d.box_L, type=d.type, bonds=d.bonds, angles=d.angles, mol=d.mol, vel=v,
+                            image=img)
+                cv, cores, sample = cpu_oracle_rate(desc, seconds=12.0)
+                line["cpu_baseline"] = {"value": cv, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+                                        "sample": sample}
+            except Exception as e:
+                line["cpu_baseline"] = {"error": str(e)}
+        line["setup_s"] = t_setup
+        print(json.dumps(line), flush=True)
+    b.close()
+    if dist is not None:
+        barrier(dist, local)
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,911 @@
+// Host side of the mixed-precision batched engine: admission of replicas into
+// the segmented batch arrays, the CUDA-graph step loop, readout, and the C ABI
+// for batches.  The single-system mixed form (fmd_sim with FMD_FORM_MIXED) is a
+// batch holding one replica.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "batch.h"
+#include "dev_common.cuh"
+#include "engine.h"
+#include "mixed.cuh"
+
+namespace fmd {
+namespace mixed {
+
+// ------------------------------------------------------------- allocator
+int64_t SegAlloc::alloc(int64_t n) {
+  if (n <= 0) n = 1;
+  for (auto it = free_.begin(); it != free_.end(); ++it) {
+    if (it->second >= n) {
+      const int64_t at = it->first;
+      const int64_t rest = it->second - n;
+      free_.erase(it);
+      if (rest > 0) free_[at + n] = rest;
+      used_[at] = n;
+      hwm_ = std::max(hwm_, at + n);
+      return at;
+    }
+  }
+  return -1;
+}
+
+void SegAlloc::release(int64_t at) {
+  auto u = used_.find(at);
+  if (u == used_.end()) return;
+  int64_t start = at, len = u->second;
+  used_.erase(u);
+  auto nx = free_.lower_bound(start);
+  if (nx != free_.end() && nx->first == start + len) {
+    len += nx->second;
+    nx = free_.erase(nx);
+  }
+  if (nx != free_.begin()) {
+    auto pv = std::prev(nx);
+    if (pv->first + pv->second == start) {
+      start = pv->first;
+      len += pv->second;
+      free_.erase(pv);
+    }
+  }
+  free_[start] = len;
+  hwm_ = 0;
+  for (auto& kv : used_) hwm_ = std::max(hwm_, kv.first + kv.second);
+}
+
+// ------------------------------------------------------------- sizing
+static int next_pow2(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+ReplicaPlan plan_replica(const RunConfig& cfg, int32_t natoms, double L) {
+  ReplicaPlan p;
+  const double rcs = cfg.rc + cfg.skin;
+  const double grow = (cfg.ensemble == FMD_NPT_NH) ? 1.3 : 1.0;
+  int G = (int)std::floor(grow * L / (rcs * 1.0001));
+  if (G < 1) G = 1;
+  if (G > kMaxG) throw Error(FMD_ERR_CONFIG, "box too large for the cell grid (more than 512 cells per axis)");
+  p.G_alloc = G;
+  p.P = next_pow2(G);
+  p.ncell = (int64_t)p.P * p.P * p.P;
+  p.slot_cap = ((natoms + 1 + kChunk - 1) / kChunk) * kChunk;
+  p.nchunks = p.slot_cap / kChunk;
+  const double rho = natoms / (L * L * L);
+  const double expect = rho * (4.0 / 3.0) * 3.14159265358979323846 * rcs * rcs * rcs;
+  int M = (int)std::ceil(1.5 * expect + 32.0);
+  M = ((M + 31) / 32) * 32;
+  p.M = std::max(64, M);
+  p.nbr_entries = (int64_t)(p.slot_cap / kTile) * p.M * kTile;
+  return p;
+}
+
+int64_t bytes_per_slot() {
+  return 6 * 16 + 2 * 16 + 7 * 4 + (int64_t)(kNumPartials * 8) / kChunk + 1;
+}
+
+int64_t estimate_bytes(const ReplicaPlan& p, int32_t nbonds, int32_t nangles) {
+  return p.slot_cap * bytes_per_slot() + p.nbr_entries * 4 + p.ncell * 12 + (int64_t)2 * nbonds * 8 +
+         (int64_t)3 * nangles * 16 + (int64_t)sizeof(Rep);
+}
+
+// ------------------------------------------------------------- batch
+Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
+  device_ = o.device;
+  FMD_CUDA(cudaSetDevice(device_));
+  FMD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  graph_steps_ = o.graph_steps > 0 ? o.graph_steps : 50;
+  max_reps_ = o.max_replicas > 0 ? o.max_replicas : 256;
+  BatchCaps c;
+  if (exact) {
+    c = *exact;
+  } else {
+    const double budget = (o.hbm_budget_gb > 0 ? o.hbm_budget_gb : 150.0) * 1e9;
+    int64_t slots = o.max_atoms > 0 ? o.max_atoms : (int64_t)4 << 20;
+    // list entries at ~160 per atom, cells at ~4 per atom (Morton padding), topology at ~3 per atom
+    int64_t per = bytes_per_slot() + 160 * 4 + 4 * 12 + 3 * 16;
+    slots = std::min<int64_t>(slots, (int64_t)(budget / per));
+    slots = ((slots + kChunk - 1) / kChunk) * kChunk;
+    c.slots = slots;
+    c.nbr = slots * 160;
+    c.cells = slots * 4 + 4096;
+    c.bonds = slots * 3;
+    c.angles = slots * 4;
+  }
+  caps_ = c;
+  budget_bytes_ = (int64_t)((o.hbm_budget_gb > 0 ? o.hbm_budget_gb : 150.0) * 1e9);
+  slot_alloc_.reset(c.slots / kChunk);
+  cell_alloc_.reset(c.cells);
+  nbr_alloc_.reset(c.nbr / 1024);  // 1024-entry units
+  bond_alloc_.reset(c.bonds);
+  angle_alloc_.reset(c.angles);
+  const size_t S = (size_t)c.slots;
+  pos_.alloc_zero(S);
+  vel_.alloc_zero(S);
+  force_.alloc_zero(S);
+  ref_.alloc_zero(S);
+  img_.alloc_zero(S);
+  tpos_.alloc(S);
+  timg_.alloc(S);
+  tvel_.alloc(S);
+  key_.alloc(S);
+  perm_.alloc(S);
+  bucket_.alloc(S);
+  slot_of_.alloc_zero(S);
+  boff_.alloc_zero(S);
+  aoff_.alloc_zero(S);
+  ncnt_.alloc_zero(S);
+  part_.alloc_zero(S / kChunk * kNumPartials);
+  cell_cnt_.alloc_zero(c.cells);
+  cell_start_.alloc_zero(c.cells);
+  cell_fill_.alloc_zero(c.cells);
+  bent_.alloc(std::max<int64_t>(1, c.bonds));
+  aent_.alloc(std::max<int64_t>(1, c.angles));
+  nbr_.alloc(c.nbr);
+  reps_.alloc_zero(max_reps_);
+  chunk_rep_.alloc(S / kChunk);
+  h_chunk_rep_.assign(S / kChunk, -1);
+  FMD_CUDA(cudaMemcpy(chunk_rep_, h_chunk_rep_.data(), h_chunk_rep_.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  h_reps_.assign(max_reps_, Rep{});
+  info_.resize(max_reps_);
+  bytes_ = (int64_t)S * bytes_per_slot() + c.nbr * 4 + c.cells * 12 + c.bonds * 8 + c.angles * 16;
+}
+
+Batch::~Batch() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (st_) cudaStreamDestroy(st_);
+}
+
+Dev Batch::dev() const {
+  Dev d;
+  d.reps = reps_;
+  d.chunk_rep = chunk_rep_;
+  d.pos = pos_;
+  d.vel = vel_;
+  d.force = force_;
+  d.ref = ref_;
+  d.img = img_;
+  d.tpos = tpos_;
+  d.timg = timg_;
+  d.tvel = tvel_;
+  d.key = key_;
+  d.perm = perm_;
+  d.bucket = bucket_;
+  d.cell_cnt = cell_cnt_;
+  d.cell_start = cell_start_;
+  d.cell_fill = cell_fill_;
+  d.slot_of = slot_of_;
+  d.boff = boff_;
+  d.aoff = aoff_;
+  d.bent = bent_;
+  d.aent = aent_;
+  d.nbr = nbr_;
+  d.ncnt = ncnt_;
+  d.part = part_;
+  return d;
+}
+
+void Batch::download_reps() {
+  FMD_CUDA(cudaMemcpyAsync(h_reps_.data(), reps_, sizeof(Rep) * max_reps_, cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Batch::upload_reps() {
+  FMD_CUDA(cudaMemcpyAsync(reps_, h_reps_.data(), sizeof(Rep) * max_reps_, cudaMemcpyHostToDevice, st_));
+}
+
+int Batch::nchunks_launch() const { return (int)std::max<int64_t>(1, slot_alloc_.hwm()); }
+int Batch::nreps_launch() const {
+  int m = 0;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used) m = r + 1;
+  return std::max(1, m);
+}
+int Batch::max_cells() const {
+  int64_t m = 1;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used) m = std::max<int64_t>(m, info_[r].plan.ncell);
+  return (int)m;
+}
+
+static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
+  R.ntypes = cfg.ntypes;
+  R.ensemble = cfg.ensemble;
+  R.chain_M = cfg.chain_length;
+  R.max_between = 20;  // main.cu:401
+  R.nsteps = cfg.nsteps;
+  R.seed = cfg.seed;
+  R.dt = cfg.dt;
+  R.rc = cfg.rc;
+  R.skin = cfg.skin;
+  R.T0 = cfg.T_start;
+  R.T1 = cfg.T_stop;
+  R.Tdamp = cfg.Tdamp;
+  R.P0 = cfg.P_start;
+  R.P1 = cfg.P_stop;
+  R.Pdamp = cfg.Pdamp;
+  R.c1 = std::exp(-(1.0 / cfg.Tdamp) * cfg.dt);
+  const double Nf = 3.0 * t.natoms, kT0 = cfg.T_start;
+  R.Q1 = Nf * kT0 * cfg.Tdamp * cfg.Tdamp;
+  R.Qr = kT0 * cfg.Tdamp * cfg.Tdamp;
+  R.W = (Nf + 3.0) * kT0 * cfg.Pdamp * cfg.Pdamp;
+  R.V0 = t.box_L * t.box_L * t.box_L;
+  for (int k = 0; k < kMaxTypes; ++k) R.invm[k] = 1.0f;
+  for (int k = 0; k < cfg.ntypes; ++k) R.invm[k] = (float)(1.0 / t.mass[k]);
+  for (int a = 0; a < cfg.ntypes; ++a)
+    for (int b = 0; b < cfg.ntypes; ++b) {
+      const double eps = cfg.lj[2 * (a * cfg.ntypes + b)], sig = cfg.lj[2 * (a * cfg.ntypes + b) + 1];
+      R.lj_eps24[a * cfg.ntypes + b] = (float)(24.0 * eps);
+      R.lj_sig2[a * cfg.ntypes + b] = (float)(sig * sig);
+    }
+  if (cfg.bond.size() > 4 || cfg.angle.size() > 4)
+    throw Error(FMD_ERR_CONFIG, "the mixed form supports up to 4 bond and 4 angle types");
+  for (size_t k = 0; k < cfg.bond.size(); ++k) {
+    R.fene[4 * k] = (float)cfg.bond[k][0];
+    R.fene[4 * k + 1] = (float)(cfg.bond[k][1] * cfg.bond[k][1]);
+    R.fene[4 * k + 2] = (float)cfg.bond[k][2];
+    R.fene[4 * k + 3] = (float)(cfg.bond[k][3] * cfg.bond[k][3]);
+  }
+  for (size_t k = 0; k < cfg.angle.size(); ++k) {
+    R.angp[2 * k] = (float)cfg.angle[k][0];
+    R.angp[2 * k + 1] = (float)cfg.angle[k][1];
+  }
+}
+
+static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
+  R.mode = kModeRun;
+  R.fcap = 0;
+  R.push_dt = R.dt;
+  R.step = 0;
+  R.stop_step = 0;
+  R.since = 0;
+  R.rebuild_now = 1;
+  R.adv = 1;
+  int G = (int)std::floor(L / (rcs * 1.0001));
+  G = std::max(1, std::min(G, G_alloc));
+  R.G = G;
+  R.L = L;
+  R.Lpos = L;
+  R.h = (float)(L / G);
+  R.maxdisp_bits = 0;
+  R.status = 0;
+  R.rebuilds = 0;
+  R.cnt_pre = R.cnt_post = 0;
+  std::memset(&R.nh, 0, sizeof(R.nh));
+  R.nh.scale = 1.0;
+  R.nh.bscale = 1.0;
+  R.nh.exp_vW = 1.0;
+  R.nh.L = L;
+  R.nh.inv_L = 1.0 / L;
+  R.nh.V = L * L * L;
+  R.pending_scale = 1.0;
+}
+
+// Positions of atoms in data-file order into the replica's slots (slot = id);
+// the first rebuild sorts them into cell order.
+void Batch::upload_atoms(int r, const double* xyz, const double* vel, const int32_t* image) {
+  const Rep& R = h_reps_[r];
+  const ReplicaInfo& I = info_[r];
+  const int n = R.natoms;
+  const double L = R.L, h = R.h;
+  std::vector<float4> hp(R.slot_cap), hv(R.slot_cap);
+  std::vector<int4> hi(R.slot_cap);
+  std::vector<int32_t> so(R.slot_cap, 0);
+  for (int s = 0; s < R.slot_cap; ++s) {
+    if (s < n) {
+      int c[3], im[3];
+      float o[3];
+      for (int a = 0; a < 3; ++a) {
+        double x = xyz[3 * s + a];
+        const double fl = std::floor(x / L);
+        x -= fl * L;
+        im[a] = (image ? image[3 * s + a] : 0) + (int)fl;
+        if (x >= L) {
+          x -= L;
+          im[a] += 1;
+        }
+        if (x < 0) x = 0;
+        int ca = (int)std::floor(x / h);
+        ca = std::max(0, std::min(ca, R.G - 1));
+        c[a] = ca;
+        o[a] = (float)(x - ca * h);
+      }
+      hp[s] = make_float4(o[0], o[1], o[2], pack_w(c[0], c[1], c[2], I.type[s]));
+      hv[s] = make_float4(vel ? (float)vel[3 * s] : 0.f, vel ? (float)vel[3 * s + 1] : 0.f,
+                          vel ? (float)vel[3 * s + 2] : 0.f, R.invm[I.type[s]]);
+      hi[s] = make_int4(im[0], im[1], im[2], s);
+      so[s] = s;
+    } else {
+      hp[s] = make_float4(0, 0, 0, pack_w(0, 0, 0, kGhostType));
+      hv[s] = make_float4(0, 0, 0, 1.0f);
+      hi[s] = make_int4(0, 0, 0, -1);
+    }
+  }
+  const size_t b = R.slot_base;
+  FMD_CUDA(cudaMemcpyAsync(pos_.p + b, hp.data(), R.slot_cap * sizeof(float4), cudaMemcpyHostToDevice, st_));
+  FMD_CUDA(cudaMemcpyAsync(ref_.p + b, hp.data(), R.slot_cap * sizeof(float4), cudaMemcpyHostToDevice, st_));
+  FMD_CUDA(cudaMemcpyAsync(vel_.p + b, hv.data(), R.slot_cap * sizeof(float4), cudaMemcpyHostToDevice, st_));
+  FMD_CUDA(cudaMemcpyAsync(img_.p + b, hi.data(), R.slot_cap * sizeof(int4), cudaMemcpyHostToDevice, st_));
+  FMD_CUDA(cudaMemcpyAsync(slot_of_.p + b, so.data(), R.slot_cap * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+  FMD_CUDA(cudaMemsetAsync(force_.p + b, 0, R.slot_cap * sizeof(float4), st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+}
+
+int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
+  int r = -1;
+  for (int k = 0; k < max_reps_; ++k)
+    if (!info_[k].used) {
+      r = k;
+      break;
+    }
+  if (r < 0) throw Error(FMD_ERR_CAPACITY, "no free replica slot");
+  const ReplicaPlan p = plan_replica(cfg, t.natoms, t.box_L);
+  const int64_t need = estimate_bytes(p, t.nbonds(), t.nangles());
+  if (bytes_in_use_ + need > budget_bytes_) throw Error(FMD_ERR_CAPACITY, "device-memory budget exhausted");
+  const int64_t ch = slot_alloc_.alloc(p.nchunks);
+  const int64_t ce = ch >= 0 ? cell_alloc_.alloc(p.ncell) : -1;
+  const int64_t nb = ce >= 0 ? nbr_alloc_.alloc((p.nbr_entries + 1023) / 1024) : -1;
+  const int64_t bo = nb >= 0 ? bond_alloc_.alloc(2ll * t.nbonds()) : -1;
+  const int64_t an = bo >= 0 ? angle_alloc_.alloc(3ll * t.nangles()) : -1;
+  if (an < 0) {
+    if (ch >= 0) slot_alloc_.release(ch);
+    if (ce >= 0) cell_alloc_.release(ce);
+    if (nb >= 0) nbr_alloc_.release(nb);
+    if (bo >= 0) bond_alloc_.release(bo);
+    throw Error(FMD_ERR_CAPACITY, "batch capacity exhausted");
+  }
+  ReplicaInfo& I = info_[r];
+  I = ReplicaInfo{};
+  I.used = true;
+  I.plan = p;
+  I.cfg = cfg;
+  I.type = t.type;
+  I.mol = t.mol;
+  I.bytes = need;
+  I.seg_chunk = ch;
+  I.seg_cell = ce;
+  I.seg_nbr = nb;
+  I.seg_bond = bo;
+  I.seg_angle = an;
+  bytes_in_use_ += need;
+  Rep& R = h_reps_[r];
+  R = Rep{};
+  R.active = 1;
+  R.slot_base = (int32_t)(ch * kChunk);
+  R.slot_cap = p.slot_cap;
+  R.natoms = t.natoms;
+  R.chunk_base = (int32_t)ch;
+  R.nchunks = p.nchunks;
+  R.cell_base = (int32_t)ce;
+  R.P = p.P;
+  R.G_alloc = p.G_alloc;
+  R.nbr_base = nb * 1024;
+  R.M = p.M;
+  R.bond_base = (int32_t)bo;
+  R.angle_base = (int32_t)an;
+  fill_static(R, cfg, t);
+  init_dynamic(R, t.box_L, p.G_alloc, cfg.rc + cfg.skin);
+  // Topology CSR by atom id.
+  {
+    const int n = t.natoms;
+    std::vector<int32_t> boff(R.slot_cap, 0), aoff(R.slot_cap, 0);
+    for (int b = 0; b < t.nbonds(); ++b) {
+      boff[t.bonds[2 * b] + 1]++;
+      boff[t.bonds[2 * b + 1] + 1]++;
+    }
+    for (int a = 0; a < t.nangles(); ++a)
+      for (int k = 0; k < 3; ++k) aoff[t.angles[3 * a + k] + 1]++;
+    for (int i = 0; i < n; ++i) {
+      boff[i + 1] += boff[i];
+      aoff[i + 1] += aoff[i];
+    }
+    std::vector<int2> be(std::max(1, 2 * t.nbonds()));
+    std::vector<int4> ae(std::max(1, 3 * t.nangles()));
+    std::vector<int32_t> fb(boff.begin(), boff.begin() + n), fa(aoff.begin(), aoff.begin() + n);
+    for (int b = 0; b < t.nbonds(); ++b) {
+      const int i = t.bonds[2 * b], j = t.bonds[2 * b + 1], ty = t.bond_type[b];
+      be[fb[i]++] = make_int2(j, ty | (1 << 8));
+      be[fb[j]++] = make_int2(i, ty);
+    }
+    for (int a = 0; a < t.nangles(); ++a) {
+      const int i = t.angles[3 * a], j = t.angles[3 * a + 1], k = t.angles[3 * a + 2], ty = t.angle_type[a];
+      ae[fa[i]++] = make_int4(i, j, k, ty | (0 << 8));
+      ae[fa[j]++] = make_int4(i, j, k, ty | (1 << 8));
+      ae[fa[k]++] = make_int4(i, j, k, ty | (2 << 8));
+    }
+    for (int i = n + 1; i < R.slot_cap; ++i) {
+      boff[i] = boff[n];
+      aoff[i] = aoff[n];
+    }
+    FMD_CUDA(cudaMemcpyAsync(boff_.p + R.slot_base, boff.data(), R.slot_cap * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+    FMD_CUDA(cudaMemcpyAsync(aoff_.p + R.slot_base, aoff.data(), R.slot_cap * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+    if (t.nbonds())
+      FMD_CUDA(cudaMemcpyAsync(bent_.p + R.bond_base, be.data(), 2 * t.nbonds() * sizeof(int2), cudaMemcpyHostToDevice, st_));
+    if (t.nangles())
+      FMD_CUDA(cudaMemcpyAsync(aent_.p + R.angle_base, ae.data(), 3 * t.nangles() * sizeof(int4), cudaMemcpyHostToDevice, st_));
+  }
+  for (int c = 0; c < p.nchunks; ++c) h_chunk_rep_[ch + c] = r;
+  FMD_CUDA(cudaMemcpyAsync(chunk_rep_.p + ch, h_chunk_rep_.data() + ch, p.nchunks * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+  FMD_CUDA(cudaMemsetAsync(cell_cnt_.p + ce, 0, p.ncell * sizeof(int32_t), st_));
+  // Other replicas must not advance while this one is being set up.
+  download_reps_keep(r);
+  upload_atoms(r, t.xyz.data(), t.vel.data(), t.image.data());
+  graph_dirty_ = true;
+  setup(r);
+  if (pushoff && pushoff->pushoff_steps > 0) run_pushoff(r, *pushoff);
+  return r;
+}
+
+// Refresh the host mirror of every replica except r (whose record the host
+// has just written) from the device.
+void Batch::download_reps_keep(int r) {
+  const Rep keep = h_reps_[r];
+  download_reps();
+  h_reps_[r] = keep;
+}
+
+void Batch::freeze_others(int r) {
+  for (int k = 0; k < max_reps_; ++k)
+    if (k != r && info_[k].used) h_reps_[k].stop_step = h_reps_[k].step;
+}
+
+// Rebuild + forces + KE reduction without integrating (main.cu:313-390).
+void Batch::setup(int r) {
+  freeze_others(r);
+  Rep& R = h_reps_[r];
+  R.adv = 1;
+  R.rebuild_now = 1;
+  R.since = 0;
+  R.maxdisp_bits = 0;
+  upload_reps();
+  const Dev d = dev();
+  launch_rebuild(d, nchunks_launch(), nreps_launch(), max_cells(), st_);
+  FMD_CUDA_LAUNCH();
+  launch_forces_only(d, nchunks_launch(), st_);
+  FMD_CUDA_LAUNCH();
+  launch_reduce_only(d, nchunks_launch(), st_);
+  FMD_CUDA_LAUNCH();
+  download_reps();
+  check_status(r, true);
+}
+
+void Batch::check_status(int r, bool throw_on_fault) {
+  const Rep& R = h_reps_[r];
+  if (R.status == 0) return;
+  if (!throw_on_fault) return;
+  if (R.status & kStatusOverflow) throw Error(FMD_ERR_OVERFLOW, "neighbor list overflow");
+  if (R.status & kStatusCellCapacity) throw Error(FMD_ERR_OVERFLOW, "cell grid capacity exceeded");
+  if (R.status & kStatusNonFinite) throw Error(FMD_ERR_FAULT, "non-finite state");
+  if (R.status & kStatusFeneStretch) throw Error(FMD_ERR_FAULT, "FENE bond stretched to R0");
+  throw Error(FMD_ERR_FAULT, "replica fault");
+}
+
+void Batch::run_pushoff(int r, const fmd_melt_spec& sp) {
+  Rep& R = h_reps_[r];
+  R.mode = kModePushoff;
+  R.fcap = sp.pushoff_fcap > 0 ? sp.pushoff_fcap : 50.0;
+  R.push_dt = sp.pushoff_dt > 0 ? sp.pushoff_dt : 0.005;
+  R.step = 0;
+  // forces of the current state must be capped before the first kick
+  setup(r);
+  Rep& R2 = h_reps_[r];
+  R2.stop_step = sp.pushoff_steps;
+  freeze_others(r);
+  upload_reps();
+  advance_direct(sp.pushoff_steps);
+  download_reps();
+  check_status(r, true);
+  Rep& R3 = h_reps_[r];
+  R3.mode = kModeRun;
+  R3.fcap = 0;
+  R3.step = 0;
+  R3.stop_step = 0;
+  std::memset(&R3.nh, 0, sizeof(R3.nh));
+  R3.nh.scale = 1.0;
+  R3.nh.bscale = 1.0;
+  R3.nh.exp_vW = 1.0;
+  R3.nh.L = R3.L;
+  R3.nh.inv_L = 1.0 / R3.L;
+  R3.nh.V = R3.L * R3.L * R3.L;
+  R3.pending_scale = 1.0;
+  R3.rebuilds = 0;
+  setup(r);
+}
+
+void Batch::advance_direct(int64_t nsteps) {
+  const Dev d = dev();
+  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
+  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, mc, st_);
+  FMD_CUDA_LAUNCH();
+  FMD_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Batch::ensure_graph() {
+  if (!graph_dirty_ && graph_exec_) return;
+  if (graph_exec_) {
+    cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+  }
+  const Dev d = dev();
+  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
+  cudaGraph_t g;
+  FMD_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  for (int k = 0; k < graph_steps_; ++k) launch_step(d, nc, nr, mc, st_);
+  FMD_CUDA(cudaStreamEndCapture(st_, &g));
+  FMD_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
+  cudaGraphDestroy(g);
+  graph_dirty_ = false;
+}
+
+void Batch::run(int64_t nsteps, bool respect_nsteps) {
+  if (nsteps <= 0) return;
+  download_reps();
+  int64_t need = 0;
+  for (int r = 0; r < max_reps_; ++r) {
+    if (!info_[r].used) continue;
+    Rep& R = h_reps_[r];
+    if (!R.active) {
+      R.stop_step = R.step;
+      continue;
+    }
+    int64_t stop = R.step + nsteps;
+    if (respect_nsteps && R.nsteps > 0) stop = std::min<int64_t>(stop, R.nsteps);
+    R.stop_step = stop;
+    need = std::max<int64_t>(need, stop - R.step);
+  }
+  if (need == 0) return;
+  upload_reps();
+  if (need >= graph_steps_) {
+    ensure_graph();
+    const int64_t reps = need / graph_steps_;
+    for (int64_t k = 0; k < reps; ++k) FMD_CUDA(cudaGraphLaunch(graph_exec_, st_));
+    need -= reps * graph_steps_;
+  }
+  if (need > 0) {
+    const Dev d = dev();
+    const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
+    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, mc, st_);
+    FMD_CUDA_LAUNCH();
+  }
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  download_reps();
+  // A faulted replica stops; the others continue.
+  bool changed = false;
+  for (int r = 0; r < max_reps_; ++r) {
+    if (!info_[r].used) continue;
+    Rep& R = h_reps_[r];
+    if (R.status != 0 && R.active) {
+      R.active = 0;
+      changed = true;
+    }
+  }
+  if (changed) upload_reps();
+}
+
+void Batch::retire(int r) {
+  if (r < 0 || r >= max_reps_ || !info_[r].used) throw Error(FMD_ERR_ARG, "no such replica");
+  download_reps();
+  ReplicaInfo& I = info_[r];
+  Rep& R = h_reps_[r];
+  for (int c = 0; c < R.nchunks; ++c) h_chunk_rep_[R.chunk_base + c] = -1;
+  FMD_CUDA(cudaMemcpyAsync(chunk_rep_.p + R.chunk_base, h_chunk_rep_.data() + R.chunk_base, R.nchunks * sizeof(int32_t),
+                           cudaMemcpyHostToDevice, st_));
+  slot_alloc_.release(I.seg_chunk);
+  cell_alloc_.release(I.seg_cell);
+  nbr_alloc_.release(I.seg_nbr);
+  bond_alloc_.release(I.seg_bond);
+  angle_alloc_.release(I.seg_angle);
+  bytes_in_use_ -= I.bytes;
+  R = Rep{};
+  I = ReplicaInfo{};
+  upload_reps();
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  graph_dirty_ = true;
+}
+
+void Batch::mark(int which) {
+  if (which < 0 || which > 1) throw Error(FMD_ERR_ARG, "event index must be 0 or 1");
+  if (!ev_[which]) FMD_CUDA(cudaEventCreate(&ev_[which]));
+  FMD_CUDA(cudaEventRecord(ev_[which], st_));
+}
+
+double Batch::elapsed_ms() {
+  if (!ev_[0] || !ev_[1]) throw Error(FMD_ERR_STATE, "both events must be recorded first");
+  FMD_CUDA(cudaEventSynchronize(ev_[1]));
+  float ms = 0;
+  FMD_CUDA(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+  return ms;
+}
+
+double Batch::time_force(int iters) {
+  download_reps();
+  // mark every replica as advancing for the force kernel only
+  std::vector<Rep> saved = h_reps_;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used && h_reps_[r].active) h_reps_[r].adv = 1;
+  upload_reps();
+  const Dev d = dev();
+  const int nc = nchunks_launch();
+  launch_forces_only(d, nc, st_);  // warm
+  FMD_CUDA_LAUNCH();
+  mark(0);
+  for (int k = 0; k < iters; ++k) launch_forces_only(d, nc, st_);
+  FMD_CUDA_LAUNCH();
+  mark(1);
+  const double ms = elapsed_ms() / std::max(1, iters);
+  h_reps_ = saved;
+  upload_reps();
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  return ms;
+}
+
+void Batch::list_stats(int64_t* entries, int32_t* max_per_atom) {
+  int64_t tot = 0;
+  int32_t mx = 0;
+  for (int r = 0; r < max_reps_; ++r) {
+    if (!info_[r].used || !h_reps_[r].active) continue;
+    const Rep& R = h_reps_[r];
+    std::vector<int32_t> c(R.natoms);
+    FMD_CUDA(cudaMemcpy(c.data(), ncnt_.p + R.slot_base, R.natoms * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    for (int32_t v : c) {
+      tot += v;
+      mx = std::max(mx, v);
+    }
+  }
+  if (entries) *entries = tot;
+  if (max_per_atom) *max_per_atom = mx;
+}
+
+void Batch::set_max_between(int r, int k) {
+  download_reps();
+  h_reps_[r].max_between = k > 0 ? k : 20;
+  upload_reps();
+  FMD_CUDA(cudaStreamSynchronize(st_));
+}
+
+const Rep& Batch::rep(int r) const {
+  if (r < 0 || r >= max_reps_ || !info_[r].used) throw Error(FMD_ERR_ARG, "no such replica");
+  return h_reps_[r];
+}
+
+void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) {
+  const Rep& R = rep(r);
+  const int n = R.natoms;
+  std::vector<float4> hp(n), hv(n);
+  std::vector<int4> hi(n);
+  FMD_CUDA(cudaMemcpyAsync(hp.data(), pos_.p + R.slot_base, n * sizeof(float4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaMemcpyAsync(hv.data(), vel_.p + R.slot_base, n * sizeof(float4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaMemcpyAsync(hi.data(), img_.p + R.slot_base, n * sizeof(int4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  const double L = R.Lpos, h = R.h;
+  for (int s = 0; s < n; ++s) {
+    const int id = hi[s].w;
+    const uint32_t u = w_bits(hp[s].w);
+    const int c[3] = {w_cx(u), w_cy(u), w_cz(u)};
+    const float o[3] = {hp[s].x, hp[s].y, hp[s].z};
+    const int im[3] = {hi[s].x, hi[s].y, hi[s].z};
+    for (int a = 0; a < 3; ++a) {
+      double x = (double)c[a] * h + (double)o[a];
+      int ia = im[a];
+      if (x < 0) {
+        x += L;
+        ia -= 1;
+      } else if (x >= L) {
+        x -= L;
+        ia += 1;
+      }
+      if (xyz) xyz[3 * id + a] = x;
+      if (image) image[3 * id + a] = ia;
+    }
+    if (vel) {
+      vel[3 * id] = (double)hv[s].x * R.pending_scale;
+      vel[3 * id + 1] = (double)hv[s].y * R.pending_scale;
+      vel[3 * id + 2] = (double)hv[s].z * R.pending_scale;
+    }
+  }
+}
+
+void Batch::set_state(int r, const double* xyz, const double* vel, const int32_t* image) {
+  const Rep& R0 = rep(r);
+  const int n = R0.natoms;
+  std::vector<double> x(3 * n), v(3 * n);
+  std::vector<int32_t> im(3 * n);
+  get_state(r, x.data(), v.data(), im.data());
+  if (xyz) std::memcpy(x.data(), xyz, 3 * n * sizeof(double));
+  if (vel) std::memcpy(v.data(), vel, 3 * n * sizeof(double));
+  if (image) std::memcpy(im.data(), image, 3 * n * sizeof(int32_t));
+  else if (xyz) std::fill(im.begin(), im.end(), 0);
+  download_reps();
+  Rep& R = h_reps_[r];
+  R.pending_scale = 1.0;
+  R.Lpos = R.L;
+  R.h = (float)(R.L / R.G);
+  upload_atoms(r, x.data(), v.data(), im.data());
+  setup(r);
+}
+
+void Batch::forces(int r, double* f, double* pe, double* vir) {
+  const Rep& R = rep(r);
+  const int n = R.natoms;
+  std::vector<float4> hf(n);
+  std::vector<int4> hi(n);
+  FMD_CUDA(cudaMemcpyAsync(hf.data(), force_.p + R.slot_base, n * sizeof(float4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaMemcpyAsync(hi.data(), img_.p + R.slot_base, n * sizeof(int4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  for (int s = 0; s < n; ++s) {
+    const int id = hi[s].w;
+    if (f) {
+      f[3 * id] = hf[s].x;
+      f[3 * id + 1] = hf[s].y;
+      f[3 * id + 2] = hf[s].z;
+    }
+    if (pe) pe[id] = hf[s].w;
+  }
+  if (vir) std::memcpy(vir, R.vir, 6 * sizeof(double));
+}
+
+void Batch::thermo(int r, fmd_thermo_row* row) {
+  const Rep& R = rep(r);
+  const int n = R.natoms;
+  const double s2 = R.pending_scale * R.pending_scale;
+  double k[6];
+  for (int c = 0; c < 6; ++c) k[c] = R.ke[c] * s2;
+  const double ke = 0.5 * (k[0] + k[3] + k[5]);
+  row->step = R.step;
+  row->ke = ke / n;
+  row->pe = R.pe / n;
+  row->temp = 2.0 * row->ke / 3.0;
+  const double V = R.L * R.L * R.L;
+  for (int c = 0; c < 6; ++c) row->stress[c] = (k[c] + R.vir[c]) / V;
+  row->box_L = R.L;
+  double e = ke + R.pe;
+  if (R.ensemble != FMD_LANGEVIN) {
+    const double frac = (double)(R.step - 1) / (double)(R.nsteps > 0 ? R.nsteps : 1);
+    const double kT = R.T0 + (R.T1 - R.T0) * frac;
+    const double Nf = 3.0 * n;
+    e += 0.5 * R.Q1 * R.nh.vxi[0] * R.nh.vxi[0] + Nf * kT * R.nh.xi[0];
+    for (int q = 1; q < R.chain_M; ++q) e += 0.5 * R.Qr * R.nh.vxi[q] * R.nh.vxi[q] + kT * R.nh.xi[q];
+    if (R.ensemble == FMD_NPT_NH) {
+      const double Pt = R.P0 + (R.P1 - R.P0) * frac;
+      e += R.nh.veps * R.nh.veps / (2.0 * R.W) + Pt * V;
+    }
+  }
+  row->conserved = e / n;
+}
+
+double Batch::rg(int r) {
+  const Rep& R = rep(r);
+  const int n = R.natoms;
+  std::vector<double> x(3 * n);
+  std::vector<int32_t> im(3 * n);
+  get_state(r, x.data(), nullptr, im.data());
+  const std::vector<int32_t>& mol = info_[r].mol;
+  std::vector<int32_t> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return mol[a] < mol[b]; });
+  double sum = 0;
+  int nch = 0;
+  const double L = R.Lpos;
+  for (int s = 0; s < n;) {
+    int e = s;
+    while (e < n && mol[order[e]] == mol[order[s]]) ++e;
+    double com[3] = {0, 0, 0};
+    for (int t = s; t < e; ++t)
+      for (int a = 0; a < 3; ++a) com[a] += x[3 * order[t] + a] + im[3 * order[t] + a] * L;
+    for (int a = 0; a < 3; ++a) com[a] /= (e - s);
+    double rg2 = 0;
+    for (int t = s; t < e; ++t)
+      for (int a = 0; a < 3; ++a) {
+        const double u = x[3 * order[t] + a] + im[3 * order[t] + a] * L - com[a];
+        rg2 += u * u;
+      }
+    sum += std::sqrt(rg2 / (e - s));
+    ++nch;
+    s = e;
+  }
+  return nch ? sum / nch : 0.0;
+}
+
+int64_t Batch::pairs(int r, int32_t* pi, int32_t* pj, int64_t cap) {
+  const Rep& R = rep(r);
+  const int n = R.natoms;
+  const int tiles = R.slot_cap / kTile;
+  std::vector<uint32_t> nb((size_t)tiles * R.M * kTile);
+  std::vector<int32_t> cnt(n);
+  std::vector<int4> hi(n);
+  FMD_CUDA(cudaMemcpyAsync(nb.data(), nbr_.p + R.nbr_base, nb.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaMemcpyAsync(cnt.data(), ncnt_.p + R.slot_base, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaMemcpyAsync(hi.data(), img_.p + R.slot_base, n * sizeof(int4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  int64_t m = 0;
+  for (int s = 0; s < n; ++s)
+    for (int k = 0; k < cnt[s]; ++k) {
+      const uint32_t w = nb[((size_t)(s >> 5) * R.M + k) * kTile + (s & 31)];
+      const int js = (int)(w & kIdxMask);
+      const int a = hi[s].w, b = hi[js].w;
+      if (a < b) {
+        if (m < cap) {
+          pi[m] = a;
+          pj[m] = b;
+        }
+        ++m;
+      }
+    }
+  return m;
+}
+
+void Batch::totals(int32_t* active, int64_t* atoms, int64_t* bytes) {
+  int32_t a = 0;
+  int64_t n = 0;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used && h_reps_[r].active) {
+      ++a;
+      n += h_reps_[r].natoms;
+    }
+  if (active) *active = a;
+  if (atoms) *atoms = n;
+  if (bytes) *bytes = bytes_in_use_;
+}
+
+// ------------------------------------------------------------- SimEngine
+class MixedEngine final : public SimEngine {
+ public:
+  MixedEngine(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
+    const ReplicaPlan p = plan_replica(cfg, t.natoms, t.box_L);
+    BatchCaps c;
+    c.slots = p.slot_cap;
+    c.nbr = ((p.nbr_entries + 1023) / 1024) * 1024;
+    c.cells = p.ncell;
+    c.bonds = std::max<int64_t>(1, 2ll * t.nbonds());
+    c.angles = std::max<int64_t>(1, 3ll * t.nangles());
+    fmd_batch_opts o{};
+    o.max_replicas = 1;
+    o.hbm_budget_gb = 1e6;
+    o.graph_steps = 20;
+    b_.reset(new Batch(o, &c));
+    nb_ = t.nbonds();
+    na_ = t.nangles();
+    r_ = b_->add(cfg, std::move(t), pushoff);
+  }
+  void step(int64_t n) override {
+    b_->run(n, false);
+    b_->check_status(r_, true);
+  }
+  void compute_forces(double* f, double* pe, double* vir) override { b_->forces(r_, f, pe, vir); }
+  void get_state(double* x, double* v, int32_t* i) override { b_->get_state(r_, x, v, i); }
+  void set_state(const double* x, const double* v, const int32_t* i) override { b_->set_state(r_, x, v, i); }
+  void thermo(fmd_thermo_row* row) override { b_->thermo(r_, row); }
+  double rg() override { return b_->rg(r_); }
+  int64_t pairs(int32_t* pi, int32_t* pj, int64_t cap) override { return b_->pairs(r_, pi, pj, cap); }
+  int32_t natoms() const override { return b_->rep(r_).natoms; }
+  int32_t nbonds() const override { return nb_; }
+  int32_t nangles() const override { return na_; }
+  int64_t step_count() const override { return b_->rep(r_).step; }
+  double box_L() override { return b_->rep(r_).L; }
+  int64_t rebuilds() const override { return b_->rep(r_).rebuilds; }
+  int32_t status_word() override { return b_->rep(r_).status; }
+  int32_t max_neighbors() const override { return b_->rep(r_).M; }
+
+ private:
+  std::unique_ptr<Batch> b_;
+  int r_ = 0;
+  int32_t nb_ = 0, na_ = 0;
+};
+
+}  // namespace mixed
+
+std::unique_ptr<SimEngine> make_mixed_engine(const RunConfig& cfg, Topology topo, const fmd_melt_spec* pushoff) {
+  return std::unique_ptr<SimEngine>(new mixed::MixedEngine(cfg, std::move(topo), pushoff));
+}
+
+}  // namespace fmd

@@ -1,0 +1,128 @@
+// Host-side batch manager for the mixed-precision engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <vector>
+
+#include "dev_common.cuh"
+#include "host.h"
+#include "mixed.cuh"
+
+namespace fmd {
+namespace mixed {
+
+// First-fit segment allocator over [0, capacity) in caller units.
+class SegAlloc {
+ public:
+  void reset(int64_t capacity) {
+    free_.clear();
+    used_.clear();
+    if (capacity > 0) free_[0] = capacity;
+    hwm_ = 0;
+  }
+  int64_t alloc(int64_t n);
+  void release(int64_t at);
+  int64_t hwm() const { return hwm_; }
+
+ private:
+  std::map<int64_t, int64_t> free_, used_;
+  int64_t hwm_ = 0;
+};
+
+struct ReplicaPlan {
+  int G_alloc = 1, P = 1;
+  int64_t ncell = 1;
+  int32_t slot_cap = 0, nchunks = 0, M = 0;
+  int64_t nbr_entries = 0;
+};
+
+struct BatchCaps {
+  int64_t slots = 0, nbr = 0, cells = 0, bonds = 0, angles = 0;
+};
+
+ReplicaPlan plan_replica(const RunConfig& cfg, int32_t natoms, double L);
+int64_t estimate_bytes(const ReplicaPlan& p, int32_t nbonds, int32_t nangles);
+
+struct ReplicaInfo {
+  bool used = false;
+  ReplicaPlan plan;
+  RunConfig cfg;
+  std::vector<int32_t> type, mol;
+  int64_t bytes = 0;
+  int64_t seg_chunk = -1, seg_cell = -1, seg_nbr = -1, seg_bond = -1, seg_angle = -1;
+};
+
+class Batch {
+ public:
+  Batch(const fmd_batch_opts& o, const BatchCaps* exact = nullptr);
+  ~Batch();
+  int add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff);
+  void run(int64_t nsteps, bool respect_nsteps);
+  void retire(int r);
+  const Rep& rep(int r) const;
+  bool used(int r) const { return r >= 0 && r < max_reps_ && info_[r].used; }
+  int max_reps() const { return max_reps_; }
+  const RunConfig& cfg(int r) const { return info_[r].cfg; }
+  void get_state(int r, double* xyz, double* vel, int32_t* image);
+  void set_state(int r, const double* xyz, const double* vel, const int32_t* image);
+  void forces(int r, double* f, double* pe, double* vir);
+  void thermo(int r, fmd_thermo_row* row);
+  double rg(int r);
+  int64_t pairs(int r, int32_t* pi, int32_t* pj, int64_t cap);
+  void totals(int32_t* active, int64_t* atoms, int64_t* bytes);
+  void check_status(int r, bool throw_on_fault);
+  int64_t budget_bytes() const { return budget_bytes_; }
+  int64_t bytes_in_use() const { return bytes_in_use_; }
+  cudaStream_t stream() const { return st_; }
+  Dev dev() const;
+  int nchunks_launch() const;
+  int nreps_launch() const;
+  int max_cells() const;
+  int graph_steps() const { return graph_steps_; }
+  void set_max_between(int r, int k);
+  void mark(int which);
+  double elapsed_ms();
+  double time_force(int iters);
+  void list_stats(int64_t* entries, int32_t* max_per_atom);
+
+ private:
+  void download_reps();
+  void download_reps_keep(int r);
+  void upload_reps();
+  void freeze_others(int r);
+  void upload_atoms(int r, const double* xyz, const double* vel, const int32_t* image);
+  void setup(int r);
+  void run_pushoff(int r, const fmd_melt_spec& sp);
+  void advance_direct(int64_t nsteps);
+  void ensure_graph();
+
+  int device_ = 0;
+  cudaStream_t st_ = nullptr;
+  int graph_steps_ = 50;
+  int max_reps_ = 256;
+  BatchCaps caps_;
+  int64_t budget_bytes_ = 0, bytes_in_use_ = 0, bytes_ = 0;
+  SegAlloc slot_alloc_, cell_alloc_, nbr_alloc_, bond_alloc_, angle_alloc_;
+  DevBuf<float4> pos_, vel_, force_, ref_, tpos_, tvel_;
+  DevBuf<int4> img_, timg_;
+  DevBuf<uint32_t> key_;
+  DevBuf<int32_t> perm_, bucket_, slot_of_, boff_, aoff_, ncnt_;
+  DevBuf<double> part_;
+  DevBuf<int32_t> cell_cnt_, cell_start_, cell_fill_;
+  DevBuf<int2> bent_;
+  DevBuf<int4> aent_;
+  DevBuf<uint32_t> nbr_;
+  DevBuf<Rep> reps_;
+  DevBuf<int32_t> chunk_rep_;
+  std::vector<int32_t> h_chunk_rep_;
+  std::vector<Rep> h_reps_;
+  std::vector<ReplicaInfo> info_;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+  bool graph_dirty_ = true;
+};
+
+}  // namespace mixed
+}  // namespace fmd

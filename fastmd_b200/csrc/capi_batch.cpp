@@ -1,0 +1,196 @@
+// extern "C" entry points for batches of replicas (include/fastmd.h).
+#include <cstring>
+#include <memory>
+
+#include "batch.h"
+#include "host.h"
+
+struct fmd_batch {
+  std::unique_ptr<fmd::mixed::Batch> b;
+};
+
+namespace {
+template <typename F>
+fmd_status guarded(F&& f) {
+  try {
+    f();
+    fmd::set_last_error("");
+    return FMD_OK;
+  } catch (const fmd::Error& e) {
+    fmd::set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    fmd::set_last_error("host out of memory");
+    return FMD_ERR_CAPACITY;
+  } catch (const std::exception& e) {
+    fmd::set_last_error(e.what());
+    return FMD_ERR_ARG;
+  }
+}
+
+fmd::mixed::Batch& B(fmd_batch* b) {
+  if (!b || !b->b) throw fmd::Error(FMD_ERR_ARG, "null batch handle");
+  return *b->b;
+}
+
+void need_slot(fmd::mixed::Batch& b, int32_t slot) {
+  if (!b.used(slot)) throw fmd::Error(FMD_ERR_ARG, "no replica in this slot");
+}
+}  // namespace
+
+extern "C" {
+
+FMD_API fmd_status fmd_batch_create(const fmd_batch_opts* opts, fmd_batch** out) {
+  return guarded([&] {
+    if (!out) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      throw fmd::Error(FMD_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    fmd_batch_opts o{};
+    if (opts) o = *opts;
+    std::unique_ptr<fmd_batch> b(new fmd_batch());
+    b->b.reset(new fmd::mixed::Batch(o));
+    *out = b.release();
+  });
+}
+
+FMD_API fmd_status fmd_batch_destroy(fmd_batch* b) {
+  return guarded([&] { delete b; });
+}
+
+FMD_API fmd_status fmd_batch_add_replica(fmd_batch* b, const char* conf, const char* data_path,
+                                         const fmd_system_desc* desc, const fmd_melt_spec* gen, int32_t* slot) {
+  return guarded([&] {
+    if (!conf || !slot) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    fmd::RunConfig cfg = fmd::parse_run_conf(conf);
+    fmd::Topology t = fmd::load_atoms(cfg, data_path, desc, gen);
+    *slot = B(b).add(cfg, std::move(t), gen);
+  });
+}
+
+FMD_API fmd_status fmd_batch_estimate_bytes(const char* conf, int32_t natoms, double box_L, int64_t* bytes) {
+  return guarded([&] {
+    if (!conf || !bytes || natoms <= 0 || box_L <= 0) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    fmd::RunConfig cfg = fmd::parse_run_conf(conf);
+    const auto p = fmd::mixed::plan_replica(cfg, natoms, box_L);
+    *bytes = fmd::mixed::estimate_bytes(p, natoms, natoms);
+  });
+}
+
+FMD_API fmd_status fmd_batch_run(fmd_batch* b, int64_t nsteps) {
+  return guarded([&] {
+    if (nsteps < 0) throw fmd::Error(FMD_ERR_ARG, "nsteps < 0");
+    B(b).run(nsteps, true);
+  });
+}
+
+FMD_API fmd_status fmd_batch_retire(fmd_batch* b, int32_t slot) {
+  return guarded([&] { B(b).retire(slot); });
+}
+
+FMD_API fmd_status fmd_batch_replica_info(fmd_batch* b, int32_t slot, fmd_replica_info* info) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!info) throw fmd::Error(FMD_ERR_ARG, "null info");
+    const auto& R = bb.rep(slot);
+    info->slot = slot;
+    info->natoms = R.natoms;
+    info->step = R.step;
+    info->nsteps = R.nsteps;
+    info->status_word = R.status;
+    info->active = R.active;
+    info->box_L = R.L;
+    info->rebuilds = R.rebuilds;
+  });
+}
+
+FMD_API fmd_status fmd_batch_get_state(fmd_batch* b, int32_t slot, double* xyz, double* vel, int32_t* image) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    bb.get_state(slot, xyz, vel, image);
+  });
+}
+
+FMD_API fmd_status fmd_batch_thermo(fmd_batch* b, int32_t slot, fmd_thermo_row* row) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!row) throw fmd::Error(FMD_ERR_ARG, "null row");
+    bb.thermo(slot, row);
+  });
+}
+
+FMD_API fmd_status fmd_batch_rg(fmd_batch* b, int32_t slot, double* rg) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!rg) throw fmd::Error(FMD_ERR_ARG, "null rg");
+    *rg = bb.rg(slot);
+  });
+}
+
+FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* f, double* pe, double* virial) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    bb.forces(slot, f, pe, virial);
+  });
+}
+
+FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!n || (cap > 0 && (!i || !j))) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    *n = bb.pairs(slot, i, j, cap);
+  });
+}
+
+FMD_API fmd_status fmd_batch_totals(fmd_batch* b, int32_t* active, int64_t* atoms, int64_t* bytes) {
+  return guarded([&] { B(b).totals(active, atoms, bytes); });
+}
+
+FMD_API fmd_status fmd_batch_mark(fmd_batch* b, int32_t which) {
+  return guarded([&] { B(b).mark(which); });
+}
+
+FMD_API fmd_status fmd_batch_elapsed_ms(fmd_batch* b, double* ms) {
+  return guarded([&] {
+    if (!ms) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    *ms = B(b).elapsed_ms();
+  });
+}
+
+FMD_API fmd_status fmd_batch_time_force(fmd_batch* b, int32_t iters, double* ms) {
+  return guarded([&] {
+    if (!ms || iters <= 0) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    *ms = B(b).time_force(iters);
+  });
+}
+
+FMD_API fmd_status fmd_batch_list_stats(fmd_batch* b, int64_t* entries, int32_t* max_per_atom) {
+  return guarded([&] { B(b).list_stats(entries, max_per_atom); });
+}
+
+FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n) {
+  return guarded([&] {
+    B(b);
+    if (!n) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    *n = 9;  // k_pre, 6 rebuild kernels (early exit unless flagged), k_force, k_post
+  });
+}
+
+FMD_API fmd_status fmd_batch_set_rebuild_cadence(fmd_batch* b, int32_t slot, int32_t max_steps) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    bb.set_max_between(slot, max_steps);
+  });
+}
+
+}  // extern "C"

@@ -36,7 +36,7 @@ struct RunConfig {
   double T_start = 0, T_stop = 0, Tdamp = 0;
   double P_start = 0, P_stop = 0, Pdamp = 0;
   int32_t chain_length = 3;
-  uint64_t seed = 42;
+  uint64_t seed = 0;  // SimParams is zero-initialized; nvt_langevin defaults it to 42 (config.cpp:11, 79-81)
   std::string data_file, coords_file, forces_dump_file;
   std::vector<double> lj;                   // [ntypes*ntypes*2] (eps, sig)
   std::vector<std::array<double, 4>> bond;  // k, R0, eps, sig

@@ -1,0 +1,371 @@
+// Reference-layout launchers: drop-in replacements for the reference's
+// in-process entry points that take raw device pointers and a stream.
+//   fmd_launch_verlet_build  <- VerletList::build   (neighbor/verlet_list.cu:337-376)
+//   fmd_launch_lj            <- launch_lj_kernel    (force/lj.cu:109-122)
+//   fmd_launch_morton_sort   <- MortonSorter::sort_and_permute (core/morton.cu:65-85)
+// Buffers keep the reference's layout: float4 positions with the type id
+// bit-cast into .w, the transposed list neighbors[k * natoms + i].
+// FP32 throughout, as the reference; this file is compiled with -fmad=false so
+// the pair predicate rounds exactly like reference/cpu_reference.hpp on the
+// host (the pair set is bit-exact against it).  Differences: neighbor overflow
+// raises a flag instead of truncating silently; the caller owns all memory.
+#include <cub/cub.cuh>
+
+#include <cstdint>
+
+#include "dev_common.cuh"
+#include "host.h"
+
+namespace fmd {
+namespace launch {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ float min_image_f(float dr, float L, float inv_L) { return dr - L * rintf(dr * inv_L); }
+
+struct VerletGeom {
+  int nx, ncell;
+  float cell, inv_cell;
+};
+
+// verlet_list.cu:3-13 (grid from the box) with the same FP32 arithmetic.
+inline VerletGeom verlet_geom(float L, float rcs) {
+  VerletGeom g;
+  g.nx = (int)(L / rcs);
+  if (g.nx < 1) g.nx = 1;
+  g.ncell = g.nx * g.nx * g.nx;
+  g.cell = L / (float)g.nx;
+  g.inv_cell = 1.0f / g.cell;
+  return g;
+}
+
+struct VerletScratch {
+  int* cid;
+  int* cid_sorted;
+  int* aid;
+  int* sorted;
+  int* start;
+  int* end;
+  void* cub;
+  size_t cub_bytes;
+  size_t total;
+};
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+VerletScratch verlet_carve(void* base, int n, int ncell) {
+  VerletScratch s{};
+  size_t cub_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (int*)nullptr, (int*)nullptr, (int*)nullptr, (int*)nullptr, n);
+  char* p = (char*)base;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* q = p ? p + off : nullptr;
+    off += align256(bytes);
+    return q;
+  };
+  s.cid = (int*)take(sizeof(int) * n);
+  s.cid_sorted = (int*)take(sizeof(int) * n);
+  s.aid = (int*)take(sizeof(int) * n);
+  s.sorted = (int*)take(sizeof(int) * n);
+  s.start = (int*)take(sizeof(int) * ncell);
+  s.end = (int*)take(sizeof(int) * ncell);
+  s.cub = take(cub_bytes);
+  s.cub_bytes = cub_bytes;
+  s.total = off;
+  return s;
+}
+
+// verlet_list.cu:58-75
+__global__ void k_assign(const float4* pos, int* cid, int* aid, int n, float inv_cell, int nx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 r = pos[i];
+  int cx = __float2int_rd(r.x * inv_cell), cy = __float2int_rd(r.y * inv_cell), cz = __float2int_rd(r.z * inv_cell);
+  cx = ((cx % nx) + nx) % nx;
+  cy = ((cy % nx) + nx) % nx;
+  cz = ((cz % nx) + nx) % nx;
+  cid[i] = (cz * nx + cy) * nx + cx;
+  aid[i] = i;
+}
+
+__global__ void k_ranges(const int* scid, int* start, int* end, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = scid[k];
+  if (k == 0 || scid[k - 1] != c) start[c] = k;
+  if (k == n - 1 || scid[k + 1] != c) end[c] = k + 1;
+}
+
+// One thread per atom in cell-sorted order; per atom the candidate order is
+// the reference's (verlet_list.cu:154-327).
+__global__ void k_build(const float4* pos, const int* sorted, const int* scid, const int* start, const int* end,
+                        const int* eoff, const int* elist, int* nbr, int* cnt, int n, int nx, float rcs2, float L,
+                        float inv_L, int max_nbr, int* overflow) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = sorted[k];
+  const int c = scid[k];
+  const int cz = c / (nx * nx), cy = (c / nx) % nx, cx = c % nx;
+  const bool dedup = nx < 3;
+  const float4 pi = pos[i];
+  int visited[27];
+  int nvis = 0, count = 0;
+  const int e0 = eoff ? eoff[i] : 0, e1 = eoff ? eoff[i + 1] : 0;
+  for (int dz = -1; dz <= 1; ++dz) {
+    int ncz = cz + dz;
+    ncz = ncz < 0 ? ncz + nx : (ncz >= nx ? ncz - nx : ncz);
+    for (int dy = -1; dy <= 1; ++dy) {
+      int ncy = cy + dy;
+      ncy = ncy < 0 ? ncy + nx : (ncy >= nx ? ncy - nx : ncy);
+      for (int dx = -1; dx <= 1; ++dx) {
+        int ncx = cx + dx;
+        ncx = ncx < 0 ? ncx + nx : (ncx >= nx ? ncx - nx : ncx);
+        const int nc = (ncz * nx + ncy) * nx + ncx;
+        if (dedup) {
+          bool seen = false;
+          for (int v = 0; v < nvis; ++v) seen |= (visited[v] == nc);
+          if (seen) continue;
+          visited[nvis++] = nc;
+        }
+        const int b1 = end[nc];
+        for (int b = start[nc]; b < b1; ++b) {
+          const int j = sorted[b];
+          if (j == i) continue;
+          const float4 pj = __ldg(&pos[j]);
+          const float ddx = min_image_f(pi.x - pj.x, L, inv_L);
+          const float ddy = min_image_f(pi.y - pj.y, L, inv_L);
+          const float ddz = min_image_f(pi.z - pj.z, L, inv_L);
+          const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+          if (r2 < rcs2) {
+            bool ex = false;
+            for (int e = e0; e < e1; ++e) ex |= (elist[e] == j);
+            if (!ex) {
+              if (count < max_nbr) nbr[(size_t)count * n + i] = j;
+              ++count;
+            }
+          }
+        }
+      }
+    }
+  }
+  cnt[i] = count < max_nbr ? count : max_nbr;
+  if (count > max_nbr && overflow) atomicOr(overflow, 1);
+}
+
+// lj.cu:4-107 semantics: force[i] = (F, pe_i) overwritten, virial accumulated.
+__global__ void k_lj(const float4* __restrict__ pos, float4* __restrict__ force, float* __restrict__ virial,
+                     const float2* __restrict__ lj, const int* __restrict__ nbr, const int* __restrict__ cnt, int n,
+                     int ntypes, float rc2, float L, float inv_L) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float fx = 0, fy = 0, fz = 0, pe = 0;
+  float v[6] = {0, 0, 0, 0, 0, 0};
+  if (i < n) {
+    const float4 pi = pos[i];
+    const int ti = __float_as_int(pi.w);
+    const int nn = __ldg(&cnt[i]);
+    for (int k = 0; k < nn; ++k) {
+      const int j = __ldg(&nbr[(size_t)k * n + i]);
+      const float4 pj = __ldg(&pos[j]);
+      const float dx = min_image_f(pi.x - pj.x, L, inv_L);
+      const float dy = min_image_f(pi.y - pj.y, L, inv_L);
+      const float dz = min_image_f(pi.z - pj.z, L, inv_L);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < rc2 && r2 > 1e-10f) {
+        const float2 p = __ldg(&lj[ti * ntypes + __float_as_int(pj.w)]);
+        const float sig2 = p.y * p.y;
+        const float r2inv = __fdividef(1.0f, r2);
+        const float sr2 = sig2 * r2inv;
+        const float sr6 = sr2 * sr2 * sr2;
+        const float sr12 = sr6 * sr6;
+        float fr = 24.0f * p.x * r2inv * (2.0f * sr12 - sr6);
+        fr = fminf(fmaxf(fr, -1000.0f), 1000.0f);
+        const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
+        fx += fxij;
+        fy += fyij;
+        fz += fzij;
+        pe += 0.5f * 4.0f * p.x * (sr12 - sr6);
+        v[0] += 0.5f * fxij * dx;
+        v[1] += 0.5f * fxij * dy;
+        v[2] += 0.5f * fxij * dz;
+        v[3] += 0.5f * fyij * dy;
+        v[4] += 0.5f * fyij * dz;
+        v[5] += 0.5f * fzij * dz;
+      }
+    }
+    force[i] = make_float4(fx, fy, fz, pe);
+  }
+  __shared__ float sm[kBlock / 32][6];
+  for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < 6; ++c) sm[threadIdx.x >> 5][c] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    float s = 0;
+    for (int w = 0; w < kBlock / 32; ++w) s += sm[w][threadIdx.x];
+    atomicAdd(&virial[threadIdx.x], s);
+  }
+}
+
+// morton.cu:4-28: 10 bits per axis from trunc(p * inv_L * 1024) clamped.
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void k_morton_keys(const float4* pos, uint32_t* keys, int* idx, int n, float inv_L) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = pos[i];
+  const uint32_t ix = min(max(__float2uint_rz(p.x * inv_L * 1024.0f), 0u), 1023u);
+  const uint32_t iy = min(max(__float2uint_rz(p.y * inv_L * 1024.0f), 0u), 1023u);
+  const uint32_t iz = min(max(__float2uint_rz(p.z * inv_L * 1024.0f), 0u), 1023u);
+  keys[i] = (spread10(iz) << 2) | (spread10(iy) << 1) | spread10(ix);
+  idx[i] = i;
+}
+
+__global__ void k_gather4(float4* dst, const float4* src, const int* perm, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[perm[i]];
+}
+
+struct MortonScratch {
+  uint32_t* keys;
+  uint32_t* keys_sorted;
+  int* idx;
+  float4* tmp;
+  void* cub;
+  size_t cub_bytes;
+  size_t total;
+};
+
+MortonScratch morton_carve(void* base, int n) {
+  MortonScratch s{};
+  size_t cub_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr, (int*)nullptr,
+                                  (int*)nullptr, n);
+  char* p = (char*)base;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* q = p ? p + off : nullptr;
+    off += align256(bytes);
+    return q;
+  };
+  s.keys = (uint32_t*)take(sizeof(uint32_t) * n);
+  s.keys_sorted = (uint32_t*)take(sizeof(uint32_t) * n);
+  s.idx = (int*)take(sizeof(int) * n);
+  s.tmp = (float4*)take(sizeof(float4) * n);
+  s.cub = take(cub_bytes);
+  s.cub_bytes = cub_bytes;
+  s.total = off;
+  return s;
+}
+
+}  // namespace launch
+}  // namespace fmd
+
+namespace {
+template <typename F>
+fmd_status guarded(F&& f) {
+  try {
+    f();
+    fmd::set_last_error("");
+    return FMD_OK;
+  } catch (const fmd::Error& e) {
+    fmd::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    fmd::set_last_error(e.what());
+    return FMD_ERR_ARG;
+  }
+}
+}  // namespace
+
+using namespace fmd;
+using namespace fmd::launch;
+
+extern "C" {
+
+FMD_API fmd_status fmd_verlet_scratch_bytes(int32_t natoms, float rc_skin, float box_L, size_t* bytes) {
+  return guarded([&] {
+    if (!bytes || natoms <= 0 || rc_skin <= 0 || box_L <= 0) throw Error(FMD_ERR_ARG, "bad argument");
+    const VerletGeom g = verlet_geom(box_L, rc_skin);
+    *bytes = verlet_carve(nullptr, natoms, g.ncell).total;
+  });
+}
+
+FMD_API fmd_status fmd_launch_verlet_build(const void* pos, int32_t natoms, float box_L, const int32_t* excl_off,
+                                           const int32_t* excl_list, float rc_skin, int32_t max_neighbors,
+                                           int32_t* neighbors, int32_t* num_neighbors, void* scratch,
+                                           size_t scratch_bytes, int32_t* overflow_flag, void* stream) {
+  return guarded([&] {
+    if (!pos || natoms <= 0 || !neighbors || !num_neighbors || !scratch || max_neighbors <= 0)
+      throw Error(FMD_ERR_ARG, "bad argument");
+    const VerletGeom g = verlet_geom(box_L, rc_skin);
+    VerletScratch s = verlet_carve(scratch, natoms, g.ncell);
+    if (s.total > scratch_bytes) throw Error(FMD_ERR_ARG, "scratch buffer too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int gr = div_up(natoms, kBlock);
+    k_assign<<<gr, kBlock, 0, st>>>((const float4*)pos, s.cid, s.aid, natoms, g.inv_cell, g.nx);
+    FMD_CUDA_LAUNCH();
+    size_t cb = s.cub_bytes;
+    FMD_CUDA(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.cid, s.cid_sorted, s.aid, s.sorted, natoms, 0, 32, st));
+    FMD_CUDA(cudaMemsetAsync(s.start, 0, sizeof(int) * g.ncell, st));
+    FMD_CUDA(cudaMemsetAsync(s.end, 0, sizeof(int) * g.ncell, st));
+    k_ranges<<<gr, kBlock, 0, st>>>(s.cid_sorted, s.start, s.end, natoms);
+    FMD_CUDA_LAUNCH();
+    const float rcs2 = rc_skin * rc_skin;
+    k_build<<<gr, kBlock, 0, st>>>((const float4*)pos, s.sorted, s.cid_sorted, s.start, s.end, excl_off, excl_list,
+                                   neighbors, num_neighbors, natoms, g.nx, rcs2, box_L, 1.0f / box_L, max_neighbors,
+                                   overflow_flag);
+    FMD_CUDA_LAUNCH();
+  });
+}
+
+FMD_API fmd_status fmd_launch_lj(const void* pos, void* force, float* virial, const void* lj_params,
+                                 const int32_t* neighbors, const int32_t* num_neighbors, int32_t natoms, int32_t ntypes,
+                                 float rc2, float box_L, float inv_L, void* stream) {
+  return guarded([&] {
+    if (!pos || !force || !virial || !lj_params || !neighbors || !num_neighbors || natoms <= 0 || ntypes <= 0)
+      throw Error(FMD_ERR_ARG, "bad argument");
+    k_lj<<<div_up(natoms, kBlock), kBlock, 0, (cudaStream_t)stream>>>(
+        (const float4*)pos, (float4*)force, virial, (const float2*)lj_params, neighbors, num_neighbors, natoms,
+        ntypes, rc2, box_L, inv_L);
+    FMD_CUDA_LAUNCH();
+  });
+}
+
+FMD_API fmd_status fmd_morton_scratch_bytes(int32_t natoms, size_t* bytes) {
+  return guarded([&] {
+    if (!bytes || natoms <= 0) throw Error(FMD_ERR_ARG, "bad argument");
+    *bytes = morton_carve(nullptr, natoms).total;
+  });
+}
+
+FMD_API fmd_status fmd_launch_morton_sort(void* pos, void* vel, int32_t natoms, float inv_L, int32_t* perm,
+                                          void* scratch, size_t scratch_bytes, void* stream) {
+  return guarded([&] {
+    if (!pos || natoms <= 0 || !perm || !scratch) throw Error(FMD_ERR_ARG, "bad argument");
+    MortonScratch s = morton_carve(scratch, natoms);
+    if (s.total > scratch_bytes) throw Error(FMD_ERR_ARG, "scratch buffer too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int gr = div_up(natoms, kBlock);
+    k_morton_keys<<<gr, kBlock, 0, st>>>((const float4*)pos, s.keys, s.idx, natoms, inv_L);
+    FMD_CUDA_LAUNCH();
+    size_t cb = s.cub_bytes;
+    FMD_CUDA(cub::DeviceRadixSort::SortPairs(s.cub, cb, s.keys, s.keys_sorted, s.idx, perm, natoms, 0, 30, st));
+    k_gather4<<<gr, kBlock, 0, st>>>(s.tmp, (const float4*)pos, perm, natoms);
+    FMD_CUDA_LAUNCH();
+    FMD_CUDA(cudaMemcpyAsync(pos, s.tmp, sizeof(float4) * natoms, cudaMemcpyDeviceToDevice, st));
+    if (vel) {
+      k_gather4<<<gr, kBlock, 0, st>>>(s.tmp, (const float4*)vel, perm, natoms);
+      FMD_CUDA_LAUNCH();
+      FMD_CUDA(cudaMemcpyAsync(vel, s.tmp, sizeof(float4) * natoms, cudaMemcpyDeviceToDevice, st));
+    }
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,164 @@
+// Mixed-precision batched engine: device data layout shared by the kernels
+// (mixed_kernels.cu) and the host batch manager (batch.cpp).
+//
+// Layout in HBM.  Replicas occupy disjoint slot segments of the batch arrays;
+// a replica's segment is padded to a multiple of kChunk slots so that no block
+// (one chunk) straddles two replicas, which makes every per-replica reduction
+// independent of what else is in the batch.
+//
+//   pos[s]   float4 {ox, oy, oz, packed}   offset from the atom's cell corner
+//                                          (absolute units) + cell (9 bits per
+//                                          axis) and type (5 bits) in .w
+//   vel[s]   float4 {vx, vy, vz, 1/m}
+//   force[s] float4 {fx, fy, fz, pe_i}
+//   ref[s]   float4 offsets at the last rebuild (displacement test)
+//   img[s]   int4   {ix, iy, iz, atom id}  image flags + replica-local atom id
+//   nbr      uint32 per (tile, k, lane): replica-local slot of j (26 bits) and
+//            the cell shift of j relative to i (2 bits per axis)
+//
+// A position is r = (c + 0) * h + o with h = L / G the cell edge; pair
+// displacements are formed as (o_i - o_j) - e * h, so their precision is set by
+// the cell edge, not by the box size.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "nhc.h"
+
+namespace fmd {
+namespace mixed {
+
+constexpr int kChunk = 128;       // slots per block / per reduction partial
+constexpr int kTile = 32;         // slots per warp tile
+constexpr int kMaxTypes = 16;
+constexpr int kGhostType = 31;
+constexpr int kMaxG = 512;        // cells per axis (9 bits)
+constexpr uint32_t kIdxMask = (1u << 26) - 1;
+constexpr int kNumPartials = 14;  // pe, vir[6], ke[6], sum m v^2
+
+enum Mode : int32_t { kModeRun = 0, kModePushoff = 1 };
+
+// Per-replica record (device).  Static fields are set at admission; dynamic
+// ones are updated by the kernels.
+struct Rep {
+  // --- static
+  int32_t active;
+  int32_t slot_base, slot_cap, natoms;
+  int32_t chunk_base, nchunks;
+  int32_t cell_base, P;          // Morton-keyed cell arrays: P^3 entries (P = pow2 >= G_alloc)
+  int32_t G_alloc;
+  int64_t nbr_base;              // first list entry of the replica's first tile
+  int32_t M;                     // list capacity per atom
+  int32_t bond_base, angle_base; // CSR entry bases
+  int32_t ntypes;
+  int32_t ensemble;
+  int32_t chain_M;
+  int32_t max_between;           // forced rebuild cadence (steps)
+  int64_t nsteps;                // run.conf nsteps (ramp denominator)
+  uint64_t seed;
+  double dt, rc, skin;
+  double T0, T1, Tdamp, P0, P1, Pdamp;
+  double c1;                     // exp(-dt / Tdamp)
+  double Q1, Qr, W, V0;
+  float invm[kMaxTypes];
+  float lj_eps24[kMaxTypes * kMaxTypes];  // 24 eps
+  float lj_sig2[kMaxTypes * kMaxTypes];   // sig^2
+  float fene[4 * 4];             // up to 4 bond types: k, R0^2, eps, sig^2
+  float angp[2 * 4];             // up to 4 angle types: k, theta0
+  // --- dynamic
+  int32_t mode;
+  double fcap;                   // force cap (push-off)
+  double push_dt;
+  int64_t step, stop_step;
+  int32_t since, rebuild_now, adv;
+  int32_t G;
+  double L;      // box edge (barostat value)
+  double Lpos;   // box the stored positions are wrapped in (last pre-force)
+  float h;
+  uint32_t maxdisp_bits;
+  int32_t status;
+  int64_t rebuilds;
+  int32_t cnt_pre, cnt_post;     // last-block counters
+  NHScalars nh;
+  double pending_scale;          // NH post-force velocity scale applied at the next pre-force
+  // reductions of the last completed step
+  double pe, vir[6], ke[6];
+  int64_t thermo_step;
+};
+
+// Device pointers of the batch arrays.
+struct Dev {
+  Rep* reps;
+  const int32_t* chunk_rep;      // replica of each chunk (-1 free)
+  float4* pos;
+  float4* vel;
+  float4* force;
+  float4* ref;
+  int4* img;
+  // rebuild scratch
+  float4* tpos;
+  int4* timg;
+  float4* tvel;
+  uint32_t* key;                 // cell key per slot during a rebuild
+  int32_t* perm;                 // new local slot -> old local slot
+  int32_t* bucket;               // cell bucket (old local slots)
+  int32_t* cell_cnt;             // per cell key
+  int32_t* cell_start;
+  int32_t* cell_fill;
+  // id-indexed (slot_base + atom id)
+  int32_t* slot_of;
+  int32_t* boff;                 // bond CSR offsets (natoms + 1 per replica, relative to bond_base)
+  int32_t* aoff;                 // angle CSR offsets
+  // topology entries
+  int2* bent;                    // {partner id, type | first << 8}
+  int4* aent;                    // {i id, j id, k id, type | role << 8}
+  // neighbor list
+  uint32_t* nbr;
+  int32_t* ncnt;
+  double* part;                  // [chunks][kNumPartials]
+};
+
+__host__ __device__ inline uint32_t spread3(uint32_t v) {
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ inline uint32_t cell_key(int x, int y, int z) {
+  return spread3((uint32_t)x) | (spread3((uint32_t)y) << 1) | (spread3((uint32_t)z) << 2);
+}
+__host__ __device__ inline float pack_w(int cx, int cy, int cz, int type) {
+  uint32_t u = (uint32_t)cx | ((uint32_t)cy << 9) | ((uint32_t)cz << 18) | ((uint32_t)type << 27);
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(u);
+#else
+  float f;
+  __builtin_memcpy(&f, &u, 4);
+  return f;
+#endif
+}
+__host__ __device__ inline uint32_t w_bits(float w) {
+#ifdef __CUDA_ARCH__
+  return __float_as_uint(w);
+#else
+  uint32_t u;
+  __builtin_memcpy(&u, &w, 4);
+  return u;
+#endif
+}
+__host__ __device__ inline int w_cx(uint32_t u) { return (int)(u & 511u); }
+__host__ __device__ inline int w_cy(uint32_t u) { return (int)((u >> 9) & 511u); }
+__host__ __device__ inline int w_cz(uint32_t u) { return (int)((u >> 18) & 511u); }
+__host__ __device__ inline int w_type(uint32_t u) { return (int)(u >> 27); }
+
+// Kernel launchers (mixed_kernels.cu).
+void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st);
+void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells_per_rep, cudaStream_t st);
+void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st);
+void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st);
+
+}  // namespace mixed
+}  // namespace fmd

@@ -1,0 +1,818 @@
+// Mixed-precision batched engine: kernels.
+//
+// One step over every replica of a batch (kernel per phase, one block per
+// 128-slot chunk; a chunk never straddles replicas):
+//   k_pre      half kick / drift (Langevin BAOAB or Nose-Hoover NVT / MTK NPT)
+//              on FP32 cell offsets; per-replica scalar work (thermostat chain,
+//              barostat) recomputed identically by every block in FP64; the
+//              last block of a replica commits it and takes the rebuild decision
+//              (skin/2 displacement test or forced cadence, done on the device).
+//   rebuild    only replicas flagged this step: re-bin into cells, per-cell
+//              deterministic order, permute state, Verlet list (k_bin, k_scan,
+//              k_scatter, k_cellsort, k_permute, k_neighbors).
+//   k_force    LJ over the list + FENE/WCA + harmonic angle gathered per atom
+//              (no atomics), FP32 with compensated sums, FP64 block partials.
+//   k_post     final half kick + FP64 KE-tensor partials; the last block of a
+//              replica reduces all partials in chunk order and runs the
+//              post-force thermostat / barostat update.
+// Reference algorithm sources: integrate/langevin.cu:34-130,
+// integrate/nose_hoover.cu:86-305, 606-898, force/lj.cu:21-65,
+// force/fene.cu:18-73, force/angle.cu:17-80, neighbor/verlet_list.cu:108-335,
+// neighbor/skin_trigger.cuh:6-33, analysis/thermo.cu:88-138.
+#include <cuda_runtime.h>
+
+#include "counter_rng.h"
+#include "dev_common.cuh"
+#include "mixed.cuh"
+#include "nhc.h"
+
+namespace fmd {
+namespace mixed {
+
+struct DExp {
+  __device__ double operator()(double x) const { return exp(x); }
+};
+struct DCbrt {
+  __device__ double operator()(double x) const { return cbrt(x); }
+};
+struct DSinh {
+  __device__ double operator()(double x) const { return sinh(x); }
+};
+
+// Per-step scalars of a replica, computed redundantly by every block.
+struct StepScalars {
+  int adv;
+  int64_t step;  // step being taken (1-based)
+  float hdt, dt;
+  float c1;      // Langevin velocity decay
+  float c2kT;    // c2 * sqrt(kT) (per-type mass applied per atom)
+  float vscale;  // velocity scale applied before the kick (pending post * pre)
+  float ev, fpos;       // NPT: position scale and drift factor
+  float dh;             // NPT: c * dh term (h_old * ev - h_new)
+  float h_new;          // NPT: new cell edge
+  uint32_t stream;
+  int ens;
+  NHScalars nh;         // updated chain / barostat state (committed by the last block)
+  double L_new;
+};
+
+__device__ __forceinline__ double ramp(const Rep& R, int64_t step, double a, double b) {
+  const double frac = (double)(step - 1) / (double)(R.nsteps > 0 ? R.nsteps : 1);
+  return a + (b - a) * frac;
+}
+
+__device__ void compute_step_scalars(const Rep& R, StepScalars& S) {
+  S.adv = R.active && R.step < R.stop_step;
+  S.step = R.step + 1;
+  S.ens = (R.mode == kModePushoff) ? FMD_LANGEVIN : R.ensemble;
+  const double dt = (R.mode == kModePushoff) ? R.push_dt : R.dt;
+  S.dt = (float)dt;
+  S.hdt = (float)(0.5 * dt);
+  S.stream = (R.mode == kModePushoff) ? kStreamPushoff : kStreamLangevin;
+  S.vscale = (float)R.pending_scale;
+  S.ev = 1.0f;
+  S.fpos = (float)dt;
+  S.dh = 0.0f;
+  S.h_new = R.h;
+  S.L_new = R.L;
+  S.nh = R.nh;
+  if (S.ens == FMD_LANGEVIN) {
+    const double kT = (R.mode == kModePushoff) ? R.T0 : ramp(R, S.step, R.T0, R.T1);
+    const double c1 = (R.mode == kModePushoff) ? exp(-dt / R.Tdamp) : R.c1;
+    S.c1 = (float)c1;
+    S.c2kT = (float)(sqrt(1.0 - c1 * c1) * sqrt(kT));
+  } else if (S.ens == FMD_NVT_NH) {
+    const double kT = ramp(R, S.step, R.T0, R.T1);
+    const double sc = nhc_half_step(S.nh.xi, S.nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, S.nh.carry, 0.5 * dt);
+    S.nh.scale = sc;
+    S.vscale = (float)(R.pending_scale * sc);
+  } else {
+    const double kT = ramp(R, S.step, R.T0, R.T1), Pt = ramp(R, S.step, R.P0, R.P1);
+    npt_chain_baro(S.nh, true, 0.0, 0.0, R.chain_M, R.Q1, R.Qr, R.W, 0.5 * dt, dt, R.V0, R.natoms, kT, Pt, DExp(),
+                   DCbrt(), DSinh());
+    S.vscale = (float)(R.pending_scale * (S.nh.scale * S.nh.bscale));
+    S.ev = (float)S.nh.exp_vW;
+    S.fpos = (float)S.nh.fpos;
+    S.L_new = S.nh.L;
+    const double hn = (double)(float)(S.nh.L / R.G);
+    S.h_new = (float)hn;
+    S.dh = (float)((double)R.h * S.nh.exp_vW - hn);
+  }
+}
+
+__device__ __forceinline__ void warp_max_u32(uint32_t& v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+}
+
+// ---------------------------------------------------------------- pre-force
+__global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
+  const int chunk = blockIdx.x;
+  const int r = d.chunk_rep[chunk];
+  if (r < 0) return;
+  Rep& R = d.reps[r];
+  __shared__ StepScalars S;
+  __shared__ uint32_t wmax[kChunk / 32];
+  __shared__ int last;
+  if (threadIdx.x == 0) compute_step_scalars(R, S);
+  __syncthreads();
+  if (!S.adv) return;
+  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  const int s = R.slot_base + local;
+  uint32_t d2bits = 0;
+  int bad = 0;
+  if (local < R.natoms) {
+    float4 p = d.pos[s];
+    float4 v = d.vel[s];
+    const float4 f = d.force[s];
+    float4 q = d.ref[s];
+    const float hm = S.hdt * v.w;
+    v.x *= S.vscale;
+    v.y *= S.vscale;
+    v.z *= S.vscale;
+    if (S.ens == FMD_LANGEVIN) {
+      double n0, n1, n2;
+      rng_normal3(R.seed, S.stream, (uint64_t)S.step, (uint32_t)d.img[s].w, &n0, &n1, &n2);
+      const float ns = S.c2kT * sqrtf(v.w);
+      v.x = fmaf(hm, f.x, v.x);
+      v.y = fmaf(hm, f.y, v.y);
+      v.z = fmaf(hm, f.z, v.z);
+      p.x = fmaf(S.hdt, v.x, p.x);
+      p.y = fmaf(S.hdt, v.y, p.y);
+      p.z = fmaf(S.hdt, v.z, p.z);
+      v.x = fmaf(S.c1, v.x, ns * (float)n0);
+      v.y = fmaf(S.c1, v.y, ns * (float)n1);
+      v.z = fmaf(S.c1, v.z, ns * (float)n2);
+      p.x = fmaf(S.hdt, v.x, p.x);
+      p.y = fmaf(S.hdt, v.y, p.y);
+      p.z = fmaf(S.hdt, v.z, p.z);
+    } else if (S.ens == FMD_NVT_NH) {
+      v.x = fmaf(hm, f.x, v.x);
+      v.y = fmaf(hm, f.y, v.y);
+      v.z = fmaf(hm, f.z, v.z);
+      p.x = fmaf(S.dt, v.x, p.x);
+      p.y = fmaf(S.dt, v.y, p.y);
+      p.z = fmaf(S.dt, v.z, p.z);
+    } else {
+      v.x = fmaf(hm, f.x, v.x);
+      v.y = fmaf(hm, f.y, v.y);
+      v.z = fmaf(hm, f.z, v.z);
+      const uint32_t u = w_bits(p.w);
+      const float cx = (float)w_cx(u), cy = (float)w_cy(u), cz = (float)w_cz(u);
+      p.x = fmaf(p.x, S.ev, fmaf(cx, S.dh, v.x * S.fpos));
+      p.y = fmaf(p.y, S.ev, fmaf(cy, S.dh, v.y * S.fpos));
+      p.z = fmaf(p.z, S.ev, fmaf(cz, S.dh, v.z * S.fpos));
+      q.x = fmaf(q.x, S.ev, cx * S.dh);
+      q.y = fmaf(q.y, S.ev, cy * S.dh);
+      q.z = fmaf(q.z, S.ev, cz * S.dh);
+      d.ref[s] = q;
+    }
+    const float ux = p.x - q.x, uy = p.y - q.y, uz = p.z - q.z;
+    const float dd = ux * ux + uy * uy + uz * uz;
+    bad = !isfinite(dd) || !isfinite(v.x + v.y + v.z);
+    d2bits = __float_as_uint(dd);
+    d.pos[s] = p;
+    d.vel[s] = v;
+  }
+  warp_max_u32(d2bits);
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2bits;
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    uint32_t m = 0;
+    for (int w = 0; w < kChunk / 32; ++w) m = max(m, wmax[w]);
+    atomicMax(&R.maxdisp_bits, m);
+    if (bad) atomicOr(&R.status, kStatusNonFinite);
+    __threadfence();
+    const int old = atomicAdd(&R.cnt_pre, 1);
+    last = (old == R.nchunks - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  // Last block of the replica: commit scalars, decide on a rebuild.
+  __threadfence();
+  R.cnt_pre = 0;
+  R.step = S.step;
+  R.nh = S.nh;
+  R.pending_scale = 1.0;
+  if (S.ens == FMD_NPT_NH) {
+    R.L = S.L_new;
+    R.h = S.h_new;
+  }
+  R.Lpos = R.L;
+  R.adv = 1;
+  R.since += 1;
+  const uint32_t mb = atomicAdd(&R.maxdisp_bits, 0u);
+  const float maxd2 = __uint_as_float(mb);
+  const float hs = (float)(0.5 * R.skin);
+  const bool trig = maxd2 > hs * hs;
+  if (trig || R.since >= R.max_between) {
+    R.since = 0;
+    R.maxdisp_bits = 0u;
+    R.rebuilds += 1;
+    R.rebuild_now = 1;
+  } else {
+    R.rebuild_now = 0;
+  }
+}
+
+// ---------------------------------------------------------------- rebuild
+// Minimum-image cell shift of j relative to i and the periodic wrap count,
+// for cell coordinates ci, cj and offsets oi, oj (one axis).
+__device__ __forceinline__ void pair_shift(int ci, int cj, float oi, float oj, int G, float inv_h, int& e, int& k) {
+  const int dc = ci - cj;
+  const float D = (float)dc + (oi - oj) * inv_h;
+  k = (int)rintf(D / (float)G);
+  e = k * G - dc;
+}
+
+// Cell shift term e*h + k*dL (exact periodic box L = G*h + dL).
+__device__ __forceinline__ float shift_term(int e, int k, float h, float dL) { return (float)e * h + (float)k * dL; }
+
+__global__ void __launch_bounds__(kChunk) k_bin(Dev d) {
+  const int chunk = blockIdx.x;
+  const int r = d.chunk_rep[chunk];
+  if (r < 0) return;
+  const Rep& R = d.reps[r];
+  if (!R.rebuild_now) return;
+  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  if (local >= R.natoms) return;
+  const int s = R.slot_base + local;
+  const float4 p = d.pos[s];
+  int4 im = d.img[s];
+  const uint32_t u = w_bits(p.w);
+  const int c[3] = {w_cx(u), w_cy(u), w_cz(u)};
+  const float o[3] = {p.x, p.y, p.z};
+  const double L = R.L, h = (double)R.h;
+  // New grid for the current box (re-derived at every rebuild).
+  int Gn = (int)floor(L / ((R.rc + R.skin) * 1.0001));
+  Gn = Gn < 1 ? 1 : (Gn > R.G_alloc ? R.G_alloc : Gn);
+  const double hn = (double)(float)(L / Gn);
+  int cn[3];
+  float on[3];
+  int dimg[3];
+  for (int a = 0; a < 3; ++a) {
+    double x = (double)c[a] * h + (double)o[a];
+    int w = 0;
+    if (x < 0.0) {
+      x += L;
+      w = -1;
+    } else if (x >= L) {
+      x -= L;
+      w = 1;
+    }
+    int ca = (int)floor(x / hn);
+    ca = ca < 0 ? 0 : (ca >= Gn ? Gn - 1 : ca);
+    cn[a] = ca;
+    on[a] = (float)(x - (double)ca * hn);
+    dimg[a] = w;
+  }
+  im.x += dimg[0];
+  im.y += dimg[1];
+  im.z += dimg[2];
+  const uint32_t key = cell_key(cn[0], cn[1], cn[2]);
+  d.tpos[s] = make_float4(on[0], on[1], on[2], pack_w(cn[0], cn[1], cn[2], w_type(u)));
+  d.timg[s] = im;
+  d.tvel[s] = d.vel[s];
+  d.key[s] = key;
+  atomicAdd(&d.cell_cnt[R.cell_base + key], 1);
+}
+
+// Exclusive scan of the replica's cell counts; one block per replica.
+__global__ void __launch_bounds__(1024) k_scan(Dev d, int nreps) {
+  const int r = blockIdx.x;
+  if (r >= nreps) return;
+  Rep& R = d.reps[r];
+  if (!R.active || !R.rebuild_now) return;
+  const int ncell = R.P * R.P * R.P;
+  const int per = (ncell + blockDim.x - 1) / blockDim.x;
+  const int b0 = threadIdx.x * per;
+  const int b1 = min(b0 + per, ncell);
+  int sum = 0;
+  for (int c = b0; c < b1; ++c) sum += d.cell_cnt[R.cell_base + c];
+  __shared__ int sm[1024];
+  sm[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int t = threadIdx.x >= off ? sm[threadIdx.x - off] : 0;
+    __syncthreads();
+    sm[threadIdx.x] += t;
+    __syncthreads();
+  }
+  int run = sm[threadIdx.x] - sum;
+  for (int c = b0; c < b1; ++c) {
+    const int n = d.cell_cnt[R.cell_base + c];
+    d.cell_start[R.cell_base + c] = run;
+    d.cell_fill[R.cell_base + c] = run;
+    d.cell_cnt[R.cell_base + c] = 0;
+    run += n;
+  }
+  if (threadIdx.x == 0) {
+    int Gn = (int)floor(R.L / ((R.rc + R.skin) * 1.0001));
+    Gn = Gn < 1 ? 1 : (Gn > R.G_alloc ? R.G_alloc : Gn);
+    R.G = Gn;
+    R.h = (float)(R.L / Gn);
+  }
+}
+
+__global__ void __launch_bounds__(kChunk) k_scatter(Dev d) {
+  const int chunk = blockIdx.x;
+  const int r = d.chunk_rep[chunk];
+  if (r < 0) return;
+  const Rep& R = d.reps[r];
+  if (!R.rebuild_now) return;
+  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  if (local >= R.natoms) return;
+  const int s = R.slot_base + local;
+  const int at = atomicAdd(&d.cell_fill[R.cell_base + d.key[s]], 1);
+  d.bucket[R.slot_base + at] = local;
+}
+
+// Per cell: order members by atom id (deterministic), write the permutation.
+// grid (cell blocks, replicas); 8 warps per block, 32 cells per warp.
+__global__ void __launch_bounds__(256) k_cellsort(Dev d, int nreps) {
+  const int r = blockIdx.y;
+  if (r >= nreps) return;
+  const Rep& R = d.reps[r];
+  if (!R.active || !R.rebuild_now) return;
+  const int ncell = R.P * R.P * R.P;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c0 = (blockIdx.x * 8 + warp) * 32;
+  for (int c = c0; c < c0 + 32 && c < ncell; ++c) {
+    const int st = d.cell_start[R.cell_base + c];
+    const int en = d.cell_fill[R.cell_base + c];
+    const int n = en - st;
+    if (n <= 0) continue;
+    for (int a = lane; a < n; a += 32) {
+      const int old = d.bucket[R.slot_base + st + a];
+      const int id = d.timg[R.slot_base + old].w;
+      int rank = 0;
+      for (int b = 0; b < n; ++b) {
+        const int ob = d.bucket[R.slot_base + st + b];
+        rank += (d.timg[R.slot_base + ob].w < id);
+      }
+      d.perm[R.slot_base + st + rank] = old;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kChunk) k_permute(Dev d) {
+  const int chunk = blockIdx.x;
+  const int r = d.chunk_rep[chunk];
+  if (r < 0) return;
+  const Rep& R = d.reps[r];
+  if (!R.rebuild_now) return;
+  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  const int s = R.slot_base + local;
+  if (local >= R.natoms) {
+    d.ncnt[s] = 0;
+    return;
+  }
+  const int old = R.slot_base + d.perm[s];
+  const float4 p = d.tpos[old];
+  const int4 im = d.timg[old];
+  d.pos[s] = p;
+  d.ref[s] = p;
+  d.vel[s] = d.tvel[old];
+  d.img[s] = im;
+  d.slot_of[R.slot_base + im.w] = local;
+}
+
+// Verlet list: one warp per home cell; candidate cells are staged through
+// registers 32 atoms at a time and broadcast with shuffles.  Pairs within
+// rc + skin, 1-2 bonded pairs excluded (verlet_list.cu:108-335 semantics).
+__global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
+  const int r = blockIdx.y;
+  if (r >= nreps) return;
+  Rep& R = d.reps[r];
+  if (!R.active || !R.rebuild_now) return;
+  const int G = R.G;
+  const int P = R.P;
+  const int ncell = G * G * G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float h = R.h, inv_h = 1.0f / h;
+  const float dL = (float)(R.L - (double)G * (double)h);
+  const float rcs = (float)(R.rc + R.skin);
+  const float rcs2 = rcs * rcs;
+  const int M = R.M;
+  const int base = R.slot_base;
+  int overflow = 0;
+  const int c0 = (blockIdx.x * 8 + warp) * 4;
+  for (int lc = c0; lc < c0 + 4 && lc < ncell; ++lc) {
+    const int hx = lc % G, hy = (lc / G) % G, hz = lc / (G * G);
+    const uint32_t hkey = cell_key(hx, hy, hz);
+    const int hs = d.cell_start[R.cell_base + hkey];
+    const int he = d.cell_fill[R.cell_base + hkey];
+    for (int hb = hs; hb < he; hb += 32) {
+      const int il = hb + lane;
+      const bool act = il < he;
+      float4 pi = make_float4(0, 0, 0, 0);
+      int idi = -1;
+      int b0 = 0, b1 = 0;
+      if (act) {
+        pi = d.pos[base + il];
+        idi = d.img[base + il].w;
+        b0 = d.boff[base + idi];
+        b1 = d.boff[base + idi + 1];
+      }
+      int count = 0;
+      uint32_t* out = d.nbr + R.nbr_base + ((size_t)(il >> 5) * M) * 32 + (il & 31);
+      // Distinct neighbor cells (all 27 when G >= 3).
+      int visited[27];
+      int nvis = 0;
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int nx = (hx + dx + G) % G, ny = (hy + dy + G) % G, nz = (hz + dz + G) % G;
+            const int lin = (nz * G + ny) * G + nx;
+            if (G < 3) {
+              bool seen = false;
+              for (int v = 0; v < nvis; ++v) seen |= (visited[v] == lin);
+              if (seen) continue;
+              visited[nvis++] = lin;
+            }
+            const uint32_t nkey = cell_key(nx, ny, nz);
+            const int ns = d.cell_start[R.cell_base + nkey];
+            const int ne = d.cell_fill[R.cell_base + nkey];
+            for (int jb = ns; jb < ne; jb += 32) {
+              const int jl = jb + lane;
+              float4 pj = make_float4(0, 0, 0, 0);
+              if (jl < ne) pj = d.pos[base + jl];
+              const int m = min(32, ne - jb);
+              for (int t = 0; t < m; ++t) {
+                const float jx = __shfl_sync(0xFFFFFFFFu, pj.x, t);
+                const float jy = __shfl_sync(0xFFFFFFFFu, pj.y, t);
+                const float jz = __shfl_sync(0xFFFFFFFFu, pj.z, t);
+                const float jw = __shfl_sync(0xFFFFFFFFu, pj.w, t);
+                const int j = jb + t;
+                if (!act || j == il) continue;
+                const uint32_t ui = w_bits(pi.w), uj = w_bits(jw);
+                int ex, kx, ey, ky, ez, kz;
+                pair_shift(w_cx(ui), w_cx(uj), pi.x, jx, G, inv_h, ex, kx);
+                pair_shift(w_cy(ui), w_cy(uj), pi.y, jy, G, inv_h, ey, ky);
+                pair_shift(w_cz(ui), w_cz(uj), pi.z, jz, G, inv_h, ez, kz);
+                const float rx = (pi.x - jx) - shift_term(ex, kx, h, dL);
+                const float ry = (pi.y - jy) - shift_term(ey, ky, h, dL);
+                const float rz = (pi.z - jz) - shift_term(ez, kz, h, dL);
+                const float r2 = rx * rx + ry * ry + rz * rz;
+                if (r2 < rcs2) {
+                  if (ex < -1 || ex > 1 || ey < -1 || ey > 1 || ez < -1 || ez > 1) {
+                    overflow |= kStatusCellCapacity;
+                    continue;
+                  }
+                  const int idj = d.img[base + j].w;
+                  bool excl = false;
+                  for (int b = b0; b < b1; ++b) excl |= (d.bent[R.bond_base + b].x == idj);
+                  if (excl) continue;
+                  if (count < M)
+                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)(ex + 1) << 26) | ((uint32_t)(ey + 1) << 28) |
+                                              ((uint32_t)(ez + 1) << 30);
+                  ++count;
+                }
+              }
+            }
+          }
+      if (act) {
+        d.ncnt[base + il] = min(count, M);
+        if (count > M) overflow |= kStatusOverflow;
+      }
+    }
+  }
+  if (overflow) atomicOr(&R.status, overflow);
+}
+
+// ---------------------------------------------------------------- forces
+struct KahanF {
+  float s, c;
+  __device__ __forceinline__ void add(float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+};
+
+__device__ __forceinline__ float sel3(int code, float m, float z, float p) {
+  return code == 0 ? m : (code == 1 ? z : p);
+}
+
+// Displacement r_i - r_j for a bonded pair (cells may differ by any amount).
+__device__ __forceinline__ float3 bonded_dr(float4 pi, float4 pj, int G, float h, float inv_h, float dL) {
+  const uint32_t ui = w_bits(pi.w), uj = w_bits(pj.w);
+  int e, k;
+  float3 r;
+  pair_shift(w_cx(ui), w_cx(uj), pi.x, pj.x, G, inv_h, e, k);
+  r.x = (pi.x - pj.x) - shift_term(e, k, h, dL);
+  pair_shift(w_cy(ui), w_cy(uj), pi.y, pj.y, G, inv_h, e, k);
+  r.y = (pi.y - pj.y) - shift_term(e, k, h, dL);
+  pair_shift(w_cz(ui), w_cz(uj), pi.z, pj.z, G, inv_h, e, k);
+  r.z = (pi.z - pj.z) - shift_term(e, k, h, dL);
+  return r;
+}
+
+template <int BS>
+__device__ __forceinline__ void block_partials(double* vals, int nv, double* out) {
+  __shared__ double sm[BS / 32][8];
+  for (int c = 0; c < nv; ++c) vals[c] = warp_sum(vals[c]);
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < nv; ++c) sm[threadIdx.x >> 5][c] = vals[c];
+  __syncthreads();
+  if (threadIdx.x < nv) {
+    double t = 0.0;
+    for (int w = 0; w < BS / 32; ++w) t += sm[w][threadIdx.x];
+    out[threadIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(kChunk) k_force(Dev d) {
+  const int chunk = blockIdx.x;
+  const int r = d.chunk_rep[chunk];
+  if (r < 0) return;
+  const Rep& R = d.reps[r];
+  if (!R.adv) return;
+  __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
+  const int nt = R.ntypes;
+  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
+    s_eps24[k] = R.lj_eps24[k];
+    s_sig2[k] = R.lj_sig2[k];
+  }
+  __syncthreads();
+  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  const int base = R.slot_base;
+  const int s = base + local;
+  const int G = R.G;
+  const float h = R.h, inv_h = 1.0f / h;
+  const float dL = (float)(R.L - (double)G * (double)h);
+  const float rc2 = (float)(R.rc * R.rc);
+  double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+  int status = 0;
+  if (local < R.natoms) {
+    const float4 pi = d.pos[s];
+    const uint32_t ui = w_bits(pi.w);
+    const int ti = w_type(ui);
+    const int cx = w_cx(ui), cy = w_cy(ui), cz = w_cz(ui);
+    // Per-axis shift for codes 0,1,2 (e = -1, 0, +1), including the periodic
+    // correction dL when the neighbor cell index wraps.
+    const float sxm = -h - (cx == 0 ? dL : 0.0f), sxp = h + (cx == G - 1 ? dL : 0.0f);
+    const float sym = -h - (cy == 0 ? dL : 0.0f), syp = h + (cy == G - 1 ? dL : 0.0f);
+    const float szm = -h - (cz == 0 ? dL : 0.0f), szp = h + (cz == G - 1 ? dL : 0.0f);
+    KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
+    float pe = 0.0f;
+    float v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+    const int nn = d.ncnt[s];
+    const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+#pragma unroll 4
+    for (int k = 0; k < nn; ++k) {
+      const uint32_t w = __ldg(lst + (size_t)k * 32);
+      const float4 pj = __ldg(&d.pos[base + (w & kIdxMask)]);
+      const float dx = (pi.x - pj.x) - sel3((w >> 26) & 3, sxm, 0.0f, sxp);
+      const float dy = (pi.y - pj.y) - sel3((w >> 28) & 3, sym, 0.0f, syp);
+      const float dz = (pi.z - pj.z) - sel3(w >> 30, szm, 0.0f, szp);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < rc2 && r2 > 1e-10f) {
+        const int pidx = ti * nt + w_type(w_bits(pj.w));
+        const float r2inv = 1.0f / r2;
+        const float sr2 = s_sig2[pidx] * r2inv;
+        const float sr6 = sr2 * sr2 * sr2;
+        const float e24 = s_eps24[pidx];
+        float fr = e24 * r2inv * sr6 * (2.0f * sr6 - 1.0f);
+        fr = fminf(fmaxf(fr, -1000.0f), 1000.0f);  // lj.cu:48
+        const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
+        fx.add(fxij);
+        fy.add(fyij);
+        fz.add(fzij);
+        pe = fmaf(e24 * (1.0f / 12.0f), sr6 * (sr6 - 1.0f), pe);  // 1/2 * 4 eps (sr12 - sr6)
+        v0 = fmaf(fxij, dx, v0);
+        v1 = fmaf(fxij, dy, v1);
+        v2 = fmaf(fxij, dz, v2);
+        v3 = fmaf(fyij, dy, v3);
+        v4 = fmaf(fyij, dz, v4);
+        v5 = fmaf(fzij, dz, v5);
+      }
+    }
+    // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
+    float bv[6] = {0.5f * v0, 0.5f * v1, 0.5f * v2, 0.5f * v3, 0.5f * v4, 0.5f * v5};
+    if (R.fcap > 0.0) {  // push-off caps the non-bonded force only
+      float lx = fx.s - fx.c, ly = fy.s - fy.c, lz = fz.s - fz.c;
+      const float m2 = lx * lx + ly * ly + lz * lz;
+      const float cap = (float)R.fcap;
+      if (m2 > cap * cap) {
+        const float sc = cap * rsqrtf(m2);
+        lx *= sc;
+        ly *= sc;
+        lz *= sc;
+      }
+      fx = {lx, 0.0f};
+      fy = {ly, 0.0f};
+      fz = {lz, 0.0f};
+    }
+    const int id = d.img[s].w;
+    // FENE + WCA (fene.cu:18-73), gathered: force on this atom only; the
+    // bond's virial and energy are counted once per atom (half each) ...
+    const int b0 = d.boff[base + id], b1 = d.boff[base + id + 1];
+    for (int b = b0; b < b1; ++b) {
+      const int2 be = d.bent[R.bond_base + b];
+      const int bt = be.y & 0xFF;
+      const int first = be.y >> 8;
+      const float4 pj = d.pos[base + d.slot_of[base + be.x]];
+      const float3 dr = bonded_dr(pi, pj, G, h, inv_h, dL);
+      const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+      const float kf = R.fene[4 * bt], R02 = R.fene[4 * bt + 1], eps = R.fene[4 * bt + 2], sig2 = R.fene[4 * bt + 3];
+      if (r2 >= R02 * 0.9999f) status |= kStatusFeneStretch;
+      const float r2s = fminf(fmaxf(r2, 1e-6f), R02 * 0.9999f);
+      float ff = -kf * R02 / (R02 - r2s);
+      float wpe = 0.0f;
+      if (r2s < sig2 * 1.2599210498948732f) {
+        const float r2inv = 1.0f / r2s;
+        const float sr2 = sig2 * r2inv;
+        const float sr6 = sr2 * sr2 * sr2;
+        ff += 24.0f * eps * r2inv * sr6 * (2.0f * sr6 - 1.0f);
+        wpe = 4.0f * eps * sr6 * (sr6 - 1.0f) + eps;
+      }
+      fx.add(ff * dr.x);
+      fy.add(ff * dr.y);
+      fz.add(ff * dr.z);
+      pe += 0.5f * (-0.5f * kf * R02 * log1pf(-r2s / R02) + wpe);
+      if (first) {
+        bv[0] = fmaf(ff * dr.x, dr.x, bv[0]);
+        bv[1] = fmaf(ff * dr.x, dr.y, bv[1]);
+        bv[2] = fmaf(ff * dr.x, dr.z, bv[2]);
+        bv[3] = fmaf(ff * dr.y, dr.y, bv[3]);
+        bv[4] = fmaf(ff * dr.y, dr.z, bv[4]);
+        bv[5] = fmaf(ff * dr.z, dr.z, bv[5]);
+      }
+    }
+    // Harmonic angle (angle.cu:17-80), gathered by role.
+    const int a0 = d.aoff[base + id], a1 = d.aoff[base + id + 1];
+    for (int a = a0; a < a1; ++a) {
+      const int4 ae = d.aent[R.angle_base + a];
+      const int at = ae.w & 0xFF, role = ae.w >> 8;
+      const float4 ri = d.pos[base + d.slot_of[base + ae.x]];
+      const float4 rj = d.pos[base + d.slot_of[base + ae.y]];
+      const float4 rk = d.pos[base + d.slot_of[base + ae.z]];
+      const float3 dij = bonded_dr(ri, rj, G, h, inv_h, dL);
+      const float3 dkj = bonded_dr(rk, rj, G, h, inv_h, dL);
+      const float rij2 = dij.x * dij.x + dij.y * dij.y + dij.z * dij.z;
+      const float rkj2 = dkj.x * dkj.x + dkj.y * dkj.y + dkj.z * dkj.z;
+      const float rij_inv = rsqrtf(rij2), rkj_inv = rsqrtf(rkj2);
+      float cs = (dij.x * dkj.x + dij.y * dkj.y + dij.z * dkj.z) * rij_inv * rkj_inv;
+      cs = fminf(fmaxf(cs, -1.0f), 1.0f);
+      const float kt = R.angp[2 * at], th0 = R.angp[2 * at + 1];
+      const float dth = acosf(cs) - th0;
+      const float sn = fmaxf(sqrtf(1.0f - cs * cs), 1e-6f);
+      const float pref = 2.0f * kt * dth / sn;
+      const float rr = rij_inv * rkj_inv, i2 = rij_inv * rij_inv, k2 = rkj_inv * rkj_inv;
+      const float fix = pref * (dkj.x * rr - cs * dij.x * i2);
+      const float fiy = pref * (dkj.y * rr - cs * dij.y * i2);
+      const float fiz = pref * (dkj.z * rr - cs * dij.z * i2);
+      const float fkx = pref * (dij.x * rr - cs * dkj.x * k2);
+      const float fky = pref * (dij.y * rr - cs * dkj.y * k2);
+      const float fkz = pref * (dij.z * rr - cs * dkj.z * k2);
+      if (role == 0) {
+        fx.add(fix);
+        fy.add(fiy);
+        fz.add(fiz);
+      } else if (role == 2) {
+        fx.add(fkx);
+        fy.add(fky);
+        fz.add(fkz);
+      } else {
+        fx.add(-(fix + fkx));
+        fy.add(-(fiy + fky));
+        fz.add(-(fiz + fkz));
+        bv[0] += fix * dij.x + fkx * dkj.x;
+        bv[1] += fix * dij.y + fkx * dkj.y;
+        bv[2] += fix * dij.z + fkx * dkj.z;
+        bv[3] += fiy * dij.y + fky * dkj.y;
+        bv[4] += fiy * dij.z + fky * dkj.z;
+        bv[5] += fiz * dij.z + fkz * dkj.z;
+      }
+      pe += kt * dth * dth * (1.0f / 3.0f);
+    }
+    const float ox = fx.s - fx.c, oy = fy.s - fy.c, oz = fz.s - fz.c;
+    if (!isfinite(ox + oy + oz + pe)) status |= kStatusNonFinite;
+    d.force[s] = make_float4(ox, oy, oz, pe);
+    vals[0] = pe;
+    for (int c = 0; c < 6; ++c) vals[1 + c] = bv[c];
+  }
+  status = __syncthreads_or(status);
+  if (threadIdx.x == 0 && status) atomicOr((int*)&d.reps[r].status, status);
+  block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
+}
+
+// ---------------------------------------------------------------- post-force
+__global__ void __launch_bounds__(kChunk) k_post(Dev d, int kick) {
+  const int chunk = blockIdx.x;
+  const int r = d.chunk_rep[chunk];
+  if (r < 0) return;
+  Rep& R = d.reps[r];
+  if (!R.adv) return;
+  __shared__ int last;
+  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  const int s = R.slot_base + local;
+  double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (local < R.natoms) {
+    float4 v = d.vel[s];
+    if (kick) {
+      const float4 f = d.force[s];
+      const double dt = (R.mode == kModePushoff) ? R.push_dt : R.dt;
+      const float hm = (float)(0.5 * dt) * v.w;
+      v.x = fmaf(hm, f.x, v.x);
+      v.y = fmaf(hm, f.y, v.y);
+      v.z = fmaf(hm, f.z, v.z);
+      d.vel[s] = v;
+    }
+    const double m = 1.0 / (double)v.w;
+    const double vx = v.x, vy = v.y, vz = v.z;
+    vals[0] = m * vx * vx;
+    vals[1] = m * vx * vy;
+    vals[2] = m * vx * vz;
+    vals[3] = m * vy * vy;
+    vals[4] = m * vy * vz;
+    vals[5] = m * vz * vz;
+  }
+  block_partials<kChunk>(vals, 6, d.part + (size_t)chunk * kNumPartials + 7);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int old = atomicAdd(&R.cnt_post, 1);
+    last = (old == R.nchunks - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // Last block: reduce the replica's partials in chunk order (warp 0).
+  if (threadIdx.x < 32) {
+    double acc[13];
+    for (int q = 0; q < 13; ++q) acc[q] = 0.0;
+    for (int c = threadIdx.x; c < R.nchunks; c += 32) {
+      const volatile double* pp = d.part + (size_t)(R.chunk_base + c) * kNumPartials;
+      for (int q = 0; q < 13; ++q) acc[q] += pp[q];
+    }
+    for (int q = 0; q < 13; ++q) acc[q] = warp_sum(acc[q]);
+    if (threadIdx.x == 0) {
+      R.cnt_post = 0;
+      R.pe = acc[0];
+      for (int q = 0; q < 6; ++q) {
+        R.vir[q] = acc[1 + q];
+        R.ke[q] = acc[7 + q];
+      }
+      const double ke_raw = acc[7] + acc[10] + acc[12];
+      const double dt = (R.mode == kModePushoff) ? R.push_dt : R.dt;
+      const int ens = (R.mode == kModePushoff) ? FMD_LANGEVIN : R.ensemble;
+      if (!kick) {
+        // Setup: the chain carry starts at the current KE (main.cu:376-390).
+        R.nh.carry = 0.5 * ke_raw;
+        R.pending_scale = 1.0;
+      } else if (ens == FMD_NVT_NH) {
+        const double kT = ramp(R, R.step, R.T0, R.T1);
+        const double ke = 0.5 * ke_raw;
+        const double sc = nhc_half_step(R.nh.xi, R.nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, ke, 0.5 * dt);
+        R.nh.scale = sc;
+        R.nh.carry = ke * sc * sc;
+        R.pending_scale = sc;
+      } else if (ens == FMD_NPT_NH) {
+        const double kT = ramp(R, R.step, R.T0, R.T1), Pt = ramp(R, R.step, R.P0, R.P1);
+        const double vtr = R.vir[0] + R.vir[3] + R.vir[5];
+        npt_chain_baro(R.nh, false, ke_raw, vtr, R.chain_M, R.Q1, R.Qr, R.W, 0.5 * dt, dt, R.V0, R.natoms, kT, Pt,
+                       DExp(), DCbrt(), DSinh());
+        R.L = R.nh.L;
+        R.pending_scale = R.nh.bscale * R.nh.scale;
+      } else {
+        R.pending_scale = 1.0;
+      }
+      R.thermo_step = R.step;
+      R.adv = 0;
+      R.rebuild_now = 0;
+    }
+  }
+}
+
+// NPT post-force: the box changed after the barostat update, so h follows L.
+// (h is re-derived from L at the next pre-force; between the post update and
+// the next pre-force nothing reads h.)
+
+// ---------------------------------------------------------------- launchers
+void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st) {
+  k_pre<<<nchunks, kChunk, 0, st>>>(d);
+  launch_rebuild(d, nchunks, nreps, max_cells, st);
+  k_force<<<nchunks, kChunk, 0, st>>>(d);
+  k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
+}
+
+void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st) {
+  if (max_cells < 1) max_cells = 1;
+  k_bin<<<nchunks, kChunk, 0, st>>>(d);
+  k_scan<<<nreps, 1024, 0, st>>>(d, nreps);
+  k_scatter<<<nchunks, kChunk, 0, st>>>(d);
+  dim3 gs((max_cells + 255) / 256, nreps);
+  k_cellsort<<<gs, 256, 0, st>>>(d, nreps);
+  k_permute<<<nchunks, kChunk, 0, st>>>(d);
+  dim3 gn((max_cells + 31) / 32, nreps);
+  k_neighbors<<<gn, 256, 0, st>>>(d, nreps);
+}
+
+void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st) { k_force<<<nchunks, kChunk, 0, st>>>(d); }
+void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st) { k_post<<<nchunks, kChunk, 0, st>>>(d, 0); }
+
+}  // namespace mixed
+}  // namespace fmd

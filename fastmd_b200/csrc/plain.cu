@@ -876,6 +876,10 @@ class PlainEngine final : public SimEngine {
     k_lj<<<div_up(n_, kBlock), kBlock, 0, st_>>>(pos_, force_, virial_, lj_, nbr_, cnt_, n_, cfg_.ntypes,
                                                  cfg_.rc * cfg_.rc, L_, 1.0 / L_, 1);
     FMD_CUDA_LAUNCH();
+    if (cap > 0) {  // push-off caps the non-bonded force only
+      k_cap<<<div_up(n_, kBlock), kBlock, 0, st_>>>(force_, n_, cap);
+      FMD_CUDA_LAUNCH();
+    }
     if (nb_) {
       k_fene<<<div_up(nb_, kBlock), kBlock, 0, st_>>>(pos_, force_, virial_, bonds_, btype_, fene_, nb_, L_,
                                                       1.0 / L_, 1, status_);
@@ -883,10 +887,6 @@ class PlainEngine final : public SimEngine {
     }
     if (na_) {
       k_angle<<<div_up(na_, kBlock), kBlock, 0, st_>>>(pos_, force_, virial_, angles_, angp_, na_, L_, 1.0 / L_);
-      FMD_CUDA_LAUNCH();
-    }
-    if (cap > 0) {
-      k_cap<<<div_up(n_, kBlock), kBlock, 0, st_>>>(force_, n_, cap);
       FMD_CUDA_LAUNCH();
     }
   }
@@ -916,7 +916,7 @@ class PlainEngine final : public SimEngine {
   }
 
   void run_pushoff(const fmd_melt_spec& sp) {
-    const double dt = sp.pushoff_dt > 0 ? sp.pushoff_dt : cfg_.dt;
+    const double dt = sp.pushoff_dt > 0 ? sp.pushoff_dt : 0.005;
     const double cap = sp.pushoff_fcap > 0 ? sp.pushoff_fcap : 50.0;
     forces(cap);
     for (int k = 0; k < sp.pushoff_steps; ++k) one_step(dt, cap, kStreamPushoff, FMD_LANGEVIN);

@@ -81,8 +81,8 @@ typedef struct fmd_melt_spec {
   double bond_length;    /* random-walk step (0 -> 0.97) */
   double min_dist;       /* reject non-bonded beads closer than this (0 -> 0.8) */
   int32_t pushoff_steps; /* capped-force Langevin steps run on the device at creation (0 -> none) */
-  double pushoff_fcap;   /* |F| cap per atom during push-off (0 -> 50) */
-  double pushoff_dt;     /* push-off time step (0 -> run.conf dt) */
+  double pushoff_fcap;   /* cap on each atom's non-bonded (LJ) force during push-off (0 -> 50) */
+  double pushoff_dt;     /* push-off time step (0 -> 0.005) */
 } fmd_melt_spec;
 
 /* An in-memory system (what a LAMMPS data file carries). */
@@ -218,6 +218,24 @@ FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* 
 FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n);
 /* Totals: active replicas, atoms, device bytes in use. */
 FMD_API fmd_status fmd_batch_totals(fmd_batch* b, int32_t* active, int64_t* atoms, int64_t* bytes);
+
+/* Measurement hooks (device time on the batch's own stream).
+ * fmd_batch_mark records CUDA event `which` (0 or 1) on the batch stream;
+ * fmd_batch_elapsed_ms gives event1 - event0 after synchronizing.
+ * fmd_batch_time_force re-evaluates the force kernel `iters` times on the
+ * current state (idempotent) and returns its mean device time per launch.
+ * fmd_batch_list_stats: total neighbor-list entries and the largest per-atom
+ * count over active replicas.
+ * fmd_batch_kernels_per_step: kernel launches one step issues. */
+FMD_API fmd_status fmd_batch_mark(fmd_batch* b, int32_t which);
+FMD_API fmd_status fmd_batch_elapsed_ms(fmd_batch* b, double* ms);
+FMD_API fmd_status fmd_batch_time_force(fmd_batch* b, int32_t iters, double* ms_per_launch);
+FMD_API fmd_status fmd_batch_list_stats(fmd_batch* b, int64_t* entries, int32_t* max_per_atom);
+FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n);
+/* Set the forced rebuild cadence of a replica (the reference rebuilds at
+ * least every 20 steps, main.cu:401); the skin/2 displacement test still
+ * triggers rebuilds in between. */
+FMD_API fmd_status fmd_batch_set_rebuild_cadence(fmd_batch* b, int32_t slot, int32_t max_steps);
 
 /* ------------------------------------------------------------- serving */
 /* A request loop on its own host thread: submitted requests are admitted as

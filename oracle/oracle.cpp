@@ -754,9 +754,10 @@ struct orc_sim {
   void forces() {
     for (int c = 0; c < 6; ++c) vir[c] = 0;
     lj_from_list(sys, x.data(), L, vl, f.data(), pe.data(), vir);
+    // Push-off caps the non-bonded (LJ) force only, so bonds stay intact.
+    cap_forces(sys.natoms, run.force_cap, f.data());
     fene_add(sys, bi, x.data(), L, f.data(), pe.data(), vir);
     angle_add(sys, bi, x.data(), L, f.data(), pe.data(), vir);
-    cap_forces(sys.natoms, run.force_cap, f.data());
   }
   double ke_raw() const {  // sum m v^2 (nose_hoover.cu:904-939)
     double s = 0;

@@ -121,6 +121,9 @@ def ref_lib():
         R.ref_brute_force_tile_list.restype = C.c_int64
         R.ref_brute_force_tile_list.argtypes = [f32p, C.c_int32, C.c_int32, C.c_float, C.c_float, i32p,
                                                 C.c_int64]
+        R.ref_pairs_within.restype = C.c_int64
+        R.ref_pairs_within.argtypes = [f32p, C.c_int32, C.c_float, C.c_float, C.c_void_p, C.c_void_p, i32p, i32p,
+                                       C.c_int64]
         R.ref_nh_chain.argtypes = [C.c_int32, C.c_float, C.c_float, C.c_int32, f32p, f32p, C.c_float,
                                    C.c_float, C.POINTER(C.c_float), f32p]
         R.ref_parse_config.restype = C.c_int32

@@ -113,6 +113,31 @@ void ref_brute_force_angle(const float* xyz, int32_t n, const int32_t* angles, c
   for (int c = 0; c < 6; ++c) vir[c] = r.virial[c];
 }
 
+// Unordered atom pairs (i < j) with ref::dist2_pbc(...) < rcs * rcs, the
+// reference's FP32 pair predicate (cpu_reference.hpp:11-18), 1-2 bonded
+// pairs given in excl CSR skipped.
+int64_t ref_pairs_within(const float* xyz, int32_t n, float L, float rcs, const int32_t* excl_off,
+                         const int32_t* excl_list, int32_t* pi, int32_t* pj, int64_t cap) {
+  const float inv_L = 1.0f / L, rcs2 = rcs * rcs;
+  int64_t m = 0;
+  for (int32_t i = 0; i < n; ++i)
+    for (int32_t j = i + 1; j < n; ++j) {
+      float d2 = ref::dist2_pbc(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], xyz[3 * j], xyz[3 * j + 1],
+                                xyz[3 * j + 2], L, inv_L);
+      if (!(d2 < rcs2)) continue;
+      bool ex = false;
+      if (excl_off)
+        for (int32_t e = excl_off[i]; e < excl_off[i + 1]; ++e) ex |= (excl_list[e] == j);
+      if (ex) continue;
+      if (m < cap) {
+        pi[m] = i;
+        pj[m] = j;
+      }
+      ++m;
+    }
+  return m;
+}
+
 // Tile pairs within rc_skin (cpu_reference.hpp:59-87): out[2k], out[2k+1].
 int64_t ref_brute_force_tile_list(const float* xyz, int32_t n, int32_t ntiles, float rcs, float L,
                                   int32_t* out, int64_t cap) {

@@ -1,0 +1,129 @@
+"""Mixed form (FP32 forces on cell-relative positions, FP64 reductions and
+thermostat scalars) on the GPU against the FP64 oracle on the same inputs.
+
+Tolerances (stated targets): force RMS error <= 1e-5 relative to the FP64
+oracle; positions after one step within 2e-6 sigma (FP32 offsets); thermo
+values within 1e-5 relative; the neighbor list holds every pair within rc and
+every pair within rc + skin except pairs within 1e-4 of the rc + skin boundary."""
+import numpy as np
+import pytest
+
+import fastmd_b200 as fm
+from oracle import pyoracle as po
+from tests.util import oracle_system, pair_set, rel_rms, run_conf
+
+pytestmark = pytest.mark.gpu
+
+FORCE_RMS_TOL = 1e-5
+
+
+def _melt(nchains, length, seed=7, type_block=0):
+    return fm.generate_melt(nchains, length, density=0.85, seed=seed, type_block=type_block)
+
+
+@pytest.mark.parametrize("nchains,length", [(6, 20), (10, 30), (30, 100), (50, 100)])
+def test_mixed_forces_match_oracle(nchains, length):
+    d = _melt(nchains, length)
+    sim = fm.Simulation(run_conf(), desc=d, form=fm.FMD_FORM_MIXED)
+    x, v, img = sim.state()
+    f, pe, vir = sim.forces()
+    fo, peo, viro = po.forces(oracle_system(d, xyz=x))
+    assert rel_rms(f, fo) < FORCE_RMS_TOL
+    assert abs(pe.sum() - peo.sum()) / abs(peo.sum()) < 1e-5
+    assert np.max(np.abs(vir - viro)) / np.max(np.abs(viro)) < 1e-5
+
+
+def test_mixed_two_types_forces():
+    d = _melt(20, 100, seed=3, type_block=50)
+    lj = [(0, 0, 1.0, 1.0), (1, 1, 1.0, 1.0), (0, 1, 0.9, 1.0)]
+    sim = fm.Simulation(run_conf(ntypes=2, lj=lj), desc=d, form=fm.FMD_FORM_MIXED)
+    x, _, _ = sim.state()
+    f, _, _ = sim.forces()
+    tab = np.ones((2, 2, 2))
+    tab[0, 1, 0] = tab[1, 0, 0] = 0.9
+    fo, _, _ = po.forces(oracle_system(d, xyz=x, lj_table=tab))
+    assert rel_rms(f, fo) < FORCE_RMS_TOL
+
+
+def test_mixed_pair_list_covers_oracle():
+    d = _melt(30, 100, seed=5)
+    sim = fm.Simulation(run_conf(), desc=d, form=fm.FMD_FORM_MIXED)
+    x, _, _ = sim.state()
+    pi, pj = sim.pairs()
+    got = pair_set(pi, pj)
+    oi, oj = po.pairs_brute(x, d.box_L, 2.8, bonds=d.bonds)
+    want = pair_set(oi, oj)
+    # every oracle pair within rc + skin - 1e-4 must be present
+    ii, jj = po.pairs_brute(x, d.box_L, 2.8 - 1e-4, bonds=d.bonds)
+    core = pair_set(ii, jj)
+    assert core <= got
+    # nothing beyond rc + skin + 1e-4
+    oi2, oj2 = po.pairs_brute(x, d.box_L, 2.8 + 1e-4, bonds=d.bonds)
+    assert got <= pair_set(oi2, oj2)
+    assert len(got ^ want) <= 2
+
+
+@pytest.mark.parametrize("ens", ["nvt_langevin 1.0 1.2 1.0 42", "nvt_nh 1.0 1.0 0.5 3",
+                                 "npt_nh 1.0 1.0 0.5 0.5 0.5 1.0 3"])
+def test_mixed_steps_track_oracle(ens):
+    d = _melt(20, 50, seed=11)
+    conf = run_conf(ensemble=ens, nsteps=100)
+    sim = fm.Simulation(conf, desc=d, form=fm.FMD_FORM_MIXED)
+    x0, v0, i0 = sim.state()
+    name = ens.split()[0]
+    a = [float(t) for t in ens.split()[1:]]
+    if name == "nvt_langevin":
+        kw = dict(ensemble="langevin", T=tuple(a[:3]), seed=int(a[3]))
+    elif name == "nvt_nh":
+        kw = dict(ensemble="nvt_nh", T=tuple(a[:3]), chain=int(a[3]))
+    else:
+        kw = dict(ensemble="npt_nh", T=tuple(a[:3]), P=tuple(a[3:6]), chain=int(a[6]))
+    osim = po.Sim(oracle_system(d, xyz=x0, vel=v0, image=i0), dt=0.001, nsteps=100, **kw)
+    for n in (1, 4, 5):
+        sim.step(n)
+        osim.step(n)
+        x, v, img = sim.state()
+        o = osim.state()
+        L = sim.box_L
+        ux = x - o["x"]
+        ux -= L * np.round(ux / L)
+        assert np.max(np.abs(ux)) < 2e-5, name
+        assert rel_rms(v, o["v"]) < 1e-4, name
+        t = sim.thermo().as_array()
+        ot = osim.thermo()
+        assert np.allclose(t, ot, rtol=2e-4, atol=2e-4), (name, t, ot)
+
+
+def test_batch_alone_equals_in_mix():
+    """Each replica's trajectory is bit-identical alone and in a mixed batch."""
+    confs = [run_conf(ensemble=f"nvt_langevin {T} {T} 1.0 {s}", nsteps=200) for T, s in
+             [(1.0, 1), (0.7, 2), (1.3, 3)]]
+    confs.append(run_conf(ensemble="nvt_nh 1.0 1.0 0.5 3", nsteps=200))
+    melts = [_melt(10, 20, seed=1), _melt(25, 40, seed=2), _melt(7, 100, seed=3), _melt(12, 30, seed=4)]
+    mix = fm.Batch(max_replicas=8, max_atoms=1 << 16)
+    slots = [mix.add(c, desc=m) for c, m in zip(confs, melts)]
+    mix.run(60)
+    for c, m, s in zip(confs, melts, slots):
+        alone = fm.Batch(max_replicas=1, max_atoms=1 << 14)
+        a = alone.add(c, desc=m)
+        alone.run(60)
+        xa, va, ia = alone.state(a)
+        xm, vm, im = mix.state(s)
+        assert np.array_equal(xa, xm) and np.array_equal(va, vm) and np.array_equal(ia, im)
+        ta = alone.thermo(a).as_array()
+        tm = mix.thermo(s).as_array()
+        assert np.array_equal(ta, tm)
+        alone.close()
+
+
+def test_pushoff_then_langevin_is_stable():
+    conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 42", nsteps=2000)
+    sim = fm.Simulation(conf, gen=dict(nchains=30, chain_length=100, density=0.85, seed=42, pushoff_steps=2000),
+                        form=fm.FMD_FORM_MIXED)
+    f, _, _ = sim.forces()
+    assert np.max(np.linalg.norm(f, axis=1)) < 2000
+    sim.step(1000)
+    t = sim.thermo()
+    assert 0.8 < t.temp < 1.2
+    assert np.isfinite(t.pe)
+    assert sim.counters()["status_word"] == 0
