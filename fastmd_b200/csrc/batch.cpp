@@ -441,9 +441,65 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
   download_reps_keep(r);
   upload_atoms(r, t.xyz.data(), t.vel.data(), t.image.data());
   graph_dirty_ = true;
-  setup(r);
-  if (pushoff && pushoff->pushoff_steps > 0) run_pushoff(r, *pushoff);
+  if (pushoff && pushoff->pushoff_steps > 0) {
+    // Capped-force push-off runs batched with every other replica admitted
+    // since the last run() (finish_pushoffs); forces are capped from setup on.
+    Rep& P = h_reps_[r];
+    P.mode = kModePushoff;
+    P.fcap = pushoff->pushoff_fcap > 0 ? pushoff->pushoff_fcap : 50.0;
+    P.push_dt = pushoff->pushoff_dt > 0 ? pushoff->pushoff_dt : 0.005;
+    info_[r].pending_pushoff = pushoff->pushoff_steps;
+  }
+  setup({r});
   return r;
+}
+
+void Batch::finish_pushoffs() {
+  std::vector<int> pend;
+  int64_t steps = 0;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used && info_[r].pending_pushoff > 0) {
+      pend.push_back(r);
+      steps = std::max(steps, info_[r].pending_pushoff);
+    }
+  if (pend.empty()) return;
+  download_reps();
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used) h_reps_[r].stop_step = h_reps_[r].step;
+  for (int r : pend) {
+    h_reps_[r].step = 0;
+    h_reps_[r].stop_step = info_[r].pending_pushoff;
+  }
+  upload_reps();
+  if (steps >= graph_steps_) {
+    ensure_graph();
+    for (int64_t k = 0; k < steps / graph_steps_; ++k) FMD_CUDA(cudaGraphLaunch(graph_exec_, st_));
+  }
+  const Dev d = dev();
+  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
+  for (int64_t k = 0; k < steps % graph_steps_; ++k) launch_step(d, nc, nr, mc, st_);
+  FMD_CUDA_LAUNCH();
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  download_reps();
+  for (int r : pend) {
+    info_[r].pending_pushoff = 0;
+    Rep& R3 = h_reps_[r];
+    R3.mode = kModeRun;
+    R3.fcap = 0;
+    R3.step = 0;
+    R3.stop_step = 0;
+    std::memset(&R3.nh, 0, sizeof(R3.nh));
+    R3.nh.scale = 1.0;
+    R3.nh.bscale = 1.0;
+    R3.nh.exp_vW = 1.0;
+    R3.nh.L = R3.L;
+    R3.nh.inv_L = 1.0 / R3.L;
+    R3.nh.V = R3.L * R3.L * R3.L;
+    R3.pending_scale = 1.0;
+    R3.rebuilds = 0;
+  }
+  upload_reps();
+  setup(pend);
 }
 
 // Refresh the host mirror of every replica except r (whose record the host
@@ -459,14 +515,18 @@ void Batch::freeze_others(int r) {
     if (k != r && info_[k].used) h_reps_[k].stop_step = h_reps_[k].step;
 }
 
-// Rebuild + forces + KE reduction without integrating (main.cu:313-390).
-void Batch::setup(int r) {
-  freeze_others(r);
-  Rep& R = h_reps_[r];
-  R.adv = 1;
-  R.rebuild_now = 1;
-  R.since = 0;
-  R.maxdisp_bits = 0;
+// Rebuild + forces + KE reduction without integrating (main.cu:313-390), for
+// the listed replicas; the others are left untouched.
+void Batch::setup(const std::vector<int>& rs) {
+  for (int k = 0; k < max_reps_; ++k)
+    if (info_[k].used) h_reps_[k].stop_step = h_reps_[k].step;
+  for (int r : rs) {
+    Rep& R = h_reps_[r];
+    R.adv = 1;
+    R.rebuild_now = 1;
+    R.since = 0;
+    R.maxdisp_bits = 0;
+  }
   upload_reps();
   const Dev d = dev();
   launch_rebuild(d, nchunks_launch(), nreps_launch(), max_cells(), st_);
@@ -476,7 +536,7 @@ void Batch::setup(int r) {
   launch_reduce_only(d, nchunks_launch(), st_);
   FMD_CUDA_LAUNCH();
   download_reps();
-  check_status(r, true);
+  for (int r : rs) check_status(r, true);
 }
 
 void Batch::check_status(int r, bool throw_on_fault) {
@@ -488,38 +548,6 @@ void Batch::check_status(int r, bool throw_on_fault) {
   if (R.status & kStatusNonFinite) throw Error(FMD_ERR_FAULT, "non-finite state");
   if (R.status & kStatusFeneStretch) throw Error(FMD_ERR_FAULT, "FENE bond stretched to R0");
   throw Error(FMD_ERR_FAULT, "replica fault");
-}
-
-void Batch::run_pushoff(int r, const fmd_melt_spec& sp) {
-  Rep& R = h_reps_[r];
-  R.mode = kModePushoff;
-  R.fcap = sp.pushoff_fcap > 0 ? sp.pushoff_fcap : 50.0;
-  R.push_dt = sp.pushoff_dt > 0 ? sp.pushoff_dt : 0.005;
-  R.step = 0;
-  // forces of the current state must be capped before the first kick
-  setup(r);
-  Rep& R2 = h_reps_[r];
-  R2.stop_step = sp.pushoff_steps;
-  freeze_others(r);
-  upload_reps();
-  advance_direct(sp.pushoff_steps);
-  download_reps();
-  check_status(r, true);
-  Rep& R3 = h_reps_[r];
-  R3.mode = kModeRun;
-  R3.fcap = 0;
-  R3.step = 0;
-  R3.stop_step = 0;
-  std::memset(&R3.nh, 0, sizeof(R3.nh));
-  R3.nh.scale = 1.0;
-  R3.nh.bscale = 1.0;
-  R3.nh.exp_vW = 1.0;
-  R3.nh.L = R3.L;
-  R3.nh.inv_L = 1.0 / R3.L;
-  R3.nh.V = R3.L * R3.L * R3.L;
-  R3.pending_scale = 1.0;
-  R3.rebuilds = 0;
-  setup(r);
 }
 
 void Batch::advance_direct(int64_t nsteps) {
@@ -548,6 +576,7 @@ void Batch::ensure_graph() {
 }
 
 void Batch::run(int64_t nsteps, bool respect_nsteps) {
+  finish_pushoffs();
   if (nsteps <= 0) return;
   download_reps();
   int64_t need = 0;
@@ -687,7 +716,9 @@ void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) {
   FMD_CUDA(cudaMemcpyAsync(hv.data(), vel_.p + R.slot_base, n * sizeof(float4), cudaMemcpyDeviceToHost, st_));
   FMD_CUDA(cudaMemcpyAsync(hi.data(), img_.p + R.slot_base, n * sizeof(int4), cudaMemcpyDeviceToHost, st_));
   FMD_CUDA(cudaStreamSynchronize(st_));
-  const double L = R.Lpos, h = R.h;
+  // Positions are reported wrapped into the current box (after an NPT step
+  // the barostat has already updated L).
+  const double L = R.L, h = R.h;
   for (int s = 0; s < n; ++s) {
     const int id = hi[s].w;
     const uint32_t u = w_bits(hp[s].w);
@@ -697,13 +728,9 @@ void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) {
     for (int a = 0; a < 3; ++a) {
       double x = (double)c[a] * h + (double)o[a];
       int ia = im[a];
-      if (x < 0) {
-        x += L;
-        ia -= 1;
-      } else if (x >= L) {
-        x -= L;
-        ia += 1;
-      }
+      const double fl = std::floor(x / L);
+      x -= fl * L;
+      ia += (int)fl;
       if (xyz) xyz[3 * id + a] = x;
       if (image) image[3 * id + a] = ia;
     }
@@ -731,7 +758,7 @@ void Batch::set_state(int r, const double* xyz, const double* vel, const int32_t
   R.Lpos = R.L;
   R.h = (float)(R.L / R.G);
   upload_atoms(r, x.data(), v.data(), im.data());
-  setup(r);
+  setup({r});
 }
 
 void Batch::forces(int r, double* f, double* pe, double* vir) {
@@ -876,6 +903,7 @@ class MixedEngine final : public SimEngine {
     nb_ = t.nbonds();
     na_ = t.nangles();
     r_ = b_->add(cfg, std::move(t), pushoff);
+    b_->finish_pushoffs();
   }
   void step(int64_t n) override {
     b_->run(n, false);

@@ -52,6 +52,7 @@ struct ReplicaInfo {
   std::vector<int32_t> type, mol;
   int64_t bytes = 0;
   int64_t seg_chunk = -1, seg_cell = -1, seg_nbr = -1, seg_bond = -1, seg_angle = -1;
+  int64_t pending_pushoff = 0;
 };
 
 class Batch {
@@ -73,6 +74,8 @@ class Batch {
   int64_t pairs(int r, int32_t* pi, int32_t* pj, int64_t cap);
   void totals(int32_t* active, int64_t* atoms, int64_t* bytes);
   void check_status(int r, bool throw_on_fault);
+  // Run the capped-force push-off of every replica admitted with one, batched.
+  void finish_pushoffs();
   int64_t budget_bytes() const { return budget_bytes_; }
   int64_t bytes_in_use() const { return bytes_in_use_; }
   cudaStream_t stream() const { return st_; }
@@ -93,8 +96,7 @@ class Batch {
   void upload_reps();
   void freeze_others(int r);
   void upload_atoms(int r, const double* xyz, const double* vel, const int32_t* image);
-  void setup(int r);
-  void run_pushoff(int r, const fmd_melt_spec& sp);
+  void setup(const std::vector<int>& rs);
   void advance_direct(int64_t nsteps);
   void ensure_graph();
 

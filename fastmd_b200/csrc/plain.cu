@@ -729,12 +729,19 @@ class PlainEngine final : public SimEngine {
 
   void get_state(double* xyz, double* vel, int32_t* image) override {
     std::vector<double4> h(n_);
-    if (xyz) {
+    std::vector<int32_t> img(3 * n_);
+    FMD_CUDA(cudaMemcpy(img.data(), image_, 3 * n_ * sizeof(int), cudaMemcpyDeviceToHost));
+    if (xyz || image) {
+      // Reported wrapped into the current box (the barostat may have changed
+      // L after the last pre-force wrap).
       FMD_CUDA(cudaMemcpy(h.data(), pos_, n_ * sizeof(double4), cudaMemcpyDeviceToHost));
       for (int i = 0; i < n_; ++i) {
-        xyz[3 * i] = h[i].x;
-        xyz[3 * i + 1] = h[i].y;
-        xyz[3 * i + 2] = h[i].z;
+        const double r[3] = {h[i].x, h[i].y, h[i].z};
+        for (int a = 0; a < 3; ++a) {
+          const double fl = std::floor(r[a] / L_);
+          if (xyz) xyz[3 * i + a] = r[a] - fl * L_;
+          img[3 * i + a] += (int32_t)fl;
+        }
       }
     }
     if (vel) {
@@ -745,7 +752,7 @@ class PlainEngine final : public SimEngine {
         vel[3 * i + 2] = h[i].z;
       }
     }
-    if (image) FMD_CUDA(cudaMemcpy(image, image_, 3 * n_ * sizeof(int), cudaMemcpyDeviceToHost));
+    if (image) std::memcpy(image, img.data(), 3 * n_ * sizeof(int32_t));
   }
 
   void set_state(const double* xyz, const double* vel, const int32_t* image) override {

@@ -1001,9 +1001,19 @@ int32_t orc_sim_step(orc_sim* s, int64_t nsteps) {
 void orc_sim_get(const orc_sim* s, double* xyz, double* vel, int32_t* image, double* f, double* pe,
                  double* vir) {
   const int32_t n = s->sys.natoms;
-  if (xyz) std::memcpy(xyz, s->x.data(), sizeof(double) * 3 * n);
+  // Positions are reported wrapped into the current box (after an NPT step the
+  // barostat has already changed L; the stored positions are still wrapped in
+  // the box of the last pre-force update).
+  for (int32_t k = 0; k < 3 * n; ++k) {
+    double x = s->x[k];
+    int32_t im = s->img[k];
+    const double fl = std::floor(x / s->L);
+    x -= fl * s->L;
+    im += (int32_t)fl;
+    if (xyz) xyz[k] = x;
+    if (image) image[k] = im;
+  }
   if (vel) std::memcpy(vel, s->v.data(), sizeof(double) * 3 * n);
-  if (image) std::memcpy(image, s->img.data(), sizeof(int32_t) * 3 * n);
   if (f) std::memcpy(f, s->f.data(), sizeof(double) * 3 * n);
   if (pe) std::memcpy(pe, s->pe.data(), sizeof(double) * n);
   if (vir) std::memcpy(vir, s->vir, sizeof(double) * 6);

@@ -1,0 +1,156 @@
+"""Reference-layout launchers (fmd_launch_*) on the GPU against the golden
+fixtures made from the reference's own CPU code.
+
+Device buffers are torch tensors (memory only); the work runs in
+libfastmd_b200.so.  Tolerances: pair sets and the Morton permutation exact
+(the reference's FP32 predicate, evaluated without fused multiply-add on both
+sides); LJ forces within 1e-5 relative RMS of the reference's FP32 brute
+force (summation order differs)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import fastmd_b200 as fm
+from tests.util import pair_set, rel_rms
+
+pytestmark = pytest.mark.gpu
+G = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden.npz"))
+
+
+def _torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _pos4(xyz, types=None):
+    n = len(xyz)
+    p = np.zeros((n, 4), np.float32)
+    p[:, :3] = xyz
+    p[:, 3] = (np.zeros(n, np.int32) if types is None else types.astype(np.int32)).view(np.float32)
+    return p
+
+
+def _excl(n, bonds):
+    per = [[] for _ in range(n)]
+    for a, b in bonds:
+        per[a].append(b)
+        per[b].append(a)
+    off = [0]
+    lst = []
+    for k in range(n):
+        lst += sorted(set(per[k]))
+        off.append(len(lst))
+    return np.array(off, np.int32), np.array(lst if lst else [0], np.int32)
+
+
+def verlet(xyz, L, rcs, bonds=None, max_nbr=256):
+    torch = _torch()
+    lib = fm.lib()
+    n = len(xyz)
+    pos = torch.from_numpy(_pos4(xyz)).cuda()
+    nbr = torch.full((max_nbr * n,), -1, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    sb = C.c_size_t()
+    lib.fmd_verlet_scratch_bytes.restype = C.c_int32
+    assert lib.fmd_verlet_scratch_bytes(C.c_int32(n), C.c_float(rcs), C.c_float(L), C.byref(sb)) == 0
+    scratch = torch.empty(sb.value, dtype=torch.uint8, device="cuda")
+    eo = el = None
+    if bonds is not None and len(bonds):
+        o, l_ = _excl(n, bonds)
+        eo = torch.from_numpy(o).cuda()
+        el = torch.from_numpy(l_).cuda()
+    lib.fmd_launch_verlet_build.restype = C.c_int32
+    st = lib.fmd_launch_verlet_build(C.c_void_p(pos.data_ptr()), C.c_int32(n), C.c_float(L),
+                                     C.c_void_p(eo.data_ptr() if eo is not None else 0),
+                                     C.c_void_p(el.data_ptr() if el is not None else 0), C.c_float(rcs),
+                                     C.c_int32(max_nbr), C.c_void_p(nbr.data_ptr()), C.c_void_p(cnt.data_ptr()),
+                                     C.c_void_p(scratch.data_ptr()), C.c_size_t(sb.value),
+                                     C.c_void_p(flag.data_ptr()), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    return pos, nbr, cnt, flag
+
+
+def list_pairs(nbr, cnt, n, max_nbr=256):
+    nb = nbr.cpu().numpy().reshape(max_nbr, n)
+    c = cnt.cpu().numpy()
+    pi, pj = [], []
+    for i in range(n):
+        for k in range(c[i]):
+            pi.append(i)
+            pj.append(nb[k, i])
+    return np.array(pi), np.array(pj)
+
+
+def test_verlet_launcher_pair_set_lj64_exact():
+    xyz = G["lj64_pos"]
+    _, nbr, cnt, flag = verlet(xyz, 8.0, 3.0)
+    pi, pj = list_pairs(nbr, cnt, len(xyz))
+    assert int(flag.item()) == 0
+    assert pair_set(pi, pj) == pair_set(G["lj64_pairs"][:, 0], G["lj64_pairs"][:, 1])
+
+
+def test_verlet_launcher_pair_set_melt_with_exclusions_exact():
+    xyz = G["melt_pos"]
+    L = float(G["melt_L"][0])
+    _, nbr, cnt, flag = verlet(xyz, L, np.float32(2.8), bonds=G["melt_bonds"])
+    pi, pj = list_pairs(nbr, cnt, len(xyz))
+    assert pair_set(pi, pj) == pair_set(G["melt_pairs"][:, 0], G["melt_pairs"][:, 1])
+
+
+def test_verlet_launcher_reports_overflow():
+    xyz = G["lj64_pos"]
+    _, nbr, cnt, flag = verlet(xyz, 8.0, 3.0, max_nbr=4)
+    assert int(flag.item()) == 1
+    assert int(cnt.max().item()) == 4
+
+
+def test_lj_launcher_matches_reference_forces():
+    torch = _torch()
+    lib = fm.lib()
+    xyz = G["lj64_pos"]
+    n = len(xyz)
+    pos, nbr, cnt, _ = verlet(xyz, 8.0, 3.0)
+    force = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6, dtype=torch.float32, device="cuda")
+    lj = torch.tensor([1.0, 1.0], dtype=torch.float32, device="cuda")
+    lib.fmd_launch_lj.restype = C.c_int32
+    st = lib.fmd_launch_lj(C.c_void_p(pos.data_ptr()), C.c_void_p(force.data_ptr()), C.c_void_p(vir.data_ptr()),
+                           C.c_void_p(lj.data_ptr()), C.c_void_p(nbr.data_ptr()), C.c_void_p(cnt.data_ptr()),
+                           C.c_int32(n), C.c_int32(1), C.c_float(6.25), C.c_float(8.0), C.c_float(0.125), None)
+    assert st == 0
+    f = force.cpu().numpy()
+    # the reference kernel clamps F/r at 1000 (lj.cu:48); its CPU oracle does not
+    mask = np.all(np.abs(G["lj64_f"]) < 500, axis=1)
+    assert rel_rms(f[mask, :3], G["lj64_f"][mask]) < 1e-5
+    assert np.max(np.abs(vir.cpu().numpy() - G["lj64_vir"]) / np.abs(G["lj64_vir"])) < 1e-2  # test_lj.cu:69
+
+
+@pytest.mark.parametrize("pos_key,perm_key,inv", [("morton_pos", "morton_perm", 0.1),
+                                                  ("morton2_pos", "morton2_perm", 1.0 / 15.0)])
+def test_morton_launcher_bit_exact(pos_key, perm_key, inv):
+    torch = _torch()
+    lib = fm.lib()
+    xyz = G[pos_key]
+    n = len(xyz)
+    pos = torch.from_numpy(_pos4(xyz)).cuda()
+    vel = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    vel[:, 0] = torch.arange(n, dtype=torch.float32, device="cuda")
+    perm = torch.zeros(n, dtype=torch.int32, device="cuda")
+    sb = C.c_size_t()
+    lib.fmd_morton_scratch_bytes(C.c_int32(n), C.byref(sb))
+    scratch = torch.empty(sb.value, dtype=torch.uint8, device="cuda")
+    lib.fmd_launch_morton_sort.restype = C.c_int32
+    st = lib.fmd_launch_morton_sort(C.c_void_p(pos.data_ptr()), C.c_void_p(vel.data_ptr()), C.c_int32(n),
+                                    C.c_float(inv), C.c_void_p(perm.data_ptr()), C.c_void_p(scratch.data_ptr()),
+                                    C.c_size_t(sb.value), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    p = perm.cpu().numpy()
+    assert np.array_equal(p, G[perm_key])
+    assert np.array_equal(pos.cpu().numpy()[:, :3], xyz[p])
+    assert np.array_equal(vel.cpu().numpy()[:, 0], p.astype(np.float32))  # test_morton.cu:48
