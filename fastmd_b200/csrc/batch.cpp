@@ -89,7 +89,8 @@ ReplicaPlan plan_replica(const RunConfig& cfg, int32_t natoms, double L) {
 }
 
 int64_t bytes_per_slot() {
-  return 6 * 16 + 2 * 16 + 7 * 4 + (int64_t)(kNumPartials * 8) / kChunk + 1;
+  return 6 * 16 + 2 * 16 + 8 * 4 + kMaxBondsPerAtom * 4 + kMaxAnglesPerAtom * 8 +
+         (int64_t)(kNumPartials * 8) / kChunk + 1;
 }
 
 int64_t estimate_bytes(const ReplicaPlan& p, int32_t nbonds, int32_t nangles) {
@@ -143,6 +144,9 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   boff_.alloc_zero(S);
   aoff_.alloc_zero(S);
   ncnt_.alloc_zero(S);
+  tcnt_.alloc_zero(S);
+  bnd_.alloc(S * kMaxBondsPerAtom);
+  ang_.alloc(S * kMaxAnglesPerAtom);
   part_.alloc_zero(S / kChunk * kNumPartials);
   cell_cnt_.alloc_zero(c.cells);
   cell_start_.alloc_zero(c.cells);
@@ -191,6 +195,9 @@ Dev Batch::dev() const {
   d.aent = aent_;
   d.nbr = nbr_;
   d.ncnt = ncnt_;
+  d.tcnt = tcnt_;
+  d.bnd = bnd_;
+  d.ang = ang_;
   d.part = part_;
   return d;
 }
@@ -333,7 +340,14 @@ void Batch::upload_atoms(int r, const double* xyz, const double* vel, const int3
   }
   const size_t b = R.slot_base;
   FMD_CUDA(cudaMemcpyAsync(pos_.p + b, hp.data(), R.slot_cap * sizeof(float4), cudaMemcpyHostToDevice, st_));
-  FMD_CUDA(cudaMemcpyAsync(ref_.p + b, hp.data(), R.slot_cap * sizeof(float4), cudaMemcpyHostToDevice, st_));
+  std::vector<float4> hr(hp);
+  for (int s = 0; s < R.slot_cap; ++s) {
+    const int32_t id = hi[s].w;
+    float idf;
+    std::memcpy(&idf, &id, 4);
+    hr[s].w = idf;  // the reference copy carries the atom id in .w
+  }
+  FMD_CUDA(cudaMemcpyAsync(ref_.p + b, hr.data(), R.slot_cap * sizeof(float4), cudaMemcpyHostToDevice, st_));
   FMD_CUDA(cudaMemcpyAsync(vel_.p + b, hv.data(), R.slot_cap * sizeof(float4), cudaMemcpyHostToDevice, st_));
   FMD_CUDA(cudaMemcpyAsync(img_.p + b, hi.data(), R.slot_cap * sizeof(int4), cudaMemcpyHostToDevice, st_));
   FMD_CUDA(cudaMemcpyAsync(slot_of_.p + b, so.data(), R.slot_cap * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
@@ -405,6 +419,11 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
     }
     for (int a = 0; a < t.nangles(); ++a)
       for (int k = 0; k < 3; ++k) aoff[t.angles[3 * a + k] + 1]++;
+    for (int i = 0; i < n; ++i) {
+      if (boff[i + 1] > kMaxBondsPerAtom || aoff[i + 1] > kMaxAnglesPerAtom) {
+        throw Error(FMD_ERR_CONFIG, "an atom has more than 4 bonds or 8 angles (mixed-form limit)");
+      }
+    }
     for (int i = 0; i < n; ++i) {
       boff[i + 1] += boff[i];
       aoff[i + 1] += aoff[i];

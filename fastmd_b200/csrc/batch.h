@@ -110,7 +110,9 @@ class Batch {
   DevBuf<float4> pos_, vel_, force_, ref_, tpos_, tvel_;
   DevBuf<int4> img_, timg_;
   DevBuf<uint32_t> key_;
-  DevBuf<int32_t> perm_, bucket_, slot_of_, boff_, aoff_, ncnt_;
+  DevBuf<int32_t> perm_, bucket_, slot_of_, boff_, aoff_, ncnt_, tcnt_;
+  DevBuf<uint32_t> bnd_;
+  DevBuf<uint2> ang_;
   DevBuf<double> part_;
   DevBuf<int32_t> cell_cnt_, cell_start_, cell_fill_;
   DevBuf<int2> bent_;

@@ -11,7 +11,7 @@
 //                                          axis) and type (5 bits) in .w
 //   vel[s]   float4 {vx, vy, vz, 1/m}
 //   force[s] float4 {fx, fy, fz, pe_i}
-//   ref[s]   float4 offsets at the last rebuild (displacement test)
+//   ref[s]   float4 offsets at the last rebuild (displacement test); .w = atom id
 //   img[s]   int4   {ix, iy, iz, atom id}  image flags + replica-local atom id
 //   nbr      uint32 per (tile, k, lane): replica-local slot of j (26 bits) and
 //            the cell shift of j relative to i (2 bits per axis)
@@ -36,6 +36,8 @@ constexpr int kGhostType = 31;
 constexpr int kMaxG = 512;        // cells per axis (9 bits)
 constexpr uint32_t kIdxMask = (1u << 26) - 1;
 constexpr int kNumPartials = 14;  // pe, vir[6], ke[6], sum m v^2
+constexpr int kMaxBondsPerAtom = 4;   // per-slot bonded tables rebuilt with the list
+constexpr int kMaxAnglesPerAtom = 8;
 
 enum Mode : int32_t { kModeRun = 0, kModePushoff = 1 };
 
@@ -113,6 +115,10 @@ struct Dev {
   // topology entries
   int2* bent;                    // {partner id, type | first << 8}
   int4* aent;                    // {i id, j id, k id, type | role << 8}
+  // per-slot bonded tables (rebuilt with the list): partner slots and roles
+  int32_t* tcnt;                 // bonds | angles << 8
+  uint32_t* bnd;                 // [slot * kMaxBondsPerAtom]: partner slot | type << 26 | first << 30
+  uint2* ang;                    // [slot * kMaxAnglesPerAtom]: {other1 | role << 26, other2 | type << 26}
   // neighbor list
   uint32_t* nbr;
   int32_t* ncnt;

@@ -50,6 +50,8 @@ struct StepScalars {
   float ev, fpos;       // NPT: position scale and drift factor
   float dh;             // NPT: c * dh term (h_old * ev - h_new)
   float h_new;          // NPT: new cell edge
+  float h_old, inv_Lold;  // NPT: frame of the stored positions
+  float dW;             // NPT: L_new - L_old * ev, applied per wrapped period
   uint32_t stream;
   int ens;
   NHScalars nh;         // updated chain / barostat state (committed by the last block)
@@ -74,6 +76,9 @@ __device__ void compute_step_scalars(const Rep& R, StepScalars& S) {
   S.fpos = (float)dt;
   S.dh = 0.0f;
   S.h_new = R.h;
+  S.h_old = R.h;
+  S.inv_Lold = (float)(1.0 / R.Lpos);
+  S.dW = 0.0f;
   S.L_new = R.L;
   S.nh = R.nh;
   if (S.ens == FMD_LANGEVIN) {
@@ -97,6 +102,11 @@ __device__ void compute_step_scalars(const Rep& R, StepScalars& S) {
     const double hn = (double)(float)(S.nh.L / R.G);
     S.h_new = (float)hn;
     S.dh = (float)((double)R.h * S.nh.exp_vW - hn);
+    // The reference scales positions wrapped into the previous box
+    // (nose_hoover.cu:729-749 after the wrap of the step before); the scale
+    // factor is not the box ratio, so an atom stored outside [0, L_old) picks
+    // up w * (L_new - L_old * ev) per period w it lies outside.
+    S.dW = (float)(S.nh.L - R.Lpos * S.nh.exp_vW);
   }
 }
 
@@ -132,7 +142,7 @@ __global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
     v.z *= S.vscale;
     if (S.ens == FMD_LANGEVIN) {
       double n0, n1, n2;
-      rng_normal3(R.seed, S.stream, (uint64_t)S.step, (uint32_t)d.img[s].w, &n0, &n1, &n2);
+      rng_normal3(R.seed, S.stream, (uint64_t)S.step, (uint32_t)__float_as_int(q.w), &n0, &n1, &n2);
       const float ns = S.c2kT * sqrtf(v.w);
       v.x = fmaf(hm, f.x, v.x);
       v.y = fmaf(hm, f.y, v.y);
@@ -159,9 +169,12 @@ __global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
       v.z = fmaf(hm, f.z, v.z);
       const uint32_t u = w_bits(p.w);
       const float cx = (float)w_cx(u), cy = (float)w_cy(u), cz = (float)w_cz(u);
-      p.x = fmaf(p.x, S.ev, fmaf(cx, S.dh, v.x * S.fpos));
-      p.y = fmaf(p.y, S.ev, fmaf(cy, S.dh, v.y * S.fpos));
-      p.z = fmaf(p.z, S.ev, fmaf(cz, S.dh, v.z * S.fpos));
+      const float wx = floorf(fmaf(cx, S.h_old, p.x) * S.inv_Lold);
+      const float wy = floorf(fmaf(cy, S.h_old, p.y) * S.inv_Lold);
+      const float wz = floorf(fmaf(cz, S.h_old, p.z) * S.inv_Lold);
+      p.x = fmaf(p.x, S.ev, fmaf(cx, S.dh, fmaf(wx, S.dW, v.x * S.fpos)));
+      p.y = fmaf(p.y, S.ev, fmaf(cy, S.dh, fmaf(wy, S.dW, v.y * S.fpos)));
+      p.z = fmaf(p.z, S.ev, fmaf(cz, S.dh, fmaf(wz, S.dW, v.z * S.fpos)));
       q.x = fmaf(q.x, S.ev, cx * S.dh);
       q.y = fmaf(q.y, S.ev, cy * S.dh);
       q.z = fmaf(q.z, S.ev, cz * S.dh);
@@ -328,7 +341,9 @@ __global__ void __launch_bounds__(kChunk) k_scatter(Dev d) {
 }
 
 // Per cell: order members by atom id (deterministic), write the permutation.
-// grid (cell blocks, replicas); 8 warps per block, 32 cells per warp.
+// grid (cell blocks, replicas); 8 warps per block, 32 cells per warp.  Cells
+// of up to 32 members rank in registers with shuffles; larger ones fall back
+// to a loop over the bucket.
 __global__ void __launch_bounds__(256) k_cellsort(Dev d, int nreps) {
   const int r = blockIdx.y;
   if (r >= nreps) return;
@@ -339,18 +354,25 @@ __global__ void __launch_bounds__(256) k_cellsort(Dev d, int nreps) {
   const int c0 = (blockIdx.x * 8 + warp) * 32;
   for (int c = c0; c < c0 + 32 && c < ncell; ++c) {
     const int st = d.cell_start[R.cell_base + c];
-    const int en = d.cell_fill[R.cell_base + c];
-    const int n = en - st;
+    const int n = d.cell_fill[R.cell_base + c] - st;
     if (n <= 0) continue;
-    for (int a = lane; a < n; a += 32) {
-      const int old = d.bucket[R.slot_base + st + a];
-      const int id = d.timg[R.slot_base + old].w;
-      int rank = 0;
-      for (int b = 0; b < n; ++b) {
-        const int ob = d.bucket[R.slot_base + st + b];
-        rank += (d.timg[R.slot_base + ob].w < id);
+    if (n <= 32) {
+      int old = 0, id = 0x7FFFFFFF;
+      if (lane < n) {
+        old = d.bucket[R.slot_base + st + lane];
+        id = d.timg[R.slot_base + old].w;
       }
-      d.perm[R.slot_base + st + rank] = old;
+      int rank = 0;
+      for (int b = 0; b < n; ++b) rank += (__shfl_sync(0xFFFFFFFFu, id, b) < id);
+      if (lane < n) d.perm[R.slot_base + st + rank] = old;
+    } else {
+      for (int a = lane; a < n; a += 32) {
+        const int old = d.bucket[R.slot_base + st + a];
+        const int id = d.timg[R.slot_base + old].w;
+        int rank = 0;
+        for (int b = 0; b < n; ++b) rank += (d.timg[R.slot_base + d.bucket[R.slot_base + st + b]].w < id);
+        d.perm[R.slot_base + st + rank] = old;
+      }
     }
   }
 }
@@ -371,10 +393,47 @@ __global__ void __launch_bounds__(kChunk) k_permute(Dev d) {
   const float4 p = d.tpos[old];
   const int4 im = d.timg[old];
   d.pos[s] = p;
-  d.ref[s] = p;
+  d.ref[s] = make_float4(p.x, p.y, p.z, __int_as_float(im.w));
   d.vel[s] = d.tvel[old];
   d.img[s] = im;
   d.slot_of[R.slot_base + im.w] = local;
+}
+
+// Per-slot bonded tables for the new order: partner slots instead of atom
+// ids, so the force kernel reaches a partner's position in one load.
+__global__ void __launch_bounds__(kChunk) k_topo(Dev d) {
+  const int chunk = blockIdx.x;
+  const int r = d.chunk_rep[chunk];
+  if (r < 0) return;
+  const Rep& R = d.reps[r];
+  if (!R.rebuild_now) return;
+  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  const int s = R.slot_base + local;
+  if (local >= R.natoms) {
+    d.tcnt[s] = 0;
+    return;
+  }
+  const int base = R.slot_base;
+  const int id = d.img[s].w;
+  const int b0 = d.boff[base + id], b1 = d.boff[base + id + 1];
+  const int a0 = d.aoff[base + id], a1 = d.aoff[base + id + 1];
+  for (int b = b0; b < b1; ++b) {
+    const int2 be = d.bent[R.bond_base + b];
+    const uint32_t ps = (uint32_t)d.slot_of[base + be.x];
+    d.bnd[(size_t)s * kMaxBondsPerAtom + (b - b0)] =
+        ps | ((uint32_t)(be.y & 0xF) << 26) | ((uint32_t)((be.y >> 8) & 1) << 30);
+  }
+  for (int a = a0; a < a1; ++a) {
+    const int4 ae = d.aent[R.angle_base + a];
+    const int role = ae.w >> 8, ty = ae.w & 0xF;
+    const uint32_t si = (uint32_t)d.slot_of[base + ae.x], sj = (uint32_t)d.slot_of[base + ae.y],
+                   sk = (uint32_t)d.slot_of[base + ae.z];
+    const uint32_t o1 = role == 0 ? sj : si;
+    const uint32_t o2 = role == 2 ? sj : sk;
+    d.ang[(size_t)s * kMaxAnglesPerAtom + (a - a0)] =
+        make_uint2(o1 | ((uint32_t)role << 26), o2 | ((uint32_t)ty << 26));
+  }
+  d.tcnt[s] = (b1 - b0) | ((a1 - a0) << 8);
 }
 
 // Verlet list: one warp per home cell; candidate cells are staged through
@@ -386,7 +445,6 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
   Rep& R = d.reps[r];
   if (!R.active || !R.rebuild_now) return;
   const int G = R.G;
-  const int P = R.P;
   const int ncell = G * G * G;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float h = R.h, inv_h = 1.0f / h;
@@ -431,6 +489,10 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
               visited[nvis++] = lin;
             }
             const uint32_t nkey = cell_key(nx, ny, nz);
+            // shift of this neighbor cell relative to the home cell (G >= 3)
+            const float csx = shift_term(dx, (hx + dx < 0) ? -1 : (hx + dx >= G ? 1 : 0), h, dL);
+            const float csy = shift_term(dy, (hy + dy < 0) ? -1 : (hy + dy >= G ? 1 : 0), h, dL);
+            const float csz = shift_term(dz, (hz + dz < 0) ? -1 : (hz + dz >= G ? 1 : 0), h, dL);
             const int ns = d.cell_start[R.cell_base + nkey];
             const int ne = d.cell_fill[R.cell_base + nkey];
             for (int jb = ns; jb < ne; jb += 32) {
@@ -445,14 +507,23 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
                 const float jw = __shfl_sync(0xFFFFFFFFu, pj.w, t);
                 const int j = jb + t;
                 if (!act || j == il) continue;
-                const uint32_t ui = w_bits(pi.w), uj = w_bits(jw);
-                int ex, kx, ey, ky, ez, kz;
-                pair_shift(w_cx(ui), w_cx(uj), pi.x, jx, G, inv_h, ex, kx);
-                pair_shift(w_cy(ui), w_cy(uj), pi.y, jy, G, inv_h, ey, ky);
-                pair_shift(w_cz(ui), w_cz(uj), pi.z, jz, G, inv_h, ez, kz);
-                const float rx = (pi.x - jx) - shift_term(ex, kx, h, dL);
-                const float ry = (pi.y - jy) - shift_term(ey, ky, h, dL);
-                const float rz = (pi.z - jz) - shift_term(ez, kz, h, dL);
+                int ex = dx, ey = dy, ez = dz;
+                float rx, ry, rz;
+                if (G >= 3) {
+                  // the stencil offset is the cell shift; the wrap count follows from it
+                  rx = (pi.x - jx) - csx;
+                  ry = (pi.y - jy) - csy;
+                  rz = (pi.z - jz) - csz;
+                } else {
+                  const uint32_t ui = w_bits(pi.w), uj = w_bits(jw);
+                  int kx, ky, kz;
+                  pair_shift(w_cx(ui), w_cx(uj), pi.x, jx, G, inv_h, ex, kx);
+                  pair_shift(w_cy(ui), w_cy(uj), pi.y, jy, G, inv_h, ey, ky);
+                  pair_shift(w_cz(ui), w_cz(uj), pi.z, jz, G, inv_h, ez, kz);
+                  rx = (pi.x - jx) - shift_term(ex, kx, h, dL);
+                  ry = (pi.y - jy) - shift_term(ey, ky, h, dL);
+                  rz = (pi.z - jz) - shift_term(ez, kz, h, dL);
+                }
                 const float r2 = rx * rx + ry * ry + rz * rz;
                 if (r2 < rcs2) {
                   if (ex < -1 || ex > 1 || ey < -1 || ey > 1 || ez < -1 || ez > 1) {
@@ -523,6 +594,84 @@ __device__ __forceinline__ void block_partials(double* vals, int nv, double* out
   }
 }
 
+// LJ contribution of one listed neighbor to this atom: force components,
+// half the pair energy and the virial half-pair (lj.cu:32-61 semantics).
+struct PairAcc {
+  float fx, fy, fz, pe, v0, v1, v2, v3, v4, v5;
+};
+
+__device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 pj, uint32_t w, float sxm, float sxp, float sym,
+                                        float syp, float szm, float szp, float rc2, float e24, float sig2) {
+  const float dx = (pi.x - pj.x) - sel3((w >> 26) & 3, sxm, 0.0f, sxp);
+  const float dy = (pi.y - pj.y) - sel3((w >> 28) & 3, sym, 0.0f, syp);
+  const float dz = (pi.z - pj.z) - sel3(w >> 30, szm, 0.0f, szp);
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 < rc2 && r2 > 1e-10f) {
+    const float r2inv = __fdividef(1.0f, r2);
+    const float sr2 = sig2 * r2inv;
+    const float sr6 = sr2 * sr2 * sr2;
+    float fr = e24 * r2inv * sr6 * (2.0f * sr6 - 1.0f);
+    fr = fminf(fmaxf(fr, -1000.0f), 1000.0f);  // lj.cu:48
+    const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
+    a.fx += fxij;
+    a.fy += fyij;
+    a.fz += fzij;
+    a.pe = fmaf(e24 * (1.0f / 12.0f), sr6 * (sr6 - 1.0f), a.pe);  // 1/2 * 4 eps (sr12 - sr6)
+    a.v0 = fmaf(fxij, dx, a.v0);
+    a.v1 = fmaf(fxij, dy, a.v1);
+    a.v2 = fmaf(fxij, dz, a.v2);
+    a.v3 = fmaf(fyij, dy, a.v3);
+    a.v4 = fmaf(fyij, dz, a.v4);
+    a.v5 = fmaf(fzij, dz, a.v5);
+  }
+}
+
+// Harmonic angle (angle.cu:17-80): force on member `role` of (i, j, k).
+__device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int role, float kt, float th0, int G,
+                                           float h, float inv_h, float dL, KahanF& fx, KahanF& fy, KahanF& fz,
+                                           float& pe, float* bv) {
+  const float3 dij = bonded_dr(ri, rj, G, h, inv_h, dL);
+  const float3 dkj = bonded_dr(rk, rj, G, h, inv_h, dL);
+  const float rij2 = dij.x * dij.x + dij.y * dij.y + dij.z * dij.z;
+  const float rkj2 = dkj.x * dkj.x + dkj.y * dkj.y + dkj.z * dkj.z;
+  const float rij_inv = rsqrtf(rij2), rkj_inv = rsqrtf(rkj2);
+  float cs = (dij.x * dkj.x + dij.y * dkj.y + dij.z * dkj.z) * rij_inv * rkj_inv;
+  cs = fminf(fmaxf(cs, -1.0f), 1.0f);
+  const float dth = acosf(cs) - th0;
+  const float sn = fmaxf(sqrtf(1.0f - cs * cs), 1e-6f);
+  const float pref = 2.0f * kt * dth / sn;
+  const float rr = rij_inv * rkj_inv, i2 = rij_inv * rij_inv, k2 = rkj_inv * rkj_inv;
+  const float fix = pref * (dkj.x * rr - cs * dij.x * i2);
+  const float fiy = pref * (dkj.y * rr - cs * dij.y * i2);
+  const float fiz = pref * (dkj.z * rr - cs * dij.z * i2);
+  const float fkx = pref * (dij.x * rr - cs * dkj.x * k2);
+  const float fky = pref * (dij.y * rr - cs * dkj.y * k2);
+  const float fkz = pref * (dij.z * rr - cs * dkj.z * k2);
+  if (role == 0) {
+    fx.add(fix);
+    fy.add(fiy);
+    fz.add(fiz);
+  } else if (role == 2) {
+    fx.add(fkx);
+    fy.add(fky);
+    fz.add(fkz);
+  } else {
+    fx.add(-(fix + fkx));
+    fy.add(-(fiy + fky));
+    fz.add(-(fiz + fkz));
+    // the vertex atom carries the angle's virial (counted once per angle)
+    bv[0] += fix * dij.x + fkx * dkj.x;
+    bv[1] += fix * dij.y + fkx * dkj.y;
+    bv[2] += fix * dij.z + fkx * dkj.z;
+    bv[3] += fiy * dij.y + fky * dkj.y;
+    bv[4] += fiy * dij.z + fky * dkj.z;
+    bv[5] += fiz * dij.z + fkz * dkj.z;
+  }
+  pe += kt * dth * dth * (1.0f / 3.0f);
+}
+
+constexpr int kBatch = 8;  // neighbors whose loads are issued together
+
 __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
@@ -556,41 +705,71 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
     const float sym = -h - (cy == 0 ? dL : 0.0f), syp = h + (cy == G - 1 ? dL : 0.0f);
     const float szm = -h - (cz == 0 ? dL : 0.0f), szp = h + (cz == G - 1 ? dL : 0.0f);
     KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
-    float pe = 0.0f;
-    float v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+    PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int nn = d.ncnt[s];
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
-#pragma unroll 4
-    for (int k = 0; k < nn; ++k) {
-      const uint32_t w = __ldg(lst + (size_t)k * 32);
-      const float4 pj = __ldg(&d.pos[base + (w & kIdxMask)]);
-      const float dx = (pi.x - pj.x) - sel3((w >> 26) & 3, sxm, 0.0f, sxp);
-      const float dy = (pi.y - pj.y) - sel3((w >> 28) & 3, sym, 0.0f, syp);
-      const float dz = (pi.z - pj.z) - sel3(w >> 30, szm, 0.0f, szp);
-      const float r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < rc2 && r2 > 1e-10f) {
-        const int pidx = ti * nt + w_type(w_bits(pj.w));
-        const float r2inv = 1.0f / r2;
-        const float sr2 = s_sig2[pidx] * r2inv;
-        const float sr6 = sr2 * sr2 * sr2;
-        const float e24 = s_eps24[pidx];
-        float fr = e24 * r2inv * sr6 * (2.0f * sr6 - 1.0f);
-        fr = fminf(fmaxf(fr, -1000.0f), 1000.0f);  // lj.cu:48
-        const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
-        fx.add(fxij);
-        fy.add(fyij);
-        fz.add(fzij);
-        pe = fmaf(e24 * (1.0f / 12.0f), sr6 * (sr6 - 1.0f), pe);  // 1/2 * 4 eps (sr12 - sr6)
-        v0 = fmaf(fxij, dx, v0);
-        v1 = fmaf(fxij, dy, v1);
-        v2 = fmaf(fxij, dz, v2);
-        v3 = fmaf(fyij, dy, v3);
-        v4 = fmaf(fyij, dz, v4);
-        v5 = fmaf(fzij, dz, v5);
+    const float4* pbase = d.pos + base;
+    const bool one_type = (nt == 1);
+    const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
+    int k = 0;
+    // Batches of kBatch: all list loads, then all position gathers, then the
+    // arithmetic, so each thread keeps 2 * kBatch loads in flight.
+    for (; k + kBatch <= nn; k += kBatch) {
+      uint32_t w[kBatch];
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) w[q] = __ldg(lst + (size_t)(k + q) * 32);
+      float4 pj[kBatch];
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+      PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q) {
+        float e24 = e24_0, sig2 = sig2_0;
+        if (!one_type) {
+          const int pidx = ti * nt + w_type(w_bits(pj[q].w));
+          e24 = s_eps24[pidx];
+          sig2 = s_sig2[pidx];
+        }
+        lj_pair(g, pi, pj[q], w[q], sxm, sxp, sym, syp, szm, szp, rc2, e24, sig2);
       }
+      fx.add(g.fx);
+      fy.add(g.fy);
+      fz.add(g.fz);
+      acc.pe = g.pe;
+      acc.v0 = g.v0;
+      acc.v1 = g.v1;
+      acc.v2 = g.v2;
+      acc.v3 = g.v3;
+      acc.v4 = g.v4;
+      acc.v5 = g.v5;
     }
+    {
+      PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
+      for (; k < nn; ++k) {
+        const uint32_t w = __ldg(lst + (size_t)k * 32);
+        const float4 pj = __ldg(pbase + (w & kIdxMask));
+        float e24 = e24_0, sig2 = sig2_0;
+        if (!one_type) {
+          const int pidx = ti * nt + w_type(w_bits(pj.w));
+          e24 = s_eps24[pidx];
+          sig2 = s_sig2[pidx];
+        }
+        lj_pair(g, pi, pj, w, sxm, sxp, sym, syp, szm, szp, rc2, e24, sig2);
+      }
+      fx.add(g.fx);
+      fy.add(g.fy);
+      fz.add(g.fz);
+      acc.pe = g.pe;
+      acc.v0 = g.v0;
+      acc.v1 = g.v1;
+      acc.v2 = g.v2;
+      acc.v3 = g.v3;
+      acc.v4 = g.v4;
+      acc.v5 = g.v5;
+    }
+    float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
-    float bv[6] = {0.5f * v0, 0.5f * v1, 0.5f * v2, 0.5f * v3, 0.5f * v4, 0.5f * v5};
+    float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
     if (R.fcap > 0.0) {  // push-off caps the non-bonded force only
       float lx = fx.s - fx.c, ly = fy.s - fy.c, lz = fz.s - fz.c;
       const float m2 = lx * lx + ly * ly + lz * lz;
@@ -605,15 +784,15 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
       fy = {ly, 0.0f};
       fz = {lz, 0.0f};
     }
-    const int id = d.img[s].w;
-    // FENE + WCA (fene.cu:18-73), gathered: force on this atom only; the
-    // bond's virial and energy are counted once per atom (half each) ...
-    const int b0 = d.boff[base + id], b1 = d.boff[base + id + 1];
-    for (int b = b0; b < b1; ++b) {
-      const int2 be = d.bent[R.bond_base + b];
-      const int bt = be.y & 0xFF;
-      const int first = be.y >> 8;
-      const float4 pj = d.pos[base + d.slot_of[base + be.x]];
+    const int tc = d.tcnt[s];
+    const int nbd = tc & 0xFF, nang = tc >> 8;
+    // FENE + WCA (fene.cu:18-73), gathered: this atom's force; the bond's
+    // energy is split half per atom and its virial carried by the first atom.
+    const uint32_t* bl = d.bnd + (size_t)s * kMaxBondsPerAtom;
+    for (int b = 0; b < nbd; ++b) {
+      const uint32_t bw = bl[b];
+      const int bt = (bw >> 26) & 0xF;
+      const float4 pj = pbase[bw & kIdxMask];
       const float3 dr = bonded_dr(pi, pj, G, h, inv_h, dL);
       const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
       const float kf = R.fene[4 * bt], R02 = R.fene[4 * bt + 1], eps = R.fene[4 * bt + 2], sig2 = R.fene[4 * bt + 3];
@@ -632,7 +811,7 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
       fy.add(ff * dr.y);
       fz.add(ff * dr.z);
       pe += 0.5f * (-0.5f * kf * R02 * log1pf(-r2s / R02) + wpe);
-      if (first) {
+      if ((bw >> 30) & 1) {
         bv[0] = fmaf(ff * dr.x, dr.x, bv[0]);
         bv[1] = fmaf(ff * dr.x, dr.y, bv[1]);
         bv[2] = fmaf(ff * dr.x, dr.z, bv[2]);
@@ -641,52 +820,20 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
         bv[5] = fmaf(ff * dr.z, dr.z, bv[5]);
       }
     }
-    // Harmonic angle (angle.cu:17-80), gathered by role.
-    const int a0 = d.aoff[base + id], a1 = d.aoff[base + id + 1];
-    for (int a = a0; a < a1; ++a) {
-      const int4 ae = d.aent[R.angle_base + a];
-      const int at = ae.w & 0xFF, role = ae.w >> 8;
-      const float4 ri = d.pos[base + d.slot_of[base + ae.x]];
-      const float4 rj = d.pos[base + d.slot_of[base + ae.y]];
-      const float4 rk = d.pos[base + d.slot_of[base + ae.z]];
-      const float3 dij = bonded_dr(ri, rj, G, h, inv_h, dL);
-      const float3 dkj = bonded_dr(rk, rj, G, h, inv_h, dL);
-      const float rij2 = dij.x * dij.x + dij.y * dij.y + dij.z * dij.z;
-      const float rkj2 = dkj.x * dkj.x + dkj.y * dkj.y + dkj.z * dkj.z;
-      const float rij_inv = rsqrtf(rij2), rkj_inv = rsqrtf(rkj2);
-      float cs = (dij.x * dkj.x + dij.y * dkj.y + dij.z * dkj.z) * rij_inv * rkj_inv;
-      cs = fminf(fmaxf(cs, -1.0f), 1.0f);
+    // Harmonic angles this atom belongs to, by role.
+    const uint2* al = d.ang + (size_t)s * kMaxAnglesPerAtom;
+    for (int a = 0; a < nang; ++a) {
+      const uint2 aw = al[a];
+      const int role = (aw.x >> 26) & 3, at = (aw.y >> 26) & 0xF;
+      const float4 p1 = pbase[aw.x & kIdxMask];
+      const float4 p2 = pbase[aw.y & kIdxMask];
       const float kt = R.angp[2 * at], th0 = R.angp[2 * at + 1];
-      const float dth = acosf(cs) - th0;
-      const float sn = fmaxf(sqrtf(1.0f - cs * cs), 1e-6f);
-      const float pref = 2.0f * kt * dth / sn;
-      const float rr = rij_inv * rkj_inv, i2 = rij_inv * rij_inv, k2 = rkj_inv * rkj_inv;
-      const float fix = pref * (dkj.x * rr - cs * dij.x * i2);
-      const float fiy = pref * (dkj.y * rr - cs * dij.y * i2);
-      const float fiz = pref * (dkj.z * rr - cs * dij.z * i2);
-      const float fkx = pref * (dij.x * rr - cs * dkj.x * k2);
-      const float fky = pref * (dij.y * rr - cs * dkj.y * k2);
-      const float fkz = pref * (dij.z * rr - cs * dkj.z * k2);
-      if (role == 0) {
-        fx.add(fix);
-        fy.add(fiy);
-        fz.add(fiz);
-      } else if (role == 2) {
-        fx.add(fkx);
-        fy.add(fky);
-        fz.add(fkz);
-      } else {
-        fx.add(-(fix + fkx));
-        fy.add(-(fiy + fky));
-        fz.add(-(fiz + fkz));
-        bv[0] += fix * dij.x + fkx * dkj.x;
-        bv[1] += fix * dij.y + fkx * dkj.y;
-        bv[2] += fix * dij.z + fkx * dkj.z;
-        bv[3] += fiy * dij.y + fky * dkj.y;
-        bv[4] += fiy * dij.z + fky * dkj.z;
-        bv[5] += fiz * dij.z + fkz * dkj.z;
-      }
-      pe += kt * dth * dth * (1.0f / 3.0f);
+      if (role == 0)
+        angle_term(pi, p1, p2, 0, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
+      else if (role == 1)
+        angle_term(p1, pi, p2, 1, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
+      else
+        angle_term(p1, p2, pi, 2, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
     }
     const float ox = fx.s - fx.c, oy = fy.s - fy.c, oz = fz.s - fz.c;
     if (!isfinite(ox + oy + oz + pe)) status |= kStatusNonFinite;
@@ -807,6 +954,7 @@ void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, cudaStr
   dim3 gs((max_cells + 255) / 256, nreps);
   k_cellsort<<<gs, 256, 0, st>>>(d, nreps);
   k_permute<<<nchunks, kChunk, 0, st>>>(d);
+  k_topo<<<nchunks, kChunk, 0, st>>>(d);
   dim3 gn((max_cells + 31) / 32, nreps);
   k_neighbors<<<gn, 256, 0, st>>>(d, nreps);
 }
