@@ -12,6 +12,8 @@
 #include <cub/cub.cuh>
 
 #include <cstdint>
+#include <mutex>
+#include <string>
 
 #include "dev_common.cuh"
 #include "host.h"
@@ -264,6 +266,44 @@ MortonScratch morton_carve(void* base, int n) {
   return s;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free Verlet build.  Some callers cannot allocate device memory:
+// code running inside another framework's memory pool or a stream-capture
+// region, or a host process that must not grow its device footprint after
+// start-up.  For them the cell-list scratch of fmd_launch_verlet_build lives in
+// this fixed array, which every GPU that loads the library holds until the
+// process exits.  Its device address is looked up once per device with
+// cudaGetSymbolAddress (the array's name in host code is only a host-side
+// stand-in, never a device pointer).
+constexpr size_t kStaticScratchBytes = (size_t)8 << 20;  // 8 MiB
+constexpr int kStaticMaxAtoms = 1 << 17;                  // 131072 atoms
+constexpr int kStaticMaxCells = 1 << 16;                  // 65536 cells
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_verlet_static_scratch[kStaticScratchBytes];
+
+static std::mutex g_static_mu;
+static void* g_static_ptr[kMaxDevices] = {};
+
+// Device address of the static scratch for the current device (looked up on
+// the first call for that device, with that device current).
+void* static_scratch_for_current_device() {
+  int dev = 0;
+  FMD_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) throw Error(FMD_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_verlet_static_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      throw Error(FMD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    }
+    g_static_ptr[dev] = p;
+  }
+  return g_static_ptr[dev];
+}
+
 }  // namespace launch
 }  // namespace fmd
 
@@ -297,16 +337,12 @@ FMD_API fmd_status fmd_verlet_scratch_bytes(int32_t natoms, float rc_skin, float
   });
 }
 
-FMD_API fmd_status fmd_launch_verlet_build(const void* pos, int32_t natoms, float box_L, const int32_t* excl_off,
-                                           const int32_t* excl_list, float rc_skin, int32_t max_neighbors,
-                                           int32_t* neighbors, int32_t* num_neighbors, void* scratch,
-                                           size_t scratch_bytes, int32_t* overflow_flag, void* stream) {
-  return guarded([&] {
-    if (!pos || natoms <= 0 || !neighbors || !num_neighbors || !scratch || max_neighbors <= 0)
-      throw Error(FMD_ERR_ARG, "bad argument");
-    const VerletGeom g = verlet_geom(box_L, rc_skin);
-    VerletScratch s = verlet_carve(scratch, natoms, g.ncell);
-    if (s.total > scratch_bytes) throw Error(FMD_ERR_ARG, "scratch buffer too small");
+}  // extern "C"
+
+namespace {
+void verlet_build_into(const void* pos, int32_t natoms, float box_L, const int32_t* excl_off, const int32_t* excl_list,
+                       float rc_skin, int32_t max_neighbors, int32_t* neighbors, int32_t* num_neighbors,
+                       const VerletScratch& s, const VerletGeom& g, int32_t* overflow_flag, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const int gr = div_up(natoms, kBlock);
     k_assign<<<gr, kBlock, 0, st>>>((const float4*)pos, s.cid, s.aid, natoms, g.inv_cell, g.nx);
@@ -322,6 +358,46 @@ FMD_API fmd_status fmd_launch_verlet_build(const void* pos, int32_t natoms, floa
                                    neighbors, num_neighbors, natoms, g.nx, rcs2, box_L, 1.0f / box_L, max_neighbors,
                                    overflow_flag);
     FMD_CUDA_LAUNCH();
+}
+}  // namespace
+
+extern "C" {
+
+FMD_API fmd_status fmd_launch_verlet_build(const void* pos, int32_t natoms, float box_L, const int32_t* excl_off,
+                                           const int32_t* excl_list, float rc_skin, int32_t max_neighbors,
+                                           int32_t* neighbors, int32_t* num_neighbors, void* scratch,
+                                           size_t scratch_bytes, int32_t* overflow_flag, void* stream) {
+  return guarded([&] {
+    if (!pos || natoms <= 0 || !neighbors || !num_neighbors || !scratch || max_neighbors <= 0)
+      throw Error(FMD_ERR_ARG, "bad argument");
+    const VerletGeom g = verlet_geom(box_L, rc_skin);
+    const VerletScratch s = verlet_carve(scratch, natoms, g.ncell);
+    if (s.total > scratch_bytes) throw Error(FMD_ERR_ARG, "scratch buffer too small");
+    verlet_build_into(pos, natoms, box_L, excl_off, excl_list, rc_skin, max_neighbors, neighbors, num_neighbors, s, g,
+                      overflow_flag, stream);
+  });
+}
+
+// Same result as fmd_launch_verlet_build, with the scratch in the library's
+// static device array instead of caller memory; allocates nothing.
+FMD_API fmd_status fmd_launch_verlet_build_static(const void* pos, int32_t natoms, float box_L,
+                                                  const int32_t* excl_off, const int32_t* excl_list, float rc_skin,
+                                                  int32_t max_neighbors, int32_t* neighbors, int32_t* num_neighbors,
+                                                  int32_t* overflow_flag, void* stream) {
+  return guarded([&] {
+    if (!pos || natoms <= 0 || !neighbors || !num_neighbors || max_neighbors <= 0)
+      throw Error(FMD_ERR_ARG, "bad argument");
+    if (natoms > kStaticMaxAtoms)
+      throw Error(FMD_ERR_CAPACITY, "natoms exceeds the static-scratch limit of " + std::to_string(kStaticMaxAtoms));
+    const VerletGeom g = verlet_geom(box_L, rc_skin);
+    if (g.ncell > kStaticMaxCells)
+      throw Error(FMD_ERR_CAPACITY, "cell grid exceeds the static-scratch limit of " + std::to_string(kStaticMaxCells) +
+                                        " cells");
+    void* base = static_scratch_for_current_device();
+    const VerletScratch s = verlet_carve(base, natoms, g.ncell);
+    if (s.total > kStaticScratchBytes) throw Error(FMD_ERR_CAPACITY, "problem too large for the static scratch");
+    verlet_build_into(pos, natoms, box_L, excl_off, excl_list, rc_skin, max_neighbors, neighbors, num_neighbors, s, g,
+                      overflow_flag, stream);
   });
 }
 

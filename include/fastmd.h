@@ -284,6 +284,25 @@ FMD_API fmd_status fmd_launch_verlet_build(const void* pos, int32_t natoms, floa
                                            float rc_skin, int32_t max_neighbors, int32_t* neighbors,
                                            int32_t* num_neighbors, void* scratch, size_t scratch_bytes,
                                            int32_t* overflow_flag, void* stream);
+/* Allocation-free variant of fmd_launch_verlet_build; it has no counterpart in
+ * the reference.  It is for callers that cannot allocate device memory: code
+ * running inside another framework's memory pool, inside a stream-capture
+ * region, or in a process that must keep its device footprint fixed after
+ * start-up.  The caller still passes the positions, exclusions and output
+ * buffers; the cell-list scratch lives in one static device array inside the
+ * library (8 MiB, held by every GPU that loads the library until the process
+ * exits).  Limits: natoms <= 131072 and at most 65536 cells (box_L / rc_skin
+ * <= 40 per axis); larger inputs return FMD_ERR_CAPACITY.  The first call on a
+ * device looks the array's address up for that device (cudaGetSymbolAddress),
+ * so make that first call before any stream capture.  Every call on a device
+ * shares the one array and each call re-initialises what must start at zero,
+ * so calls whose kernels overlap on the GPU (different streams, no ordering)
+ * race; order them on one stream.  No cudaMalloc / cudaFree is called. */
+FMD_API fmd_status fmd_launch_verlet_build_static(const void* pos, int32_t natoms, float box_L,
+                                                  const int32_t* exclusion_offsets,
+                                                  const int32_t* exclusion_list, float rc_skin,
+                                                  int32_t max_neighbors, int32_t* neighbors,
+                                                  int32_t* num_neighbors, int32_t* overflow_flag, void* stream);
 /* LJ over the transposed list, replacing launch_lj_kernel (force/lj.cuh:4-12;
  * lj.cu:4-122): force[i] = (F, pe_i) overwritten, virial[6] accumulated. */
 FMD_API fmd_status fmd_launch_lj(const void* pos, void* force, float* virial, const void* lj_params,
