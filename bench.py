@@ -294,7 +294,7 @@ def main():
         lib.fmd_batch_list_stats(b._h, C.byref(entries), C.byref(mx))
         fms = C.c_double()
         lib.fmd_batch_time_force(b._h, 50, C.byref(fms))
-        per_atom_fixed = 180  # see DESIGN.md: pos_i, pos_j set, force, count, id, bonded topology
+        per_atom_fixed = 88  # pos_i, pos_j set, force write, list count, bonded count, bond and angle tables
         alg_bytes = natoms * per_atom_fixed + 4 * entries.value
         achieved = alg_bytes / (fms.value * 1e-3) / 1e9
         peak, kind = measured_peaks()

@@ -230,6 +230,7 @@ static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
   R.ensemble = cfg.ensemble;
   R.chain_M = cfg.chain_length;
   R.max_between = 20;  // main.cu:401
+  R.thermo_freq = cfg.thermo_on ? cfg.thermo_freq : 0;
   R.nsteps = cfg.nsteps;
   R.seed = cfg.seed;
   R.dt = cfg.dt;
@@ -296,6 +297,8 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   R.nh.inv_L = 1.0 / L;
   R.nh.V = L * L * L;
   R.pending_scale = 1.0;
+  R.force_ev = 0;
+  R.ev_step = -1;
 }
 
 // Positions of atoms in data-file order into the replica's slots (slot = id);
@@ -545,6 +548,7 @@ void Batch::setup(const std::vector<int>& rs) {
     R.rebuild_now = 1;
     R.since = 0;
     R.maxdisp_bits = 0;
+    R.force_ev = 1;
   }
   upload_reps();
   const Dev d = dev();
@@ -552,7 +556,7 @@ void Batch::setup(const std::vector<int>& rs) {
   FMD_CUDA_LAUNCH();
   launch_forces_only(d, nchunks_launch(), st_);
   FMD_CUDA_LAUNCH();
-  launch_reduce_only(d, nchunks_launch(), st_);
+  launch_reduce_only(d, nchunks_launch(), st_, 0);
   FMD_CUDA_LAUNCH();
   download_reps();
   for (int r : rs) check_status(r, true);
@@ -780,7 +784,29 @@ void Batch::set_state(int r, const double* xyz, const double* vel, const int32_t
   setup({r});
 }
 
+// Energies and virial of the current state for replica r: steps between
+// thermo steps skip them, so a readout re-evaluates the forces (same
+// positions, same list, same result) with energies on.
+void Batch::ensure_ev(int r) {
+  rep(r);
+  if (h_reps_[r].ev_step == h_reps_[r].step) return;
+  for (int k = 0; k < max_reps_; ++k)
+    if (info_[k].used) h_reps_[k].stop_step = h_reps_[k].step;
+  Rep& R = h_reps_[r];
+  R.adv = 1;
+  R.force_ev = 1;
+  R.rebuild_now = 0;
+  upload_reps();
+  const Dev d = dev();
+  launch_forces_only(d, nchunks_launch(), st_);
+  FMD_CUDA_LAUNCH();
+  launch_reduce_only(d, nchunks_launch(), st_, 2);
+  FMD_CUDA_LAUNCH();
+  download_reps();
+}
+
 void Batch::forces(int r, double* f, double* pe, double* vir) {
+  ensure_ev(r);
   const Rep& R = rep(r);
   const int n = R.natoms;
   std::vector<float4> hf(n);
@@ -801,6 +827,7 @@ void Batch::forces(int r, double* f, double* pe, double* vir) {
 }
 
 void Batch::thermo(int r, fmd_thermo_row* row) {
+  ensure_ev(r);
   const Rep& R = rep(r);
   const int n = R.natoms;
   const double s2 = R.pending_scale * R.pending_scale;

@@ -74,6 +74,7 @@ class Batch {
   int64_t pairs(int r, int32_t* pi, int32_t* pj, int64_t cap);
   void totals(int32_t* active, int64_t* atoms, int64_t* bytes);
   void check_status(int r, bool throw_on_fault);
+  void ensure_ev(int r);
   // Run the capped-force push-off of every replica admitted with one, batched.
   void finish_pushoffs();
   int64_t budget_bytes() const { return budget_bytes_; }

@@ -181,7 +181,7 @@ FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n) {
   return guarded([&] {
     B(b);
     if (!n) throw fmd::Error(FMD_ERR_ARG, "null argument");
-    *n = 9;  // k_pre, 6 rebuild kernels (early exit unless flagged), k_force, k_post
+    *n = 11;  // k_pre, 7 rebuild kernels (early exit unless flagged), k_force x2 (with and without energies), k_post
   });
 }
 

@@ -13,8 +13,9 @@
 //   force[s] float4 {fx, fy, fz, pe_i}
 //   ref[s]   float4 offsets at the last rebuild (displacement test); .w = atom id
 //   img[s]   int4   {ix, iy, iz, atom id}  image flags + replica-local atom id
-//   nbr      uint32 per (tile, k, lane): replica-local slot of j (26 bits) and
-//            the cell shift of j relative to i (2 bits per axis)
+//   nbr      uint32 per (tile, k, lane): replica-local slot of j (27 bits) and
+//            the cell shift of j relative to i as one code
+//            (ex + 1) * 9 + (ey + 1) * 3 + (ez + 1) in the top 5 bits
 //
 // A position is r = (c + 0) * h + o with h = L / G the cell edge; pair
 // displacements are formed as (o_i - o_j) - e * h, so their precision is set by
@@ -34,7 +35,8 @@ constexpr int kTile = 32;         // slots per warp tile
 constexpr int kMaxTypes = 16;
 constexpr int kGhostType = 31;
 constexpr int kMaxG = 512;        // cells per axis (9 bits)
-constexpr uint32_t kIdxMask = (1u << 26) - 1;
+constexpr uint32_t kIdxMask = (1u << 27) - 1;     // neighbor-list slot field
+constexpr uint32_t kSlotMask26 = (1u << 26) - 1;  // bonded-table slot field
 constexpr int kNumPartials = 14;  // pe, vir[6], ke[6], sum m v^2
 constexpr int kMaxBondsPerAtom = 4;   // per-slot bonded tables rebuilt with the list
 constexpr int kMaxAnglesPerAtom = 8;
@@ -87,6 +89,9 @@ struct Rep {
   // reductions of the last completed step
   double pe, vir[6], ke[6];
   int64_t thermo_step;
+  int32_t thermo_freq;           // run.conf thermo cadence (0: off); energies/virial computed on those steps
+  int32_t force_ev;              // host request: compute energies/virial at the next force evaluation
+  int64_t ev_step;               // step whose energies/virial are in pe/vir
 };
 
 // Device pointers of the batch arrays.
@@ -164,7 +169,7 @@ __host__ __device__ inline int w_type(uint32_t u) { return (int)(u >> 27); }
 void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st);
 void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells_per_rep, cudaStream_t st);
 void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st);
-void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st);
+void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode);  // 0 setup, 2 re-evaluation
 
 }  // namespace mixed
 }  // namespace fmd

@@ -535,8 +535,7 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
                   for (int b = b0; b < b1; ++b) excl |= (d.bent[R.bond_base + b].x == idj);
                   if (excl) continue;
                   if (count < M)
-                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)(ex + 1) << 26) | ((uint32_t)(ey + 1) << 28) |
-                                              ((uint32_t)(ez + 1) << 30);
+                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)((ex + 1) * 9 + (ey + 1) * 3 + (ez + 1)) << 27);
                   ++count;
                 }
               }
@@ -552,6 +551,8 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
 }
 
 // ---------------------------------------------------------------- forces
+constexpr int kBatch = 8;  // neighbors whose loads are issued together
+
 struct KahanF {
   float s, c;
   __device__ __forceinline__ void add(float x) {
@@ -594,17 +595,18 @@ __device__ __forceinline__ void block_partials(double* vals, int nv, double* out
   }
 }
 
-// LJ contribution of one listed neighbor to this atom: force components,
-// half the pair energy and the virial half-pair (lj.cu:32-61 semantics).
+// LJ contribution of one listed neighbor (lj.cu:32-61 semantics).  t is
+// pos_i - shift for the entry's cell-shift code, so r_ij = t - pos_j.
+// EV: also accumulate half the pair energy and the virial half-pair.
 struct PairAcc {
   float fx, fy, fz, pe, v0, v1, v2, v3, v4, v5;
 };
 
-__device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 pj, uint32_t w, float sxm, float sxp, float sym,
-                                        float syp, float szm, float szp, float rc2, float e24, float sig2) {
-  const float dx = (pi.x - pj.x) - sel3((w >> 26) & 3, sxm, 0.0f, sxp);
-  const float dy = (pi.y - pj.y) - sel3((w >> 28) & 3, sym, 0.0f, syp);
-  const float dz = (pi.z - pj.z) - sel3(w >> 30, szm, 0.0f, szp);
+template <bool EV>
+__device__ __forceinline__ void lj_pair(PairAcc& a, float4 t, float4 pj, float rc2, float e24, float sig2) {
+  const float dx = t.x - pj.x;
+  const float dy = t.y - pj.y;
+  const float dz = t.z - pj.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   if (r2 < rc2 && r2 > 1e-10f) {
     const float r2inv = __fdividef(1.0f, r2);
@@ -616,14 +618,65 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 pj, uint32
     a.fx += fxij;
     a.fy += fyij;
     a.fz += fzij;
-    a.pe = fmaf(e24 * (1.0f / 12.0f), sr6 * (sr6 - 1.0f), a.pe);  // 1/2 * 4 eps (sr12 - sr6)
-    a.v0 = fmaf(fxij, dx, a.v0);
-    a.v1 = fmaf(fxij, dy, a.v1);
-    a.v2 = fmaf(fxij, dz, a.v2);
-    a.v3 = fmaf(fyij, dy, a.v3);
-    a.v4 = fmaf(fyij, dz, a.v4);
-    a.v5 = fmaf(fzij, dz, a.v5);
+    if (EV) {
+      a.pe = fmaf(e24 * (1.0f / 12.0f), sr6 * (sr6 - 1.0f), a.pe);  // 1/2 * 4 eps (sr12 - sr6)
+      a.v0 = fmaf(fxij, dx, a.v0);
+      a.v1 = fmaf(fxij, dy, a.v1);
+      a.v2 = fmaf(fxij, dz, a.v2);
+      a.v3 = fmaf(fyij, dy, a.v3);
+      a.v4 = fmaf(fyij, dz, a.v4);
+      a.v5 = fmaf(fzij, dz, a.v5);
+    }
   }
+}
+
+// The LJ loop over one atom's list: batches of kBatch entries (all list
+// loads, then all position gathers, then the arithmetic).
+template <bool EV>
+__device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, const float4* tab, int tid,
+                                        bool one_type, int ti, int nt, const float* s_eps24, const float* s_sig2,
+                                        float rc2, KahanF& fx, KahanF& fy, KahanF& fz, PairAcc& acc) {
+  const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
+  int k = 0;
+  for (; k + kBatch <= nn; k += kBatch) {
+    uint32_t w[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) w[q] = __ldg(lst + (size_t)(k + q) * 32);
+    float4 pj[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+    PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      float e24 = e24_0, sig2 = sig2_0;
+      if (!one_type) {
+        const int pidx = ti * nt + w_type(w_bits(pj[q].w));
+        e24 = s_eps24[pidx];
+        sig2 = s_sig2[pidx];
+      }
+      lj_pair<EV>(g, tab[(w[q] >> 27) * kChunk + tid], pj[q], rc2, e24, sig2);
+    }
+    fx.add(g.fx);
+    fy.add(g.fy);
+    fz.add(g.fz);
+    acc = g;
+  }
+  PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
+  for (; k < nn; ++k) {
+    const uint32_t w = __ldg(lst + (size_t)k * 32);
+    const float4 pj = __ldg(pbase + (w & kIdxMask));
+    float e24 = e24_0, sig2 = sig2_0;
+    if (!one_type) {
+      const int pidx = ti * nt + w_type(w_bits(pj.w));
+      e24 = s_eps24[pidx];
+      sig2 = s_sig2[pidx];
+    }
+    lj_pair<EV>(g, tab[(w >> 27) * kChunk + tid], pj, rc2, e24, sig2);
+  }
+  fx.add(g.fx);
+  fy.add(g.fy);
+  fz.add(g.fz);
+  acc = g;
 }
 
 // Harmonic angle (angle.cu:17-80): force on member `role` of (i, j, k).
@@ -670,14 +723,27 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
   pe += kt * dth * dth * (1.0f / 3.0f);
 }
 
-constexpr int kBatch = 8;  // neighbors whose loads are issued together
+// Energies and virial are needed on thermo steps, for NPT (the barostat uses
+// the virial every step) and when the host asks for them.
+__device__ __forceinline__ bool need_ev(const Rep& R) {
+  if (R.force_ev) return true;
+  if (R.mode != kModePushoff && R.ensemble == FMD_NPT_NH) return true;
+  return R.thermo_freq > 0 && (R.step % R.thermo_freq) == 0;
+}
 
+// Two instantiations: with energies / virial (thermo steps, NPT, host
+// requests) and without (all other steps); a block runs in the one that
+// matches its replica's need this step and the other returns at once.
+template <bool EV>
 __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
   const Rep& R = d.reps[r];
   if (!R.adv) return;
+  if (need_ev(R) != EV) return;
+  extern __shared__ float4 tab[];  // [27][kChunk]
+  constexpr bool ev = EV;
   __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
   const int nt = R.ntypes;
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
@@ -704,69 +770,20 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
     const float sxm = -h - (cx == 0 ? dL : 0.0f), sxp = h + (cx == G - 1 ? dL : 0.0f);
     const float sym = -h - (cy == 0 ? dL : 0.0f), syp = h + (cy == G - 1 ? dL : 0.0f);
     const float szm = -h - (cz == 0 ? dL : 0.0f), szp = h + (cz == G - 1 ? dL : 0.0f);
+    // pos_i - shift for the 27 cell-shift codes, in this thread's column.
+#pragma unroll
+    for (int c = 0; c < 27; ++c) {
+      const int ex = c / 9, ey = (c / 3) % 3, ez = c % 3;
+      tab[c * kChunk + threadIdx.x] = make_float4(pi.x - sel3(ex, sxm, 0.0f, sxp), pi.y - sel3(ey, sym, 0.0f, syp),
+                                                  pi.z - sel3(ez, szm, 0.0f, szp), 0.0f);
+    }
     KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
     PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int nn = d.ncnt[s];
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
     const bool one_type = (nt == 1);
-    const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
-    int k = 0;
-    // Batches of kBatch: all list loads, then all position gathers, then the
-    // arithmetic, so each thread keeps 2 * kBatch loads in flight.
-    for (; k + kBatch <= nn; k += kBatch) {
-      uint32_t w[kBatch];
-#pragma unroll
-      for (int q = 0; q < kBatch; ++q) w[q] = __ldg(lst + (size_t)(k + q) * 32);
-      float4 pj[kBatch];
-#pragma unroll
-      for (int q = 0; q < kBatch; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
-      PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
-#pragma unroll
-      for (int q = 0; q < kBatch; ++q) {
-        float e24 = e24_0, sig2 = sig2_0;
-        if (!one_type) {
-          const int pidx = ti * nt + w_type(w_bits(pj[q].w));
-          e24 = s_eps24[pidx];
-          sig2 = s_sig2[pidx];
-        }
-        lj_pair(g, pi, pj[q], w[q], sxm, sxp, sym, syp, szm, szp, rc2, e24, sig2);
-      }
-      fx.add(g.fx);
-      fy.add(g.fy);
-      fz.add(g.fz);
-      acc.pe = g.pe;
-      acc.v0 = g.v0;
-      acc.v1 = g.v1;
-      acc.v2 = g.v2;
-      acc.v3 = g.v3;
-      acc.v4 = g.v4;
-      acc.v5 = g.v5;
-    }
-    {
-      PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
-      for (; k < nn; ++k) {
-        const uint32_t w = __ldg(lst + (size_t)k * 32);
-        const float4 pj = __ldg(pbase + (w & kIdxMask));
-        float e24 = e24_0, sig2 = sig2_0;
-        if (!one_type) {
-          const int pidx = ti * nt + w_type(w_bits(pj.w));
-          e24 = s_eps24[pidx];
-          sig2 = s_sig2[pidx];
-        }
-        lj_pair(g, pi, pj, w, sxm, sxp, sym, syp, szm, szp, rc2, e24, sig2);
-      }
-      fx.add(g.fx);
-      fy.add(g.fy);
-      fz.add(g.fz);
-      acc.pe = g.pe;
-      acc.v0 = g.v0;
-      acc.v1 = g.v1;
-      acc.v2 = g.v2;
-      acc.v3 = g.v3;
-      acc.v4 = g.v4;
-      acc.v5 = g.v5;
-    }
+    lj_loop<EV>(lst, nn, pbase, tab, threadIdx.x, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
@@ -792,7 +809,7 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
     for (int b = 0; b < nbd; ++b) {
       const uint32_t bw = bl[b];
       const int bt = (bw >> 26) & 0xF;
-      const float4 pj = pbase[bw & kIdxMask];
+      const float4 pj = pbase[bw & kSlotMask26];
       const float3 dr = bonded_dr(pi, pj, G, h, inv_h, dL);
       const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
       const float kf = R.fene[4 * bt], R02 = R.fene[4 * bt + 1], eps = R.fene[4 * bt + 2], sig2 = R.fene[4 * bt + 3];
@@ -825,8 +842,8 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
     for (int a = 0; a < nang; ++a) {
       const uint2 aw = al[a];
       const int role = (aw.x >> 26) & 3, at = (aw.y >> 26) & 0xF;
-      const float4 p1 = pbase[aw.x & kIdxMask];
-      const float4 p2 = pbase[aw.y & kIdxMask];
+      const float4 p1 = pbase[aw.x & kSlotMask26];
+      const float4 p2 = pbase[aw.y & kSlotMask26];
       const float kt = R.angp[2 * at], th0 = R.angp[2 * at + 1];
       if (role == 0)
         angle_term(pi, p1, p2, 0, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
@@ -838,8 +855,10 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
     const float ox = fx.s - fx.c, oy = fy.s - fy.c, oz = fz.s - fz.c;
     if (!isfinite(ox + oy + oz + pe)) status |= kStatusNonFinite;
     d.force[s] = make_float4(ox, oy, oz, pe);
-    vals[0] = pe;
-    for (int c = 0; c < 6; ++c) vals[1 + c] = bv[c];
+    if (ev) {
+      vals[0] = pe;
+      for (int c = 0; c < 6; ++c) vals[1 + c] = bv[c];
+    }
   }
   status = __syncthreads_or(status);
   if (threadIdx.x == 0 && status) atomicOr((int*)&d.reps[r].status, status);
@@ -859,7 +878,7 @@ __global__ void __launch_bounds__(kChunk) k_post(Dev d, int kick) {
   double vals[7] = {0, 0, 0, 0, 0, 0, 0};
   if (local < R.natoms) {
     float4 v = d.vel[s];
-    if (kick) {
+    if (kick == 1) {
       const float4 f = d.force[s];
       const double dt = (R.mode == kModePushoff) ? R.push_dt : R.dt;
       const float hm = (float)(0.5 * dt) * v.w;
@@ -898,15 +917,19 @@ __global__ void __launch_bounds__(kChunk) k_post(Dev d, int kick) {
     for (int q = 0; q < 13; ++q) acc[q] = warp_sum(acc[q]);
     if (threadIdx.x == 0) {
       R.cnt_post = 0;
-      R.pe = acc[0];
-      for (int q = 0; q < 6; ++q) {
-        R.vir[q] = acc[1 + q];
-        R.ke[q] = acc[7 + q];
+      if (need_ev(R)) {
+        R.pe = acc[0];
+        for (int q = 0; q < 6; ++q) R.vir[q] = acc[1 + q];
       }
+      for (int q = 0; q < 6; ++q) R.ke[q] = acc[7 + q];
       const double ke_raw = acc[7] + acc[10] + acc[12];
       const double dt = (R.mode == kModePushoff) ? R.push_dt : R.dt;
       const int ens = (R.mode == kModePushoff) ? FMD_LANGEVIN : R.ensemble;
-      if (!kick) {
+      if (need_ev(R)) R.ev_step = R.step;
+      R.force_ev = 0;
+      if (kick == 2) {
+        // re-evaluation of the current state: reductions only
+      } else if (!kick) {
         // Setup: the chain carry starts at the current KE (main.cu:376-390).
         R.nh.carry = 0.5 * ke_raw;
         R.pending_scale = 1.0;
@@ -939,10 +962,23 @@ __global__ void __launch_bounds__(kChunk) k_post(Dev d, int kick) {
 // the next pre-force nothing reads h.)
 
 // ---------------------------------------------------------------- launchers
+constexpr size_t kForceSmem = 27 * kChunk * sizeof(float4);
+
+void force_kernel_setup() {
+  static bool done = false;
+  if (!done) {
+    FMD_CUDA(cudaFuncSetAttribute(k_force<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem));
+    FMD_CUDA(cudaFuncSetAttribute(k_force<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem));
+    done = true;
+  }
+}
+
 void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st) {
+  force_kernel_setup();
   k_pre<<<nchunks, kChunk, 0, st>>>(d);
   launch_rebuild(d, nchunks, nreps, max_cells, st);
-  k_force<<<nchunks, kChunk, 0, st>>>(d);
+  k_force<false><<<nchunks, kChunk, kForceSmem, st>>>(d);
+  k_force<true><<<nchunks, kChunk, kForceSmem, st>>>(d);
   k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
 }
 
@@ -959,8 +995,14 @@ void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, cudaStr
   k_neighbors<<<gn, 256, 0, st>>>(d, nreps);
 }
 
-void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st) { k_force<<<nchunks, kChunk, 0, st>>>(d); }
-void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st) { k_post<<<nchunks, kChunk, 0, st>>>(d, 0); }
+void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st) {
+  force_kernel_setup();
+  k_force<false><<<nchunks, kChunk, kForceSmem, st>>>(d);
+  k_force<true><<<nchunks, kChunk, kForceSmem, st>>>(d);
+}
+void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode) {
+  k_post<<<nchunks, kChunk, 0, st>>>(d, mode);
+}
 
 }  // namespace mixed
 }  // namespace fmd
