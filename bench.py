@@ -60,6 +60,17 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def profiler_range(start):
+    """cudaProfilerStart / Stop around the timed region, so that a profiler
+    run with --profile-from-start off sees exactly the timed launches."""
+    import ctypes as C
+    try:
+        rt = C.CDLL("libcudart.so.12")
+    except OSError:
+        return
+    (rt.cudaProfilerStart if start else rt.cudaProfilerStop)()
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -212,6 +223,35 @@ def run_reference(args, rank, world, local, dist):
 
 
 # --------------------------------------------------------------------- GPU
+def reference_gpu_leg(fm, xyz, vel, image, steps):
+    """The reference's own FP32 GPU engine (src/main.cu and its core library,
+    built for sm_100a into oracle/_ref/fastMD_ref by `make -C oracle refbin`)
+    stepping one 30K replica of the same melt: one system per process, its
+    own wall clock (the "Steps/s" it prints, main.cu:750-756).  A datapoint
+    beside the batched number, not a bench arm."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "fastMD_ref")
+    if not os.path.exists(exe):
+        return {"unavailable": "reference GPU engine not built (make -C oracle refbin)"}
+    import tempfile
+    d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0)
+    d.xyz, d.vel, d.image = xyz, vel, image
+    with tempfile.TemporaryDirectory() as td:
+        data = os.path.join(td, "melt.data")
+        fm.write_lammps_data(data, d)
+        conf = os.path.join(td, "run.conf")
+        with open(conf, "w") as f:
+            f.write(run_conf(42, nsteps=steps) + f"lammps_data_file {data}\n")
+        out = subprocess.run([exe, conf], capture_output=True, text=True, timeout=600, cwd=td)
+    m = re.search(r"Steps/s:\s*([0-9.]+)", out.stdout)
+    if out.returncode != 0 or not m:
+        tail = (out.stdout + out.stderr).strip().splitlines()[-3:]
+        return {"unavailable": f"reference run failed (rc {out.returncode}): {' | '.join(tail)}"}
+    sps = float(m.group(1))
+    n = len(d.type)
+    return {"value": n * sps, "unit": "atom-steps/s", "steps": steps, "natoms": n,
+            "how": "oracle/_ref/fastMD_ref <run.conf> on a LAMMPS data file of replica 0, its printed Steps/s"}
+
+
 def force_profile_traffic():
     """Per-launch DRAM bytes of the force kernel from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "k_force_kg30k_langevin.md")
@@ -228,7 +268,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=100)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--replicas", type=int, default=64)
-    ap.add_argument("--no-extras", action="store_true", help="skip e2e / plain / CPU legs")
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e / plain / CPU / reference-GPU legs")
+    ap.add_argument("--ref-gpu-steps", type=int, default=5000, help="steps of the reference GPU datapoint")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local, dist = dist_setup(args.gpus)
@@ -255,13 +296,17 @@ def main():
     # warm-up
     b.run(args.warmup)
     barrier(dist, local)
+    counts0 = b.launch_counts()
     with ClockSampler(local) as clk:
+        profiler_range(True)
         lib.fmd_batch_mark(b._h, 0)
         b.run(args.steps)
         lib.fmd_batch_mark(b._h, 1)
+        profiler_range(False)
         import ctypes as C
         ms = C.c_double()
         lib.fmd_batch_elapsed_ms(b._h, C.byref(ms))
+    counts1 = b.launch_counts()
     barrier(dist, local)
     dev_ms = allmax(dist, ms.value, local)
     total_atoms = allmax(dist, float(natoms), local) * world  # equal per rank
@@ -285,9 +330,9 @@ def main():
 
     if rank == 0:
         line["clocks"] = clk.summary()
-        kps = C.c_int32()
-        lib.fmd_batch_kernels_per_step(b._h, C.byref(kps))
-        line["gpu_launches"] = int(kps.value) * args.steps
+        launched = {k: counts1[k] - counts0[k] for k in counts0}
+        line["gpu_launches"] = int(sum(launched.values()))
+        line["launches_by_kernel"] = launched
         # ---- roofline of the force kernel
         entries = C.c_int64()
         mx = C.c_int32()
@@ -343,6 +388,12 @@ def main():
                 ps.close()
             except Exception as e:  # reported, not fatal
                 line["plain_fp64_one_replica"] = {"error": str(e)}
+            # ---- the reference's own FP32 GPU engine on one replica
+            try:
+                x, v, img = b.state(slots[0])
+                line["reference_gpu_fp32_one_replica"] = reference_gpu_leg(fm, x, v, img, args.ref_gpu_steps)
+            except Exception as e:
+                line["reference_gpu_fp32_one_replica"] = {"unavailable": str(e)}
             # ---- CPU baseline (FP64 oracle port on the host cores)
             try:
                 x, v, img = b.state(slots[0])

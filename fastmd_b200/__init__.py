@@ -33,6 +33,7 @@ from ._lib import (  # noqa: F401
     lib_path,
     parse_run_conf,
     read_lammps_data,
+    write_lammps_data,
 )
 
 __version__ = "0.1.0"

@@ -170,6 +170,12 @@ class SystemDesc:
         return d, keep
 
 
+def write_lammps_data(path, desc: SystemDesc, step=0):
+    """Write a system as a LAMMPS data file (the reference's restart layout)."""
+    d, keep = desc.to_c()
+    _call("fmd_write_lammps_data", str(path).encode(), C.byref(d), C.c_int64(step))
+
+
 def generate_melt(nchains, chain_length, density=0.85, seed=42, type_block=0, bond_length=0.0, min_dist=0.0):
     """Host-side seeded random-walk melt (no push-off).  Returns a SystemDesc."""
     spec = MeltSpec(nchains=nchains, chain_length=chain_length, density=density, seed=seed,
@@ -340,6 +346,9 @@ class Simulation:
         _call("fmd_sim_counters", self._h, C.byref(r), C.byref(s), C.byref(m))
         return dict(rebuilds=r.value, status_word=s.value, max_neighbors=m.value)
 
+    def write_restart(self, path):
+        _call("fmd_write_restart", self._h, str(path).encode())
+
 
 class Batch:
     """Many replicas advanced together (the mixed form)."""
@@ -417,6 +426,18 @@ class Batch:
         b = C.c_int64()
         _call("fmd_batch_totals", self._h, C.byref(a), C.byref(n), C.byref(b))
         return dict(active=a.value, atoms=n.value, bytes=b.value)
+
+    def write_restart(self, slot, path):
+        _call("fmd_batch_write_restart", self._h, C.c_int32(slot), str(path).encode())
+
+    LAUNCH_KINDS = ("pre", "bin", "scan", "scatter", "cellsort", "permute", "topo", "neighbors", "force",
+                    "force_ev", "post")
+
+    def launch_counts(self):
+        """Kernel launches executed so far, per kernel (counted on the device)."""
+        c = np.zeros(len(self.LAUNCH_KINDS), np.int64)
+        _call("fmd_batch_launch_counts", self._h, _ptr(c), C.c_int32(len(c)))
+        return dict(zip(self.LAUNCH_KINDS, c.tolist()))
 
 
 class Server:

@@ -103,6 +103,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   device_ = o.device;
   FMD_CUDA(cudaSetDevice(device_));
   FMD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  FMD_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
   graph_steps_ = o.graph_steps > 0 ? o.graph_steps : 50;
   max_reps_ = o.max_replicas > 0 ? o.max_replicas : 256;
   BatchCaps c;
@@ -148,6 +149,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   bnd_.alloc(S * kMaxBondsPerAtom);
   ang_.alloc(S * kMaxAnglesPerAtom);
   part_.alloc_zero(S / kChunk * kNumPartials);
+  kcount_.alloc_zero(kKernelKinds);
   cell_cnt_.alloc_zero(c.cells);
   cell_start_.alloc_zero(c.cells);
   cell_fill_.alloc_zero(c.cells);
@@ -168,6 +170,7 @@ Batch::~Batch() {
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
   if (st_) cudaStreamDestroy(st_);
+  if (side_) cudaStreamDestroy(side_);
 }
 
 Dev Batch::dev() const {
@@ -199,6 +202,7 @@ Dev Batch::dev() const {
   d.bnd = bnd_;
   d.ang = ang_;
   d.part = part_;
+  d.kcount = kcount_;
   return d;
 }
 
@@ -208,6 +212,8 @@ void Batch::download_reps() {
 }
 
 void Batch::upload_reps() {
+  // a host change may touch any input of the precomputed step scalars
+  for (int r = 0; r < max_reps_; ++r) h_reps_[r].next_valid = 0;
   FMD_CUDA(cudaMemcpyAsync(reps_, h_reps_.data(), sizeof(Rep) * max_reps_, cudaMemcpyHostToDevice, st_));
 }
 
@@ -222,6 +228,15 @@ int Batch::max_cells() const {
   int64_t m = 1;
   for (int r = 0; r < max_reps_; ++r)
     if (info_[r].used) m = std::max<int64_t>(m, info_[r].plan.ncell);
+  return (int)m;
+}
+int Batch::max_home_cells() const {
+  int64_t m = 1;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used) {
+      const int64_t g = info_[r].plan.G_alloc;
+      m = std::max<int64_t>(m, g * g * g);
+    }
   return (int)m;
 }
 
@@ -366,6 +381,8 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
       break;
     }
   if (r < 0) throw Error(FMD_ERR_CAPACITY, "no free replica slot");
+  // neighbor-list entries address a replica's slots with 25 bits
+  if ((int64_t)t.natoms + kChunk >= (int64_t)kIdxMask) throw Error(FMD_ERR_CAPACITY, "replica too large (max 33,554,000 atoms)");
   const ReplicaPlan p = plan_replica(cfg, t.natoms, t.box_L);
   const int64_t need = estimate_bytes(p, t.nbonds(), t.nangles());
   if (bytes_in_use_ + need > budget_bytes_) throw Error(FMD_ERR_CAPACITY, "device-memory budget exhausted");
@@ -388,6 +405,10 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
   I.cfg = cfg;
   I.type = t.type;
   I.mol = t.mol;
+  I.topo = t;
+  I.topo.xyz.clear();
+  I.topo.vel.clear();
+  I.topo.image.clear();
   I.bytes = need;
   I.seg_chunk = ch;
   I.seg_cell = ce;
@@ -498,8 +519,8 @@ void Batch::finish_pushoffs() {
     for (int64_t k = 0; k < steps / graph_steps_; ++k) FMD_CUDA(cudaGraphLaunch(graph_exec_, st_));
   }
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
-  for (int64_t k = 0; k < steps % graph_steps_; ++k) launch_step(d, nc, nr, mc, st_);
+  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
+  for (int64_t k = 0; k < steps % graph_steps_; ++k) launch_step(d, nc, nr, mc, mh, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
   download_reps();
@@ -552,7 +573,7 @@ void Batch::setup(const std::vector<int>& rs) {
   }
   upload_reps();
   const Dev d = dev();
-  launch_rebuild(d, nchunks_launch(), nreps_launch(), max_cells(), st_);
+  launch_rebuild(d, nchunks_launch(), nreps_launch(), max_cells(), max_home_cells(), st_);
   FMD_CUDA_LAUNCH();
   launch_forces_only(d, nchunks_launch(), st_);
   FMD_CUDA_LAUNCH();
@@ -575,8 +596,8 @@ void Batch::check_status(int r, bool throw_on_fault) {
 
 void Batch::advance_direct(int64_t nsteps) {
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
-  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, mc, st_);
+  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
+  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, mc, mh, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
 }
@@ -588,10 +609,17 @@ void Batch::ensure_graph() {
     graph_exec_ = nullptr;
   }
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
+  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
   cudaGraph_t g;
   FMD_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-  for (int k = 0; k < graph_steps_; ++k) launch_step(d, nc, nr, mc, st_);
+  try {
+    for (int k = 0; k < graph_steps_; ++k) capture_step(d, nc, nr, mc, mh, st_, side_);
+  } catch (...) {
+    cudaGraph_t partial = nullptr;
+    cudaStreamEndCapture(st_, &partial);
+    if (partial) cudaGraphDestroy(partial);
+    throw;
+  }
   FMD_CUDA(cudaStreamEndCapture(st_, &g));
   FMD_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
   cudaGraphDestroy(g);
@@ -625,8 +653,8 @@ void Batch::run(int64_t nsteps, bool respect_nsteps) {
   }
   if (need > 0) {
     const Dev d = dev();
-    const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells();
-    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, mc, st_);
+    const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
+    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, mc, mh, st_);
     FMD_CUDA_LAUNCH();
   }
   FMD_CUDA(cudaStreamSynchronize(st_));
@@ -730,7 +758,9 @@ const Rep& Batch::rep(int r) const {
   return h_reps_[r];
 }
 
-void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) {
+void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) { read_state(r, xyz, vel, image, true); }
+
+void Batch::read_state(int r, double* xyz, double* vel, int32_t* image, bool rewrap) {
   const Rep& R = rep(r);
   const int n = R.natoms;
   std::vector<float4> hp(n), hv(n);
@@ -739,9 +769,10 @@ void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) {
   FMD_CUDA(cudaMemcpyAsync(hv.data(), vel_.p + R.slot_base, n * sizeof(float4), cudaMemcpyDeviceToHost, st_));
   FMD_CUDA(cudaMemcpyAsync(hi.data(), img_.p + R.slot_base, n * sizeof(int4), cudaMemcpyDeviceToHost, st_));
   FMD_CUDA(cudaStreamSynchronize(st_));
-  // Positions are reported wrapped into the current box (after an NPT step
-  // the barostat has already updated L).
-  const double L = R.L, h = R.h;
+  // The reference wraps positions in the box of the last pre-force update
+  // (Lpos); an NPT barostat has changed L since, and positions are reported
+  // re-wrapped into the current box L (two wraps, the first one in Lpos).
+  const double Lp = R.Lpos, L = R.L, h = R.h;
   for (int s = 0; s < n; ++s) {
     const int id = hi[s].w;
     const uint32_t u = w_bits(hp[s].w);
@@ -751,9 +782,14 @@ void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) {
     for (int a = 0; a < 3; ++a) {
       double x = (double)c[a] * h + (double)o[a];
       int ia = im[a];
-      const double fl = std::floor(x / L);
-      x -= fl * L;
+      double fl = std::floor(x / Lp);
+      x -= fl * Lp;
       ia += (int)fl;
+      if (rewrap) {
+        fl = std::floor(x / L);
+        x -= fl * L;
+        ia += (int)fl;
+      }
       if (xyz) xyz[3 * id + a] = x;
       if (image) image[3 * id + a] = ia;
     }
@@ -763,6 +799,25 @@ void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) {
       vel[3 * id + 2] = (double)hv[s].z * R.pending_scale;
     }
   }
+}
+
+void Batch::launch_counts(int64_t* counts, int n) {
+  unsigned long long h[kKernelKinds];
+  FMD_CUDA(cudaMemcpyAsync(h, kcount_.p, sizeof(h), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  for (int k = 0; k < n && k < kKernelKinds; ++k) counts[k] = (int64_t)h[k];
+}
+
+void Batch::write_restart(int r, const std::string& path) {
+  const Rep& R = rep(r);
+  Topology t = info_[r].topo;
+  const size_t n = (size_t)R.natoms;
+  t.xyz.resize(3 * n);
+  t.vel.resize(3 * n);
+  t.image.resize(3 * n);
+  get_state(r, t.xyz.data(), t.vel.data(), t.image.data());
+  t.box_L = rep(r).L;
+  write_lammps_data(path, t, rep(r).step);
 }
 
 void Batch::set_state(int r, const double* xyz, const double* vel, const int32_t* image) {
@@ -861,14 +916,16 @@ double Batch::rg(int r) {
   const int n = R.natoms;
   std::vector<double> x(3 * n);
   std::vector<int32_t> im(3 * n);
-  get_state(r, x.data(), nullptr, im.data());
+  // The reference unwraps the stored positions (wrapped in Lpos) with the
+  // current box L (analysis/rg.cu).
+  read_state(r, x.data(), nullptr, im.data(), false);
   const std::vector<int32_t>& mol = info_[r].mol;
   std::vector<int32_t> order(n);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return mol[a] < mol[b]; });
   double sum = 0;
   int nch = 0;
-  const double L = R.Lpos;
+  const double L = R.L;
   for (int s = 0; s < n;) {
     int e = s;
     while (e < n && mol[order[e]] == mol[order[s]]) ++e;

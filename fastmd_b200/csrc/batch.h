@@ -50,6 +50,7 @@ struct ReplicaInfo {
   ReplicaPlan plan;
   RunConfig cfg;
   std::vector<int32_t> type, mol;
+  Topology topo;  // bonds, angles, types, masses (positions live on the device)
   int64_t bytes = 0;
   int64_t seg_chunk = -1, seg_cell = -1, seg_nbr = -1, seg_bond = -1, seg_angle = -1;
   int64_t pending_pushoff = 0;
@@ -67,6 +68,9 @@ class Batch {
   int max_reps() const { return max_reps_; }
   const RunConfig& cfg(int r) const { return info_[r].cfg; }
   void get_state(int r, double* xyz, double* vel, int32_t* image);
+  void write_restart(int r, const std::string& path);
+  void launch_counts(int64_t* counts, int n);
+  void read_state(int r, double* xyz, double* vel, int32_t* image, bool rewrap);
   void set_state(int r, const double* xyz, const double* vel, const int32_t* image);
   void forces(int r, double* f, double* pe, double* vir);
   void thermo(int r, fmd_thermo_row* row);
@@ -84,6 +88,7 @@ class Batch {
   int nchunks_launch() const;
   int nreps_launch() const;
   int max_cells() const;
+  int max_home_cells() const;
   int graph_steps() const { return graph_steps_; }
   void set_max_between(int r, int k);
   void mark(int which);
@@ -103,6 +108,7 @@ class Batch {
 
   int device_ = 0;
   cudaStream_t st_ = nullptr;
+  cudaStream_t side_ = nullptr;  // captures conditional-node bodies
   int graph_steps_ = 50;
   int max_reps_ = 256;
   BatchCaps caps_;
@@ -115,6 +121,7 @@ class Batch {
   DevBuf<uint32_t> bnd_;
   DevBuf<uint2> ang_;
   DevBuf<double> part_;
+  DevBuf<unsigned long long> kcount_;
   DevBuf<int32_t> cell_cnt_, cell_start_, cell_fill_;
   DevBuf<int2> bent_;
   DevBuf<int4> aent_;

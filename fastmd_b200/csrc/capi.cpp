@@ -18,6 +18,7 @@ const std::string& last_error();
 struct fmd_sim {
   std::unique_ptr<fmd::SimEngine> eng;
   int32_t form = 0;
+  fmd::Topology topo;  // topology and masses (the state lives in the engine)
 };
 
 namespace {
@@ -150,6 +151,13 @@ FMD_API fmd_status fmd_read_lammps_data(const char* path, int32_t* counts, doubl
   });
 }
 
+FMD_API fmd_status fmd_write_lammps_data(const char* path, const fmd_system_desc* desc, int64_t step) {
+  return guarded([&] {
+    if (!path || !desc) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    fmd::write_lammps_data(path, fmd::topology_from_desc(*desc), step);
+  });
+}
+
 FMD_API fmd_status fmd_format_thermo_row(const fmd_thermo_row* r, char* buf, size_t len) {
   return guarded([&] {
     if (!r || !buf) throw fmd::Error(FMD_ERR_ARG, "null argument");
@@ -175,6 +183,10 @@ FMD_API fmd_status fmd_sim_create(const char* conf, const char* data_path, const
     require_device();
     std::unique_ptr<fmd_sim> s(new fmd_sim());
     s->form = form;
+    s->topo = t;
+    s->topo.xyz.clear();
+    s->topo.vel.clear();
+    s->topo.image.clear();
     if (form == FMD_FORM_PLAIN_FP64)
       s->eng = fmd::make_plain_engine(cfg, std::move(t), gen);
     else if (form == FMD_FORM_MIXED)
@@ -230,6 +242,21 @@ FMD_API fmd_status fmd_set_state(fmd_sim* sim, const double* xyz, const double* 
   return guarded([&] {
     SIM_CHECK();
     sim->eng->set_state(xyz, vel, image);
+  });
+}
+
+FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (!path) throw fmd::Error(FMD_ERR_ARG, "null path");
+    fmd::Topology t = sim->topo;
+    const int n = sim->eng->natoms();
+    t.xyz.resize(3 * (size_t)n);
+    t.vel.resize(3 * (size_t)n);
+    t.image.resize(3 * (size_t)n);
+    sim->eng->get_state(t.xyz.data(), t.vel.data(), t.image.data());
+    t.box_L = sim->eng->box_L();
+    fmd::write_lammps_data(path, t, sim->eng->step_count());
   });
 }
 

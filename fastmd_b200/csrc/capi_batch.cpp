@@ -116,6 +116,15 @@ FMD_API fmd_status fmd_batch_get_state(fmd_batch* b, int32_t slot, double* xyz, 
   });
 }
 
+FMD_API fmd_status fmd_batch_write_restart(fmd_batch* b, int32_t slot, const char* path) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!path) throw fmd::Error(FMD_ERR_ARG, "null path");
+    bb.write_restart(slot, path);
+  });
+}
+
 FMD_API fmd_status fmd_batch_thermo(fmd_batch* b, int32_t slot, fmd_thermo_row* row) {
   return guarded([&] {
     auto& bb = B(b);
@@ -182,6 +191,13 @@ FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n) {
     B(b);
     if (!n) throw fmd::Error(FMD_ERR_ARG, "null argument");
     *n = 11;  // k_pre, 7 rebuild kernels (early exit unless flagged), k_force x2 (with and without energies), k_post
+  });
+}
+
+FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_t n) {
+  return guarded([&] {
+    if (!counts || n < 0) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    B(b).launch_counts(counts, n);
   });
 }
 

@@ -65,6 +65,10 @@ struct Topology {
 };
 
 Topology read_lammps_data(const std::string& path);
+// Restart / data file in the reference's layout (io/lammps_data.cpp:269-385:
+// header, Masses, "Atoms # full" with image flags, Velocities, Bonds,
+// Angles), FP64 values written with enough digits to read back exactly.
+void write_lammps_data(const std::string& path, const Topology& t, int64_t step);
 Topology read_xyz_coords(const std::string& path, double box_L);
 Topology topology_from_desc(const fmd_system_desc& d);
 Topology generate_melt(const fmd_melt_spec& spec);

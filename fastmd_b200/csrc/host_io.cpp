@@ -287,6 +287,52 @@ Topology read_xyz_coords(const std::string& path, double box_L) {
   return t;
 }
 
+void write_lammps_data(const std::string& path, const Topology& t, int64_t step) {
+  FILE* fp = std::fopen(path.c_str(), "w");
+  if (!fp) throw Error(FMD_ERR_IO, "cannot open " + path + " for writing");
+  int nbt = 0, nat = 0;
+  for (int32_t b : t.bond_type) nbt = std::max(nbt, b + 1);
+  for (int32_t a : t.angle_type) nat = std::max(nat, a + 1);
+  const int nb = t.nbonds(), na = t.nangles(), n = t.natoms;
+  std::fprintf(fp, "# Restart from step %lld\n", (long long)step);
+  std::fprintf(fp, "%d atoms\n%d atom types\n", n, t.ntypes);
+  if (nb > 0) std::fprintf(fp, "%d bonds\n%d bond types\n", nb, nbt);
+  if (na > 0) std::fprintf(fp, "%d angles\n%d angle types\n", na, nat);
+  // all three box lines carry the edge (the reference's writer drops it from
+  // the zhi line, io/lammps_data.cpp:335)
+  std::fprintf(fp, "\n0.0 %.17g xlo xhi\n0.0 %.17g ylo yhi\n0.0 %.17g zlo zhi\n\n", t.box_L, t.box_L, t.box_L);
+  std::fprintf(fp, "Masses\n\n");
+  for (int k = 0; k < t.ntypes; ++k)
+    std::fprintf(fp, "%d %.17g\n", k + 1, k < (int)t.mass.size() ? t.mass[k] : 1.0);
+  std::fprintf(fp, "\nAtoms # full\n\n");
+  for (int i = 0; i < n; ++i) {
+    const int mol = t.mol.empty() ? 1 : t.mol[i];
+    const int ix = t.image.empty() ? 0 : t.image[3 * i], iy = t.image.empty() ? 0 : t.image[3 * i + 1],
+              iz = t.image.empty() ? 0 : t.image[3 * i + 2];
+    std::fprintf(fp, "%d %d %d 0.0 %.17g %.17g %.17g %d %d %d\n", i + 1, mol, t.type[i] + 1, t.xyz[3 * i],
+                 t.xyz[3 * i + 1], t.xyz[3 * i + 2], ix, iy, iz);
+  }
+  std::fprintf(fp, "\nVelocities\n\n");
+  for (int i = 0; i < n; ++i) {
+    const double vx = t.vel.empty() ? 0.0 : t.vel[3 * i], vy = t.vel.empty() ? 0.0 : t.vel[3 * i + 1],
+                 vz = t.vel.empty() ? 0.0 : t.vel[3 * i + 2];
+    std::fprintf(fp, "%d %.17g %.17g %.17g\n", i + 1, vx, vy, vz);
+  }
+  if (nb > 0) {
+    std::fprintf(fp, "\nBonds\n\n");
+    for (int b = 0; b < nb; ++b)
+      std::fprintf(fp, "%d %d %d %d\n", b + 1, t.bond_type[b] + 1, t.bonds[2 * b] + 1, t.bonds[2 * b + 1] + 1);
+  }
+  if (na > 0) {
+    std::fprintf(fp, "\nAngles\n\n");
+    for (int a = 0; a < na; ++a)
+      std::fprintf(fp, "%d %d %d %d %d\n", a + 1, t.angle_type[a] + 1, t.angles[3 * a] + 1, t.angles[3 * a + 1] + 1,
+                   t.angles[3 * a + 2] + 1);
+  }
+  const bool bad = std::ferror(fp) != 0;
+  if (std::fclose(fp) != 0 || bad) throw Error(FMD_ERR_IO, "write failed: " + path);
+}
+
 Topology topology_from_desc(const fmd_system_desc& d) {
   if (d.natoms <= 0 || !d.xyz || !d.type || d.box_L <= 0) throw Error(FMD_ERR_ARG, "system descriptor incomplete");
   Topology t;

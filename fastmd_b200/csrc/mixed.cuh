@@ -35,7 +35,13 @@ constexpr int kTile = 32;         // slots per warp tile
 constexpr int kMaxTypes = 16;
 constexpr int kGhostType = 31;
 constexpr int kMaxG = 512;        // cells per axis (9 bits)
-constexpr uint32_t kIdxMask = (1u << 27) - 1;     // neighbor-list slot field
+// Neighbor-list entry: slot (25 bits) | shift code (7 bits).  The shift
+// code names one of 125 periodic shift vectors: per axis a in 0..4 for
+// e*h + k*dL with (e, k) = (-1,-1), (-1,0), (0,0), (1,0), (1,1), code =
+// 25 ax + 5 ay + az.  The vector is the same for every atom of a replica.
+constexpr uint32_t kIdxMask = (1u << 25) - 1;
+constexpr int kCodeShift = 25;
+constexpr int kShiftCodes = 125;
 constexpr uint32_t kSlotMask26 = (1u << 26) - 1;  // bonded-table slot field
 constexpr int kNumPartials = 14;  // pe, vir[6], ke[6], sum m v^2
 constexpr int kMaxBondsPerAtom = 4;   // per-slot bonded tables rebuilt with the list
@@ -43,8 +49,35 @@ constexpr int kMaxAnglesPerAtom = 8;
 
 enum Mode : int32_t { kModeRun = 0, kModePushoff = 1 };
 
+// Per-kernel launch counters (executed launches, graph conditionals included).
+enum KernelKind : int {
+  kKPre = 0, kKBin, kKScan, kKScatter, kKCellsort, kKPermute, kKTopo, kKNeighbors, kKForce, kKForceEv, kKPost,
+  kKernelKinds
+};
+
 // Per-replica record (device).  Static fields are set at admission; dynamic
 // ones are updated by the kernels.
+// Per-step scalars of a replica's pre-force update: thermostat / barostat
+// factors for the step about to be taken.  Computed once per replica (by the
+// last block of the previous post-force) and read by every block.
+struct StepScalars {
+  int adv;
+  int64_t step;  // step being taken (1-based)
+  float hdt, dt;
+  float c1;      // Langevin velocity decay
+  float c2kT;    // c2 * sqrt(kT) (per-type mass applied per atom)
+  float vscale;  // velocity scale applied before the kick (pending post * pre)
+  float ev, fpos;       // NPT: position scale and drift factor
+  float dh;             // NPT: c * dh term (h_old * ev - h_new)
+  float h_new;          // NPT: new cell edge
+  float h_old, inv_Lold;  // NPT: frame of the stored positions
+  float dW;             // NPT: L_new - L_old * ev, applied per wrapped period
+  uint32_t stream;
+  int ens;
+  NHScalars nh;         // updated chain / barostat state (committed by the last block)
+  double L_new;
+};
+
 struct Rep {
   // --- static
   int32_t active;
@@ -92,6 +125,8 @@ struct Rep {
   int32_t thermo_freq;           // run.conf thermo cadence (0: off); energies/virial computed on those steps
   int32_t force_ev;              // host request: compute energies/virial at the next force evaluation
   int64_t ev_step;               // step whose energies/virial are in pe/vir
+  StepScalars next;              // scalars of the next pre-force (valid when next_valid)
+  int32_t next_valid;            // cleared by every host upload and by each pre-force
 };
 
 // Device pointers of the batch arrays.
@@ -128,7 +163,19 @@ struct Dev {
   uint32_t* nbr;
   int32_t* ncnt;
   double* part;                  // [chunks][kNumPartials]
+  unsigned long long* kcount;    // [kKernelKinds] launches executed (block 0 of each launch counts)
 };
+
+// Axis part of the shift code for cell shift e and wrap count k; -1 when
+// (e, k) is not one of the five representable cases.
+__host__ __device__ inline int axis_shift_code(int e, int k) {
+  if (e == 0) return k == 0 ? 2 : -1;
+  if (e == -1) return k == -1 ? 0 : (k == 0 ? 1 : -1);
+  if (e == 1) return k == 1 ? 4 : (k == 0 ? 3 : -1);
+  return -1;
+}
+__host__ __device__ inline int axis_code_e(int a) { return a < 2 ? -1 : (a == 2 ? 0 : 1); }
+__host__ __device__ inline int axis_code_k(int a) { return a == 0 ? -1 : (a == 4 ? 1 : 0); }
 
 __host__ __device__ inline uint32_t spread3(uint32_t v) {
   v &= 0x3FFu;
@@ -166,8 +213,20 @@ __host__ __device__ inline int w_cz(uint32_t u) { return (int)((u >> 18) & 511u)
 __host__ __device__ inline int w_type(uint32_t u) { return (int)(u >> 27); }
 
 // Kernel launchers (mixed_kernels.cu).
-void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st);
-void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells_per_rep, cudaStream_t st);
+// Conditional-node handles of one captured step (CUDA graph IF nodes around
+// the rebuild and the two force-kernel variants); set from the device by the
+// pre-force kernel.  use == 0 outside a graph (every kernel launched, blocks
+// of replicas that need no work return at once).
+struct StepConds {
+  int use;
+  cudaGraphConditionalHandle rebuild, force_plain, force_ev;
+};
+void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st);
+// The same step recorded into the graph being captured on st, with the
+// conditional nodes; side is a second stream used to capture their bodies.
+void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st,
+                  cudaStream_t side);
+void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells_per_rep, int max_home_cells, cudaStream_t st);
 void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st);
 void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode);  // 0 setup, 2 re-evaluation
 

@@ -39,31 +39,12 @@ struct DSinh {
   __device__ double operator()(double x) const { return sinh(x); }
 };
 
-// Per-step scalars of a replica, computed redundantly by every block.
-struct StepScalars {
-  int adv;
-  int64_t step;  // step being taken (1-based)
-  float hdt, dt;
-  float c1;      // Langevin velocity decay
-  float c2kT;    // c2 * sqrt(kT) (per-type mass applied per atom)
-  float vscale;  // velocity scale applied before the kick (pending post * pre)
-  float ev, fpos;       // NPT: position scale and drift factor
-  float dh;             // NPT: c * dh term (h_old * ev - h_new)
-  float h_new;          // NPT: new cell edge
-  float h_old, inv_Lold;  // NPT: frame of the stored positions
-  float dW;             // NPT: L_new - L_old * ev, applied per wrapped period
-  uint32_t stream;
-  int ens;
-  NHScalars nh;         // updated chain / barostat state (committed by the last block)
-  double L_new;
-};
-
 __device__ __forceinline__ double ramp(const Rep& R, int64_t step, double a, double b) {
   const double frac = (double)(step - 1) / (double)(R.nsteps > 0 ? R.nsteps : 1);
   return a + (b - a) * frac;
 }
 
-__device__ void compute_step_scalars(const Rep& R, StepScalars& S) {
+__device__ __noinline__ void compute_step_scalars(const Rep& R, StepScalars& S) {
   S.adv = R.active && R.step < R.stop_step;
   S.step = R.step + 1;
   S.ens = (R.mode == kModePushoff) ? FMD_LANGEVIN : R.ensemble;
@@ -110,13 +91,58 @@ __device__ void compute_step_scalars(const Rep& R, StepScalars& S) {
   }
 }
 
+// Three standard normals from the same Philox words as rng_normal3 (seed,
+// stream, step, atom id), transformed in FP32: Box-Muller with u1 = (a + 1)
+// 2^-32 and the angle split into quadrant (top two bits of b) and a quarter
+// turn fraction, evaluated with the CUDA math library's logf / sincospif.
+// Agrees with the FP64 transform to FP32 rounding (the mixed form casts the
+// deviates to FP32 in any case).
+__device__ __forceinline__ void normal_pair_f32(uint32_t a, uint32_t b, float& z0, float& z1) {
+  const float u1 = ((float)a + 1.0f) * 0x1.0p-32f;
+  const float r = sqrtf(-2.0f * logf(u1));
+  const float f = (float)(b & 0x3FFFFFFFu) * 0x1.0p-30f;
+  float s, c;
+  sincospif(0.5f * f, &s, &c);
+  const uint32_t q = b >> 30;
+  const float cs = q == 0 ? c : (q == 1 ? -s : (q == 2 ? -c : s));
+  const float sn = q == 0 ? s : (q == 1 ? c : (q == 2 ? -s : -c));
+  z0 = r * cs;
+  z1 = r * sn;
+}
+
+__device__ __forceinline__ void normal3_f32(uint64_t seed, uint32_t stream, uint64_t step, uint32_t id, float& n0,
+                                            float& n1, float& n2) {
+  U32x4 c;
+  c.x = id;
+  c.y = (uint32_t)step;
+  c.z = (uint32_t)(step >> 32);
+  c.w = stream;
+  const U32x4 w = philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  float z3;
+  normal_pair_f32(w.x, w.y, n0, n1);
+  normal_pair_f32(w.z, w.w, n2, z3);
+}
+
 __device__ __forceinline__ void warp_max_u32(uint32_t& v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
 }
 
+// Energies and virial are needed on thermo steps, for NPT (the barostat uses
+// the virial every step) and when the host asks for them.
+__device__ __forceinline__ bool need_ev(const Rep& R) {
+  if (R.force_ev) return true;
+  if (R.mode != kModePushoff && R.ensemble == FMD_NPT_NH) return true;
+  return R.thermo_freq > 0 && (R.step % R.thermo_freq) == 0;
+}
+
+__device__ __forceinline__ void count_launch(const Dev& d, int kind) {
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(d.kcount + kind, 1ull);
+}
+
 // ---------------------------------------------------------------- pre-force
-__global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
+__global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
+  count_launch(d, kKPre);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
@@ -124,25 +150,37 @@ __global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
   __shared__ StepScalars S;
   __shared__ uint32_t wmax[kChunk / 32];
   __shared__ int last;
-  if (threadIdx.x == 0) compute_step_scalars(R, S);
-  __syncthreads();
-  if (!S.adv) return;
+  if (!(R.active && R.step < R.stop_step)) return;
   const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
   const int s = R.slot_base + local;
+  const bool have = local < R.natoms;
+  // The atom's data does not depend on the step scalars: load it first.
+  float4 p = make_float4(0, 0, 0, 0), v = p, f = p, q = p;
+  if (have) {
+    p = d.pos[s];
+    v = d.vel[s];
+    f = d.force[s];
+    q = d.ref[s];
+  }
+  if (R.next_valid) {
+    constexpr int nw = (int)(sizeof(StepScalars) / sizeof(uint32_t));
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&R.next);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&S);
+    for (int k = threadIdx.x; k < nw; k += kChunk) dst[k] = src[k];
+  } else if (threadIdx.x == 0) {
+    compute_step_scalars(R, S);
+  }
+  __syncthreads();
   uint32_t d2bits = 0;
   int bad = 0;
-  if (local < R.natoms) {
-    float4 p = d.pos[s];
-    float4 v = d.vel[s];
-    const float4 f = d.force[s];
-    float4 q = d.ref[s];
+  if (have) {
     const float hm = S.hdt * v.w;
     v.x *= S.vscale;
     v.y *= S.vscale;
     v.z *= S.vscale;
     if (S.ens == FMD_LANGEVIN) {
-      double n0, n1, n2;
-      rng_normal3(R.seed, S.stream, (uint64_t)S.step, (uint32_t)__float_as_int(q.w), &n0, &n1, &n2);
+      float n0, n1, n2;
+      normal3_f32(R.seed, S.stream, (uint64_t)S.step, (uint32_t)__float_as_int(q.w), n0, n1, n2);
       const float ns = S.c2kT * sqrtf(v.w);
       v.x = fmaf(hm, f.x, v.x);
       v.y = fmaf(hm, f.y, v.y);
@@ -150,9 +188,9 @@ __global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
       p.x = fmaf(S.hdt, v.x, p.x);
       p.y = fmaf(S.hdt, v.y, p.y);
       p.z = fmaf(S.hdt, v.z, p.z);
-      v.x = fmaf(S.c1, v.x, ns * (float)n0);
-      v.y = fmaf(S.c1, v.y, ns * (float)n1);
-      v.z = fmaf(S.c1, v.z, ns * (float)n2);
+      v.x = fmaf(S.c1, v.x, ns * n0);
+      v.y = fmaf(S.c1, v.y, ns * n1);
+      v.z = fmaf(S.c1, v.z, ns * n2);
       p.x = fmaf(S.hdt, v.x, p.x);
       p.y = fmaf(S.hdt, v.y, p.y);
       p.z = fmaf(S.hdt, v.z, p.z);
@@ -204,6 +242,7 @@ __global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
   // Last block of the replica: commit scalars, decide on a rebuild.
   __threadfence();
   R.cnt_pre = 0;
+  R.next_valid = 0;
   R.step = S.step;
   R.nh = S.nh;
   R.pending_scale = 1.0;
@@ -226,6 +265,11 @@ __global__ void __launch_bounds__(kChunk) k_pre(Dev d) {
   } else {
     R.rebuild_now = 0;
   }
+  if (cond.use) {
+    // any replica that rebuilds / needs a force variant switches it on
+    if (R.rebuild_now) cudaGraphSetConditional(cond.rebuild, 1u);
+    cudaGraphSetConditional(need_ev(R) ? cond.force_ev : cond.force_plain, 1u);
+  }
 }
 
 // ---------------------------------------------------------------- rebuild
@@ -242,6 +286,7 @@ __device__ __forceinline__ void pair_shift(int ci, int cj, float oi, float oj, i
 __device__ __forceinline__ float shift_term(int e, int k, float h, float dL) { return (float)e * h + (float)k * dL; }
 
 __global__ void __launch_bounds__(kChunk) k_bin(Dev d) {
+  count_launch(d, kKBin);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
@@ -292,6 +337,7 @@ __global__ void __launch_bounds__(kChunk) k_bin(Dev d) {
 
 // Exclusive scan of the replica's cell counts; one block per replica.
 __global__ void __launch_bounds__(1024) k_scan(Dev d, int nreps) {
+  count_launch(d, kKScan);
   const int r = blockIdx.x;
   if (r >= nreps) return;
   Rep& R = d.reps[r];
@@ -328,6 +374,7 @@ __global__ void __launch_bounds__(1024) k_scan(Dev d, int nreps) {
 }
 
 __global__ void __launch_bounds__(kChunk) k_scatter(Dev d) {
+  count_launch(d, kKScatter);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
@@ -341,21 +388,22 @@ __global__ void __launch_bounds__(kChunk) k_scatter(Dev d) {
 }
 
 // Per cell: order members by atom id (deterministic), write the permutation.
-// grid (cell blocks, replicas); 8 warps per block, 32 cells per warp.  Cells
-// of up to 32 members rank in registers with shuffles; larger ones fall back
-// to a loop over the bucket.
+// grid (cell blocks, replicas); one warp per cell.  Cells of up to 32
+// members rank in registers with shuffles; larger ones fall back to a loop
+// over the bucket.
 __global__ void __launch_bounds__(256) k_cellsort(Dev d, int nreps) {
+  count_launch(d, kKCellsort);
   const int r = blockIdx.y;
   if (r >= nreps) return;
   const Rep& R = d.reps[r];
   if (!R.active || !R.rebuild_now) return;
   const int ncell = R.P * R.P * R.P;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int c0 = (blockIdx.x * 8 + warp) * 32;
-  for (int c = c0; c < c0 + 32 && c < ncell; ++c) {
+  const int c = blockIdx.x * 8 + warp;
+  if (c < ncell) {
     const int st = d.cell_start[R.cell_base + c];
     const int n = d.cell_fill[R.cell_base + c] - st;
-    if (n <= 0) continue;
+    if (n <= 0) return;
     if (n <= 32) {
       int old = 0, id = 0x7FFFFFFF;
       if (lane < n) {
@@ -378,6 +426,7 @@ __global__ void __launch_bounds__(256) k_cellsort(Dev d, int nreps) {
 }
 
 __global__ void __launch_bounds__(kChunk) k_permute(Dev d) {
+  count_launch(d, kKPermute);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
@@ -402,6 +451,7 @@ __global__ void __launch_bounds__(kChunk) k_permute(Dev d) {
 // Per-slot bonded tables for the new order: partner slots instead of atom
 // ids, so the force kernel reaches a partner's position in one load.
 __global__ void __launch_bounds__(kChunk) k_topo(Dev d) {
+  count_launch(d, kKTopo);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
@@ -436,17 +486,12 @@ __global__ void __launch_bounds__(kChunk) k_topo(Dev d) {
   d.tcnt[s] = (b1 - b0) | ((a1 - a0) << 8);
 }
 
-// Verlet list: one warp per home cell; candidate cells are staged through
-// registers 32 atoms at a time and broadcast with shuffles.  Pairs within
-// rc + skin, 1-2 bonded pairs excluded (verlet_list.cu:108-335 semantics).
-__global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
-  const int r = blockIdx.y;
-  if (r >= nreps) return;
-  Rep& R = d.reps[r];
-  if (!R.active || !R.rebuild_now) return;
+// Verlet list for boxes of fewer than three cells per axis (L < 3 (rc +
+// skin)): one warp per home cell, the distinct neighbor cells de-duplicated,
+// each pair's periodic shift derived from the two cells and offsets.
+// Candidates are broadcast 32 at a time with shuffles.
+__device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
   const int G = R.G;
-  const int ncell = G * G * G;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const float h = R.h, inv_h = 1.0f / h;
   const float dL = (float)(R.L - (double)G * (double)h);
   const float rcs = (float)(R.rc + R.skin);
@@ -454,8 +499,7 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
   const int M = R.M;
   const int base = R.slot_base;
   int overflow = 0;
-  const int c0 = (blockIdx.x * 8 + warp) * 4;
-  for (int lc = c0; lc < c0 + 4 && lc < ncell; ++lc) {
+  {
     const int hx = lc % G, hy = (lc / G) % G, hz = lc / (G * G);
     const uint32_t hkey = cell_key(hx, hy, hz);
     const int hs = d.cell_start[R.cell_base + hkey];
@@ -474,25 +518,18 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
       }
       int count = 0;
       uint32_t* out = d.nbr + R.nbr_base + ((size_t)(il >> 5) * M) * 32 + (il & 31);
-      // Distinct neighbor cells (all 27 when G >= 3).
-      int visited[27];
+      int visited[27];  // distinct neighbor cells
       int nvis = 0;
       for (int dz = -1; dz <= 1; ++dz)
         for (int dy = -1; dy <= 1; ++dy)
           for (int dx = -1; dx <= 1; ++dx) {
             const int nx = (hx + dx + G) % G, ny = (hy + dy + G) % G, nz = (hz + dz + G) % G;
             const int lin = (nz * G + ny) * G + nx;
-            if (G < 3) {
-              bool seen = false;
-              for (int v = 0; v < nvis; ++v) seen |= (visited[v] == lin);
-              if (seen) continue;
-              visited[nvis++] = lin;
-            }
+            bool seen = false;
+            for (int v = 0; v < nvis; ++v) seen |= (visited[v] == lin);
+            if (seen) continue;
+            visited[nvis++] = lin;
             const uint32_t nkey = cell_key(nx, ny, nz);
-            // shift of this neighbor cell relative to the home cell (G >= 3)
-            const float csx = shift_term(dx, (hx + dx < 0) ? -1 : (hx + dx >= G ? 1 : 0), h, dL);
-            const float csy = shift_term(dy, (hy + dy < 0) ? -1 : (hy + dy >= G ? 1 : 0), h, dL);
-            const float csz = shift_term(dz, (hz + dz < 0) ? -1 : (hz + dz >= G ? 1 : 0), h, dL);
             const int ns = d.cell_start[R.cell_base + nkey];
             const int ne = d.cell_fill[R.cell_base + nkey];
             for (int jb = ns; jb < ne; jb += 32) {
@@ -507,26 +544,18 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
                 const float jw = __shfl_sync(0xFFFFFFFFu, pj.w, t);
                 const int j = jb + t;
                 if (!act || j == il) continue;
-                int ex = dx, ey = dy, ez = dz;
-                float rx, ry, rz;
-                if (G >= 3) {
-                  // the stencil offset is the cell shift; the wrap count follows from it
-                  rx = (pi.x - jx) - csx;
-                  ry = (pi.y - jy) - csy;
-                  rz = (pi.z - jz) - csz;
-                } else {
-                  const uint32_t ui = w_bits(pi.w), uj = w_bits(jw);
-                  int kx, ky, kz;
-                  pair_shift(w_cx(ui), w_cx(uj), pi.x, jx, G, inv_h, ex, kx);
-                  pair_shift(w_cy(ui), w_cy(uj), pi.y, jy, G, inv_h, ey, ky);
-                  pair_shift(w_cz(ui), w_cz(uj), pi.z, jz, G, inv_h, ez, kz);
-                  rx = (pi.x - jx) - shift_term(ex, kx, h, dL);
-                  ry = (pi.y - jy) - shift_term(ey, ky, h, dL);
-                  rz = (pi.z - jz) - shift_term(ez, kz, h, dL);
-                }
+                int ex, ey, ez, kx, ky, kz;
+                const uint32_t ui = w_bits(pi.w), uj = w_bits(jw);
+                pair_shift(w_cx(ui), w_cx(uj), pi.x, jx, G, inv_h, ex, kx);
+                pair_shift(w_cy(ui), w_cy(uj), pi.y, jy, G, inv_h, ey, ky);
+                pair_shift(w_cz(ui), w_cz(uj), pi.z, jz, G, inv_h, ez, kz);
+                const float rx = (pi.x - jx) - shift_term(ex, kx, h, dL);
+                const float ry = (pi.y - jy) - shift_term(ey, ky, h, dL);
+                const float rz = (pi.z - jz) - shift_term(ez, kz, h, dL);
                 const float r2 = rx * rx + ry * ry + rz * rz;
                 if (r2 < rcs2) {
-                  if (ex < -1 || ex > 1 || ey < -1 || ey > 1 || ez < -1 || ez > 1) {
+                  const int ax = axis_shift_code(ex, kx), ay = axis_shift_code(ey, ky), az = axis_shift_code(ez, kz);
+                  if (ax < 0 || ay < 0 || az < 0) {
                     overflow |= kStatusCellCapacity;
                     continue;
                   }
@@ -535,7 +564,7 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
                   for (int b = b0; b < b1; ++b) excl |= (d.bent[R.bond_base + b].x == idj);
                   if (excl) continue;
                   if (count < M)
-                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)((ex + 1) * 9 + (ey + 1) * 3 + (ez + 1)) << 27);
+                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)(ax * 25 + ay * 5 + az) << kCodeShift);
                   ++count;
                 }
               }
@@ -547,11 +576,148 @@ __global__ void __launch_bounds__(256) k_neighbors(Dev d, int nreps) {
       }
     }
   }
+  return overflow;
+}
+
+// Verlet list, one block per home cell (G >= 3).  The 27 neighbor cells'
+// atoms are staged in shared memory in stencil order (dz, dy, dx; slot order
+// inside a cell) with the cell's periodic shift already added, so a pair's
+// separation is one subtraction.  Each warp takes one home atom at a time;
+// its lanes test 32 candidates, a ballot compacts the hits and they are
+// stored in candidate order, so the list (and the force sums that follow it)
+// is deterministic.  Pairs within rc + skin, 1-2 bonded pairs excluded
+// (verlet_list.cu:108-335 semantics), exclusions compared as slots from the
+// per-slot bond table.
+constexpr int kNbrThreads = 128;
+constexpr int kNbrWarps = kNbrThreads / 32;
+constexpr int kNbrWin = 1024;     // staged candidates per window
+constexpr int kNbrGroup = 64;     // home atoms per pass
+
+__global__ void __launch_bounds__(kNbrThreads) k_neighbors(Dev d, int nreps) {
+  count_launch(d, kKNeighbors);
+  const int r = blockIdx.y;
+  if (r >= nreps) return;
+  Rep& R = d.reps[r];
+  if (!R.active || !R.rebuild_now) return;
+  const int G = R.G;
+  const int lc = blockIdx.x;
+  if (lc >= G * G * G) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (G < 3) {
+    if (warp == 0) {
+      const int ov = neighbors_small_box(d, R, lc, lane);
+      if (ov) atomicOr(&R.status, ov);
+    }
+    return;
+  }
+  const int M = R.M;
+  const int base = R.slot_base;
+  const int cell_base = R.cell_base;
+  uint32_t* const list = d.nbr + R.nbr_base;
+  const float h = R.h;
+  const float dL = (float)(R.L - (double)G * (double)h);
+  const float rcs = (float)(R.rc + R.skin);
+  const float rcs2 = rcs * rcs;
+
+  __shared__ float4 s_c[kNbrWin];
+  __shared__ int s_ns[27], s_off[28], s_cnt[kNbrGroup];
+  __shared__ float s_sx[27], s_sy[27], s_sz[27];
+  __shared__ uint32_t s_code[27];
+  const int hx = lc % G, hy = (lc / G) % G, hz = lc / (G * G);
+  if (threadIdx.x < 27) {
+    const int t = threadIdx.x;
+    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+    const int nx = (hx + dx + G) % G, ny = (hy + dy + G) % G, nz = (hz + dz + G) % G;
+    const uint32_t nkey = cell_key(nx, ny, nz);
+    const int ns = d.cell_start[cell_base + nkey];
+    s_ns[t] = ns;
+    s_off[t + 1] = d.cell_fill[cell_base + nkey] - ns;
+    // a candidate's position relative to the home cell: offset + shift
+    const int kx = (hx + dx < 0) ? -1 : (hx + dx >= G ? 1 : 0);
+    const int ky = (hy + dy < 0) ? -1 : (hy + dy >= G ? 1 : 0);
+    const int kz = (hz + dz < 0) ? -1 : (hz + dz >= G ? 1 : 0);
+    s_sx[t] = shift_term(dx, kx, h, dL);
+    s_sy[t] = shift_term(dy, ky, h, dL);
+    s_sz[t] = shift_term(dz, kz, h, dL);
+    s_code[t] = (uint32_t)(axis_shift_code(dx, kx) * 25 + axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz))
+                << kCodeShift;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_off[0] = 0;
+    for (int t = 0; t < 27; ++t) s_off[t + 1] += s_off[t];
+  }
+  __syncthreads();
+  const int total = s_off[27];
+  const int hs = s_ns[13];
+  const int nh = s_off[14] - s_off[13];
+  if (nh == 0) return;
+  int overflow = 0;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int hg = 0; hg < nh; hg += kNbrGroup) {
+    const int gn = min(kNbrGroup, nh - hg);
+    for (int w0 = 0; w0 < total; w0 += kNbrWin) {
+      const int wn = min(kNbrWin, total - w0);
+      if (hg == 0 || total > kNbrWin) {
+        __syncthreads();
+        for (int t = warp; t < 27; t += kNbrWarps) {
+          const int o0 = s_off[t], o1 = s_off[t + 1];
+          const int lo = max(o0, w0), hi = min(o1, w0 + wn);
+          const float sx = s_sx[t], sy = s_sy[t], sz = s_sz[t];
+          const uint32_t code = s_code[t];
+          const int ns = s_ns[t];
+          for (int k = lo + lane; k < hi; k += 32) {
+            const int j = ns + (k - o0);
+            const float4 p = d.pos[base + j];
+            s_c[k - w0] = make_float4(p.x + sx, p.y + sy, p.z + sz, __uint_as_float((uint32_t)j | code));
+          }
+        }
+        __syncthreads();
+      }
+      for (int a = warp; a < gn; a += kNbrWarps) {
+        const int i = hs + hg + a;
+        const float4 pi = d.pos[base + i];
+        const int nb = d.tcnt[base + i] & 0xFF;
+        uint32_t ex[kMaxBondsPerAtom];
+#pragma unroll
+        for (int b = 0; b < kMaxBondsPerAtom; ++b)
+          ex[b] = b < nb ? (d.bnd[(size_t)(base + i) * kMaxBondsPerAtom + b] & kSlotMask26) : 0xFFFFFFFFu;
+        int count = w0 == 0 ? 0 : s_cnt[a];
+        uint32_t* out = list + ((size_t)(i >> 5) * M) * 32 + (i & 31);
+        for (int c0 = 0; c0 < wn; c0 += 32) {
+          const int k = c0 + lane;
+          bool acc = false;
+          uint32_t e = 0;
+          if (k < wn) {
+            const float4 c = s_c[k];
+            const float rx = pi.x - c.x, ry = pi.y - c.y, rz = pi.z - c.z;
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            e = __float_as_uint(c.w);
+            const uint32_t j = e & kIdxMask;
+            acc = r2 < rcs2 && j != (uint32_t)i && j != ex[0] && j != ex[1] && j != ex[2] && j != ex[3];
+          }
+          const uint32_t m = __ballot_sync(0xFFFFFFFFu, acc);
+          const int at = count + __popc(m & lt);
+          if (acc && at < M) out[(size_t)at * 32] = e;
+          count += __popc(m);
+        }
+        if (w0 + kNbrWin >= total) {
+          if (lane == 0) {
+            d.ncnt[base + i] = min(count, M);
+            if (count > M) overflow |= kStatusOverflow;
+          }
+        } else if (lane == 0) {
+          s_cnt[a] = count;
+        }
+      }
+    }
+  }
   if (overflow) atomicOr(&R.status, overflow);
 }
 
 // ---------------------------------------------------------------- forces
 constexpr int kBatch = 8;  // neighbors whose loads are issued together
+constexpr int kForceBlocksPerSM = 6;
 
 struct KahanF {
   float s, c;
@@ -562,10 +728,6 @@ struct KahanF {
     s = t;
   }
 };
-
-__device__ __forceinline__ float sel3(int code, float m, float z, float p) {
-  return code == 0 ? m : (code == 1 ? z : p);
-}
 
 // Displacement r_i - r_j for a bonded pair (cells may differ by any amount).
 __device__ __forceinline__ float3 bonded_dr(float4 pi, float4 pj, int G, float h, float inv_h, float dL) {
@@ -595,18 +757,20 @@ __device__ __forceinline__ void block_partials(double* vals, int nv, double* out
   }
 }
 
-// LJ contribution of one listed neighbor (lj.cu:32-61 semantics).  t is
-// pos_i - shift for the entry's cell-shift code, so r_ij = t - pos_j.
-// EV: also accumulate half the pair energy and the virial half-pair.
+// LJ contribution of one listed neighbor (lj.cu:32-61 semantics).  sh is
+// the periodic shift vector named by the entry's code, so
+// r_ij = (pos_i - pos_j) - sh.  EV: also accumulate half the pair energy and
+// the virial half-pair.
 struct PairAcc {
   float fx, fy, fz, pe, v0, v1, v2, v3, v4, v5;
 };
 
 template <bool EV>
-__device__ __forceinline__ void lj_pair(PairAcc& a, float4 t, float4 pj, float rc2, float e24, float sig2) {
-  const float dx = t.x - pj.x;
-  const float dy = t.y - pj.y;
-  const float dz = t.z - pj.z;
+__device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4 pj, float rc2, float e24,
+                                        float sig2) {
+  const float dx = (pi.x - pj.x) - sh.x;
+  const float dy = (pi.y - pj.y) - sh.y;
+  const float dz = (pi.z - pj.z) - sh.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   if (r2 < rc2 && r2 > 1e-10f) {
     const float r2inv = __fdividef(1.0f, r2);
@@ -633,9 +797,10 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 t, float4 pj, float r
 // The LJ loop over one atom's list: batches of kBatch entries (all list
 // loads, then all position gathers, then the arithmetic).
 template <bool EV>
-__device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, const float4* tab, int tid,
-                                        bool one_type, int ti, int nt, const float* s_eps24, const float* s_sig2,
-                                        float rc2, KahanF& fx, KahanF& fy, KahanF& fz, PairAcc& acc) {
+__device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
+                                        const float4* s_shift, bool one_type, int ti, int nt, const float* s_eps24,
+                                        const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
+                                        PairAcc& acc) {
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
   int k = 0;
   for (; k + kBatch <= nn; k += kBatch) {
@@ -654,7 +819,7 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
         e24 = s_eps24[pidx];
         sig2 = s_sig2[pidx];
       }
-      lj_pair<EV>(g, tab[(w[q] >> 27) * kChunk + tid], pj[q], rc2, e24, sig2);
+      lj_pair<EV>(g, pi, s_shift[w[q] >> kCodeShift], pj[q], rc2, e24, sig2);
     }
     fx.add(g.fx);
     fy.add(g.fy);
@@ -671,7 +836,7 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
       e24 = s_eps24[pidx];
       sig2 = s_sig2[pidx];
     }
-    lj_pair<EV>(g, tab[(w >> 27) * kChunk + tid], pj, rc2, e24, sig2);
+    lj_pair<EV>(g, pi, s_shift[w >> kCodeShift], pj, rc2, e24, sig2);
   }
   fx.add(g.fx);
   fy.add(g.fy);
@@ -723,40 +888,40 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
   pe += kt * dth * dth * (1.0f / 3.0f);
 }
 
-// Energies and virial are needed on thermo steps, for NPT (the barostat uses
-// the virial every step) and when the host asks for them.
-__device__ __forceinline__ bool need_ev(const Rep& R) {
-  if (R.force_ev) return true;
-  if (R.mode != kModePushoff && R.ensemble == FMD_NPT_NH) return true;
-  return R.thermo_freq > 0 && (R.step % R.thermo_freq) == 0;
-}
-
 // Two instantiations: with energies / virial (thermo steps, NPT, host
 // requests) and without (all other steps); a block runs in the one that
 // matches its replica's need this step and the other returns at once.
 template <bool EV>
-__global__ void __launch_bounds__(kChunk) k_force(Dev d) {
+__global__ void __launch_bounds__(kChunk, EV ? kForceBlocksPerSM - 1 : kForceBlocksPerSM) k_force(Dev d) {
+  count_launch(d, EV ? kKForceEv : kKForce);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
   const Rep& R = d.reps[r];
   if (!R.adv) return;
   if (need_ev(R) != EV) return;
-  extern __shared__ float4 tab[];  // [27][kChunk]
   constexpr bool ev = EV;
+  __shared__ float4 s_shift[kShiftCodes];
   __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
   const int nt = R.ntypes;
+  const int G = R.G;
+  const float h = R.h, inv_h = 1.0f / h;
+  const float dL = (float)(R.L - (double)G * (double)h);
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
     s_eps24[k] = R.lj_eps24[k];
     s_sig2[k] = R.lj_sig2[k];
+  }
+  if (threadIdx.x < kShiftCodes) {
+    const int c = threadIdx.x;
+    const int ax = c / 25, ay = (c / 5) % 5, az = c % 5;
+    s_shift[c] = make_float4(shift_term(axis_code_e(ax), axis_code_k(ax), h, dL),
+                             shift_term(axis_code_e(ay), axis_code_k(ay), h, dL),
+                             shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
   }
   __syncthreads();
   const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
   const int base = R.slot_base;
   const int s = base + local;
-  const int G = R.G;
-  const float h = R.h, inv_h = 1.0f / h;
-  const float dL = (float)(R.L - (double)G * (double)h);
   const float rc2 = (float)(R.rc * R.rc);
   double vals[7] = {0, 0, 0, 0, 0, 0, 0};
   int status = 0;
@@ -764,26 +929,13 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
     const float4 pi = d.pos[s];
     const uint32_t ui = w_bits(pi.w);
     const int ti = w_type(ui);
-    const int cx = w_cx(ui), cy = w_cy(ui), cz = w_cz(ui);
-    // Per-axis shift for codes 0,1,2 (e = -1, 0, +1), including the periodic
-    // correction dL when the neighbor cell index wraps.
-    const float sxm = -h - (cx == 0 ? dL : 0.0f), sxp = h + (cx == G - 1 ? dL : 0.0f);
-    const float sym = -h - (cy == 0 ? dL : 0.0f), syp = h + (cy == G - 1 ? dL : 0.0f);
-    const float szm = -h - (cz == 0 ? dL : 0.0f), szp = h + (cz == G - 1 ? dL : 0.0f);
-    // pos_i - shift for the 27 cell-shift codes, in this thread's column.
-#pragma unroll
-    for (int c = 0; c < 27; ++c) {
-      const int ex = c / 9, ey = (c / 3) % 3, ez = c % 3;
-      tab[c * kChunk + threadIdx.x] = make_float4(pi.x - sel3(ex, sxm, 0.0f, sxp), pi.y - sel3(ey, sym, 0.0f, syp),
-                                                  pi.z - sel3(ez, szm, 0.0f, szp), 0.0f);
-    }
     KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
     PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int nn = d.ncnt[s];
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
     const bool one_type = (nt == 1);
-    lj_loop<EV>(lst, nn, pbase, tab, threadIdx.x, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    lj_loop<EV>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
@@ -862,11 +1014,12 @@ __global__ void __launch_bounds__(kChunk) k_force(Dev d) {
   }
   status = __syncthreads_or(status);
   if (threadIdx.x == 0 && status) atomicOr((int*)&d.reps[r].status, status);
-  block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
+  if (EV) block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
 }
 
 // ---------------------------------------------------------------- post-force
-__global__ void __launch_bounds__(kChunk) k_post(Dev d, int kick) {
+__global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
+  count_launch(d, kKPost);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
@@ -953,6 +1106,9 @@ __global__ void __launch_bounds__(kChunk) k_post(Dev d, int kick) {
       R.thermo_step = R.step;
       R.adv = 0;
       R.rebuild_now = 0;
+      // scalars of the next pre-force, computed once here for all its blocks
+      compute_step_scalars(R, R.next);
+      R.next_valid = 1;
     }
   }
 }
@@ -962,43 +1118,75 @@ __global__ void __launch_bounds__(kChunk) k_post(Dev d, int kick) {
 // the next pre-force nothing reads h.)
 
 // ---------------------------------------------------------------- launchers
-constexpr size_t kForceSmem = 27 * kChunk * sizeof(float4);
 
-void force_kernel_setup() {
-  static bool done = false;
-  if (!done) {
-    FMD_CUDA(cudaFuncSetAttribute(k_force<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem));
-    FMD_CUDA(cudaFuncSetAttribute(k_force<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kForceSmem));
-    done = true;
-  }
-}
-
-void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st) {
-  force_kernel_setup();
-  k_pre<<<nchunks, kChunk, 0, st>>>(d);
-  launch_rebuild(d, nchunks, nreps, max_cells, st);
-  k_force<false><<<nchunks, kChunk, kForceSmem, st>>>(d);
-  k_force<true><<<nchunks, kChunk, kForceSmem, st>>>(d);
+void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st) {
+  k_pre<<<nchunks, kChunk, 0, st>>>(d, StepConds{0, 0, 0, 0});
+  launch_rebuild(d, nchunks, nreps, max_cells, max_home, st);
+  k_force<false><<<nchunks, kChunk, 0, st>>>(d);
+  k_force<true><<<nchunks, kChunk, 0, st>>>(d);
   k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
 }
 
-void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, cudaStream_t st) {
+namespace {
+// Append an IF node on handle h to the graph being captured on st; its body
+// is recorded on side by fn(side).
+template <typename F>
+void capture_if(cudaStream_t st, cudaStream_t side, cudaGraphConditionalHandle h, F&& fn) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  FMD_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) throw Error(FMD_ERR_CUDA, "conditional node outside a capture");
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeIf;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  FMD_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  FMD_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  fn(side);
+  cudaGraph_t done;
+  FMD_CUDA(cudaStreamEndCapture(side, &done));
+  FMD_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+}
+}  // namespace
+
+void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st,
+                  cudaStream_t side) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g;
+  FMD_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
+  StepConds c{1, 0, 0, 0};
+  FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild, g, 0u, cudaGraphCondAssignDefault));
+  FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_plain, g, 0u, cudaGraphCondAssignDefault));
+  FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
+  k_pre<<<nchunks, kChunk, 0, st>>>(d, c);
+  capture_if(st, side, c.rebuild, [&](cudaStream_t s) { launch_rebuild(d, nchunks, nreps, max_cells, max_home, s); });
+  capture_if(st, side, c.force_plain, [&](cudaStream_t s) { k_force<false><<<nchunks, kChunk, 0, s>>>(d); });
+  capture_if(st, side, c.force_ev, [&](cudaStream_t s) { k_force<true><<<nchunks, kChunk, 0, s>>>(d); });
+  k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
+}
+
+void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st) {
   if (max_cells < 1) max_cells = 1;
+  if (max_home < 1) max_home = 1;
   k_bin<<<nchunks, kChunk, 0, st>>>(d);
   k_scan<<<nreps, 1024, 0, st>>>(d, nreps);
   k_scatter<<<nchunks, kChunk, 0, st>>>(d);
-  dim3 gs((max_cells + 255) / 256, nreps);
+  dim3 gs((max_cells + 7) / 8, nreps);
   k_cellsort<<<gs, 256, 0, st>>>(d, nreps);
   k_permute<<<nchunks, kChunk, 0, st>>>(d);
   k_topo<<<nchunks, kChunk, 0, st>>>(d);
-  dim3 gn((max_cells + 31) / 32, nreps);
-  k_neighbors<<<gn, 256, 0, st>>>(d, nreps);
+  dim3 gn(max_home, nreps);
+  k_neighbors<<<gn, kNbrThreads, 0, st>>>(d, nreps);
 }
 
 void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st) {
-  force_kernel_setup();
-  k_force<false><<<nchunks, kChunk, kForceSmem, st>>>(d);
-  k_force<true><<<nchunks, kChunk, kForceSmem, st>>>(d);
+  k_force<false><<<nchunks, kChunk, 0, st>>>(d);
+  k_force<true><<<nchunks, kChunk, 0, st>>>(d);
 }
 void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode) {
   k_post<<<nchunks, kChunk, 0, st>>>(d, mode);

@@ -146,6 +146,12 @@ FMD_API fmd_status fmd_read_lammps_data(const char* path, int32_t* counts, doubl
                                         int32_t* image, int32_t* type, int32_t* mol, double* vel,
                                         int32_t* bonds, int32_t* bond_type, int32_t* angles,
                                         int32_t* angle_type, double* masses);
+/* Write a system as a LAMMPS data file in the layout of the reference's
+ * restart writer (src/io/lammps_data.cpp:269-385): header with the step,
+ * Masses, "Atoms # full" with image flags, Velocities, Bonds, Angles.  Values
+ * carry 17 significant digits (the reference writes %.6f); the zhi line
+ * carries the box edge (the reference's writer omits it, :335). */
+FMD_API fmd_status fmd_write_lammps_data(const char* path, const fmd_system_desc* desc, int64_t step);
 /* Reference text rows: "%d  %.4f ..." (thermo.cu:192) and "%d  %.4f" (rg.cu:127). */
 FMD_API fmd_status fmd_format_thermo_row(const fmd_thermo_row* row, char* buf, size_t len);
 FMD_API fmd_status fmd_format_rg_row(int64_t step, double rg, char* buf, size_t len);
@@ -168,6 +174,9 @@ FMD_API fmd_status fmd_compute_forces(fmd_sim* sim, double* f, double* pe, doubl
 FMD_API fmd_status fmd_get_state(fmd_sim* sim, double* xyz, double* vel, int32_t* image);
 FMD_API fmd_status fmd_set_state(fmd_sim* sim, const double* xyz, const double* vel, const int32_t* image);
 FMD_API fmd_status fmd_thermo(fmd_sim* sim, fmd_thermo_row* row);
+/* Restart file of the current state (write_lammps_data, io/lammps_data.cpp:269;
+ * main.cu:681-691, 738-745 call it every restart_freq steps and at the end). */
+FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path);
 FMD_API fmd_status fmd_rg(fmd_sim* sim, double* rg);
 /* Current Verlet pair set (unordered pairs i < j within rc + skin at the last
  * rebuild, 1-2 bonded pairs excluded), in data-file indices. */
@@ -213,6 +222,7 @@ FMD_API fmd_status fmd_batch_retire(fmd_batch* b, int32_t slot);
 FMD_API fmd_status fmd_batch_replica_info(fmd_batch* b, int32_t slot, fmd_replica_info* info);
 FMD_API fmd_status fmd_batch_get_state(fmd_batch* b, int32_t slot, double* xyz, double* vel, int32_t* image);
 FMD_API fmd_status fmd_batch_thermo(fmd_batch* b, int32_t slot, fmd_thermo_row* row);
+FMD_API fmd_status fmd_batch_write_restart(fmd_batch* b, int32_t slot, const char* path);
 FMD_API fmd_status fmd_batch_rg(fmd_batch* b, int32_t slot, double* rg);
 FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* f, double* pe, double* virial);
 FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n);
@@ -226,12 +236,18 @@ FMD_API fmd_status fmd_batch_totals(fmd_batch* b, int32_t* active, int64_t* atom
  * current state (idempotent) and returns its mean device time per launch.
  * fmd_batch_list_stats: total neighbor-list entries and the largest per-atom
  * count over active replicas.
- * fmd_batch_kernels_per_step: kernel launches one step issues. */
+ * fmd_batch_kernels_per_step: kernel launches one step issues at most.
+ * fmd_batch_launch_counts: launches executed so far per kernel, counted on
+ * the device (a graph step skips the rebuild kernels and a force variant no
+ * replica needs): counts[0..10] = pre-force, bin, scan, scatter, cell sort,
+ * permute, bonded tables, neighbor list, force, force with energies,
+ * post-force; n = entries to fill. */
 FMD_API fmd_status fmd_batch_mark(fmd_batch* b, int32_t which);
 FMD_API fmd_status fmd_batch_elapsed_ms(fmd_batch* b, double* ms);
 FMD_API fmd_status fmd_batch_time_force(fmd_batch* b, int32_t iters, double* ms_per_launch);
 FMD_API fmd_status fmd_batch_list_stats(fmd_batch* b, int64_t* entries, int32_t* max_per_atom);
 FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n);
+FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_t n);
 /* Set the forced rebuild cadence of a replica (the reference rebuilds at
  * least every 20 steps, main.cu:401); the skin/2 displacement test still
  * triggers rebuilds in between. */

@@ -154,3 +154,50 @@ def test_bad_arguments_are_status_codes():
     buf = C.create_string_buffer(128)
     lib.fmd_last_error(buf, 128)
     assert b"null" in buf.value
+
+
+def test_lammps_data_writer_round_trip(tmp_path):
+    d = fm.generate_melt(5, 20, density=0.85, seed=3, type_block=10)
+    rng = np.random.default_rng(0)
+    d.vel = rng.normal(size=d.xyz.shape)
+    d.mass = np.array([1.0, 2.5])
+    d.ntypes = 2
+    p = tmp_path / "rt.data"
+    fm.write_lammps_data(p, d, step=1234)
+    text = p.read_text()
+    assert text.startswith("# Restart from step 1234")
+    assert "zlo zhi" in text and "Atoms # full" in text
+    e = fm.read_lammps_data(str(p))
+    assert np.array_equal(e.xyz, d.xyz) and np.array_equal(e.vel, d.vel)
+    assert np.array_equal(e.image, d.image) and np.array_equal(e.type, d.type)
+    assert np.array_equal(e.mol, d.mol) and np.array_equal(e.bonds, d.bonds)
+    assert np.array_equal(e.angles, d.angles) and np.allclose(e.mass, d.mass)
+    assert e.box_L == d.box_L
+
+
+def test_lammps_data_writer_is_read_by_reference_reader(tmp_path):
+    """The reference's own parser (io/lammps_data.cpp) reads the written file."""
+    R = po.ref_lib()
+    if R is None:
+        pytest.skip("reference CPU code not built")
+    d = fm.generate_melt(4, 10, density=0.85, seed=5)
+    p = tmp_path / "ref.data"
+    fm.write_lammps_data(p, d)
+    counts = np.zeros(4, np.int32)
+    Lc = C.c_float()
+    err = C.create_string_buffer(256)
+    assert R.ref_parse_lammps_data(str(p).encode(), counts, C.byref(Lc),
+                                   *([None] * 10), err, 256) == 0, err.value
+    n, nb, na = (int(x) for x in counts[:3])
+    assert (n, nb, na) == (40, 36, 32)
+    assert abs(Lc.value - d.box_L) < 1e-5
+    xyz = np.zeros(3 * n, np.float32)
+    i32 = lambda k: np.zeros(k, np.int32)
+    # xyz, type, mol, image, vel, bonds, bond types, angles, angle types, masses
+    arrs = [xyz, i32(n), i32(n), i32(3 * n), np.zeros(3 * n, np.float32), i32(2 * nb), i32(nb), i32(3 * na), i32(na),
+            np.zeros(8, np.float32)]
+    assert R.ref_parse_lammps_data(str(p).encode(), counts, C.byref(Lc),
+                                   *[a.ctypes.data for a in arrs], err, 256) == 0
+    assert np.allclose(xyz, d.xyz.reshape(-1), atol=1e-5)
+    assert np.array_equal(arrs[3], d.image.reshape(-1))
+    assert np.array_equal(arrs[5], d.bonds.reshape(-1)) and np.array_equal(arrs[7], d.angles.reshape(-1))

@@ -98,6 +98,7 @@ def test_mixed_steps_track_oracle(ens):
         t = sim.thermo().as_array()
         ot = osim.thermo()
         assert np.allclose(t, ot, rtol=2e-4, atol=2e-4), (name, t, ot)
+        assert abs(sim.rg() - osim.rg()) < 1e-5 * osim.rg(), (name, sim.rg(), osim.rg())
 
 
 def test_batch_alone_equals_in_mix():
