@@ -240,7 +240,8 @@ def reference_gpu_leg(fm, xyz, vel, image, steps):
         fm.write_lammps_data(data, d)
         conf = os.path.join(td, "run.conf")
         with open(conf, "w") as f:
-            f.write(run_conf(42, nsteps=steps) + f"lammps_data_file {data}\n")
+            # the reference sizes its arrays from natoms (main.cu:62-99)
+            f.write(run_conf(42, nsteps=steps) + f"natoms {len(d.type)}\nlammps_data_file {data}\n")
         out = subprocess.run([exe, conf], capture_output=True, text=True, timeout=600, cwd=td)
     m = re.search(r"Steps/s:\s*([0-9.]+)", out.stdout)
     if out.returncode != 0 or not m:
@@ -270,6 +271,8 @@ def main():
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / plain / CPU / reference-GPU legs")
     ap.add_argument("--ref-gpu-steps", type=int, default=5000, help="steps of the reference GPU datapoint")
+    ap.add_argument("--graph-steps", type=int, default=50,
+                    help="steps per CUDA graph launch; < 0 launches every step directly (for kernel profilers)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local, dist = dist_setup(args.gpus)
@@ -282,7 +285,8 @@ def main():
     import fastmd_b200 as fm
 
     R = args.replicas
-    b = fm.Batch(max_replicas=R, max_atoms=R * 30080 + 4096, hbm_budget_gb=150.0, graph_steps=50, device=local)
+    b = fm.Batch(max_replicas=R, max_atoms=R * 30080 + 4096, hbm_budget_gb=150.0, graph_steps=args.graph_steps,
+                 device=local)
     t_setup = time.perf_counter()
     slots = []
     for r in range(R):
@@ -293,8 +297,10 @@ def main():
     natoms = sum(b.info(s).natoms for s in slots)
     lib = fm.lib()
 
-    # warm-up
+    # warm-up, then the force-kernel autotuner on the live state
     b.run(args.warmup)
+    variant, variant_ms = b.autotune(20)
+    b.run(3)
     barrier(dist, local)
     counts0 = b.launch_counts()
     with ClockSampler(local) as clk:
@@ -324,7 +330,7 @@ def main():
         "config": {"workload": "kg_melt_64x30k_langevin_batched", "replicas_per_gpu": R,
                    "beads_per_replica": NCHAINS * CHAIN_LEN, "chains": NCHAINS, "chain_length": CHAIN_LEN,
                    "density": DENSITY, "rc": 2.5, "skin": 0.3, "dt": 0.001, "ensemble": "nvt_langevin T=1 Tdamp=1",
-                   "form": "mixed (FP32 cell-offset forces, FP64 reductions)", "graph_steps": 50,
+                   "form": "mixed (FP32 cell-offset forces, FP64 reductions)", "graph_steps": args.graph_steps,
                    "l2": "working set > L2 (no flush needed)", "parallelism": f"replicas x{world} (no collective)"},
     }
 
@@ -332,6 +338,10 @@ def main():
         line["clocks"] = clk.summary()
         launched = {k: counts1[k] - counts0[k] for k in counts0}
         line["gpu_launches"] = int(sum(launched.values()))
+        line["autotune"] = {"force_variant": variant,
+                            "ms_per_variant": [round(float(x), 4) for x in variant_ms[:5]],
+                            "variants": ["batch8/6 blocks", "batch4/8 blocks", "batch8/5 blocks pipelined",
+                                         "batch4/6 blocks pipelined", "batch8/8 blocks"]}
         line["launches_by_kernel"] = launched
         # ---- roofline of the force kernel
         entries = C.c_int64()

@@ -433,6 +433,13 @@ class Batch:
     LAUNCH_KINDS = ("pre", "bin", "scan", "scatter", "cellsort", "permute", "topo", "neighbors", "force",
                     "force_ev", "post")
 
+    def autotune(self, iters=20):
+        """Pick the fastest force-kernel variant on the current state."""
+        ms = np.zeros(8)
+        v = C.c_int32()
+        _call("fmd_batch_autotune", self._h, C.c_int32(iters), C.byref(v), _ptr(ms), C.c_int32(len(ms)))
+        return v.value, ms
+
     def launch_counts(self):
         """Kernel launches executed so far, per kernel (counted on the device)."""
         c = np.zeros(len(self.LAUNCH_KINDS), np.int64)

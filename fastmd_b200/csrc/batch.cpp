@@ -104,7 +104,9 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   FMD_CUDA(cudaSetDevice(device_));
   FMD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
   FMD_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-  graph_steps_ = o.graph_steps > 0 ? o.graph_steps : 50;
+  // graph_steps < 0: no graph (every step launched directly; for profilers
+  // that cannot see into graphs with conditional nodes)
+  graph_steps_ = o.graph_steps > 0 ? o.graph_steps : (o.graph_steps < 0 ? 0 : 50);
   max_reps_ = o.max_replicas > 0 ? o.max_replicas : 256;
   BatchCaps c;
   if (exact) {
@@ -312,6 +314,7 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   R.nh.inv_L = 1.0 / L;
   R.nh.V = L * L * L;
   R.pending_scale = 1.0;
+  R.defer = 0;
   R.force_ev = 0;
   R.ev_step = -1;
 }
@@ -514,13 +517,15 @@ void Batch::finish_pushoffs() {
     h_reps_[r].stop_step = info_[r].pending_pushoff;
   }
   upload_reps();
-  if (steps >= graph_steps_) {
+  int64_t direct = steps;
+  if (graph_steps_ > 0 && steps >= graph_steps_) {
     ensure_graph();
     for (int64_t k = 0; k < steps / graph_steps_; ++k) FMD_CUDA(cudaGraphLaunch(graph_exec_, st_));
+    direct = steps % graph_steps_;
   }
   const Dev d = dev();
   const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
-  for (int64_t k = 0; k < steps % graph_steps_; ++k) launch_step(d, nc, nr, mc, mh, st_);
+  for (int64_t k = 0; k < direct; ++k) launch_step(d, nc, nr, mc, mh, force_variant_, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
   download_reps();
@@ -575,7 +580,7 @@ void Batch::setup(const std::vector<int>& rs) {
   const Dev d = dev();
   launch_rebuild(d, nchunks_launch(), nreps_launch(), max_cells(), max_home_cells(), st_);
   FMD_CUDA_LAUNCH();
-  launch_forces_only(d, nchunks_launch(), st_);
+  launch_forces_only(d, nchunks_launch(), force_variant_, st_);
   FMD_CUDA_LAUNCH();
   launch_reduce_only(d, nchunks_launch(), st_, 0);
   FMD_CUDA_LAUNCH();
@@ -597,7 +602,7 @@ void Batch::check_status(int r, bool throw_on_fault) {
 void Batch::advance_direct(int64_t nsteps) {
   const Dev d = dev();
   const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
-  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, mc, mh, st_);
+  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, mc, mh, force_variant_, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
 }
@@ -613,7 +618,7 @@ void Batch::ensure_graph() {
   cudaGraph_t g;
   FMD_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   try {
-    for (int k = 0; k < graph_steps_; ++k) capture_step(d, nc, nr, mc, mh, st_, side_);
+    for (int k = 0; k < graph_steps_; ++k) capture_step(d, nc, nr, mc, mh, force_variant_, st_, side_);
   } catch (...) {
     cudaGraph_t partial = nullptr;
     cudaStreamEndCapture(st_, &partial);
@@ -645,7 +650,7 @@ void Batch::run(int64_t nsteps, bool respect_nsteps) {
   }
   if (need == 0) return;
   upload_reps();
-  if (need >= graph_steps_) {
+  if (graph_steps_ > 0 && need >= graph_steps_) {
     ensure_graph();
     const int64_t reps = need / graph_steps_;
     for (int64_t k = 0; k < reps; ++k) FMD_CUDA(cudaGraphLaunch(graph_exec_, st_));
@@ -654,7 +659,7 @@ void Batch::run(int64_t nsteps, bool respect_nsteps) {
   if (need > 0) {
     const Dev d = dev();
     const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
-    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, mc, mh, st_);
+    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, mc, mh, force_variant_, st_);
     FMD_CUDA_LAUNCH();
   }
   FMD_CUDA(cudaStreamSynchronize(st_));
@@ -707,19 +712,31 @@ double Batch::elapsed_ms() {
   return ms;
 }
 
-double Batch::time_force(int iters) {
+// Device time per launch of the force kernel on the current state (the
+// evaluation is idempotent); variant < 0: the batch's current variant.  Only
+// the kernel flavour the replicas need (with or without energies) is timed.
+double Batch::time_force(int iters, int variant) {
+  if (variant < 0) variant = force_variant_;
   download_reps();
   // mark every replica as advancing for the force kernel only
   std::vector<Rep> saved = h_reps_;
+  bool any_ev = false, any_plain = false;
   for (int r = 0; r < max_reps_; ++r)
-    if (info_[r].used && h_reps_[r].active) h_reps_[r].adv = 1;
+    if (info_[r].used && h_reps_[r].active) {
+      h_reps_[r].adv = 1;
+      (need_ev(h_reps_[r]) ? any_ev : any_plain) = true;
+    }
   upload_reps();
   const Dev d = dev();
   const int nc = nchunks_launch();
-  launch_forces_only(d, nc, st_);  // warm
+  auto once = [&] {
+    if (any_plain) launch_force(d, nc, false, variant, st_);
+    if (any_ev) launch_force(d, nc, true, variant, st_);
+  };
+  once();  // warm
   FMD_CUDA_LAUNCH();
   mark(0);
-  for (int k = 0; k < iters; ++k) launch_forces_only(d, nc, st_);
+  for (int k = 0; k < iters; ++k) once();
   FMD_CUDA_LAUNCH();
   mark(1);
   const double ms = elapsed_ms() / std::max(1, iters);
@@ -727,6 +744,24 @@ double Batch::time_force(int iters) {
   upload_reps();
   FMD_CUDA(cudaStreamSynchronize(st_));
   return ms;
+}
+
+// Time every force-kernel variant on the live state and keep the fastest
+// (the step graph is re-captured with it).
+int Batch::autotune(int iters, double* ms_out, int cap) {
+  int best = 0;
+  double best_ms = 0;
+  for (int v = 0; v < kForceVariants; ++v) {
+    const double ms = time_force(iters, v);
+    if (ms_out && v < cap) ms_out[v] = ms;
+    if (v == 0 || ms < best_ms) {
+      best = v;
+      best_ms = ms;
+    }
+  }
+  if (best != force_variant_) graph_dirty_ = true;
+  force_variant_ = best;
+  return best;
 }
 
 void Batch::list_stats(int64_t* entries, int32_t* max_per_atom) {
@@ -833,6 +868,7 @@ void Batch::set_state(int r, const double* xyz, const double* vel, const int32_t
   download_reps();
   Rep& R = h_reps_[r];
   R.pending_scale = 1.0;
+  R.defer = 0;
   R.Lpos = R.L;
   R.h = (float)(R.L / R.G);
   upload_atoms(r, x.data(), v.data(), im.data());
@@ -853,7 +889,7 @@ void Batch::ensure_ev(int r) {
   R.rebuild_now = 0;
   upload_reps();
   const Dev d = dev();
-  launch_forces_only(d, nchunks_launch(), st_);
+  launch_forces_only(d, nchunks_launch(), force_variant_, st_);
   FMD_CUDA_LAUNCH();
   launch_reduce_only(d, nchunks_launch(), st_, 2);
   FMD_CUDA_LAUNCH();

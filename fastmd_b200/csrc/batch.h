@@ -93,7 +93,9 @@ class Batch {
   void set_max_between(int r, int k);
   void mark(int which);
   double elapsed_ms();
-  double time_force(int iters);
+  double time_force(int iters, int variant = -1);
+  int autotune(int iters, double* ms_out, int cap);
+  int force_variant() const { return force_variant_; }
   void list_stats(int64_t* entries, int32_t* max_per_atom);
 
  private:
@@ -110,6 +112,7 @@ class Batch {
   cudaStream_t st_ = nullptr;
   cudaStream_t side_ = nullptr;  // captures conditional-node bodies
   int graph_steps_ = 50;
+  int force_variant_ = 0;
   int max_reps_ = 256;
   BatchCaps caps_;
   int64_t budget_bytes_ = 0, bytes_in_use_ = 0, bytes_ = 0;

@@ -182,6 +182,15 @@ FMD_API fmd_status fmd_batch_time_force(fmd_batch* b, int32_t iters, double* ms)
   });
 }
 
+FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chosen, double* ms_per_variant,
+                                      int32_t cap) {
+  return guarded([&] {
+    if (iters <= 0 || cap < 0) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    const int v = B(b).autotune(iters, ms_per_variant, cap);
+    if (chosen) *chosen = v;
+  });
+}
+
 FMD_API fmd_status fmd_batch_list_stats(fmd_batch* b, int64_t* entries, int32_t* max_per_atom) {
   return guarded([&] { B(b).list_stats(entries, max_per_atom); });
 }

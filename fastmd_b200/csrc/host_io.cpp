@@ -494,6 +494,12 @@ Topology generate_melt(const fmd_melt_spec& sp) {
 
 void validate(const RunConfig& cfg, Topology& t) {
   if (t.natoms <= 0) throw Error(FMD_ERR_CONFIG, "system has no atoms");
+  // The reference sizes every array from run.conf natoms (main.cu:62-99) and
+  // overruns them when the data file holds more atoms; here a given natoms
+  // must match the system, and an absent one is taken from it.
+  if (cfg.natoms > 0 && cfg.natoms != t.natoms)
+    throw Error(FMD_ERR_CONFIG, "run.conf natoms " + std::to_string(cfg.natoms) + " does not match the system's " +
+                                    std::to_string(t.natoms) + " atoms");
   if (t.box_L <= 0) throw Error(FMD_ERR_CONFIG, "box edge must be > 0");
   for (int ty : t.type)
     if (ty < 0 || ty >= cfg.ntypes) throw Error(FMD_ERR_CONFIG, "atom type outside run.conf ntypes");

@@ -42,6 +42,11 @@ constexpr int kMaxG = 512;        // cells per axis (9 bits)
 constexpr uint32_t kIdxMask = (1u << 25) - 1;
 constexpr int kCodeShift = 25;
 constexpr int kShiftCodes = 125;
+constexpr uint32_t kZeroShiftCode = 62;  // (0, 0, 0): 2 * 25 + 2 * 5 + 2
+// Lists are padded to a multiple of kListPad entries with the atom's own
+// slot and the zero shift (r = 0, excluded by the r^2 > 1e-10 guard), so the
+// force loop runs whole batches.
+constexpr int kListPad = 8;
 constexpr uint32_t kSlotMask26 = (1u << 26) - 1;  // bonded-table slot field
 constexpr int kNumPartials = 14;  // pe, vir[6], ke[6], sum m v^2
 constexpr int kMaxBondsPerAtom = 4;   // per-slot bonded tables rebuilt with the list
@@ -125,9 +130,18 @@ struct Rep {
   int32_t thermo_freq;           // run.conf thermo cadence (0: off); energies/virial computed on those steps
   int32_t force_ev;              // host request: compute energies/virial at the next force evaluation
   int64_t ev_step;               // step whose energies/virial are in pe/vir
+  int32_t defer;                 // this step's post-force kick is applied by the next pre-force
   StepScalars next;              // scalars of the next pre-force (valid when next_valid)
   int32_t next_valid;            // cleared by every host upload and by each pre-force
 };
+
+// Energies and virial are needed on thermo steps, for NPT (the barostat uses
+// the virial every step) and when the host asks for them.
+__host__ __device__ inline bool need_ev(const Rep& R) {
+  if (R.force_ev) return true;
+  if (R.mode != kModePushoff && R.ensemble == FMD_NPT_NH) return true;
+  return R.thermo_freq > 0 && (R.step % R.thermo_freq) == 0;
+}
 
 // Device pointers of the batch arrays.
 struct Dev {
@@ -219,15 +233,18 @@ __host__ __device__ inline int w_type(uint32_t u) { return (int)(u >> 27); }
 // of replicas that need no work return at once).
 struct StepConds {
   int use;
-  cudaGraphConditionalHandle rebuild, force_plain, force_ev;
+  cudaGraphConditionalHandle rebuild, force_plain, force_ev, post;
 };
-void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st);
+constexpr int kForceVariants = 5;
+void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
+                 cudaStream_t st);
 // The same step recorded into the graph being captured on st, with the
 // conditional nodes; side is a second stream used to capture their bodies.
-void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st,
-                  cudaStream_t side);
+void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
+                  cudaStream_t st, cudaStream_t side);
+void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st);
 void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells_per_rep, int max_home_cells, cudaStream_t st);
-void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st);
+void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st);
 void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode);  // 0 setup, 2 re-evaluation
 
 }  // namespace mixed

@@ -128,13 +128,6 @@ __device__ __forceinline__ void warp_max_u32(uint32_t& v) {
   for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
 }
 
-// Energies and virial are needed on thermo steps, for NPT (the barostat uses
-// the virial every step) and when the host asks for them.
-__device__ __forceinline__ bool need_ev(const Rep& R) {
-  if (R.force_ev) return true;
-  if (R.mode != kModePushoff && R.ensemble == FMD_NPT_NH) return true;
-  return R.thermo_freq > 0 && (R.step % R.thermo_freq) == 0;
-}
 
 __device__ __forceinline__ void count_launch(const Dev& d, int kind) {
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(d.kcount + kind, 1ull);
@@ -154,6 +147,7 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
   const int s = R.slot_base + local;
   const bool have = local < R.natoms;
+  const bool deferred = R.defer != 0;
   // The atom's data does not depend on the step scalars: load it first.
   float4 p = make_float4(0, 0, 0, 0), v = p, f = p, q = p;
   if (have) {
@@ -175,6 +169,13 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   int bad = 0;
   if (have) {
     const float hm = S.hdt * v.w;
+    if (deferred) {
+      // the previous step's post-force half kick (same step size, same
+      // operation as the post-force kernel would have done)
+      v.x = fmaf(hm, f.x, v.x);
+      v.y = fmaf(hm, f.y, v.y);
+      v.z = fmaf(hm, f.z, v.z);
+    }
     v.x *= S.vscale;
     v.y *= S.vscale;
     v.z *= S.vscale;
@@ -265,10 +266,24 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   } else {
     R.rebuild_now = 0;
   }
+  // Langevin steps inside a graph leave their post-force kick to the next
+  // pre-force (the post-force kernel then has nothing else to do); the post
+  // runs on energy steps, for the Nose-Hoover chains and on a replica's last
+  // step of the run, so every state the host can read is complete.
+  const bool langevin = R.mode == kModePushoff || R.ensemble == FMD_LANGEVIN;
+  const bool post = !cond.use || !langevin || need_ev(R) || R.step >= R.stop_step;
+  R.defer = post ? 0 : 1;
   if (cond.use) {
-    // any replica that rebuilds / needs a force variant switches it on
+    // any replica that rebuilds / needs a force variant / a post switches it on
     if (R.rebuild_now) cudaGraphSetConditional(cond.rebuild, 1u);
     cudaGraphSetConditional(need_ev(R) ? cond.force_ev : cond.force_plain, 1u);
+    if (post) cudaGraphSetConditional(cond.post, 1u);
+  }
+  if (!post) {
+    // a skipped post-force computes no scalars for the next step: do it here
+    // (a Langevin post changes none of their inputs)
+    compute_step_scalars(R, R.next);
+    R.next_valid = 1;
   }
 }
 
@@ -573,6 +588,8 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
       if (act) {
         d.ncnt[base + il] = min(count, M);
         if (count > M) overflow |= kStatusOverflow;
+        for (int k = count; k < ((count + kListPad - 1) & ~(kListPad - 1)) && k < M; ++k)
+          out[(size_t)k * 32] = (uint32_t)il | (kZeroShiftCode << kCodeShift);
       }
     }
   }
@@ -702,6 +719,11 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors(Dev d, int nreps) {
           count += __popc(m);
         }
         if (w0 + kNbrWin >= total) {
+          if (count <= M) {
+            const int padded = (count + kListPad - 1) & ~(kListPad - 1);
+            if (lane < padded - count)
+              out[(size_t)(count + lane) * 32] = (uint32_t)i | (kZeroShiftCode << kCodeShift);
+          }
           if (lane == 0) {
             d.ncnt[base + i] = min(count, M);
             if (count > M) overflow |= kStatusOverflow;
@@ -716,8 +738,6 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors(Dev d, int nreps) {
 }
 
 // ---------------------------------------------------------------- forces
-constexpr int kBatch = 8;  // neighbors whose loads are issued together
-constexpr int kForceBlocksPerSM = 6;
 
 struct KahanF {
   float s, c;
@@ -729,18 +749,29 @@ struct KahanF {
   }
 };
 
-// Displacement r_i - r_j for a bonded pair (cells may differ by any amount).
+// One axis of r_i - r_j for a bonded pair.  A bond is shorter than a cell
+// edge and cells are fixed between rebuilds, so the two cells differ by at
+// most one modulo the periodic wrap: for G >= 3 the shift follows from the
+// cell indices alone (integer arithmetic); smaller grids take the general
+// offset-based form.  Both give the same e, k and hence the same value.
+__device__ __forceinline__ float bonded_axis(int ci, int cj, float oi, float oj, int G, float h, float inv_h,
+                                             float dL) {
+  int e, k;
+  if (G >= 3) {
+    const int dc = ci - cj;
+    k = dc > 1 ? 1 : (dc < -1 ? -1 : 0);
+    e = k * G - dc;
+  } else {
+    pair_shift(ci, cj, oi, oj, G, inv_h, e, k);
+  }
+  return (oi - oj) - shift_term(e, k, h, dL);
+}
+
 __device__ __forceinline__ float3 bonded_dr(float4 pi, float4 pj, int G, float h, float inv_h, float dL) {
   const uint32_t ui = w_bits(pi.w), uj = w_bits(pj.w);
-  int e, k;
-  float3 r;
-  pair_shift(w_cx(ui), w_cx(uj), pi.x, pj.x, G, inv_h, e, k);
-  r.x = (pi.x - pj.x) - shift_term(e, k, h, dL);
-  pair_shift(w_cy(ui), w_cy(uj), pi.y, pj.y, G, inv_h, e, k);
-  r.y = (pi.y - pj.y) - shift_term(e, k, h, dL);
-  pair_shift(w_cz(ui), w_cz(uj), pi.z, pj.z, G, inv_h, e, k);
-  r.z = (pi.z - pj.z) - shift_term(e, k, h, dL);
-  return r;
+  return make_float3(bonded_axis(w_cx(ui), w_cx(uj), pi.x, pj.x, G, h, inv_h, dL),
+                     bonded_axis(w_cy(ui), w_cy(uj), pi.y, pj.y, G, h, inv_h, dL),
+                     bonded_axis(w_cz(ui), w_cz(uj), pi.z, pj.z, G, h, inv_h, dL));
 }
 
 template <int BS>
@@ -772,47 +803,64 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
   const float dy = (pi.y - pj.y) - sh.y;
   const float dz = (pi.z - pj.z) - sh.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
-  if (r2 < rc2 && r2 > 1e-10f) {
-    const float r2inv = __fdividef(1.0f, r2);
-    const float sr2 = sig2 * r2inv;
-    const float sr6 = sr2 * sr2 * sr2;
-    float fr = e24 * r2inv * sr6 * (2.0f * sr6 - 1.0f);
-    fr = fminf(fmaxf(fr, -1000.0f), 1000.0f);  // lj.cu:48
-    const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
-    a.fx += fxij;
-    a.fy += fyij;
-    a.fz += fzij;
-    if (EV) {
-      a.pe = fmaf(e24 * (1.0f / 12.0f), sr6 * (sr6 - 1.0f), a.pe);  // 1/2 * 4 eps (sr12 - sr6)
-      a.v0 = fmaf(fxij, dx, a.v0);
-      a.v1 = fmaf(fxij, dy, a.v1);
-      a.v2 = fmaf(fxij, dz, a.v2);
-      a.v3 = fmaf(fyij, dy, a.v3);
-      a.v4 = fmaf(fyij, dz, a.v4);
-      a.v5 = fmaf(fzij, dz, a.v5);
-    }
+  // Branch-free: every listed pair is evaluated and pairs outside the cutoff
+  // (or the r = 0 padding entries) contribute an exact zero through selects.
+  const bool in = r2 < rc2 && r2 > 1e-10f;
+  const float r2inv = __fdividef(1.0f, r2);
+  const float sr2 = sig2 * r2inv;
+  const float sr6 = sr2 * sr2 * sr2;
+  float fr = e24 * r2inv * sr6 * (2.0f * sr6 - 1.0f);
+  fr = in ? fminf(fmaxf(fr, -1000.0f), 1000.0f) : 0.0f;  // lj.cu:48
+  const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
+  a.fx += fxij;
+  a.fy += fyij;
+  a.fz += fzij;
+  if (EV) {
+    const float e = in ? e24 * (1.0f / 12.0f) * (sr6 * (sr6 - 1.0f)) : 0.0f;  // 1/2 * 4 eps (sr12 - sr6)
+    a.pe += e;
+    a.v0 = fmaf(fxij, dx, a.v0);
+    a.v1 = fmaf(fxij, dy, a.v1);
+    a.v2 = fmaf(fxij, dz, a.v2);
+    a.v3 = fmaf(fyij, dy, a.v3);
+    a.v4 = fmaf(fyij, dz, a.v4);
+    a.v5 = fmaf(fzij, dz, a.v5);
   }
 }
 
-// The LJ loop over one atom's list: batches of kBatch entries (all list
-// loads, then all position gathers, then the arithmetic).
-template <bool EV>
+// The LJ loop over one atom's list in batches of B entries: all list loads,
+// then all position gathers, then the arithmetic.  PF: the next batch's list
+// words are loaded before this batch's gathers (software pipelining, B more
+// registers).  nn is the padded length (a multiple of B).
+template <bool EV, int B, bool PF>
 __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
                                         const float4* s_shift, bool one_type, int ti, int nt, const float* s_eps24,
                                         const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
                                         PairAcc& acc) {
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
-  int k = 0;
-  for (; k + kBatch <= nn; k += kBatch) {
-    uint32_t w[kBatch];
+  uint32_t wn[B];
+  if (PF) {
 #pragma unroll
-    for (int q = 0; q < kBatch; ++q) w[q] = __ldg(lst + (size_t)(k + q) * 32);
-    float4 pj[kBatch];
+    for (int q = 0; q < B; ++q) wn[q] = nn > 0 ? __ldg(lst + (size_t)q * 32) : 0u;
+  }
+  for (int k = 0; k < nn; k += B) {
+    uint32_t w[B];
+    if (PF) {
 #pragma unroll
-    for (int q = 0; q < kBatch; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+      for (int q = 0; q < B; ++q) w[q] = wn[q];
+      if (k + B < nn) {
+#pragma unroll
+        for (int q = 0; q < B; ++q) wn[q] = __ldg(lst + (size_t)(k + B + q) * 32);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < B; ++q) w[q] = __ldg(lst + (size_t)(k + q) * 32);
+    }
+    float4 pj[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
     PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
 #pragma unroll
-    for (int q = 0; q < kBatch; ++q) {
+    for (int q = 0; q < B; ++q) {
       float e24 = e24_0, sig2 = sig2_0;
       if (!one_type) {
         const int pidx = ti * nt + w_type(w_bits(pj[q].w));
@@ -826,25 +874,13 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
     fz.add(g.fz);
     acc = g;
   }
-  PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
-  for (; k < nn; ++k) {
-    const uint32_t w = __ldg(lst + (size_t)k * 32);
-    const float4 pj = __ldg(pbase + (w & kIdxMask));
-    float e24 = e24_0, sig2 = sig2_0;
-    if (!one_type) {
-      const int pidx = ti * nt + w_type(w_bits(pj.w));
-      e24 = s_eps24[pidx];
-      sig2 = s_sig2[pidx];
-    }
-    lj_pair<EV>(g, pi, s_shift[w >> kCodeShift], pj, rc2, e24, sig2);
-  }
-  fx.add(g.fx);
-  fy.add(g.fy);
-  fz.add(g.fz);
-  acc = g;
 }
 
-// Harmonic angle (angle.cu:17-80): force on member `role` of (i, j, k).
+// Harmonic angle (angle.cu:17-80) on (ri, rj = vertex, rk): force on the
+// member `role` (0: i, 1: j, 2: k), selected without branching so that lanes
+// in different roles follow one path.  EV: a third of the energy per member,
+// the angle's virial carried by the vertex.
+template <bool EV>
 __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int role, float kt, float th0, int G,
                                            float h, float inv_h, float dL, KahanF& fx, KahanF& fy, KahanF& fz,
                                            float& pe, float* bv) {
@@ -857,7 +893,7 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
   cs = fminf(fmaxf(cs, -1.0f), 1.0f);
   const float dth = acosf(cs) - th0;
   const float sn = fmaxf(sqrtf(1.0f - cs * cs), 1e-6f);
-  const float pref = 2.0f * kt * dth / sn;
+  const float pref = 2.0f * kt * dth * __fdividef(1.0f, sn);
   const float rr = rij_inv * rkj_inv, i2 = rij_inv * rij_inv, k2 = rkj_inv * rkj_inv;
   const float fix = pref * (dkj.x * rr - cs * dij.x * i2);
   const float fiy = pref * (dkj.y * rr - cs * dij.y * i2);
@@ -865,34 +901,27 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
   const float fkx = pref * (dij.x * rr - cs * dkj.x * k2);
   const float fky = pref * (dij.y * rr - cs * dkj.y * k2);
   const float fkz = pref * (dij.z * rr - cs * dkj.z * k2);
-  if (role == 0) {
-    fx.add(fix);
-    fy.add(fiy);
-    fz.add(fiz);
-  } else if (role == 2) {
-    fx.add(fkx);
-    fy.add(fky);
-    fz.add(fkz);
-  } else {
-    fx.add(-(fix + fkx));
-    fy.add(-(fiy + fky));
-    fz.add(-(fiz + fkz));
-    // the vertex atom carries the angle's virial (counted once per angle)
-    bv[0] += fix * dij.x + fkx * dkj.x;
-    bv[1] += fix * dij.y + fkx * dkj.y;
-    bv[2] += fix * dij.z + fkx * dkj.z;
-    bv[3] += fiy * dij.y + fky * dkj.y;
-    bv[4] += fiy * dij.z + fky * dkj.z;
-    bv[5] += fiz * dij.z + fkz * dkj.z;
+  fx.add(role == 0 ? fix : (role == 2 ? fkx : -(fix + fkx)));
+  fy.add(role == 0 ? fiy : (role == 2 ? fky : -(fiy + fky)));
+  fz.add(role == 0 ? fiz : (role == 2 ? fkz : -(fiz + fkz)));
+  if (EV) {
+    if (role == 1) {
+      bv[0] += fix * dij.x + fkx * dkj.x;
+      bv[1] += fix * dij.y + fkx * dkj.y;
+      bv[2] += fix * dij.z + fkx * dkj.z;
+      bv[3] += fiy * dij.y + fky * dkj.y;
+      bv[4] += fiy * dij.z + fky * dkj.z;
+      bv[5] += fiz * dij.z + fkz * dkj.z;
+    }
+    pe += kt * dth * dth * (1.0f / 3.0f);
   }
-  pe += kt * dth * dth * (1.0f / 3.0f);
 }
 
 // Two instantiations: with energies / virial (thermo steps, NPT, host
 // requests) and without (all other steps); a block runs in the one that
 // matches its replica's need this step and the other returns at once.
-template <bool EV>
-__global__ void __launch_bounds__(kChunk, EV ? kForceBlocksPerSM - 1 : kForceBlocksPerSM) k_force(Dev d) {
+template <bool EV, int B, int MINB, bool PF>
+__global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
   count_launch(d, EV ? kKForceEv : kKForce);
   const int chunk = blockIdx.x;
   const int r = d.chunk_rep[chunk];
@@ -931,11 +960,12 @@ __global__ void __launch_bounds__(kChunk, EV ? kForceBlocksPerSM - 1 : kForceBlo
     const int ti = w_type(ui);
     KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
     PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const int nn = d.ncnt[s];
+    static_assert(kListPad % B == 0, "list padding must cover whole batches");
+    const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
     const bool one_type = (nt == 1);
-    lj_loop<EV>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    lj_loop<EV, B, PF>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
@@ -967,10 +997,10 @@ __global__ void __launch_bounds__(kChunk, EV ? kForceBlocksPerSM - 1 : kForceBlo
       const float kf = R.fene[4 * bt], R02 = R.fene[4 * bt + 1], eps = R.fene[4 * bt + 2], sig2 = R.fene[4 * bt + 3];
       if (r2 >= R02 * 0.9999f) status |= kStatusFeneStretch;
       const float r2s = fminf(fmaxf(r2, 1e-6f), R02 * 0.9999f);
-      float ff = -kf * R02 / (R02 - r2s);
+      float ff = -kf * R02 * __fdividef(1.0f, R02 - r2s);
       float wpe = 0.0f;
       if (r2s < sig2 * 1.2599210498948732f) {
-        const float r2inv = 1.0f / r2s;
+        const float r2inv = __fdividef(1.0f, r2s);
         const float sr2 = sig2 * r2inv;
         const float sr6 = sr2 * sr2 * sr2;
         ff += 24.0f * eps * r2inv * sr6 * (2.0f * sr6 - 1.0f);
@@ -979,14 +1009,16 @@ __global__ void __launch_bounds__(kChunk, EV ? kForceBlocksPerSM - 1 : kForceBlo
       fx.add(ff * dr.x);
       fy.add(ff * dr.y);
       fz.add(ff * dr.z);
-      pe += 0.5f * (-0.5f * kf * R02 * log1pf(-r2s / R02) + wpe);
-      if ((bw >> 30) & 1) {
-        bv[0] = fmaf(ff * dr.x, dr.x, bv[0]);
-        bv[1] = fmaf(ff * dr.x, dr.y, bv[1]);
-        bv[2] = fmaf(ff * dr.x, dr.z, bv[2]);
-        bv[3] = fmaf(ff * dr.y, dr.y, bv[3]);
-        bv[4] = fmaf(ff * dr.y, dr.z, bv[4]);
-        bv[5] = fmaf(ff * dr.z, dr.z, bv[5]);
+      if (EV) {
+        pe += 0.5f * (-0.5f * kf * R02 * log1pf(-r2s / R02) + wpe);
+        if ((bw >> 30) & 1) {
+          bv[0] = fmaf(ff * dr.x, dr.x, bv[0]);
+          bv[1] = fmaf(ff * dr.x, dr.y, bv[1]);
+          bv[2] = fmaf(ff * dr.x, dr.z, bv[2]);
+          bv[3] = fmaf(ff * dr.y, dr.y, bv[3]);
+          bv[4] = fmaf(ff * dr.y, dr.z, bv[4]);
+          bv[5] = fmaf(ff * dr.z, dr.z, bv[5]);
+        }
       }
     }
     // Harmonic angles this atom belongs to, by role.
@@ -997,12 +1029,11 @@ __global__ void __launch_bounds__(kChunk, EV ? kForceBlocksPerSM - 1 : kForceBlo
       const float4 p1 = pbase[aw.x & kSlotMask26];
       const float4 p2 = pbase[aw.y & kSlotMask26];
       const float kt = R.angp[2 * at], th0 = R.angp[2 * at + 1];
-      if (role == 0)
-        angle_term(pi, p1, p2, 0, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
-      else if (role == 1)
-        angle_term(p1, pi, p2, 1, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
-      else
-        angle_term(p1, p2, pi, 2, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
+      // members in angle order (i, j = vertex, k); the table holds the other two
+      const float4 ri = role == 0 ? pi : p1;
+      const float4 rj = role == 1 ? pi : (role == 0 ? p1 : p2);
+      const float4 rk = role == 2 ? pi : p2;
+      angle_term<EV>(ri, rj, rk, role, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
     }
     const float ox = fx.s - fx.c, oy = fy.s - fy.c, oz = fz.s - fz.c;
     if (!isfinite(ox + oy + oz + pe)) status |= kStatusNonFinite;
@@ -1024,7 +1055,7 @@ __global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
   const int r = d.chunk_rep[chunk];
   if (r < 0) return;
   Rep& R = d.reps[r];
-  if (!R.adv) return;
+  if (!R.adv || (kick == 1 && R.defer)) return;
   __shared__ int last;
   const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
   const int s = R.slot_base + local;
@@ -1119,11 +1150,12 @@ __global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
 
 // ---------------------------------------------------------------- launchers
 
-void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st) {
-  k_pre<<<nchunks, kChunk, 0, st>>>(d, StepConds{0, 0, 0, 0});
+void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
+                 cudaStream_t st) {
+  k_pre<<<nchunks, kChunk, 0, st>>>(d, StepConds{0, 0, 0, 0, 0});
   launch_rebuild(d, nchunks, nreps, max_cells, max_home, st);
-  k_force<false><<<nchunks, kChunk, 0, st>>>(d);
-  k_force<true><<<nchunks, kChunk, 0, st>>>(d);
+  launch_force(d, nchunks, false, force_variant, st);
+  launch_force(d, nchunks, true, force_variant, st);
   k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
 }
 
@@ -1154,20 +1186,21 @@ void capture_if(cudaStream_t st, cudaStream_t side, cudaGraphConditionalHandle h
 }
 }  // namespace
 
-void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st,
-                  cudaStream_t side) {
+void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
+                  cudaStream_t st, cudaStream_t side) {
   cudaStreamCaptureStatus cs;
   cudaGraph_t g;
   FMD_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
-  StepConds c{1, 0, 0, 0};
+  StepConds c{1, 0, 0, 0, 0};
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_plain, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
+  FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
   k_pre<<<nchunks, kChunk, 0, st>>>(d, c);
   capture_if(st, side, c.rebuild, [&](cudaStream_t s) { launch_rebuild(d, nchunks, nreps, max_cells, max_home, s); });
-  capture_if(st, side, c.force_plain, [&](cudaStream_t s) { k_force<false><<<nchunks, kChunk, 0, s>>>(d); });
-  capture_if(st, side, c.force_ev, [&](cudaStream_t s) { k_force<true><<<nchunks, kChunk, 0, s>>>(d); });
-  k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
+  capture_if(st, side, c.force_plain, [&](cudaStream_t s) { launch_force(d, nchunks, false, force_variant, s); });
+  capture_if(st, side, c.force_ev, [&](cudaStream_t s) { launch_force(d, nchunks, true, force_variant, s); });
+  capture_if(st, side, c.post, [&](cudaStream_t s) { k_post<<<nchunks, kChunk, 0, s>>>(d, 1); });
 }
 
 void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st) {
@@ -1184,9 +1217,25 @@ void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, int max
   k_neighbors<<<gn, kNbrThreads, 0, st>>>(d, nreps);
 }
 
-void launch_forces_only(const Dev& d, int nchunks, cudaStream_t st) {
-  k_force<false><<<nchunks, kChunk, 0, st>>>(d);
-  k_force<true><<<nchunks, kChunk, 0, st>>>(d);
+// Force-kernel variants (list batch, blocks per SM, pipelined list loads);
+// the batch's autotuner picks one.  The energy variant is fixed.
+void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st) {
+  if (ev) {
+    k_force<true, 8, 5, false><<<nchunks, kChunk, 0, st>>>(d);
+    return;
+  }
+  switch (variant) {
+    case 1: k_force<false, 4, 8, false><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 2: k_force<false, 8, 5, true><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 3: k_force<false, 4, 6, true><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 4: k_force<false, 8, 8, false><<<nchunks, kChunk, 0, st>>>(d); break;
+    default: k_force<false, 8, 6, false><<<nchunks, kChunk, 0, st>>>(d); break;
+  }
+}
+
+void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st) {
+  launch_force(d, nchunks, false, variant, st);
+  launch_force(d, nchunks, true, variant, st);
 }
 void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode) {
   k_post<<<nchunks, kChunk, 0, st>>>(d, mode);

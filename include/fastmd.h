@@ -191,7 +191,7 @@ typedef struct fmd_batch_opts {
   int32_t max_replicas;    /* slot count */
   int64_t max_atoms;       /* total atom capacity (padded); 0 -> sized from budget */
   double hbm_budget_gb;    /* device-memory budget for the batch (0 -> 150) */
-  int32_t graph_steps;     /* steps captured per CUDA graph launch (0 -> 50) */
+  int32_t graph_steps;     /* steps captured per CUDA graph launch (0 -> 50; < 0: no graph) */
 } fmd_batch_opts;
 
 typedef struct fmd_replica_info {
@@ -248,6 +248,12 @@ FMD_API fmd_status fmd_batch_time_force(fmd_batch* b, int32_t iters, double* ms_
 FMD_API fmd_status fmd_batch_list_stats(fmd_batch* b, int64_t* entries, int32_t* max_per_atom);
 FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n);
 FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_t n);
+/* Autotuner: time each force-kernel variant (neighbor batch 4 or 8, blocks
+ * per SM, pipelined list loads) `iters` times on the current state, keep the
+ * fastest for all following steps.  chosen = its index; ms_per_variant (cap
+ * entries, may be NULL) = device ms per launch of each variant. */
+FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chosen, double* ms_per_variant,
+                                      int32_t cap);
 /* Set the forced rebuild cadence of a replica (the reference rebuilds at
  * least every 20 steps, main.cu:401); the skin/2 displacement test still
  * triggers rebuilds in between. */

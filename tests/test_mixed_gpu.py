@@ -134,3 +134,25 @@ def test_pushoff_then_langevin_is_stable():
     assert 0.8 < t.temp < 1.2
     assert np.isfinite(t.pe)
     assert sim.counters()["status_word"] == 0
+
+
+@pytest.mark.parametrize("ens", ["nvt_langevin 1.0 1.0 1.0 7", "nvt_nh 1.0 1.0 0.5 3",
+                                 "npt_nh 1.0 1.0 0.5 0.5 0.5 1.0 3"])
+def test_graph_steps_equal_direct_steps(ens):
+    """A CUDA-graph run (conditional rebuild / force / post nodes, Langevin
+    post-force kicks folded into the next pre-force) gives bit-identical
+    states to launching every kernel of every step directly."""
+    conf = run_conf(ensemble=ens, nsteps=10_000)
+    melts = [_melt(10, 30, seed=21), _melt(12, 50, seed=22)]
+    out = []
+    for gs in (-1, 10):
+        b = fm.Batch(max_replicas=4, max_atoms=1 << 14, graph_steps=gs)
+        slots = [b.add(conf, desc=m) for m in melts]
+        b.run(37)
+        b.run(25)
+        out.append([(b.state(s), b.thermo(s).as_array()) for s in slots])
+        b.close()
+    for (sa, ta), (sb, tb) in zip(out[0], out[1]):
+        for a, c in zip(sa, sb):
+            assert np.array_equal(a, c)
+        assert np.array_equal(ta, tb)
