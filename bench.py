@@ -131,7 +131,7 @@ def dist_setup(n_gpus):
         backend = "nccl" if torch.cuda.is_available() else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         return rank, world, local, dist
     return 0, 1, 0, None
 
@@ -338,10 +338,15 @@ def main():
         line["clocks"] = clk.summary()
         launched = {k: counts1[k] - counts0[k] for k in counts0}
         line["gpu_launches"] = int(sum(launched.values()))
-        line["autotune"] = {"force_variant": variant,
-                            "ms_per_variant": [round(float(x), 4) for x in variant_ms[:5]],
-                            "variants": ["batch8/6 blocks", "batch4/8 blocks", "batch8/5 blocks pipelined",
-                                         "batch4/6 blocks pipelined", "batch8/8 blocks"]}
+        line["autotune"] = {"force_variant": variant, "neighbor_variant": int(variant_ms[9]),
+                            "ms_per_full_rebuild": {"ballot": round(float(variant_ms[7]), 4),
+                                                    "rows": round(float(variant_ms[8]), 4)},
+                            "ms_per_variant": [round(float(x), 4) for x in variant_ms[:7]],
+                            "variants": ["b4 m6 pipelined k1", "b4 m8 pipelined k1", "b4 m6 pipelined k2",
+                                         "b4 m8 pipelined k2", "b2 m8 pipelined k4", "b4 m7 pipelined k2",
+                                         "b8 m6 k1"],
+                            "legend": "b = list entries per batch, m = min blocks per SM, pipelined = next batch's "
+                                      "list words loaded ahead, k = batches per compensated add"}
         line["launches_by_kernel"] = launched
         # ---- roofline of the force kernel
         entries = C.c_int64()

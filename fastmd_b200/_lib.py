@@ -431,11 +431,11 @@ class Batch:
         _call("fmd_batch_write_restart", self._h, C.c_int32(slot), str(path).encode())
 
     LAUNCH_KINDS = ("pre", "bin", "scan", "scatter", "cellsort", "permute", "topo", "neighbors", "force",
-                    "force_ev", "post")
+                    "force_ev", "post", "plan", "commit")
 
     def autotune(self, iters=20):
         """Pick the fastest force-kernel variant on the current state."""
-        ms = np.zeros(8)
+        ms = np.zeros(16)
         v = C.c_int32()
         _call("fmd_batch_autotune", self._h, C.c_int32(iters), C.byref(v), _ptr(ms), C.c_int32(len(ms)))
         return v.value, ms

@@ -152,6 +152,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   ang_.alloc(S * kMaxAnglesPerAtom);
   part_.alloc_zero(S / kChunk * kNumPartials);
   kcount_.alloc_zero(kKernelKinds);
+  rb_.alloc_zero(2 + (size_t)max_reps_ + 3 * ((size_t)max_reps_ + 1));
   cell_cnt_.alloc_zero(c.cells);
   cell_start_.alloc_zero(c.cells);
   cell_fill_.alloc_zero(c.cells);
@@ -160,8 +161,8 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   nbr_.alloc(c.nbr);
   reps_.alloc_zero(max_reps_);
   chunk_rep_.alloc(S / kChunk);
-  h_chunk_rep_.assign(S / kChunk, -1);
-  FMD_CUDA(cudaMemcpy(chunk_rep_, h_chunk_rep_.data(), h_chunk_rep_.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  h_chunk_rep_.assign(S / kChunk, make_int4(-1, 0, 0, 0));
+  FMD_CUDA(cudaMemcpy(chunk_rep_, h_chunk_rep_.data(), h_chunk_rep_.size() * sizeof(int4), cudaMemcpyHostToDevice));
   h_reps_.assign(max_reps_, Rep{});
   info_.resize(max_reps_);
   bytes_ = (int64_t)S * bytes_per_slot() + c.nbr * 4 + c.cells * 12 + c.bonds * 8 + c.angles * 16;
@@ -205,6 +206,8 @@ Dev Batch::dev() const {
   d.ang = ang_;
   d.part = part_;
   d.kcount = kcount_;
+  d.rb = rb_;
+  d.rb_cap = max_reps_;
   return d;
 }
 
@@ -214,9 +217,12 @@ void Batch::download_reps() {
 }
 
 void Batch::upload_reps() {
-  // a host change may touch any input of the precomputed step scalars
+  // a host change may touch any input of the precomputed step scalars:
+  // recompute them once per replica on the device
   for (int r = 0; r < max_reps_; ++r) h_reps_[r].next_valid = 0;
   FMD_CUDA(cudaMemcpyAsync(reps_, h_reps_.data(), sizeof(Rep) * max_reps_, cudaMemcpyHostToDevice, st_));
+  launch_prepare(dev(), nreps_launch(), st_);
+  FMD_CUDA_LAUNCH();
 }
 
 int Batch::nchunks_launch() const { return (int)std::max<int64_t>(1, slot_alloc_.hwm()); }
@@ -226,22 +232,6 @@ int Batch::nreps_launch() const {
     if (info_[r].used) m = r + 1;
   return std::max(1, m);
 }
-int Batch::max_cells() const {
-  int64_t m = 1;
-  for (int r = 0; r < max_reps_; ++r)
-    if (info_[r].used) m = std::max<int64_t>(m, info_[r].plan.ncell);
-  return (int)m;
-}
-int Batch::max_home_cells() const {
-  int64_t m = 1;
-  for (int r = 0; r < max_reps_; ++r)
-    if (info_[r].used) {
-      const int64_t g = info_[r].plan.G_alloc;
-      m = std::max<int64_t>(m, g * g * g);
-    }
-  return (int)m;
-}
-
 static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
   R.ntypes = cfg.ntypes;
   R.ensemble = cfg.ensemble;
@@ -305,7 +295,6 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   R.maxdisp_bits = 0;
   R.status = 0;
   R.rebuilds = 0;
-  R.cnt_pre = R.cnt_post = 0;
   std::memset(&R.nh, 0, sizeof(R.nh));
   R.nh.scale = 1.0;
   R.nh.bscale = 1.0;
@@ -480,8 +469,9 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
     if (t.nangles())
       FMD_CUDA(cudaMemcpyAsync(aent_.p + R.angle_base, ae.data(), 3 * t.nangles() * sizeof(int4), cudaMemcpyHostToDevice, st_));
   }
-  for (int c = 0; c < p.nchunks; ++c) h_chunk_rep_[ch + c] = r;
-  FMD_CUDA(cudaMemcpyAsync(chunk_rep_.p + ch, h_chunk_rep_.data() + ch, p.nchunks * sizeof(int32_t), cudaMemcpyHostToDevice, st_));
+  for (int c = 0; c < p.nchunks; ++c)
+    h_chunk_rep_[ch + c] = make_int4(r, (int)(ch * kChunk) + c * kChunk, std::max(0, std::min(kChunk, t.natoms - c * kChunk)), c);
+  FMD_CUDA(cudaMemcpyAsync(chunk_rep_.p + ch, h_chunk_rep_.data() + ch, p.nchunks * sizeof(int4), cudaMemcpyHostToDevice, st_));
   FMD_CUDA(cudaMemsetAsync(cell_cnt_.p + ce, 0, p.ncell * sizeof(int32_t), st_));
   // Other replicas must not advance while this one is being set up.
   download_reps_keep(r);
@@ -524,8 +514,8 @@ void Batch::finish_pushoffs() {
     direct = steps % graph_steps_;
   }
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
-  for (int64_t k = 0; k < direct; ++k) launch_step(d, nc, nr, mc, mh, force_variant_, st_);
+  const int nc = nchunks_launch(), nr = nreps_launch();
+  for (int64_t k = 0; k < direct; ++k) launch_step(d, nc, nr, force_variant_, nbr_variant_, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
   download_reps();
@@ -577,12 +567,18 @@ void Batch::setup(const std::vector<int>& rs) {
     R.force_ev = 1;
   }
   upload_reps();
+  // the rebuild work list holds exactly these replicas
+  std::vector<int> wl(2 + rs.size());
+  wl[0] = (int)rs.size();
+  wl[1] = 0;
+  std::copy(rs.begin(), rs.end(), wl.begin() + 2);
+  FMD_CUDA(cudaMemcpyAsync(rb_.p, wl.data(), wl.size() * sizeof(int), cudaMemcpyHostToDevice, st_));
   const Dev d = dev();
-  launch_rebuild(d, nchunks_launch(), nreps_launch(), max_cells(), max_home_cells(), st_);
+  launch_rebuild(d, nreps_launch(), nbr_variant_, st_);
   FMD_CUDA_LAUNCH();
   launch_forces_only(d, nchunks_launch(), force_variant_, st_);
   FMD_CUDA_LAUNCH();
-  launch_reduce_only(d, nchunks_launch(), st_, 0);
+  launch_reduce_only(d, nchunks_launch(), nreps_launch(), st_, 0);
   FMD_CUDA_LAUNCH();
   download_reps();
   for (int r : rs) check_status(r, true);
@@ -601,8 +597,8 @@ void Batch::check_status(int r, bool throw_on_fault) {
 
 void Batch::advance_direct(int64_t nsteps) {
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
-  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, mc, mh, force_variant_, st_);
+  const int nc = nchunks_launch(), nr = nreps_launch();
+  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, force_variant_, nbr_variant_, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
 }
@@ -614,11 +610,11 @@ void Batch::ensure_graph() {
     graph_exec_ = nullptr;
   }
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
+  const int nc = nchunks_launch(), nr = nreps_launch();
   cudaGraph_t g;
   FMD_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   try {
-    for (int k = 0; k < graph_steps_; ++k) capture_step(d, nc, nr, mc, mh, force_variant_, st_, side_);
+    for (int k = 0; k < graph_steps_; ++k) capture_step(d, nc, nr, force_variant_, nbr_variant_, st_, side_);
   } catch (...) {
     cudaGraph_t partial = nullptr;
     cudaStreamEndCapture(st_, &partial);
@@ -658,8 +654,8 @@ void Batch::run(int64_t nsteps, bool respect_nsteps) {
   }
   if (need > 0) {
     const Dev d = dev();
-    const int nc = nchunks_launch(), nr = nreps_launch(), mc = max_cells(), mh = max_home_cells();
-    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, mc, mh, force_variant_, st_);
+    const int nc = nchunks_launch(), nr = nreps_launch();
+    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, force_variant_, nbr_variant_, st_);
     FMD_CUDA_LAUNCH();
   }
   FMD_CUDA(cudaStreamSynchronize(st_));
@@ -682,8 +678,8 @@ void Batch::retire(int r) {
   download_reps();
   ReplicaInfo& I = info_[r];
   Rep& R = h_reps_[r];
-  for (int c = 0; c < R.nchunks; ++c) h_chunk_rep_[R.chunk_base + c] = -1;
-  FMD_CUDA(cudaMemcpyAsync(chunk_rep_.p + R.chunk_base, h_chunk_rep_.data() + R.chunk_base, R.nchunks * sizeof(int32_t),
+  for (int c = 0; c < R.nchunks; ++c) h_chunk_rep_[R.chunk_base + c] = make_int4(-1, 0, 0, 0);
+  FMD_CUDA(cudaMemcpyAsync(chunk_rep_.p + R.chunk_base, h_chunk_rep_.data() + R.chunk_base, R.nchunks * sizeof(int4),
                            cudaMemcpyHostToDevice, st_));
   slot_alloc_.release(I.seg_chunk);
   cell_alloc_.release(I.seg_cell);
@@ -746,9 +742,51 @@ double Batch::time_force(int iters, int variant) {
   return ms;
 }
 
-// Time every force-kernel variant on the live state and keep the fastest
-// (the step graph is re-captured with it).
+// Device time of a rebuild of every active replica with neighbor-list
+// variant v.  A rebuild of an unchanged state reproduces it (same cells, same
+// in-cell order, identity permutation); it resets the displacement reference.
+double Batch::time_rebuild(int iters, int v) {
+  download_reps();
+  std::vector<int> rs;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used && h_reps_[r].active) rs.push_back(r);
+  if (rs.empty()) return 0.0;
+  std::vector<int> wl(2 + rs.size());
+  wl[0] = (int)rs.size();
+  wl[1] = 0;
+  std::copy(rs.begin(), rs.end(), wl.begin() + 2);
+  const Dev d = dev();
+  auto once = [&] {
+    FMD_CUDA(cudaMemcpyAsync(rb_.p, wl.data(), wl.size() * sizeof(int), cudaMemcpyHostToDevice, st_));
+    launch_rebuild(d, nreps_launch(), v, st_);
+  };
+  once();
+  FMD_CUDA_LAUNCH();
+  mark(0);
+  for (int k = 0; k < iters; ++k) once();
+  FMD_CUDA_LAUNCH();
+  mark(1);
+  const double ms = elapsed_ms() / std::max(1, iters);
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  return ms;
+}
+
+// Time every force-kernel variant on the live state and keep the fastest,
+// then every neighbor-list variant on a full rebuild (the step graph is
+// re-captured with the choices).
 int Batch::autotune(int iters, double* ms_out, int cap) {
+  int nb = 0;
+  double nb_ms = 0;
+  for (int v = 0; v < kNbrVariants; ++v) {
+    const double ms = time_rebuild(std::max(1, iters / 5), v);
+    nbr_ms_[v] = ms;
+    if (v == 0 || ms < nb_ms) {
+      nb = v;
+      nb_ms = ms;
+    }
+  }
+  if (nb != nbr_variant_) graph_dirty_ = true;
+  nbr_variant_ = nb;
   int best = 0;
   double best_ms = 0;
   for (int v = 0; v < kForceVariants; ++v) {
@@ -891,7 +929,7 @@ void Batch::ensure_ev(int r) {
   const Dev d = dev();
   launch_forces_only(d, nchunks_launch(), force_variant_, st_);
   FMD_CUDA_LAUNCH();
-  launch_reduce_only(d, nchunks_launch(), st_, 2);
+  launch_reduce_only(d, nchunks_launch(), nreps_launch(), st_, 2);
   FMD_CUDA_LAUNCH();
   download_reps();
 }

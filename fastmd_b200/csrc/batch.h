@@ -87,14 +87,15 @@ class Batch {
   Dev dev() const;
   int nchunks_launch() const;
   int nreps_launch() const;
-  int max_cells() const;
-  int max_home_cells() const;
   int graph_steps() const { return graph_steps_; }
   void set_max_between(int r, int k);
   void mark(int which);
   double elapsed_ms();
   double time_force(int iters, int variant = -1);
   int autotune(int iters, double* ms_out, int cap);
+  double time_rebuild(int iters, int variant);
+  int nbr_variant() const { return nbr_variant_; }
+  const double* nbr_variant_ms() const { return nbr_ms_; }
   int force_variant() const { return force_variant_; }
   void list_stats(int64_t* entries, int32_t* max_per_atom);
 
@@ -113,6 +114,8 @@ class Batch {
   cudaStream_t side_ = nullptr;  // captures conditional-node bodies
   int graph_steps_ = 50;
   int force_variant_ = 0;
+  int nbr_variant_ = 0;
+  double nbr_ms_[kNbrVariants] = {0, 0};
   int max_reps_ = 256;
   BatchCaps caps_;
   int64_t budget_bytes_ = 0, bytes_in_use_ = 0, bytes_ = 0;
@@ -125,13 +128,14 @@ class Batch {
   DevBuf<uint2> ang_;
   DevBuf<double> part_;
   DevBuf<unsigned long long> kcount_;
+  DevBuf<int> rb_;  // rebuild work list
   DevBuf<int32_t> cell_cnt_, cell_start_, cell_fill_;
   DevBuf<int2> bent_;
   DevBuf<int4> aent_;
   DevBuf<uint32_t> nbr_;
   DevBuf<Rep> reps_;
-  DevBuf<int32_t> chunk_rep_;
-  std::vector<int32_t> h_chunk_rep_;
+  DevBuf<int4> chunk_rep_;
+  std::vector<int4> h_chunk_rep_;
   std::vector<Rep> h_reps_;
   std::vector<ReplicaInfo> info_;
   cudaGraphExec_t graph_exec_ = nullptr;

@@ -188,6 +188,14 @@ FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chos
     if (iters <= 0 || cap < 0) throw fmd::Error(FMD_ERR_ARG, "bad argument");
     const int v = B(b).autotune(iters, ms_per_variant, cap);
     if (chosen) *chosen = v;
+    // entries after the force variants: neighbor-list variant times (ms per
+    // full rebuild), then the chosen neighbor variant
+    if (ms_per_variant) {
+      for (int k = 0; k < fmd::mixed::kNbrVariants && fmd::mixed::kForceVariants + k < cap; ++k)
+        ms_per_variant[fmd::mixed::kForceVariants + k] = B(b).nbr_variant_ms()[k];
+      const int at = fmd::mixed::kForceVariants + fmd::mixed::kNbrVariants;
+      if (at < cap) ms_per_variant[at] = B(b).nbr_variant();
+    }
   });
 }
 
@@ -199,7 +207,9 @@ FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n) {
   return guarded([&] {
     B(b);
     if (!n) throw fmd::Error(FMD_ERR_ARG, "null argument");
-    *n = 11;  // k_pre, 7 rebuild kernels (early exit unless flagged), k_force x2 (with and without energies), k_post
+    // k_pre, k_commit, 9 rebuild kernels (plan, bin, scan, scatter, cell sort,
+    // permute, bonded tables, home plan, list), k_force x2, k_post, k_post_commit
+    *n = 15;
   });
 }
 

@@ -57,7 +57,7 @@ enum Mode : int32_t { kModeRun = 0, kModePushoff = 1 };
 // Per-kernel launch counters (executed launches, graph conditionals included).
 enum KernelKind : int {
   kKPre = 0, kKBin, kKScan, kKScatter, kKCellsort, kKPermute, kKTopo, kKNeighbors, kKForce, kKForceEv, kKPost,
-  kKernelKinds
+  kKPlan, kKCommit, kKernelKinds
 };
 
 // Per-replica record (device).  Static fields are set at admission; dynamic
@@ -121,7 +121,6 @@ struct Rep {
   uint32_t maxdisp_bits;
   int32_t status;
   int64_t rebuilds;
-  int32_t cnt_pre, cnt_post;     // last-block counters
   NHScalars nh;
   double pending_scale;          // NH post-force velocity scale applied at the next pre-force
   // reductions of the last completed step
@@ -146,7 +145,7 @@ __host__ __device__ inline bool need_ev(const Rep& R) {
 // Device pointers of the batch arrays.
 struct Dev {
   Rep* reps;
-  const int32_t* chunk_rep;      // replica of each chunk (-1 free)
+  const int4* chunk_rep;         // per chunk: replica (-1 free), first slot, atoms in it, index in the replica
   float4* pos;
   float4* vel;
   float4* force;
@@ -178,6 +177,11 @@ struct Dev {
   int32_t* ncnt;
   double* part;                  // [chunks][kNumPartials]
   unsigned long long* kcount;    // [kKernelKinds] launches executed (block 0 of each launch counts)
+  // rebuild work list: [0] count, [1] done blocks, [2, 2 + rb_cap) replicas,
+  // then three offset arrays of rb_cap + 1 (chunk items, cell-group items,
+  // home-cell items)
+  int* rb;
+  int rb_cap;
 };
 
 // Axis part of the shift code for cell shift e and wrap count k; -1 when
@@ -235,17 +239,21 @@ struct StepConds {
   int use;
   cudaGraphConditionalHandle rebuild, force_plain, force_ev, post;
 };
-constexpr int kForceVariants = 5;
-void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
-                 cudaStream_t st);
+constexpr int kForceVariants = 7;
+constexpr int kNbrVariants = 2;
+void launch_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st);
 // The same step recorded into the graph being captured on st, with the
 // conditional nodes; side is a second stream used to capture their bodies.
-void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
-                  cudaStream_t st, cudaStream_t side);
+void capture_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st,
+                  cudaStream_t side);
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st);
-void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells_per_rep, int max_home_cells, cudaStream_t st);
+// Rebuild of the replicas on the work list (rb): bin, scan, scatter, cell sort,
+// permute, bonded tables, neighbor lists.
+void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st);
 void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st);
-void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode);  // 0 setup, 2 re-evaluation
+void launch_reduce_only(const Dev& d, int nchunks, int nreps, cudaStream_t st, int mode);
+// Scalars of the next pre-force for replicas whose copy a host upload made stale.
+void launch_prepare(const Dev& d, int nreps, cudaStream_t st);  // 0 setup, 2 re-evaluation
 
 }  // namespace mixed
 }  // namespace fmd

@@ -1,20 +1,25 @@
 // Mixed-precision batched engine: kernels.
 //
-// One step over every replica of a batch (kernel per phase, one block per
-// 128-slot chunk; a chunk never straddles replicas):
-//   k_pre      half kick / drift (Langevin BAOAB or Nose-Hoover NVT / MTK NPT)
-//              on FP32 cell offsets; per-replica scalar work (thermostat chain,
-//              barostat) recomputed identically by every block in FP64; the
-//              last block of a replica commits it and takes the rebuild decision
-//              (skin/2 displacement test or forced cadence, done on the device).
-//   rebuild    only replicas flagged this step: re-bin into cells, per-cell
-//              deterministic order, permute state, Verlet list (k_bin, k_scan,
-//              k_scatter, k_cellsort, k_permute, k_neighbors).
-//   k_force    LJ over the list + FENE/WCA + harmonic angle gathered per atom
-//              (no atomics), FP32 with compensated sums, FP64 block partials.
-//   k_post     final half kick + FP64 KE-tensor partials; the last block of a
-//              replica reduces all partials in chunk order and runs the
-//              post-force thermostat / barostat update.
+// One step over every replica of a batch (one block per 128-slot chunk for
+// per-atom work; a chunk never straddles replicas):
+//   k_pre        half kick / drift (Langevin BAOAB or Nose-Hoover NVT / MTK NPT)
+//                on FP32 cell offsets with the replica's precomputed FP64 step
+//                scalars; per-replica max displacement.
+//   k_commit     one thread per replica: commits the step (chain / barostat
+//                state, box), takes the rebuild decision (skin/2 displacement
+//                or forced cadence) and appends to the rebuild work list; in a
+//                CUDA graph it switches the conditional nodes below.
+//   rebuild      [IF any replica rebuilds] work-list kernels over the flagged
+//                replicas only: re-bin into cells, per-cell deterministic order,
+//                permute state, per-slot bonded tables, Verlet lists.
+//   k_force      [IF needed, with / without energies] LJ over the list +
+//                FENE/WCA + harmonic angle gathered per atom (no atomics),
+//                FP32 with compensated sums, FP64 block partials.
+//   k_post       [IF needed] final half kick + FP64 KE-tensor partials, then
+//   k_post_commit  one warp per replica reduces the partials in chunk order
+//                and runs the post-force thermostat / barostat.  Langevin
+//                steps inside a graph fold the final half kick into the next
+//                k_pre instead (same operations, same order).
 // Reference algorithm sources: integrate/langevin.cu:34-130,
 // integrate/nose_hoover.cu:86-305, 606-898, force/lj.cu:21-65,
 // force/fene.cu:18-73, force/angle.cu:17-80, neighbor/verlet_list.cu:108-335,
@@ -136,19 +141,12 @@ __device__ __forceinline__ void count_launch(const Dev& d, int kind) {
 // ---------------------------------------------------------------- pre-force
 __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   count_launch(d, kKPre);
-  const int chunk = blockIdx.x;
-  const int r = d.chunk_rep[chunk];
-  if (r < 0) return;
-  Rep& R = d.reps[r];
-  __shared__ StepScalars S;
-  __shared__ uint32_t wmax[kChunk / 32];
-  __shared__ int last;
-  if (!(R.active && R.step < R.stop_step)) return;
-  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
-  const int s = R.slot_base + local;
-  const bool have = local < R.natoms;
-  const bool deferred = R.defer != 0;
-  // The atom's data does not depend on the step scalars: load it first.
+  const int4 ci = d.chunk_rep[blockIdx.x];
+  if (ci.x < 0) return;
+  const int s = ci.y + threadIdx.x;
+  const bool have = (int)threadIdx.x < ci.z;
+  // The atom's data depends neither on the replica record nor on the step
+  // scalars: issue its loads first.
   float4 p = make_float4(0, 0, 0, 0), v = p, f = p, q = p;
   if (have) {
     p = d.pos[s];
@@ -156,6 +154,11 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
     f = d.force[s];
     q = d.ref[s];
   }
+  Rep& R = d.reps[ci.x];
+  __shared__ StepScalars S;
+  __shared__ uint32_t wmax[kChunk / 32];
+  if (!(R.active && R.step < R.stop_step)) return;
+  const bool deferred = R.defer != 0;
   if (R.next_valid) {
     constexpr int nw = (int)(sizeof(StepScalars) / sizeof(uint32_t));
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&R.next);
@@ -234,15 +237,21 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
     for (int w = 0; w < kChunk / 32; ++w) m = max(m, wmax[w]);
     atomicMax(&R.maxdisp_bits, m);
     if (bad) atomicOr(&R.status, kStatusNonFinite);
-    __threadfence();
-    const int old = atomicAdd(&R.cnt_pre, 1);
-    last = (old == R.nchunks - 1);
   }
-  __syncthreads();
-  if (!last || threadIdx.x != 0) return;
-  // Last block of the replica: commit scalars, decide on a rebuild.
-  __threadfence();
-  R.cnt_pre = 0;
+}
+
+// Per-replica commit of the pre-force update (one thread per replica, after
+// every pre-force block finished): step counter, chain / barostat state, box,
+// the rebuild decision and the graph's conditional switches.
+__global__ void __launch_bounds__(32) k_commit(Dev d, StepConds cond) {
+  count_launch(d, kKCommit);
+  const int r = blockIdx.x;
+  if (threadIdx.x != 0 || r >= d.rb_cap) return;
+  Rep& R = d.reps[r];
+  if (!(R.active && R.step < R.stop_step)) return;  // did not advance this step
+  StepScalars S;
+  if (R.next_valid) S = R.next;
+  else compute_step_scalars(R, S);
   R.next_valid = 0;
   R.step = S.step;
   R.nh = S.nh;
@@ -254,8 +263,7 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   R.Lpos = R.L;
   R.adv = 1;
   R.since += 1;
-  const uint32_t mb = atomicAdd(&R.maxdisp_bits, 0u);
-  const float maxd2 = __uint_as_float(mb);
+  const float maxd2 = __uint_as_float(R.maxdisp_bits);
   const float hs = (float)(0.5 * R.skin);
   const bool trig = maxd2 > hs * hs;
   if (trig || R.since >= R.max_between) {
@@ -263,6 +271,7 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
     R.maxdisp_bits = 0u;
     R.rebuilds += 1;
     R.rebuild_now = 1;
+    d.rb[2 + atomicAdd(d.rb, 1)] = r;
   } else {
     R.rebuild_now = 0;
   }
@@ -287,6 +296,18 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   }
 }
 
+// Scalars of the next pre-force for every active replica whose copy is
+// stale (after a host upload), so that no pre-force block computes them.
+__global__ void __launch_bounds__(32) k_prepare(Dev d) {
+  count_launch(d, kKCommit);
+  const int r = blockIdx.x;
+  if (threadIdx.x != 0 || r >= d.rb_cap) return;
+  Rep& R = d.reps[r];
+  if (!R.active || R.next_valid) return;
+  compute_step_scalars(R, R.next);
+  R.next_valid = 1;
+}
+
 // ---------------------------------------------------------------- rebuild
 // Minimum-image cell shift of j relative to i and the periodic wrap count,
 // for cell coordinates ci, cj and offsets oi, oj (one axis).
@@ -300,14 +321,99 @@ __device__ __forceinline__ void pair_shift(int ci, int cj, float oi, float oj, i
 // Cell shift term e*h + k*dL (exact periodic box L = G*h + dL).
 __device__ __forceinline__ float shift_term(int e, int k, float h, float dL) { return (float)e * h + (float)k * dL; }
 
-__global__ void __launch_bounds__(kChunk) k_bin(Dev d) {
-  count_launch(d, kKBin);
-  const int chunk = blockIdx.x;
-  const int r = d.chunk_rep[chunk];
-  if (r < 0) return;
-  const Rep& R = d.reps[r];
-  if (!R.rebuild_now) return;
-  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+// Neighbor-list work items: rows of kNbrRow home cells along x (G >= 3),
+// single home cells for smaller grids.
+constexpr int kNbrThreads = 128;
+constexpr int kNbrRow = kNbrThreads / 32;  // home cells per item, one warp each
+constexpr int kNbrCap = 1536;              // staged candidates (24 KB)
+constexpr int kNbrUnion = (kNbrRow + 2) * 9;
+
+__host__ __device__ inline int nbr_items(int G) { return G >= 3 ? G * G * ((G + kNbrRow - 1) / kNbrRow) : G * G * G; }
+
+// ---- rebuild work list.  The pre-force kernel appends each replica that
+// rebuilds this step; k_rbplan turns the list into prefix offsets of chunk
+// and cell-group work items; the rebuild kernels run fixed grids that stride
+// over those items only, so a step where a few replicas rebuild costs work
+// for those replicas, not early exits over the whole batch.  The last block
+// of the neighbor-list kernel empties the list for the next step.
+__device__ __forceinline__ int rb_count(const Dev& d) { return d.rb[0]; }
+__device__ __forceinline__ int rb_rep(const Dev& d, int i) { return d.rb[2 + i]; }
+__device__ __forceinline__ int* rb_off(const Dev& d, int which) { return d.rb + 2 + d.rb_cap + which * (d.rb_cap + 1); }
+
+// index i with off[i] <= item < off[i + 1]
+__device__ __forceinline__ int rb_find(const int* off, int n, int item) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= item) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Block-wide exclusive scan of v over the list (1024 threads), into off[0..n].
+template <typename F>
+__device__ void rb_scan(const Dev& d, int n, int* off, F value) {
+  __shared__ int sm[1024];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < n ? value(rb_rep(d, i)) : 0;
+    sm[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      const int t = threadIdx.x >= o ? sm[threadIdx.x - o] : 0;
+      __syncthreads();
+      sm[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < n) off[i] = carry + sm[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += sm[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) off[n] = carry;
+}
+
+constexpr int kCellGroup = 8;  // cells per cell-sort work item (one warp each)
+
+// Offsets of chunk items and cell-group items (P^3 Morton cells per replica).
+__global__ void __launch_bounds__(1024) k_rbplan(Dev d) {
+  count_launch(d, kKPlan);
+  const int n = rb_count(d);
+  rb_scan(d, n, rb_off(d, 0), [&](int r) { return d.reps[r].nchunks; });
+  rb_scan(d, n, rb_off(d, 1), [&](int r) {
+    const int P = d.reps[r].P;
+    return (P * P * P + kCellGroup - 1) / kCellGroup;
+  });
+}
+
+// Offsets of home-cell items (G^3 per replica, G as set by k_scan).
+__global__ void __launch_bounds__(1024) k_rbplan_home(Dev d, int variant) {
+  count_launch(d, kKPlan);
+  const int n = rb_count(d);
+  rb_scan(d, n, rb_off(d, 2), [&](int r) {
+    const int G = d.reps[r].G;
+    return variant == 0 ? G * G * G : nbr_items(G);
+  });
+}
+
+// Calls body(R, r, chunk index within the replica) for this block's chunk items.
+template <typename F>
+__device__ __forceinline__ void for_rebuild_chunks(const Dev& d, F body) {
+  const int n = rb_count(d);
+  const int* off = rb_off(d, 0);
+  const int total = n > 0 ? off[n] : 0;
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    const int i = rb_find(off, n, item);
+    const int r = rb_rep(d, i);
+    body(d.reps[r], r, item - off[i]);
+  }
+}
+
+__device__ __forceinline__ void bin_chunk(const Dev& d, const Rep& R, int ci) {
+  const int local = ci * kChunk + threadIdx.x;
   if (local >= R.natoms) return;
   const int s = R.slot_base + local;
   const float4 p = d.pos[s];
@@ -350,13 +456,16 @@ __global__ void __launch_bounds__(kChunk) k_bin(Dev d) {
   atomicAdd(&d.cell_cnt[R.cell_base + key], 1);
 }
 
+__global__ void __launch_bounds__(kChunk) k_bin(Dev d) {
+  count_launch(d, kKBin);
+  for_rebuild_chunks(d, [&](const Rep& R, int, int ci) { bin_chunk(d, R, ci); });
+}
+
 // Exclusive scan of the replica's cell counts; one block per replica.
-__global__ void __launch_bounds__(1024) k_scan(Dev d, int nreps) {
+__global__ void __launch_bounds__(1024) k_scan(Dev d) {
   count_launch(d, kKScan);
-  const int r = blockIdx.x;
-  if (r >= nreps) return;
-  Rep& R = d.reps[r];
-  if (!R.active || !R.rebuild_now) return;
+  if ((int)blockIdx.x >= rb_count(d)) return;
+  Rep& R = d.reps[rb_rep(d, blockIdx.x)];
   const int ncell = R.P * R.P * R.P;
   const int per = (ncell + blockDim.x - 1) / blockDim.x;
   const int b0 = threadIdx.x * per;
@@ -390,32 +499,21 @@ __global__ void __launch_bounds__(1024) k_scan(Dev d, int nreps) {
 
 __global__ void __launch_bounds__(kChunk) k_scatter(Dev d) {
   count_launch(d, kKScatter);
-  const int chunk = blockIdx.x;
-  const int r = d.chunk_rep[chunk];
-  if (r < 0) return;
-  const Rep& R = d.reps[r];
-  if (!R.rebuild_now) return;
-  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
-  if (local >= R.natoms) return;
-  const int s = R.slot_base + local;
-  const int at = atomicAdd(&d.cell_fill[R.cell_base + d.key[s]], 1);
-  d.bucket[R.slot_base + at] = local;
+  for_rebuild_chunks(d, [&](const Rep& R, int, int ci) {
+    const int local = ci * kChunk + threadIdx.x;
+    if (local >= R.natoms) return;
+    const int s = R.slot_base + local;
+    const int at = atomicAdd(&d.cell_fill[R.cell_base + d.key[s]], 1);
+    d.bucket[R.slot_base + at] = local;
+  });
 }
 
 // Per cell: order members by atom id (deterministic), write the permutation.
 // grid (cell blocks, replicas); one warp per cell.  Cells of up to 32
 // members rank in registers with shuffles; larger ones fall back to a loop
 // over the bucket.
-__global__ void __launch_bounds__(256) k_cellsort(Dev d, int nreps) {
-  count_launch(d, kKCellsort);
-  const int r = blockIdx.y;
-  if (r >= nreps) return;
-  const Rep& R = d.reps[r];
-  if (!R.active || !R.rebuild_now) return;
-  const int ncell = R.P * R.P * R.P;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int c = blockIdx.x * 8 + warp;
-  if (c < ncell) {
+__device__ __forceinline__ void cellsort_cell(const Dev& d, const Rep& R, int c, int lane) {
+  {
     const int st = d.cell_start[R.cell_base + c];
     const int n = d.cell_fill[R.cell_base + c] - st;
     if (n <= 0) return;
@@ -440,14 +538,22 @@ __global__ void __launch_bounds__(256) k_cellsort(Dev d, int nreps) {
   }
 }
 
-__global__ void __launch_bounds__(kChunk) k_permute(Dev d) {
-  count_launch(d, kKPermute);
-  const int chunk = blockIdx.x;
-  const int r = d.chunk_rep[chunk];
-  if (r < 0) return;
-  const Rep& R = d.reps[r];
-  if (!R.rebuild_now) return;
-  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+__global__ void __launch_bounds__(32 * kCellGroup) k_cellsort(Dev d) {
+  count_launch(d, kKCellsort);
+  const int n = rb_count(d);
+  const int* off = rb_off(d, 1);
+  const int total = n > 0 ? off[n] : 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    const int i = rb_find(off, n, item);
+    const Rep& R = d.reps[rb_rep(d, i)];
+    const int c = (item - off[i]) * kCellGroup + warp;
+    if (c < R.P * R.P * R.P) cellsort_cell(d, R, c, lane);
+  }
+}
+
+__device__ __forceinline__ void permute_chunk(const Dev& d, const Rep& R, int ci) {
+  const int local = ci * kChunk + threadIdx.x;
   const int s = R.slot_base + local;
   if (local >= R.natoms) {
     d.ncnt[s] = 0;
@@ -463,16 +569,15 @@ __global__ void __launch_bounds__(kChunk) k_permute(Dev d) {
   d.slot_of[R.slot_base + im.w] = local;
 }
 
+__global__ void __launch_bounds__(kChunk) k_permute(Dev d) {
+  count_launch(d, kKPermute);
+  for_rebuild_chunks(d, [&](const Rep& R, int, int ci) { permute_chunk(d, R, ci); });
+}
+
 // Per-slot bonded tables for the new order: partner slots instead of atom
 // ids, so the force kernel reaches a partner's position in one load.
-__global__ void __launch_bounds__(kChunk) k_topo(Dev d) {
-  count_launch(d, kKTopo);
-  const int chunk = blockIdx.x;
-  const int r = d.chunk_rep[chunk];
-  if (r < 0) return;
-  const Rep& R = d.reps[r];
-  if (!R.rebuild_now) return;
-  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+__device__ __forceinline__ void topo_chunk(const Dev& d, const Rep& R, int ci) {
+  const int local = ci * kChunk + threadIdx.x;
   const int s = R.slot_base + local;
   if (local >= R.natoms) {
     d.tcnt[s] = 0;
@@ -499,6 +604,11 @@ __global__ void __launch_bounds__(kChunk) k_topo(Dev d) {
         make_uint2(o1 | ((uint32_t)role << 26), o2 | ((uint32_t)ty << 26));
   }
   d.tcnt[s] = (b1 - b0) | ((a1 - a0) << 8);
+}
+
+__global__ void __launch_bounds__(kChunk) k_topo(Dev d) {
+  count_launch(d, kKTopo);
+  for_rebuild_chunks(d, [&](const Rep& R, int, int ci) { topo_chunk(d, R, ci); });
 }
 
 // Verlet list for boxes of fewer than three cells per axis (L < 3 (rc +
@@ -596,7 +706,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
   return overflow;
 }
 
-// Verlet list, one block per home cell (G >= 3).  The 27 neighbor cells'
+// Verlet list, ballot form: one block per home cell (G >= 3).  The 27 neighbor cells'
 // atoms are staged in shared memory in stencil order (dz, dy, dx; slot order
 // inside a cell) with the cell's periodic shift already added, so a pair's
 // separation is one subtraction.  Each warp takes one home atom at a time;
@@ -605,20 +715,12 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
 // is deterministic.  Pairs within rc + skin, 1-2 bonded pairs excluded
 // (verlet_list.cu:108-335 semantics), exclusions compared as slots from the
 // per-slot bond table.
-constexpr int kNbrThreads = 128;
 constexpr int kNbrWarps = kNbrThreads / 32;
 constexpr int kNbrWin = 1024;     // staged candidates per window
 constexpr int kNbrGroup = 64;     // home atoms per pass
 
-__global__ void __launch_bounds__(kNbrThreads) k_neighbors(Dev d, int nreps) {
-  count_launch(d, kKNeighbors);
-  const int r = blockIdx.y;
-  if (r >= nreps) return;
-  Rep& R = d.reps[r];
-  if (!R.active || !R.rebuild_now) return;
+__device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
   const int G = R.G;
-  const int lc = blockIdx.x;
-  if (lc >= G * G * G) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (G < 3) {
     if (warp == 0) {
@@ -715,14 +817,14 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors(Dev d, int nreps) {
           }
           const uint32_t m = __ballot_sync(0xFFFFFFFFu, acc);
           const int at = count + __popc(m & lt);
-          if (acc && at < M) out[(size_t)at * 32] = e;
+          if (acc && at < M) __stcg(out + (size_t)at * 32, e);
           count += __popc(m);
         }
         if (w0 + kNbrWin >= total) {
           if (count <= M) {
             const int padded = (count + kListPad - 1) & ~(kListPad - 1);
             if (lane < padded - count)
-              out[(size_t)(count + lane) * 32] = (uint32_t)i | (kZeroShiftCode << kCodeShift);
+              __stcg(out + (size_t)(count + lane) * 32, (uint32_t)i | (kZeroShiftCode << kCodeShift));
           }
           if (lane == 0) {
             d.ncnt[base + i] = min(count, M);
@@ -735,6 +837,179 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors(Dev d, int nreps) {
     }
   }
   if (overflow) atomicOr(&R.status, overflow);
+}
+
+// Verlet list (G >= 3): one block per row of up to kNbrRow home cells along
+// x.  The union of their neighbor cells (a (row + 2) x 3 x 3 block of cells)
+// is staged once in shared memory, each candidate with its cell's periodic
+// shift relative to the row origin already added; cells beyond the staging
+// capacity are read from global memory instead.  Each warp owns one home
+// cell, its lanes are that cell's atoms (32 at a time), and it walks its own
+// 27 cells in stencil order (dz, dy, dx; slot order inside a cell) with every
+// lane reading the same candidate (shared-memory broadcast); hits are
+// appended per lane, so each list is in candidate order and deterministic.
+// Pairs within rc + skin, 1-2 bonded pairs excluded (verlet_list.cu:108-335
+// semantics), exclusions compared as slots from the per-slot bond table.
+
+__device__ void neighbors_row(const Dev& d, Rep& R, int item) {
+  const int G = R.G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (G < 3) {
+    if (warp == 0) {
+      const int ov = neighbors_small_box(d, R, item, lane);
+      if (ov) atomicOr(&R.status, ov);
+    }
+    return;
+  }
+  const int nrow = (G + kNbrRow - 1) / kNbrRow;
+  const int bx = item % nrow, hy = (item / nrow) % G, hz = item / (nrow * G);
+  const int hx0 = bx * kNbrRow;
+  const int nhome = min(kNbrRow, G - hx0);
+  const int ux = nhome + 2;  // union columns: x = hx0 - 1 ... hx0 + nhome
+  const int nu = ux * 9;
+  const int M = R.M;
+  const int base = R.slot_base;
+  const int cell_base = R.cell_base;
+  uint32_t* const list = d.nbr + R.nbr_base;
+  const float h = R.h;
+  const float dL = (float)(R.L - (double)G * (double)h);
+  const float rcs = (float)(R.rc + R.skin);
+  const float rcs2 = rcs * rcs;
+
+  __shared__ float4 s_c[kNbrCap];
+  __shared__ int s_ns[kNbrUnion], s_off[kNbrUnion + 1];
+  __shared__ float s_sx[kNbrUnion], s_sy[kNbrUnion], s_sz[kNbrUnion];
+  __shared__ int s_ax[kNbrUnion];   // wrap count kx of the union column
+  __shared__ int s_ayz[kNbrUnion];  // (axis code y) * 5 + (axis code z)
+  if (threadIdx.x < nu) {
+    const int u = threadIdx.x;
+    const int row = u / ux, col = u % ux;
+    const int dz = row / 3 - 1, dy = row % 3 - 1;
+    const int xu = hx0 - 1 + col;
+    const int kx = xu < 0 ? -1 : (xu >= G ? 1 : 0);
+    const int ky = hy + dy < 0 ? -1 : (hy + dy >= G ? 1 : 0);
+    const int kz = hz + dz < 0 ? -1 : (hz + dz >= G ? 1 : 0);
+    const int nx = xu - kx * G, ny = hy + dy - ky * G, nz = hz + dz - kz * G;
+    const uint32_t key = cell_key(nx, ny, nz);
+    const int ns = d.cell_start[cell_base + key];
+    s_ns[u] = ns;
+    s_off[u + 1] = d.cell_fill[cell_base + key] - ns;
+    // relative to the row origin: x shift (xu - hx0) h + kx dL
+    s_sx[u] = shift_term(xu - hx0, kx, h, dL);
+    s_sy[u] = shift_term(dy, ky, h, dL);
+    s_sz[u] = shift_term(dz, kz, h, dL);
+    s_ax[u] = kx;
+    s_ayz[u] = axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_off[0] = 0;
+    for (int u = 0; u < nu; ++u) s_off[u + 1] += s_off[u];
+  }
+  __syncthreads();
+  const int staged = min(s_off[nu], kNbrCap);
+  for (int u = warp; u < nu; u += kNbrRow) {
+    const int o0 = s_off[u], o1 = min(s_off[u + 1], kNbrCap);
+    const float sx = s_sx[u], sy = s_sy[u], sz = s_sz[u];
+    const int ns = s_ns[u];
+    for (int k = o0 + lane; k < o1; k += 32) {
+      const int j = ns + (k - o0);
+      const float4 p = d.pos[base + j];
+      s_c[k] = make_float4(p.x + sx, p.y + sy, p.z + sz, __int_as_float(j));
+    }
+  }
+  __syncthreads();
+  int overflow = 0;
+  if (warp < nhome) {
+    const int a = warp;  // this warp's home cell: x = hx0 + a
+    const int uh = 4 * ux + a + 1;
+    const int hs = s_ns[uh];
+    const int nh = s_off[uh + 1] - s_off[uh];
+    const float ah = (float)a * h;
+    for (int hb = 0; hb < nh; hb += 32) {
+      const bool act = hb + lane < nh;
+      const int i = hs + hb + lane;
+      float4 pi = make_float4(0, 0, 0, 0);
+      uint32_t ex0 = 0xFFFFFFFFu, ex1 = ex0, ex2 = ex0, ex3 = ex0;
+      if (act) {
+        pi = d.pos[base + i];
+        pi.x += ah;
+        const int nb = d.tcnt[base + i] & 0xFF;
+        const uint32_t* bl = d.bnd + (size_t)(base + i) * kMaxBondsPerAtom;
+        if (nb > 0) ex0 = bl[0] & kSlotMask26;
+        if (nb > 1) ex1 = bl[1] & kSlotMask26;
+        if (nb > 2) ex2 = bl[2] & kSlotMask26;
+        if (nb > 3) ex3 = bl[3] & kSlotMask26;
+      }
+      uint32_t* out = list + ((size_t)(i >> 5) * M) * 32 + (i & 31);
+      int count = 0;
+      for (int row = 0; row < 9; ++row) {
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int u = row * ux + a + 1 + dx;
+          const uint32_t code =
+              (uint32_t)(axis_shift_code(dx, s_ax[u]) * 25 + s_ayz[u]) << kCodeShift;
+          const int k0 = s_off[u], k1 = s_off[u + 1];
+          const float sx = s_sx[u], sy = s_sy[u], sz = s_sz[u];
+          const int ns = s_ns[u];
+#pragma unroll 4
+          for (int k = k0; k < k1; ++k) {
+            float4 c;
+            if (k < staged) {
+              c = s_c[k];
+            } else {
+              const int j = ns + (k - k0);
+              const float4 p = d.pos[base + j];
+              c = make_float4(p.x + sx, p.y + sy, p.z + sz, __int_as_float(j));
+            }
+            const uint32_t j = (uint32_t)__float_as_int(c.w);
+            const float rx = pi.x - c.x, ry = pi.y - c.y, rz = pi.z - c.z;
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            const bool hit = act && r2 < rcs2 && j != (uint32_t)i && j != ex0 && j != ex1 && j != ex2 && j != ex3;
+            if (hit && count < M) __stcg(out + (size_t)count * 32, j | code);
+            count += hit ? 1 : 0;
+          }
+        }
+      }
+      if (act) {
+        d.ncnt[base + i] = min(count, M);
+        if (count > M) {
+          overflow |= kStatusOverflow;
+        } else {
+          for (int k = count; k < ((count + kListPad - 1) & ~(kListPad - 1)); ++k)
+            __stcg(out + (size_t)k * 32, (uint32_t)i | (kZeroShiftCode << kCodeShift));
+        }
+      }
+    }
+  }
+  if (overflow) atomicOr(&R.status, overflow);
+}
+
+// Neighbor-list kernel variants: 0 = ballot form (one home cell per item),
+// 1 = row form (kNbrRow home cells per item); the autotuner picks one.
+template <int V>
+__global__ void __launch_bounds__(kNbrThreads, V == 0 ? 8 : 6) k_neighbors(Dev d) {
+  count_launch(d, kKNeighbors);
+  const int n = rb_count(d);
+  const int* off = rb_off(d, 2);
+  const int total = n > 0 ? off[n] : 0;
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    const int i = rb_find(off, n, item);
+    __syncthreads();  // the previous item's shared staging is no longer read
+    if (V == 0)
+      neighbors_cell_ballot(d, d.reps[rb_rep(d, i)], item - off[i]);
+    else
+      neighbors_row(d, d.reps[rb_rep(d, i)], item - off[i]);
+  }
+  // the last block to finish empties the work list for the next step
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(d.rb + 1, 1) == (int)gridDim.x - 1) {
+      d.rb[0] = 0;
+      d.rb[1] = 0;
+      __threadfence();
+    }
+  }
 }
 
 // ---------------------------------------------------------------- forces
@@ -831,7 +1106,7 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
 // then all position gathers, then the arithmetic.  PF: the next batch's list
 // words are loaded before this batch's gathers (software pipelining, B more
 // registers).  nn is the padded length (a multiple of B).
-template <bool EV, int B, bool PF>
+template <bool EV, int B, bool PF, int KB>
 __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
                                         const float4* s_shift, bool one_type, int ti, int nt, const float* s_eps24,
                                         const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
@@ -842,6 +1117,9 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
 #pragma unroll
     for (int q = 0; q < B; ++q) wn[q] = nn > 0 ? __ldg(lst + (size_t)q * 32) : 0u;
   }
+  // plain sums over KB batches (KB * B <= 8 pairs), then one compensated add
+  PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
+  int kb = 0;
   for (int k = 0; k < nn; k += B) {
     uint32_t w[B];
     if (PF) {
@@ -858,7 +1136,6 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
     float4 pj[B];
 #pragma unroll
     for (int q = 0; q < B; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
-    PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
 #pragma unroll
     for (int q = 0; q < B; ++q) {
       float e24 = e24_0, sig2 = sig2_0;
@@ -869,11 +1146,21 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
       }
       lj_pair<EV>(g, pi, s_shift[w[q] >> kCodeShift], pj[q], rc2, e24, sig2);
     }
-    fx.add(g.fx);
-    fy.add(g.fy);
-    fz.add(g.fz);
-    acc = g;
+    if (++kb == KB || k + B >= nn) {
+      fx.add(g.fx);
+      fy.add(g.fy);
+      fz.add(g.fz);
+      g.fx = g.fy = g.fz = 0.0f;
+      kb = 0;
+    }
   }
+  acc.pe = g.pe;
+  acc.v0 = g.v0;
+  acc.v1 = g.v1;
+  acc.v2 = g.v2;
+  acc.v3 = g.v3;
+  acc.v4 = g.v4;
+  acc.v5 = g.v5;
 }
 
 // Harmonic angle (angle.cu:17-80) on (ri, rj = vertex, rk): force on the
@@ -920,11 +1207,12 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
 // Two instantiations: with energies / virial (thermo steps, NPT, host
 // requests) and without (all other steps); a block runs in the one that
 // matches its replica's need this step and the other returns at once.
-template <bool EV, int B, int MINB, bool PF>
+template <bool EV, int B, int MINB, bool PF, int KB>
 __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
   count_launch(d, EV ? kKForceEv : kKForce);
   const int chunk = blockIdx.x;
-  const int r = d.chunk_rep[chunk];
+  const int4 ci = d.chunk_rep[chunk];
+  const int r = ci.x;
   if (r < 0) return;
   const Rep& R = d.reps[r];
   if (!R.adv) return;
@@ -948,9 +1236,9 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
                              shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
   }
   __syncthreads();
-  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
+  const int local = ci.w * kChunk + threadIdx.x;
   const int base = R.slot_base;
-  const int s = base + local;
+  const int s = ci.y + threadIdx.x;
   const float rc2 = (float)(R.rc * R.rc);
   double vals[7] = {0, 0, 0, 0, 0, 0, 0};
   int status = 0;
@@ -965,7 +1253,7 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
     const bool one_type = (nt == 1);
-    lj_loop<EV, B, PF>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    lj_loop<EV, B, PF, KB>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
@@ -1052,18 +1340,20 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
 __global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
   count_launch(d, kKPost);
   const int chunk = blockIdx.x;
-  const int r = d.chunk_rep[chunk];
-  if (r < 0) return;
-  Rep& R = d.reps[r];
+  const int4 ci = d.chunk_rep[chunk];
+  if (ci.x < 0) return;
+  const int s = ci.y + threadIdx.x;
+  const bool have = (int)threadIdx.x < ci.z;
+  float4 v = make_float4(0, 0, 0, 1), f = make_float4(0, 0, 0, 0);
+  if (have) {
+    v = d.vel[s];
+    f = d.force[s];
+  }
+  Rep& R = d.reps[ci.x];
   if (!R.adv || (kick == 1 && R.defer)) return;
-  __shared__ int last;
-  const int local = (chunk - R.chunk_base) * kChunk + threadIdx.x;
-  const int s = R.slot_base + local;
   double vals[7] = {0, 0, 0, 0, 0, 0, 0};
-  if (local < R.natoms) {
-    float4 v = d.vel[s];
+  if (have) {
     if (kick == 1) {
-      const float4 f = d.force[s];
       const double dt = (R.mode == kModePushoff) ? R.push_dt : R.dt;
       const float hm = (float)(0.5 * dt) * v.w;
       v.x = fmaf(hm, f.x, v.x);
@@ -1081,26 +1371,27 @@ __global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
     vals[5] = m * vz * vz;
   }
   block_partials<kChunk>(vals, 6, d.part + (size_t)chunk * kNumPartials + 7);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const int old = atomicAdd(&R.cnt_post, 1);
-    last = (old == R.nchunks - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // Last block: reduce the replica's partials in chunk order (warp 0).
-  if (threadIdx.x < 32) {
+}
+
+// Per-replica commit of the post-force update (one warp per replica, after
+// every post-force block finished): reduce the chunk partials in chunk order
+// (deterministic), store energies / virial / KE, run the post-force chain or
+// barostat, and precompute the next pre-force's scalars.
+__global__ void __launch_bounds__(32) k_post_commit(Dev d, int kick) {
+  count_launch(d, kKCommit);
+  const int r = blockIdx.x;
+  if (r >= d.rb_cap) return;
+  Rep& R = d.reps[r];
+  if (!R.adv || (kick == 1 && R.defer)) return;
+  {
     double acc[13];
     for (int q = 0; q < 13; ++q) acc[q] = 0.0;
     for (int c = threadIdx.x; c < R.nchunks; c += 32) {
-      const volatile double* pp = d.part + (size_t)(R.chunk_base + c) * kNumPartials;
+      const double* pp = d.part + (size_t)(R.chunk_base + c) * kNumPartials;
       for (int q = 0; q < 13; ++q) acc[q] += pp[q];
     }
     for (int q = 0; q < 13; ++q) acc[q] = warp_sum(acc[q]);
     if (threadIdx.x == 0) {
-      R.cnt_post = 0;
       if (need_ev(R)) {
         R.pe = acc[0];
         for (int q = 0; q < 6; ++q) R.vir[q] = acc[1 + q];
@@ -1144,19 +1435,26 @@ __global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
   }
 }
 
-// NPT post-force: the box changed after the barostat update, so h follows L.
-// (h is re-derived from L at the next pre-force; between the post update and
-// the next pre-force nothing reads h.)
-
 // ---------------------------------------------------------------- launchers
+namespace {
+int num_sms() {
+  int dev = 0;
+  FMD_CUDA(cudaGetDevice(&dev));
+  static int cache[256] = {0};
+  if (dev < 0 || dev >= 256) return 148;
+  if (!cache[dev]) FMD_CUDA(cudaDeviceGetAttribute(&cache[dev], cudaDevAttrMultiProcessorCount, dev));
+  return cache[dev];
+}
+}  // namespace
 
-void launch_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
-                 cudaStream_t st) {
+void launch_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st) {
   k_pre<<<nchunks, kChunk, 0, st>>>(d, StepConds{0, 0, 0, 0, 0});
-  launch_rebuild(d, nchunks, nreps, max_cells, max_home, st);
+  k_commit<<<nreps, 32, 0, st>>>(d, StepConds{0, 0, 0, 0, 0});
+  launch_rebuild(d, nreps, nbr_variant, st);
   launch_force(d, nchunks, false, force_variant, st);
   launch_force(d, nchunks, true, force_variant, st);
   k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
+  k_post_commit<<<nreps, 32, 0, st>>>(d, 1);
 }
 
 namespace {
@@ -1186,8 +1484,8 @@ void capture_if(cudaStream_t st, cudaStream_t side, cudaGraphConditionalHandle h
 }
 }  // namespace
 
-void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, int force_variant,
-                  cudaStream_t st, cudaStream_t side) {
+void capture_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st,
+                  cudaStream_t side) {
   cudaStreamCaptureStatus cs;
   cudaGraph_t g;
   FMD_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
@@ -1197,39 +1495,61 @@ void capture_step(const Dev& d, int nchunks, int nreps, int max_cells, int max_h
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
   k_pre<<<nchunks, kChunk, 0, st>>>(d, c);
-  capture_if(st, side, c.rebuild, [&](cudaStream_t s) { launch_rebuild(d, nchunks, nreps, max_cells, max_home, s); });
+  k_commit<<<nreps, 32, 0, st>>>(d, c);
+  capture_if(st, side, c.rebuild, [&](cudaStream_t s) { launch_rebuild(d, nreps, nbr_variant, s); });
   capture_if(st, side, c.force_plain, [&](cudaStream_t s) { launch_force(d, nchunks, false, force_variant, s); });
   capture_if(st, side, c.force_ev, [&](cudaStream_t s) { launch_force(d, nchunks, true, force_variant, s); });
-  capture_if(st, side, c.post, [&](cudaStream_t s) { k_post<<<nchunks, kChunk, 0, s>>>(d, 1); });
+  capture_if(st, side, c.post, [&](cudaStream_t s) {
+    k_post<<<nchunks, kChunk, 0, s>>>(d, 1);
+    k_post_commit<<<nreps, 32, 0, s>>>(d, 1);
+  });
 }
 
-void launch_rebuild(const Dev& d, int nchunks, int nreps, int max_cells, int max_home, cudaStream_t st) {
-  if (max_cells < 1) max_cells = 1;
-  if (max_home < 1) max_home = 1;
-  k_bin<<<nchunks, kChunk, 0, st>>>(d);
-  k_scan<<<nreps, 1024, 0, st>>>(d, nreps);
-  k_scatter<<<nchunks, kChunk, 0, st>>>(d);
-  dim3 gs((max_cells + 7) / 8, nreps);
-  k_cellsort<<<gs, 256, 0, st>>>(d, nreps);
-  k_permute<<<nchunks, kChunk, 0, st>>>(d);
-  k_topo<<<nchunks, kChunk, 0, st>>>(d);
-  dim3 gn(max_home, nreps);
-  k_neighbors<<<gn, kNbrThreads, 0, st>>>(d, nreps);
+namespace {
+// Blocks of a persistent (grid-stride) kernel: exactly the number that are
+// resident at once, so no block waits for a second wave.
+template <typename K>
+int resident_grid(K kernel, int threads) {
+  int per_sm = 0;
+  FMD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+  return num_sms() * (per_sm > 0 ? per_sm : 1);
+}
+}  // namespace
+
+void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
+  static const int g_bin = resident_grid(k_bin, kChunk), g_scatter = resident_grid(k_scatter, kChunk),
+                   g_sort = resident_grid(k_cellsort, 32 * kCellGroup), g_perm = resident_grid(k_permute, kChunk),
+                   g_topo = resident_grid(k_topo, kChunk), g_nbr0 = resident_grid(k_neighbors<0>, kNbrThreads),
+                   g_nbr1 = resident_grid(k_neighbors<1>, kNbrThreads);
+  k_rbplan<<<1, 1024, 0, st>>>(d);
+  k_bin<<<g_bin, kChunk, 0, st>>>(d);
+  k_scan<<<nreps, 1024, 0, st>>>(d);
+  k_scatter<<<g_scatter, kChunk, 0, st>>>(d);
+  k_cellsort<<<g_sort, 32 * kCellGroup, 0, st>>>(d);
+  k_permute<<<g_perm, kChunk, 0, st>>>(d);
+  k_topo<<<g_topo, kChunk, 0, st>>>(d);
+  k_rbplan_home<<<1, 1024, 0, st>>>(d, nbr_variant);
+  if (nbr_variant == 0)
+    k_neighbors<0><<<g_nbr0, kNbrThreads, 0, st>>>(d);
+  else
+    k_neighbors<1><<<g_nbr1, kNbrThreads, 0, st>>>(d);
 }
 
 // Force-kernel variants (list batch, blocks per SM, pipelined list loads);
 // the batch's autotuner picks one.  The energy variant is fixed.
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st) {
   if (ev) {
-    k_force<true, 8, 5, false><<<nchunks, kChunk, 0, st>>>(d);
+    k_force<true, 4, 5, true, 2><<<nchunks, kChunk, 0, st>>>(d);
     return;
   }
   switch (variant) {
-    case 1: k_force<false, 4, 8, false><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 2: k_force<false, 8, 5, true><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 3: k_force<false, 4, 6, true><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 4: k_force<false, 8, 8, false><<<nchunks, kChunk, 0, st>>>(d); break;
-    default: k_force<false, 8, 6, false><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 1: k_force<false, 4, 8, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 2: k_force<false, 4, 6, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 3: k_force<false, 4, 8, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 4: k_force<false, 2, 8, true, 4><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 5: k_force<false, 4, 7, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 6: k_force<false, 8, 6, false, 1><<<nchunks, kChunk, 0, st>>>(d); break;
+    default: k_force<false, 4, 6, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
   }
 }
 
@@ -1237,9 +1557,12 @@ void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st)
   launch_force(d, nchunks, false, variant, st);
   launch_force(d, nchunks, true, variant, st);
 }
-void launch_reduce_only(const Dev& d, int nchunks, cudaStream_t st, int mode) {
+void launch_reduce_only(const Dev& d, int nchunks, int nreps, cudaStream_t st, int mode) {
   k_post<<<nchunks, kChunk, 0, st>>>(d, mode);
+  k_post_commit<<<nreps, 32, 0, st>>>(d, mode);
 }
+
+void launch_prepare(const Dev& d, int nreps, cudaStream_t st) { k_prepare<<<nreps, 32, 0, st>>>(d); }
 
 }  // namespace mixed
 }  // namespace fmd

@@ -239,19 +239,22 @@ FMD_API fmd_status fmd_batch_totals(fmd_batch* b, int32_t* active, int64_t* atom
  * fmd_batch_kernels_per_step: kernel launches one step issues at most.
  * fmd_batch_launch_counts: launches executed so far per kernel, counted on
  * the device (a graph step skips the rebuild kernels and a force variant no
- * replica needs): counts[0..10] = pre-force, bin, scan, scatter, cell sort,
+ * replica needs): counts[0..12] = pre-force, bin, scan, scatter, cell sort,
  * permute, bonded tables, neighbor list, force, force with energies,
- * post-force; n = entries to fill. */
+ * post-force, rebuild planning, per-replica commits; n = entries to fill. */
 FMD_API fmd_status fmd_batch_mark(fmd_batch* b, int32_t which);
 FMD_API fmd_status fmd_batch_elapsed_ms(fmd_batch* b, double* ms);
 FMD_API fmd_status fmd_batch_time_force(fmd_batch* b, int32_t iters, double* ms_per_launch);
 FMD_API fmd_status fmd_batch_list_stats(fmd_batch* b, int64_t* entries, int32_t* max_per_atom);
 FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n);
 FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_t n);
-/* Autotuner: time each force-kernel variant (neighbor batch 4 or 8, blocks
- * per SM, pipelined list loads) `iters` times on the current state, keep the
- * fastest for all following steps.  chosen = its index; ms_per_variant (cap
- * entries, may be NULL) = device ms per launch of each variant. */
+/* Autotuner: time each force-kernel variant (list entries per batch, blocks
+ * per SM, pipelined list loads) `iters` times on the current state and each
+ * neighbor-list variant on a full rebuild (ballot form, row form), keep the
+ * fastest for all following steps.  chosen = force variant index;
+ * ms_per_variant (cap entries, may be NULL) = device ms per launch of each
+ * force variant (7), then ms per full rebuild of each neighbor variant (2),
+ * then the chosen neighbor variant. */
 FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chosen, double* ms_per_variant,
                                       int32_t cap);
 /* Set the forced rebuild cadence of a replica (the reference rebuilds at
