@@ -262,6 +262,254 @@ def force_profile_traffic():
     return float(m.group(1)) if m else None
 
 
+# --------------------------------------------------------------- workloads
+# The scope table's reported cases beside the headline (one JSON line each):
+#   c0  3,000 beads (30 x 100), Langevin, 5,000 steps: mixed vs plain FP64 vs CPU oracle
+#   c1  30,000 beads: force RMS error vs the FP64 oracle on 10 snapshots; <T>, <P>, Rg
+#       of the mixed form against the plain FP64 form; NVT conserved-quantity drift
+#   c2  1,000,000 beads, two types, NPT: throughput and conserved-quantity drift
+#   c3  256 replicas of uneven size: batched vs the plain form one at a time
+#   c4  served request stream (Poisson arrivals): p50 / p99 latency, throughput
+
+
+def _conf(ens, nsteps, ntypes=1, lj=((0, 0, 1.0, 1.0),), thermo=0):
+    text = (f"ntypes {ntypes}\nrc 2.5\nskin 0.3\ndt 0.001\nnsteps {nsteps}\n{ens}\n"
+            "bond_type 0 30.0 1.5 1.0 1.0\nangle_type 0 5.0 180.0\n")
+    text += "".join(f"lj {a} {b} {e} {g}\n" for a, b, e, g in lj)
+    if thermo:
+        text += f"thermo 1 {thermo} thermo.dat\n"
+    return text
+
+
+def _dev_run(fm, b, nsteps):
+    """Advance a batch nsteps; device milliseconds between events on its stream."""
+    import ctypes as C
+    lib = fm.lib()
+    lib.fmd_batch_mark(b._h, 0)
+    b.run(nsteps)
+    lib.fmd_batch_mark(b._h, 1)
+    ms = C.c_double()
+    lib.fmd_batch_elapsed_ms(b._h, C.byref(ms))
+    return ms.value
+
+
+def _oracle_sim(desc, ens_kw, nthreads=None):
+    from oracle import pyoracle as po
+    s = po.System(xyz=desc.xyz, L=desc.box_L, type=desc.type, mass=np.ones(max(1, int(desc.type.max()) + 1)),
+                  lj=np.ones((1, 1, 2)), bonds=desc.bonds, bond_type=np.zeros(len(desc.bonds), np.int32),
+                  fene=np.array([[30.0, 1.5, 1.0, 1.0]]), angles=desc.angles,
+                  angle_type=np.zeros(len(desc.angles), np.int32), angle_p=np.array([[5.0, np.pi]]),
+                  mol=desc.mol, vel=desc.vel, image=desc.image)
+    return po, s
+
+
+def wl_c0(args, fm):
+    conf = _conf("nvt_langevin 1.0 1.0 1.0 42", 5000, thermo=100)
+    b = fm.Batch(max_replicas=1, max_atoms=4096, device=0)
+    s = b.add(conf, gen=dict(nchains=30, chain_length=100, density=DENSITY, seed=42, pushoff_steps=PUSHOFF))
+    b.run(1)  # push-off and setup
+    x0, v0, i0 = b.state(s)
+    ms = _dev_run(fm, b, 4999)
+    n = 3000
+    mixed = n * 4999 / (ms * 1e-3)
+    t_mixed = b.thermo(s)
+    d = fm.generate_melt(30, 100, density=DENSITY, seed=42)
+    d.xyz, d.vel, d.image = x0, v0, i0
+    ps = fm.Simulation(conf, desc=d, form=fm.FMD_FORM_PLAIN_FP64)
+    t0 = time.perf_counter()
+    ps.step(4999)
+    plain = n * 4999 / (time.perf_counter() - t0)
+    t_plain = ps.thermo()
+    ps.close()
+    po, sysm = _oracle_sim(d, None)
+    threads = os.cpu_count() or 1
+    sim = po.Sim(sysm, ensemble="langevin", T=(1.0, 1.0, 1.0), seed=42, nsteps=5000, nthreads=threads)
+    t0 = time.perf_counter()
+    sim.step(4999)
+    cpu = n * 4999 / (time.perf_counter() - t0)
+    return {"workload": "c0_3k_langevin_5000", "metric": "atom-steps/s", "unit": "atom-steps/s",
+            "mixed_device": mixed, "plain_fp64_wall": plain, "cpu_oracle": cpu, "cpu_threads": threads,
+            "T_final": {"mixed": t_mixed.temp, "plain_fp64": t_plain.temp},
+            "steps": 4999, "note": "one replica; mixed timed on the device, plain and CPU by wall clock"}
+
+
+def wl_c1(args, fm):
+    from oracle import pyoracle as po
+    conf = _conf("nvt_langevin 1.0 1.0 1.0 7", 10 ** 7)
+    b = fm.Batch(max_replicas=2, max_atoms=65536, device=0)
+    s = b.add(conf, gen=dict(nchains=NCHAINS, chain_length=CHAIN_LEN, density=DENSITY, seed=7, pushoff_steps=PUSHOFF))
+    b.run(200)
+    d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=7)
+    errs = []
+    for k in range(10):
+        b.run(100)
+        x, v, img = b.state(s)
+        f, _, _ = b.forces(s)
+        osys = po.System(xyz=x, L=d.box_L, type=d.type, mass=np.ones(1), lj=np.ones((1, 1, 2)), bonds=d.bonds,
+                         bond_type=np.zeros(len(d.bonds), np.int32), fene=np.array([[30.0, 1.5, 1.0, 1.0]]),
+                         angles=d.angles, angle_type=np.zeros(len(d.angles), np.int32),
+                         angle_p=np.array([[5.0, np.pi]]), mol=d.mol)
+        fo, _, _ = po.forces(osys)
+        errs.append(float(np.sqrt(np.mean((f - fo) ** 2)) / np.sqrt(np.mean(fo ** 2))))
+    # <T>, <P>, Rg: mixed and plain FP64 from the same state, 2,000 steps sampled every 20
+    x, v, img = b.state(s)
+    d.xyz, d.vel, d.image = x, v, img
+
+    def sample_batch():
+        out = []
+        for _ in range(100):
+            b.run(20)
+            t = b.thermo(s)
+            p = (t.stress[0] + t.stress[3] + t.stress[5]) / 3.0
+            out.append((t.temp, p, b.rg(s)))
+        return np.array(out)
+
+    def sample_plain():
+        ps = fm.Simulation(conf, desc=d, form=fm.FMD_FORM_PLAIN_FP64)
+        out = []
+        for _ in range(100):
+            ps.step(20)
+            t = ps.thermo()
+            p = (t.stress[0] + t.stress[3] + t.stress[5]) / 3.0
+            out.append((t.temp, p, ps.rg()))
+        ps.close()
+        return np.array(out)
+
+    mb, pl = sample_batch(), sample_plain()
+
+    def ms(a):
+        # mean and standard error with blocks of 10 samples (correlated series)
+        blocks = a[: len(a) // 10 * 10].reshape(10, -1, a.shape[1]).mean(axis=1)
+        return a.mean(axis=0).tolist(), (blocks.std(axis=0, ddof=1) / np.sqrt(len(blocks))).tolist()
+
+    (m_mean, m_err), (p_mean, p_err) = ms(mb), ms(pl)
+    # NVT conserved-quantity drift (nose_hoover test definition), mixed form
+    cn = _conf("nvt_nh 1.0 1.0 0.5 3", 10 ** 7, thermo=0)
+    b2 = fm.Batch(max_replicas=1, max_atoms=65536, device=0)
+    s2 = b2.add(cn, desc=d)
+    b2.run(10)
+    e = []
+    for _ in range(args.drift_chunks):
+        b2.run(1000)
+        e.append(b2.thermo(s2).conserved)
+    e = np.array(e)
+    steps = np.arange(1, len(e) + 1) * 1000.0
+    slope = float(np.polyfit(steps, e, 1)[0]) if len(e) > 1 else 0.0
+    rel_per_1e6 = slope * 1e6 / abs(e[0]) if len(e) else 0.0
+    return {"workload": "c1_30k", "force_rel_rms_vs_fp64_oracle": {"max": max(errs), "mean": float(np.mean(errs)),
+                                                                   "snapshots": len(errs), "target": 1e-5},
+            "langevin_T_P_Rg": {"mixed": {"mean": m_mean, "stderr": m_err},
+                                "plain_fp64": {"mean": p_mean, "stderr": p_err},
+                                "samples": "100 per form, every 20 steps, 2,000 steps from the same state"},
+            "nvt_conserved_drift": {"steps": int(steps[-1]) if len(e) else 0, "E0": float(e[0]) if len(e) else 0.0,
+                                    "slope_per_step": slope, "relative_per_1e6_steps": rel_per_1e6,
+                                    "target_relative_per_1e6": 1e-4}}
+
+
+def wl_c2(args, fm):
+    conf = _conf("npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3", 10 ** 7, ntypes=2,
+                 lj=((0, 0, 1.0, 1.0), (1, 1, 1.0, 1.0), (0, 1, 0.9, 1.0)))
+    b = fm.Batch(max_replicas=1, max_atoms=1_000_200, device=0)
+    t0 = time.perf_counter()
+    s = b.add(conf, gen=dict(nchains=10_000, chain_length=100, density=DENSITY, seed=2, pushoff_steps=PUSHOFF,
+                             type_block=50))
+    b.run(10)
+    setup = time.perf_counter() - t0
+    e, ms_total = [], 0.0
+    for _ in range(args.drift_chunks):
+        ms_total += _dev_run(fm, b, 200)
+        e.append(b.thermo(s).conserved)
+    e = np.array(e)
+    steps = np.arange(1, len(e) + 1) * 200.0
+    slope = float(np.polyfit(steps, e, 1)[0]) if len(e) > 1 else 0.0
+    n = 1_000_000
+    return {"workload": "c2_1m_npt_two_types", "value": n * steps[-1] / (ms_total * 1e-3), "unit": "atom-steps/s",
+            "steps": int(steps[-1]), "setup_s": setup, "box_L_final": b.info(s).box_L,
+            "conserved_drift": {"E0": float(e[0]), "slope_per_step": slope,
+                                "relative_per_1e6_steps": slope * 1e6 / abs(e[0])}}
+
+
+def wl_c3(args, fm):
+    rng = np.random.default_rng(3)
+    reps = []
+    for i in range(256):
+        cl = int(rng.choice([10, 20, 50, 100, 200]))
+        beads = float(np.exp(rng.uniform(np.log(500), np.log(20000))))
+        nc = max(1, int(round(beads / cl)))
+        T = float(rng.uniform(0.5, 1.5))
+        reps.append((nc, cl, T, i))
+    b = fm.Batch(max_replicas=256, max_atoms=sum(nc * cl + 128 for nc, cl, _, _ in reps) + 4096, device=0)
+    slots = [b.add(_conf(f"nvt_langevin {T} {T} 1.0 {i}", 10 ** 7),
+                   gen=dict(nchains=nc, chain_length=cl, density=DENSITY, seed=i, pushoff_steps=PUSHOFF))
+             for nc, cl, T, i in reps]
+    b.run(20)
+    b.autotune(10)
+    k = 1000
+    ms = _dev_run(fm, b, k)
+    natoms = [nc * cl for nc, cl, _, _ in reps]
+    batched = sum(natoms) * k / (ms * 1e-3)
+    # plain FP64, one replica at a time: timed on 8 replicas spread over the
+    # sizes, per-step cost interpolated in size for all 256
+    order = np.argsort(natoms)
+    pick = [int(order[j]) for j in np.linspace(0, len(order) - 1, 8).astype(int)]
+    sizes, per_step = [], []
+    for j in pick:
+        x, v, img = b.state(slots[j])
+        nc, cl, T, i = reps[j]
+        d = fm.generate_melt(nc, cl, density=DENSITY, seed=i)
+        d.xyz, d.vel, d.image = x, v, img
+        ps = fm.Simulation(_conf(f"nvt_langevin {T} {T} 1.0 {i}", 10 ** 7), desc=d, form=fm.FMD_FORM_PLAIN_FP64)
+        ps.step(10)
+        t0 = time.perf_counter()
+        ps.step(200)
+        per_step.append((time.perf_counter() - t0) / 200)
+        sizes.append(natoms[j])
+        ps.close()
+    est = float(np.sum(np.interp(natoms, sizes, per_step))) * k
+    plain = sum(natoms) * k / est
+    return {"workload": "c3_256_uneven_replicas", "value": batched, "unit": "atom-steps/s", "steps": k,
+            "total_atoms": int(sum(natoms)), "plain_fp64_one_at_a_time": plain, "speedup": batched / plain,
+            "plain_sample": {"sizes": sizes, "s_per_step": per_step}}
+
+
+def wl_c4(args, fm):
+    rng = np.random.default_rng(4)
+    srv = fm.Server(max_replicas=256, hbm_budget_gb=150.0, steps_per_round=200, device=0)
+    rate, dur = 20.0, args.serve_seconds
+    t_start = time.perf_counter()
+    t_next, ids, work = 0.0, {}, {}
+    while t_next < dur:
+        now = time.perf_counter() - t_start
+        if now < t_next:
+            time.sleep(min(0.01, t_next - now))
+            continue
+        cl = int(rng.choice([20, 50, 100]))
+        beads = float(np.exp(rng.uniform(np.log(1e3), np.log(1e5))))
+        nc = max(1, int(round(beads / cl)))
+        T = float(rng.uniform(0.8, 1.2))
+        nsteps = int(np.exp(rng.uniform(np.log(1e3), np.log(5e4))) * args.serve_step_scale)
+        rid = srv.submit(_conf(f"nvt_langevin {T} {T} 1.0 {len(ids) + 1}", max(nsteps, 100)),
+                         dict(nchains=nc, chain_length=cl, density=DENSITY, seed=len(ids) + 1, pushoff_steps=200))
+        ids[rid] = time.perf_counter() - t_start
+        work[rid] = nc * cl * max(nsteps, 100)
+        t_next += float(rng.exponential(1.0 / rate))
+    srv.drain(3600.0)
+    res = srv.poll(len(ids) + 8)
+    stats = srv.stats()
+    srv.close()
+    lat = np.array([r.finish_time - r.submit_time for r in res if r.status == 0])
+    span = max(r.finish_time for r in res) - min(r.submit_time for r in res)
+    return {"workload": "c4_served_stream", "requests": len(ids), "completed": int(len(lat)),
+            "arrival_rate_per_s": rate, "duration_s": dur, "nsteps_scale": args.serve_step_scale,
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "mean": float(lat.mean())},
+            "value": stats["atom_steps"] / span, "unit": "atom-steps/s",
+            "offered_atom_steps_per_s": sum(work.values()) / dur}
+
+
+WORKLOADS = {"c0": wl_c0, "c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c4": wl_c4}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -273,8 +521,17 @@ def main():
     ap.add_argument("--ref-gpu-steps", type=int, default=5000, help="steps of the reference GPU datapoint")
     ap.add_argument("--graph-steps", type=int, default=50,
                     help="steps per CUDA graph launch; < 0 launches every step directly (for kernel profilers)")
+    ap.add_argument("--workload", default="headline", choices=["headline"] + sorted(WORKLOADS),
+                    help="headline = the 64 x 30K benchmark; c0..c4 = the reported cases (one GPU)")
+    ap.add_argument("--drift-chunks", type=int, default=20, help="c1 / c2: conserved-quantity samples")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="c4: arrival window")
+    ap.add_argument("--serve-step-scale", type=float, default=0.25, help="c4: scale of the requests' nsteps")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.workload != "headline" and args.impl == "ours":
+        import fastmd_b200 as fm
+        print(json.dumps(WORKLOADS[args.workload](args, fm)), flush=True)
+        return
     rank, world, local, dist = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world, local, dist)
@@ -338,9 +595,10 @@ def main():
         line["clocks"] = clk.summary()
         launched = {k: counts1[k] - counts0[k] for k in counts0}
         line["gpu_launches"] = int(sum(launched.values()))
-        line["autotune"] = {"force_variant": variant, "neighbor_variant": int(variant_ms[9]),
-                            "ms_per_full_rebuild": {"ballot": round(float(variant_ms[7]), 4),
-                                                    "rows": round(float(variant_ms[8]), 4)},
+        line["autotune"] = {"force_variant": variant, "neighbor_variant": int(variant_ms[10]),
+                            "ms_per_full_rebuild": {"ballot m8": round(float(variant_ms[7]), 4),
+                                                    "rows m6": round(float(variant_ms[8]), 4),
+                                                    "ballot m6": round(float(variant_ms[9]), 4)},
                             "ms_per_variant": [round(float(x), 4) for x in variant_ms[:7]],
                             "variants": ["b4 m6 pipelined k1", "b4 m8 pipelined k1", "b4 m6 pipelined k2",
                                          "b4 m8 pipelined k2", "b2 m8 pipelined k4", "b4 m7 pipelined k2",

@@ -104,6 +104,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   FMD_CUDA(cudaSetDevice(device_));
   FMD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
   FMD_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+  FMD_CUDA(cudaStreamCreateWithFlags(&branch_, cudaStreamNonBlocking));
   // graph_steps < 0: no graph (every step launched directly; for profilers
   // that cannot see into graphs with conditional nodes)
   graph_steps_ = o.graph_steps > 0 ? o.graph_steps : (o.graph_steps < 0 ? 0 : 50);
@@ -152,7 +153,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   ang_.alloc(S * kMaxAnglesPerAtom);
   part_.alloc_zero(S / kChunk * kNumPartials);
   kcount_.alloc_zero(kKernelKinds);
-  rb_.alloc_zero(2 + (size_t)max_reps_ + 3 * ((size_t)max_reps_ + 1));
+  rb_.alloc_zero(kRbHead + (size_t)max_reps_ + 3 * ((size_t)max_reps_ + 1));
   cell_cnt_.alloc_zero(c.cells);
   cell_start_.alloc_zero(c.cells);
   cell_fill_.alloc_zero(c.cells);
@@ -174,6 +175,7 @@ Batch::~Batch() {
     if (e) cudaEventDestroy(e);
   if (st_) cudaStreamDestroy(st_);
   if (side_) cudaStreamDestroy(side_);
+  if (branch_) cudaStreamDestroy(branch_);
 }
 
 Dev Batch::dev() const {
@@ -226,6 +228,23 @@ void Batch::upload_reps() {
 }
 
 int Batch::nchunks_launch() const { return (int)std::max<int64_t>(1, slot_alloc_.hwm()); }
+StepShape Batch::shape() const {
+  StepShape g{};
+  g.nchunks = nchunks_launch();
+  g.nreps = nreps_launch();
+  int64_t mc = 1, mh = 1;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used) {
+      const int64_t ga = info_[r].plan.G_alloc;
+      mc = std::max<int64_t>(mc, info_[r].plan.ncell);
+      mh = std::max<int64_t>(mh, ga * ga * ga);
+    }
+  g.max_cells = (int)mc;
+  g.max_home = (int)mh;
+  g.force_variant = force_variant_;
+  g.nbr_variant = nbr_variant_;
+  return g;
+}
 int Batch::nreps_launch() const {
   int m = 0;
   for (int r = 0; r < max_reps_; ++r)
@@ -514,8 +533,7 @@ void Batch::finish_pushoffs() {
     direct = steps % graph_steps_;
   }
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch();
-  for (int64_t k = 0; k < direct; ++k) launch_step(d, nc, nr, force_variant_, nbr_variant_, st_);
+    for (int64_t k = 0; k < direct; ++k) launch_step(d, shape(), &host_mode_, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
   download_reps();
@@ -568,11 +586,7 @@ void Batch::setup(const std::vector<int>& rs) {
   }
   upload_reps();
   // the rebuild work list holds exactly these replicas
-  std::vector<int> wl(2 + rs.size());
-  wl[0] = (int)rs.size();
-  wl[1] = 0;
-  std::copy(rs.begin(), rs.end(), wl.begin() + 2);
-  FMD_CUDA(cudaMemcpyAsync(rb_.p, wl.data(), wl.size() * sizeof(int), cudaMemcpyHostToDevice, st_));
+  write_rebuild_list(rs);
   const Dev d = dev();
   launch_rebuild(d, nreps_launch(), nbr_variant_, st_);
   FMD_CUDA_LAUNCH();
@@ -597,8 +611,7 @@ void Batch::check_status(int r, bool throw_on_fault) {
 
 void Batch::advance_direct(int64_t nsteps) {
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch();
-  for (int64_t k = 0; k < nsteps; ++k) launch_step(d, nc, nr, force_variant_, nbr_variant_, st_);
+    for (int64_t k = 0; k < nsteps; ++k) launch_step(d, shape(), &host_mode_, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
 }
@@ -610,11 +623,10 @@ void Batch::ensure_graph() {
     graph_exec_ = nullptr;
   }
   const Dev d = dev();
-  const int nc = nchunks_launch(), nr = nreps_launch();
-  cudaGraph_t g;
+    cudaGraph_t g;
   FMD_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   try {
-    for (int k = 0; k < graph_steps_; ++k) capture_step(d, nc, nr, force_variant_, nbr_variant_, st_, side_);
+    for (int k = 0; k < graph_steps_; ++k) capture_step(d, shape(), st_, side_, branch_);
   } catch (...) {
     cudaGraph_t partial = nullptr;
     cudaStreamEndCapture(st_, &partial);
@@ -654,8 +666,7 @@ void Batch::run(int64_t nsteps, bool respect_nsteps) {
   }
   if (need > 0) {
     const Dev d = dev();
-    const int nc = nchunks_launch(), nr = nreps_launch();
-    for (int64_t k = 0; k < need; ++k) launch_step(d, nc, nr, force_variant_, nbr_variant_, st_);
+        for (int64_t k = 0; k < need; ++k) launch_step(d, shape(), &host_mode_, st_);
     FMD_CUDA_LAUNCH();
   }
   FMD_CUDA(cudaStreamSynchronize(st_));
@@ -751,13 +762,9 @@ double Batch::time_rebuild(int iters, int v) {
   for (int r = 0; r < max_reps_; ++r)
     if (info_[r].used && h_reps_[r].active) rs.push_back(r);
   if (rs.empty()) return 0.0;
-  std::vector<int> wl(2 + rs.size());
-  wl[0] = (int)rs.size();
-  wl[1] = 0;
-  std::copy(rs.begin(), rs.end(), wl.begin() + 2);
   const Dev d = dev();
   auto once = [&] {
-    FMD_CUDA(cudaMemcpyAsync(rb_.p, wl.data(), wl.size() * sizeof(int), cudaMemcpyHostToDevice, st_));
+    write_rebuild_list(rs);
     launch_rebuild(d, nreps_launch(), v, st_);
   };
   once();
@@ -872,6 +879,15 @@ void Batch::read_state(int r, double* xyz, double* vel, int32_t* image, bool rew
       vel[3 * id + 2] = (double)hv[s].z * R.pending_scale;
     }
   }
+}
+
+// The rebuild work list holds exactly these replicas (a host-driven rebuild).
+void Batch::write_rebuild_list(const std::vector<int>& rs) {
+  wl_.assign(kRbHead + rs.size(), 0);
+  wl_[kRbCount] = (int)rs.size();
+  wl_[kRbMode] = kRbList;
+  std::copy(rs.begin(), rs.end(), wl_.begin() + kRbHead);
+  FMD_CUDA(cudaMemcpyAsync(rb_.p, wl_.data(), wl_.size() * sizeof(int), cudaMemcpyHostToDevice, st_));
 }
 
 void Batch::launch_counts(int64_t* counts, int n) {

@@ -87,6 +87,8 @@ class Batch {
   Dev dev() const;
   int nchunks_launch() const;
   int nreps_launch() const;
+  StepShape shape() const;
+  void write_rebuild_list(const std::vector<int>& rs);
   int graph_steps() const { return graph_steps_; }
   void set_max_between(int r, int k);
   void mark(int which);
@@ -111,11 +113,12 @@ class Batch {
 
   int device_ = 0;
   cudaStream_t st_ = nullptr;
-  cudaStream_t side_ = nullptr;  // captures conditional-node bodies
+  cudaStream_t side_ = nullptr;    // captures conditional-node bodies
+  cudaStream_t branch_ = nullptr;  // second branch of a captured step
   int graph_steps_ = 50;
   int force_variant_ = 0;
   int nbr_variant_ = 0;
-  double nbr_ms_[kNbrVariants] = {0, 0};
+  double nbr_ms_[kNbrVariants] = {0, 0, 0};
   int max_reps_ = 256;
   BatchCaps caps_;
   int64_t budget_bytes_ = 0, bytes_in_use_ = 0, bytes_ = 0;
@@ -129,6 +132,8 @@ class Batch {
   DevBuf<double> part_;
   DevBuf<unsigned long long> kcount_;
   DevBuf<int> rb_;  // rebuild work list
+  std::vector<int> wl_;  // host staging of a host-written work list (kept alive for the async copy)
+  int host_mode_ = 0;  // rebuild form of the current step, read back by direct-launch steps
   DevBuf<int32_t> cell_cnt_, cell_start_, cell_fill_;
   DevBuf<int2> bent_;
   DevBuf<int4> aent_;

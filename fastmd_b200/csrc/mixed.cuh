@@ -177,9 +177,9 @@ struct Dev {
   int32_t* ncnt;
   double* part;                  // [chunks][kNumPartials]
   unsigned long long* kcount;    // [kKernelKinds] launches executed (block 0 of each launch counts)
-  // rebuild work list: [0] count, [1] done blocks, [2, 2 + rb_cap) replicas,
-  // then three offset arrays of rb_cap + 1 (chunk items, cell-group items,
-  // home-cell items)
+  // rebuild work list: header (RbHeader), rb_cap replicas, then three
+  // offset arrays of rb_cap + 1 (chunk items, cell-group items, home-cell
+  // items)
   int* rb;
   int rb_cap;
 };
@@ -237,15 +237,32 @@ __host__ __device__ inline int w_type(uint32_t u) { return (int)(u >> 27); }
 // of replicas that need no work return at once).
 struct StepConds {
   int use;
-  cudaGraphConditionalHandle rebuild, force_plain, force_ev, post;
+  cudaGraphConditionalHandle rebuild, rebuild_full, force_plain, force_ev, post;
 };
+
+// Rebuild work list header (ints at the front of Dev::rb).
+enum RbHeader : int { kRbCount = 0, kRbCommits = 1, kRbMode = 2, kRbHead = 4 };
+enum RbMode : int { kRbNone = 0, kRbList = 1, kRbFull = 2 };
+constexpr int kRbFullMin = 8;  // replicas rebuilding in one step before full grids pay
+
+// Launch geometry of a step for the current batch layout.
+struct StepShape {
+  int nchunks, nreps;   // chunk blocks, replica-indexed blocks
+  int max_cells;        // largest P^3 (Morton cells) over replicas
+  int max_home;         // largest G_alloc^3 (home cells) over replicas
+  int force_variant, nbr_variant;
+};
+using RebuildShape = StepShape;
 constexpr int kForceVariants = 7;
-constexpr int kNbrVariants = 2;
-void launch_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st);
+constexpr int kNbrVariants = 3;
+// One step with direct launches.  The rebuild form is read back from the
+// device after the per-replica commits (one small host read per step).
+void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t st);
 // The same step recorded into the graph being captured on st, with the
 // conditional nodes; side is a second stream used to capture their bodies.
-void capture_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st,
-                  cudaStream_t side);
+// st2: a second capture stream for the parallel branches of a step.
+void capture_step(const Dev& d, const StepShape& g, cudaStream_t st, cudaStream_t side, cudaStream_t st2);
+void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st);
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st);
 // Rebuild of the replicas on the work list (rb): bin, scan, scatter, cell sort,
 // permute, bonded tables, neighbor lists.

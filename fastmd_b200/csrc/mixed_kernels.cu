@@ -141,6 +141,12 @@ __device__ __forceinline__ void count_launch(const Dev& d, int kind) {
 // ---------------------------------------------------------------- pre-force
 __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   count_launch(d, kKPre);
+  // the previous step's rebuild has finished: empty the work list before
+  // this step's commits append to it
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d.rb[kRbCount] = 0;
+    d.rb[kRbMode] = kRbNone;
+  }
   const int4 ci = d.chunk_rep[blockIdx.x];
   if (ci.x < 0) return;
   const int s = ci.y + threadIdx.x;
@@ -243,12 +249,31 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
 // Per-replica commit of the pre-force update (one thread per replica, after
 // every pre-force block finished): step counter, chain / barostat state, box,
 // the rebuild decision and the graph's conditional switches.
+__device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& cond);
+
 __global__ void __launch_bounds__(32) k_commit(Dev d, StepConds cond) {
   count_launch(d, kKCommit);
   const int r = blockIdx.x;
-  if (threadIdx.x != 0 || r >= d.rb_cap) return;
-  Rep& R = d.reps[r];
-  if (!(R.active && R.step < R.stop_step)) return;  // did not advance this step
+  if (threadIdx.x != 0) return;
+  if (r < d.rb_cap) {
+    Rep& R = d.reps[r];
+    if (R.active && R.step < R.stop_step) commit_replica(d, R, r, cond);  // advanced this step
+  }
+  // The last block chooses how this step rebuilds: the work-list kernels for
+  // a few replicas, full grids (one block per chunk / home cell of every
+  // replica) when many rebuild at once.
+  __threadfence();
+  if (atomicAdd(d.rb + kRbCommits, 1) != (int)gridDim.x - 1) return;
+  __threadfence();
+  d.rb[kRbCommits] = 0;
+  const int n = d.rb[kRbCount];
+  const int mode = n == 0 ? kRbNone : (n >= kRbFullMin && 4 * n >= (int)gridDim.x ? kRbFull : kRbList);
+  d.rb[kRbMode] = mode;
+  if (cond.use && mode == kRbList) cudaGraphSetConditional(cond.rebuild, 1u);
+  if (cond.use && mode == kRbFull) cudaGraphSetConditional(cond.rebuild_full, 1u);
+}
+
+__device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& cond) {
   StepScalars S;
   if (R.next_valid) S = R.next;
   else compute_step_scalars(R, S);
@@ -271,7 +296,7 @@ __global__ void __launch_bounds__(32) k_commit(Dev d, StepConds cond) {
     R.maxdisp_bits = 0u;
     R.rebuilds += 1;
     R.rebuild_now = 1;
-    d.rb[2 + atomicAdd(d.rb, 1)] = r;
+    d.rb[kRbHead + atomicAdd(d.rb + kRbCount, 1)] = r;
   } else {
     R.rebuild_now = 0;
   }
@@ -283,8 +308,7 @@ __global__ void __launch_bounds__(32) k_commit(Dev d, StepConds cond) {
   const bool post = !cond.use || !langevin || need_ev(R) || R.step >= R.stop_step;
   R.defer = post ? 0 : 1;
   if (cond.use) {
-    // any replica that rebuilds / needs a force variant / a post switches it on
-    if (R.rebuild_now) cudaGraphSetConditional(cond.rebuild, 1u);
+    // any replica that needs a force variant / a post switches it on
     cudaGraphSetConditional(need_ev(R) ? cond.force_ev : cond.force_plain, 1u);
     if (post) cudaGraphSetConditional(cond.post, 1u);
   }
@@ -334,11 +358,13 @@ __host__ __device__ inline int nbr_items(int G) { return G >= 3 ? G * G * ((G + 
 // rebuilds this step; k_rbplan turns the list into prefix offsets of chunk
 // and cell-group work items; the rebuild kernels run fixed grids that stride
 // over those items only, so a step where a few replicas rebuild costs work
-// for those replicas, not early exits over the whole batch.  The last block
-// of the neighbor-list kernel empties the list for the next step.
-__device__ __forceinline__ int rb_count(const Dev& d) { return d.rb[0]; }
-__device__ __forceinline__ int rb_rep(const Dev& d, int i) { return d.rb[2 + i]; }
-__device__ __forceinline__ int* rb_off(const Dev& d, int which) { return d.rb + 2 + d.rb_cap + which * (d.rb_cap + 1); }
+// for those replicas, not early exits over the whole batch.  The next step's
+// pre-force kernel empties the list.
+__device__ __forceinline__ int rb_count(const Dev& d) { return d.rb[kRbCount]; }
+__device__ __forceinline__ int rb_rep(const Dev& d, int i) { return d.rb[kRbHead + i]; }
+__device__ __forceinline__ int* rb_off(const Dev& d, int which) {
+  return d.rb + kRbHead + d.rb_cap + which * (d.rb_cap + 1);
+}
 
 // index i with off[i] <= item < off[i + 1]
 __device__ __forceinline__ int rb_find(const int* off, int n, int item) {
@@ -395,9 +421,31 @@ __global__ void __launch_bounds__(1024) k_rbplan_home(Dev d, int variant) {
   const int n = rb_count(d);
   rb_scan(d, n, rb_off(d, 2), [&](int r) {
     const int G = d.reps[r].G;
-    return variant == 0 ? G * G * G : nbr_items(G);
+    return variant == 1 ? nbr_items(G) : G * G * G;
   });
 }
+
+// A block visits its items in increasing order, so the list entry of an item
+// only moves forward: one search for the first item, then a step when an
+// item passes the next offset.
+struct RbCursor {
+  const int* off;
+  int n, i, lo, hi;
+  __device__ __forceinline__ RbCursor(const int* o, int nn, int first) : off(o), n(nn), i(0), lo(0), hi(0) {
+    if (n > 0 && first < off[n]) {
+      i = rb_find(off, n, first);
+      lo = off[i];
+      hi = off[i + 1];
+    }
+  }
+  __device__ __forceinline__ void seek(int item) {
+    while (item >= hi) {
+      ++i;
+      lo = hi;
+      hi = off[i + 1];
+    }
+  }
+};
 
 // Calls body(R, r, chunk index within the replica) for this block's chunk items.
 template <typename F>
@@ -405,10 +453,11 @@ __device__ __forceinline__ void for_rebuild_chunks(const Dev& d, F body) {
   const int n = rb_count(d);
   const int* off = rb_off(d, 0);
   const int total = n > 0 ? off[n] : 0;
+  RbCursor cur(off, n, blockIdx.x);
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int i = rb_find(off, n, item);
-    const int r = rb_rep(d, i);
-    body(d.reps[r], r, item - off[i]);
+    cur.seek(item);
+    const int r = rb_rep(d, cur.i);
+    body(d.reps[r], r, item - cur.lo);
   }
 }
 
@@ -544,10 +593,11 @@ __global__ void __launch_bounds__(32 * kCellGroup) k_cellsort(Dev d) {
   const int* off = rb_off(d, 1);
   const int total = n > 0 ? off[n] : 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  RbCursor cur(off, n, blockIdx.x);
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int i = rb_find(off, n, item);
-    const Rep& R = d.reps[rb_rep(d, i)];
-    const int c = (item - off[i]) * kCellGroup + warp;
+    cur.seek(item);
+    const Rep& R = d.reps[rb_rep(d, cur.i)];
+    const int c = (item - cur.lo) * kCellGroup + warp;
     if (c < R.P * R.P * R.P) cellsort_cell(d, R, c, lane);
   }
 }
@@ -984,31 +1034,23 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
   if (overflow) atomicOr(&R.status, overflow);
 }
 
-// Neighbor-list kernel variants: 0 = ballot form (one home cell per item),
-// 1 = row form (kNbrRow home cells per item); the autotuner picks one.
-template <int V>
-__global__ void __launch_bounds__(kNbrThreads, V == 0 ? 8 : 6) k_neighbors(Dev d) {
+// Neighbor-list kernel variants: V = 0 ballot form (one home cell per item),
+// V = 1 row form (kNbrRow home cells per item); MINB = blocks per SM the
+// registers are fitted to.  The autotuner picks one.
+template <int V, int MINB>
+__global__ void __launch_bounds__(kNbrThreads, MINB) k_neighbors(Dev d) {
   count_launch(d, kKNeighbors);
   const int n = rb_count(d);
   const int* off = rb_off(d, 2);
   const int total = n > 0 ? off[n] : 0;
+  RbCursor cur(off, n, blockIdx.x);
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
-    const int i = rb_find(off, n, item);
+    cur.seek(item);
     __syncthreads();  // the previous item's shared staging is no longer read
     if (V == 0)
-      neighbors_cell_ballot(d, d.reps[rb_rep(d, i)], item - off[i]);
+      neighbors_cell_ballot(d, d.reps[rb_rep(d, cur.i)], item - cur.lo);
     else
-      neighbors_row(d, d.reps[rb_rep(d, i)], item - off[i]);
-  }
-  // the last block to finish empties the work list for the next step
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(d.rb + 1, 1) == (int)gridDim.x - 1) {
-      d.rb[0] = 0;
-      d.rb[1] = 0;
-      __threadfence();
-    }
+      neighbors_row(d, d.reps[rb_rep(d, cur.i)], item - cur.lo);
   }
 }
 
@@ -1086,11 +1128,13 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
   const float sr6 = sr2 * sr2 * sr2;
   float fr = e24 * r2inv * sr6 * (2.0f * sr6 - 1.0f);
   fr = in ? fminf(fmaxf(fr, -1000.0f), 1000.0f) : 0.0f;  // lj.cu:48
-  const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
-  a.fx += fxij;
-  a.fy += fyij;
-  a.fz += fzij;
+  // The force sums are written as explicit FMAs, so both flavours (with and
+  // without energies) round them identically.
+  a.fx = fmaf(fr, dx, a.fx);
+  a.fy = fmaf(fr, dy, a.fy);
+  a.fz = fmaf(fr, dz, a.fz);
   if (EV) {
+    const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
     const float e = in ? e24 * (1.0f / 12.0f) * (sr6 * (sr6 - 1.0f)) : 0.0f;  // 1/2 * 4 eps (sr12 - sr6)
     a.pe += e;
     a.v0 = fmaf(fxij, dx, a.v0);
@@ -1182,12 +1226,14 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
   const float sn = fmaxf(sqrtf(1.0f - cs * cs), 1e-6f);
   const float pref = 2.0f * kt * dth * __fdividef(1.0f, sn);
   const float rr = rij_inv * rkj_inv, i2 = rij_inv * rij_inv, k2 = rkj_inv * rkj_inv;
-  const float fix = pref * (dkj.x * rr - cs * dij.x * i2);
-  const float fiy = pref * (dkj.y * rr - cs * dij.y * i2);
-  const float fiz = pref * (dkj.z * rr - cs * dij.z * i2);
-  const float fkx = pref * (dij.x * rr - cs * dkj.x * k2);
-  const float fky = pref * (dij.y * rr - cs * dkj.y * k2);
-  const float fkz = pref * (dij.z * rr - cs * dkj.z * k2);
+  // explicit roundings: the products feed the force sums in both flavours
+  const float ci2 = __fmul_rn(cs, i2), ck2 = __fmul_rn(cs, k2);
+  const float fix = __fmul_rn(pref, fmaf(dkj.x, rr, -__fmul_rn(ci2, dij.x)));
+  const float fiy = __fmul_rn(pref, fmaf(dkj.y, rr, -__fmul_rn(ci2, dij.y)));
+  const float fiz = __fmul_rn(pref, fmaf(dkj.z, rr, -__fmul_rn(ci2, dij.z)));
+  const float fkx = __fmul_rn(pref, fmaf(dij.x, rr, -__fmul_rn(ck2, dkj.x)));
+  const float fky = __fmul_rn(pref, fmaf(dij.y, rr, -__fmul_rn(ck2, dkj.y)));
+  const float fkz = __fmul_rn(pref, fmaf(dij.z, rr, -__fmul_rn(ck2, dkj.z)));
   fx.add(role == 0 ? fix : (role == 2 ? fkx : -(fix + fkx)));
   fy.add(role == 0 ? fiy : (role == 2 ? fky : -(fiy + fky)));
   fz.add(role == 0 ? fiz : (role == 2 ? fkz : -(fiz + fkz)));
@@ -1291,12 +1337,12 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
         const float r2inv = __fdividef(1.0f, r2s);
         const float sr2 = sig2 * r2inv;
         const float sr6 = sr2 * sr2 * sr2;
-        ff += 24.0f * eps * r2inv * sr6 * (2.0f * sr6 - 1.0f);
-        wpe = 4.0f * eps * sr6 * (sr6 - 1.0f) + eps;
+        ff = fmaf(24.0f * eps * r2inv * sr6, 2.0f * sr6 - 1.0f, ff);
+        if (EV) wpe = 4.0f * eps * sr6 * (sr6 - 1.0f) + eps;
       }
-      fx.add(ff * dr.x);
-      fy.add(ff * dr.y);
-      fz.add(ff * dr.z);
+      fx.add(__fmul_rn(ff, dr.x));
+      fy.add(__fmul_rn(ff, dr.y));
+      fz.add(__fmul_rn(ff, dr.z));
       if (EV) {
         pe += 0.5f * (-0.5f * kf * R02 * log1pf(-r2s / R02) + wpe);
         if ((bw >> 30) & 1) {
@@ -1435,6 +1481,60 @@ __global__ void __launch_bounds__(32) k_post_commit(Dev d, int kick) {
   }
 }
 
+// ---- full-grid rebuild kernels: one block per chunk / cell group / home
+// cell of every replica (blocks of replicas that do not rebuild return at
+// once).  Used when many replicas rebuild in the same step, where they beat
+// the persistent work-list kernels.
+__global__ void __launch_bounds__(kChunk) k_bin_g(Dev d) {
+  count_launch(d, kKBin);
+  const int4 ci = d.chunk_rep[blockIdx.x];
+  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  bin_chunk(d, d.reps[ci.x], ci.w);
+}
+
+__global__ void __launch_bounds__(kChunk) k_scatter_g(Dev d) {
+  count_launch(d, kKScatter);
+  const int4 ci = d.chunk_rep[blockIdx.x];
+  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  const Rep& R = d.reps[ci.x];
+  const int local = ci.w * kChunk + threadIdx.x;
+  if (local >= R.natoms) return;
+  const int s = R.slot_base + local;
+  const int at = atomicAdd(&d.cell_fill[R.cell_base + d.key[s]], 1);
+  d.bucket[R.slot_base + at] = local;
+}
+
+__global__ void __launch_bounds__(32 * kCellGroup) k_cellsort_g(Dev d) {
+  count_launch(d, kKCellsort);
+  if ((int)blockIdx.y >= rb_count(d)) return;
+  const Rep& R = d.reps[rb_rep(d, blockIdx.y)];
+  const int c = blockIdx.x * kCellGroup + (threadIdx.x >> 5);
+  if (c < R.P * R.P * R.P) cellsort_cell(d, R, c, threadIdx.x & 31);
+}
+
+__global__ void __launch_bounds__(kChunk) k_permute_g(Dev d) {
+  count_launch(d, kKPermute);
+  const int4 ci = d.chunk_rep[blockIdx.x];
+  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  permute_chunk(d, d.reps[ci.x], ci.w);
+}
+
+__global__ void __launch_bounds__(kChunk) k_topo_g(Dev d) {
+  count_launch(d, kKTopo);
+  const int4 ci = d.chunk_rep[blockIdx.x];
+  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  topo_chunk(d, d.reps[ci.x], ci.w);
+}
+
+__global__ void __launch_bounds__(kNbrThreads) k_neighbors_g(Dev d) {
+  count_launch(d, kKNeighbors);
+  if ((int)blockIdx.y >= rb_count(d)) return;
+  Rep& R = d.reps[rb_rep(d, blockIdx.y)];
+  const int G = R.G;
+  if ((int)blockIdx.x >= G * G * G) return;
+  neighbors_cell_ballot(d, R, blockIdx.x);
+}
+
 // ---------------------------------------------------------------- launchers
 namespace {
 int num_sms() {
@@ -1447,14 +1547,18 @@ int num_sms() {
 }
 }  // namespace
 
-void launch_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st) {
-  k_pre<<<nchunks, kChunk, 0, st>>>(d, StepConds{0, 0, 0, 0, 0});
-  k_commit<<<nreps, 32, 0, st>>>(d, StepConds{0, 0, 0, 0, 0});
-  launch_rebuild(d, nreps, nbr_variant, st);
-  launch_force(d, nchunks, false, force_variant, st);
-  launch_force(d, nchunks, true, force_variant, st);
-  k_post<<<nchunks, kChunk, 0, st>>>(d, 1);
-  k_post_commit<<<nreps, 32, 0, st>>>(d, 1);
+void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t st) {
+  const StepConds none{0, 0, 0, 0, 0, 0};
+  k_pre<<<g.nchunks, kChunk, 0, st>>>(d, none);
+  k_commit<<<g.nreps, 32, 0, st>>>(d, none);
+  FMD_CUDA(cudaMemcpyAsync(host_mode, d.rb + kRbMode, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FMD_CUDA(cudaStreamSynchronize(st));
+  if (*host_mode == kRbList) launch_rebuild(d, g.nreps, g.nbr_variant, st);
+  if (*host_mode == kRbFull) launch_rebuild_full(d, g, st);
+  launch_force(d, g.nchunks, false, g.force_variant, st);
+  launch_force(d, g.nchunks, true, g.force_variant, st);
+  k_post<<<g.nchunks, kChunk, 0, st>>>(d, 1);
+  k_post_commit<<<g.nreps, 32, 0, st>>>(d, 1);
 }
 
 namespace {
@@ -1484,25 +1588,54 @@ void capture_if(cudaStream_t st, cudaStream_t side, cudaGraphConditionalHandle h
 }
 }  // namespace
 
-void capture_step(const Dev& d, int nchunks, int nreps, int force_variant, int nbr_variant, cudaStream_t st,
-                  cudaStream_t side) {
+void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStream_t side, cudaStream_t st2) {
+  const int nchunks = shape.nchunks, nreps = shape.nreps, force_variant = shape.force_variant,
+            nbr_variant = shape.nbr_variant;
   cudaStreamCaptureStatus cs;
   cudaGraph_t g;
   FMD_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
-  StepConds c{1, 0, 0, 0, 0};
+  StepConds c{1, 0, 0, 0, 0, 0};
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild, g, 0u, cudaGraphCondAssignDefault));
+  FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild_full, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_plain, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
   k_pre<<<nchunks, kChunk, 0, st>>>(d, c);
   k_commit<<<nreps, 32, 0, st>>>(d, c);
-  capture_if(st, side, c.rebuild, [&](cudaStream_t s) { launch_rebuild(d, nreps, nbr_variant, s); });
-  capture_if(st, side, c.force_plain, [&](cudaStream_t s) { launch_force(d, nchunks, false, force_variant, s); });
-  capture_if(st, side, c.force_ev, [&](cudaStream_t s) { launch_force(d, nchunks, true, force_variant, s); });
+  // The two rebuild forms exclude each other, and so do the replicas each
+  // force flavour serves: each pair is captured as parallel branches so the
+  // step's critical path has one conditional node per phase.
+  cudaEvent_t fork, join;
+  FMD_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  FMD_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  auto parallel = [&](auto&& a, auto&& b) {
+    FMD_CUDA(cudaEventRecord(fork, st));
+    FMD_CUDA(cudaStreamWaitEvent(st2, fork, 0));
+    a(st);
+    b(st2);
+    FMD_CUDA(cudaEventRecord(join, st2));
+    FMD_CUDA(cudaStreamWaitEvent(st, join, 0));
+  };
+  parallel(
+      [&](cudaStream_t s0) {
+        capture_if(s0, side, c.rebuild, [&](cudaStream_t s) { launch_rebuild(d, nreps, nbr_variant, s); });
+      },
+      [&](cudaStream_t s1) {
+        capture_if(s1, side, c.rebuild_full, [&](cudaStream_t s) { launch_rebuild_full(d, shape, s); });
+      });
+  parallel(
+      [&](cudaStream_t s0) {
+        capture_if(s0, side, c.force_plain, [&](cudaStream_t s) { launch_force(d, nchunks, false, force_variant, s); });
+      },
+      [&](cudaStream_t s1) {
+        capture_if(s1, side, c.force_ev, [&](cudaStream_t s) { launch_force(d, nchunks, true, force_variant, s); });
+      });
   capture_if(st, side, c.post, [&](cudaStream_t s) {
     k_post<<<nchunks, kChunk, 0, s>>>(d, 1);
     k_post_commit<<<nreps, 32, 0, s>>>(d, 1);
   });
+  FMD_CUDA(cudaEventDestroy(fork));
+  FMD_CUDA(cudaEventDestroy(join));
 }
 
 namespace {
@@ -1516,11 +1649,23 @@ int resident_grid(K kernel, int threads) {
 }
 }  // namespace
 
+void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st) {
+  const int nr = g.nreps;
+  k_bin_g<<<g.nchunks, kChunk, 0, st>>>(d);
+  k_scan<<<nr, 1024, 0, st>>>(d);
+  k_scatter_g<<<g.nchunks, kChunk, 0, st>>>(d);
+  k_cellsort_g<<<dim3((g.max_cells + kCellGroup - 1) / kCellGroup, nr), 32 * kCellGroup, 0, st>>>(d);
+  k_permute_g<<<g.nchunks, kChunk, 0, st>>>(d);
+  k_topo_g<<<g.nchunks, kChunk, 0, st>>>(d);
+  k_neighbors_g<<<dim3(g.max_home, nr), kNbrThreads, 0, st>>>(d);
+}
+
 void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
   static const int g_bin = resident_grid(k_bin, kChunk), g_scatter = resident_grid(k_scatter, kChunk),
                    g_sort = resident_grid(k_cellsort, 32 * kCellGroup), g_perm = resident_grid(k_permute, kChunk),
-                   g_topo = resident_grid(k_topo, kChunk), g_nbr0 = resident_grid(k_neighbors<0>, kNbrThreads),
-                   g_nbr1 = resident_grid(k_neighbors<1>, kNbrThreads);
+                   g_topo = resident_grid(k_topo, kChunk), g_nbr0 = resident_grid(k_neighbors<0, 8>, kNbrThreads),
+                   g_nbr1 = resident_grid(k_neighbors<1, 6>, kNbrThreads),
+                   g_nbr2 = resident_grid(k_neighbors<0, 6>, kNbrThreads);
   k_rbplan<<<1, 1024, 0, st>>>(d);
   k_bin<<<g_bin, kChunk, 0, st>>>(d);
   k_scan<<<nreps, 1024, 0, st>>>(d);
@@ -1529,28 +1674,38 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
   k_permute<<<g_perm, kChunk, 0, st>>>(d);
   k_topo<<<g_topo, kChunk, 0, st>>>(d);
   k_rbplan_home<<<1, 1024, 0, st>>>(d, nbr_variant);
-  if (nbr_variant == 0)
-    k_neighbors<0><<<g_nbr0, kNbrThreads, 0, st>>>(d);
+  if (nbr_variant == 1)
+    k_neighbors<1, 6><<<g_nbr1, kNbrThreads, 0, st>>>(d);
+  else if (nbr_variant == 2)
+    k_neighbors<0, 6><<<g_nbr2, kNbrThreads, 0, st>>>(d);
   else
-    k_neighbors<1><<<g_nbr1, kNbrThreads, 0, st>>>(d);
+    k_neighbors<0, 8><<<g_nbr0, kNbrThreads, 0, st>>>(d);
 }
 
-// Force-kernel variants (list batch, blocks per SM, pipelined list loads);
-// the batch's autotuner picks one.  The energy variant is fixed.
-void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st) {
-  if (ev) {
-    k_force<true, 4, 5, true, 2><<<nchunks, kChunk, 0, st>>>(d);
-    return;
-  }
+// Force-kernel variants (list entries per batch, blocks per SM, pipelined
+// list loads, batches per compensated add); the batch's autotuner picks one.
+// The energy flavour of a variant walks the list in the same batches with
+// the same compensated adds, so its forces are bit-identical: energy steps
+// and host re-evaluations do not perturb a trajectory.
+template <bool EV>
+void launch_force_t(const Dev& d, int nchunks, int variant, cudaStream_t st) {
+  constexpr int E = 5;  // blocks per SM of the energy flavours (more registers)
   switch (variant) {
-    case 1: k_force<false, 4, 8, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 2: k_force<false, 4, 6, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 3: k_force<false, 4, 8, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 4: k_force<false, 2, 8, true, 4><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 5: k_force<false, 4, 7, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 6: k_force<false, 8, 6, false, 1><<<nchunks, kChunk, 0, st>>>(d); break;
-    default: k_force<false, 4, 6, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 1: k_force<EV, 4, EV ? E : 8, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 2: k_force<EV, 4, EV ? E : 6, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 3: k_force<EV, 4, EV ? E : 8, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 4: k_force<EV, 2, EV ? E : 8, true, 4><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 5: k_force<EV, 4, EV ? E : 7, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 6: k_force<EV, 8, EV ? E : 6, false, 1><<<nchunks, kChunk, 0, st>>>(d); break;
+    default: k_force<EV, 4, EV ? E : 6, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
   }
+}
+
+void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st) {
+  if (ev)
+    launch_force_t<true>(d, nchunks, variant, st);
+  else
+    launch_force_t<false>(d, nchunks, variant, st);
 }
 
 void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st) {

@@ -250,10 +250,11 @@ FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n);
 FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_t n);
 /* Autotuner: time each force-kernel variant (list entries per batch, blocks
  * per SM, pipelined list loads) `iters` times on the current state and each
- * neighbor-list variant on a full rebuild (ballot form, row form), keep the
+ * neighbor-list variant on a full rebuild (ballot form with 8 or 6 blocks
+ * per SM, row form), keep the
  * fastest for all following steps.  chosen = force variant index;
  * ms_per_variant (cap entries, may be NULL) = device ms per launch of each
- * force variant (7), then ms per full rebuild of each neighbor variant (2),
+ * force variant (7), then ms per full rebuild of each neighbor variant (3),
  * then the chosen neighbor variant. */
 FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chosen, double* ms_per_variant,
                                       int32_t cap);

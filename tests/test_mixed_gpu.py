@@ -156,3 +156,57 @@ def test_graph_steps_equal_direct_steps(ens):
         for a, c in zip(sa, sb):
             assert np.array_equal(a, c)
         assert np.array_equal(ta, tb)
+
+
+@pytest.mark.parametrize("ens", ["nvt_langevin 1.0 1.0 1.0 9", "nvt_nh 1.0 1.0 0.5 3"])
+def test_observing_does_not_perturb(ens):
+    """Reading thermo / Rg / forces between runs re-evaluates energies with
+    the energy flavour of the force kernel; the trajectory stays bit-identical
+    to an unobserved run."""
+    conf = run_conf(ensemble=ens, nsteps=10_000)
+    m = _melt(15, 40, seed=31)
+    a = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    sa = a.add(conf, desc=m)
+    a.run(120)
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    sb = b.add(conf, desc=m)
+    for _ in range(4):
+        b.run(30)
+        b.thermo(sb)
+        b.rg(sb)
+        b.forces(sb)
+    for x, y in zip(a.state(sa), b.state(sb)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.thermo(sa).as_array(), b.thermo(sb).as_array())
+    a.close()
+    b.close()
+
+
+def test_server_results_equal_alone_and_in_mix():
+    """Continuous batching: requests admitted while others run, retired and
+    back-filled, give the same final thermo row and Rg as the same request
+    run alone."""
+    reqs = []
+    for k, (nc, cl, steps) in enumerate([(10, 20, 300), (8, 50, 500), (20, 30, 200), (5, 100, 400), (12, 40, 350)]):
+        T = 0.8 + 0.1 * k
+        conf = run_conf(ensemble=f"nvt_langevin {T} {T} 1.0 {k + 1}", nsteps=steps)
+        gen = dict(nchains=nc, chain_length=cl, density=0.85, seed=100 + k, pushoff_steps=300)
+        reqs.append((conf, gen))
+    srv = fm.Server(max_replicas=3, hbm_budget_gb=8.0, steps_per_round=50)
+    ids = []
+    for conf, gen in reqs:
+        ids.append(srv.submit(conf, gen))
+    srv.drain(600.0)
+    got = {r.request_id: r for r in srv.poll(64)}
+    srv.close()
+    assert sorted(got) == sorted(ids)
+    for rid, (conf, gen) in zip(ids, reqs):
+        r = got[rid]
+        assert r.status == 0
+        alone = fm.Batch(max_replicas=1, max_atoms=1 << 14)
+        s = alone.add(conf, gen=gen)
+        alone.run(10_000)  # stops at the request's nsteps
+        assert alone.info(s).step == r.steps
+        assert np.array_equal(alone.thermo(s).as_array(), np.asarray(r.thermo.as_array()))
+        assert alone.rg(s) == r.rg
+        alone.close()
