@@ -489,22 +489,28 @@ def wl_c4(args, fm):
         T = float(rng.uniform(0.8, 1.2))
         nsteps = int(np.exp(rng.uniform(np.log(1e3), np.log(5e4))) * args.serve_step_scale)
         rid = srv.submit(_conf(f"nvt_langevin {T} {T} 1.0 {len(ids) + 1}", max(nsteps, 100)),
-                         dict(nchains=nc, chain_length=cl, density=DENSITY, seed=len(ids) + 1, pushoff_steps=200))
+                         dict(nchains=nc, chain_length=cl, density=DENSITY, seed=len(ids) + 1, pushoff_steps=1000))
         ids[rid] = time.perf_counter() - t_start
         work[rid] = nc * cl * max(nsteps, 100)
         t_next += float(rng.exponential(1.0 / rate))
     srv.drain(3600.0)
     res = srv.poll(len(ids) + 8)
     stats = srv.stats()
+    timing = srv.timing()
     srv.close()
     lat = np.array([r.finish_time - r.submit_time for r in res if r.status == 0])
+    failed = {}
+    for r in res:
+        if r.status != 0:
+            failed[str(r.status)] = failed.get(str(r.status), 0) + 1
     span = max(r.finish_time for r in res) - min(r.submit_time for r in res)
     return {"workload": "c4_served_stream", "requests": len(ids), "completed": int(len(lat)),
+            "failed_by_status": failed,
             "arrival_rate_per_s": rate, "duration_s": dur, "nsteps_scale": args.serve_step_scale,
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "mean": float(lat.mean())},
             "value": stats["atom_steps"] / span, "unit": "atom-steps/s",
-            "offered_atom_steps_per_s": sum(work.values()) / dur}
+            "offered_atom_steps_per_s": sum(work.values()) / dur, "server_thread": timing}
 
 
 WORKLOADS = {"c0": wl_c0, "c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c4": wl_c4}
@@ -560,6 +566,7 @@ def main():
     b.run(3)
     barrier(dist, local)
     counts0 = b.launch_counts()
+    rebuilds0 = sum(b.info(s).rebuilds for s in slots)
     with ClockSampler(local) as clk:
         profiler_range(True)
         lib.fmd_batch_mark(b._h, 0)
@@ -570,6 +577,7 @@ def main():
         ms = C.c_double()
         lib.fmd_batch_elapsed_ms(b._h, C.byref(ms))
     counts1 = b.launch_counts()
+    rebuilds1 = sum(b.info(s).rebuilds for s in slots)
     barrier(dist, local)
     dev_ms = allmax(dist, ms.value, local)
     total_atoms = allmax(dist, float(natoms), local) * world  # equal per rank
@@ -606,6 +614,8 @@ def main():
                             "legend": "b = list entries per batch, m = min blocks per SM, pipelined = next batch's "
                                       "list words loaded ahead, k = batches per compensated add"}
         line["launches_by_kernel"] = launched
+        line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
+                                    "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0)}
         # ---- roofline of the force kernel
         entries = C.c_int64()
         mx = C.c_int32()

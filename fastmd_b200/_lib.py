@@ -475,6 +475,13 @@ class Server:
         _call("fmd_server_stats", self._h, C.byref(q), C.byref(r), C.byref(f), C.byref(a), C.byref(s))
         return dict(queued=q.value, running=r.value, finished=f.value, atoms_resident=a.value, atom_steps=s.value)
 
+    def timing(self):
+        """Host seconds of the batch thread per phase, rounds, graph captures."""
+        a, r, t = C.c_double(), C.c_double(), C.c_double()
+        n, g = C.c_int64(), C.c_int64()
+        _call("fmd_server_timing", self._h, C.byref(a), C.byref(r), C.byref(t), C.byref(n), C.byref(g))
+        return dict(admit_s=a.value, run_s=r.value, retire_s=t.value, rounds=n.value, graph_captures=g.value)
+
     def drain(self, timeout_s=600.0):
         _call("fmd_server_drain", self._h, C.c_double(timeout_s))
 

@@ -162,6 +162,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   nbr_.alloc(c.nbr);
   reps_.alloc_zero(max_reps_);
   chunk_rep_.alloc(S / kChunk);
+  slot_cap_chunks_ = (int)(S / kChunk);
   h_chunk_rep_.assign(S / kChunk, make_int4(-1, 0, 0, 0));
   FMD_CUDA(cudaMemcpy(chunk_rep_, h_chunk_rep_.data(), h_chunk_rep_.size() * sizeof(int4), cudaMemcpyHostToDevice));
   h_reps_.assign(max_reps_, Rep{});
@@ -228,19 +229,24 @@ void Batch::upload_reps() {
 }
 
 int Batch::nchunks_launch() const { return (int)std::max<int64_t>(1, slot_alloc_.hwm()); }
+// Launch geometry: high-water marks of the layout (they only grow, so
+// admitting and retiring replicas in a steady mix keeps the captured graph).
+// The marks are rounded up (chunks to a multiple of 1024, replicas of 32,
+// cell counts to a power of two) so that a growing mix re-captures rarely;
+// blocks past the live layout return at once.
+static int round_up(int x, int q) { return (x + q - 1) / q * q; }
+static int pow2_at_least(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
 StepShape Batch::shape() const {
   StepShape g{};
-  g.nchunks = nchunks_launch();
-  g.nreps = nreps_launch();
-  int64_t mc = 1, mh = 1;
-  for (int r = 0; r < max_reps_; ++r)
-    if (info_[r].used) {
-      const int64_t ga = info_[r].plan.G_alloc;
-      mc = std::max<int64_t>(mc, info_[r].plan.ncell);
-      mh = std::max<int64_t>(mh, ga * ga * ga);
-    }
-  g.max_cells = (int)mc;
-  g.max_home = (int)mh;
+  g.nchunks = std::min(round_up(nchunks_launch(), 1024), std::max(1, slot_cap_chunks_));
+  g.nreps = std::min(round_up(std::max(nreps_launch(), hw_nreps_), 32), max_reps_);
+  g.max_cells = pow2_at_least(std::max(1, hw_cells_));
+  g.max_home = pow2_at_least(std::max(1, hw_home_));
   g.force_variant = force_variant_;
   g.nbr_variant = nbr_variant_;
   return g;
@@ -492,10 +498,12 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
     h_chunk_rep_[ch + c] = make_int4(r, (int)(ch * kChunk) + c * kChunk, std::max(0, std::min(kChunk, t.natoms - c * kChunk)), c);
   FMD_CUDA(cudaMemcpyAsync(chunk_rep_.p + ch, h_chunk_rep_.data() + ch, p.nchunks * sizeof(int4), cudaMemcpyHostToDevice, st_));
   FMD_CUDA(cudaMemsetAsync(cell_cnt_.p + ce, 0, p.ncell * sizeof(int32_t), st_));
+  hw_nreps_ = std::max(hw_nreps_, r + 1);
+  hw_cells_ = std::max<int>(hw_cells_, (int)p.ncell);
+  hw_home_ = std::max<int>(hw_home_, p.G_alloc * p.G_alloc * p.G_alloc);
   // Other replicas must not advance while this one is being set up.
   download_reps_keep(r);
   upload_atoms(r, t.xyz.data(), t.vel.data(), t.image.data());
-  graph_dirty_ = true;
   if (pushoff && pushoff->pushoff_steps > 0) {
     // Capped-force push-off runs batched with every other replica admitted
     // since the last run() (finish_pushoffs); forces are capped from setup on.
@@ -533,10 +541,27 @@ void Batch::finish_pushoffs() {
     direct = steps % graph_steps_;
   }
   const Dev d = dev();
-    for (int64_t k = 0; k < direct; ++k) launch_step(d, shape(), &host_mode_, st_);
+  for (int64_t k = 0; k < direct; ++k) launch_step(d, shape(), &host_mode_, st_);
   FMD_CUDA_LAUNCH();
   FMD_CUDA(cudaStreamSynchronize(st_));
   download_reps();
+  complete_pushoffs(pend);
+}
+
+// Concurrent push-offs (run() advanced them beside the running replicas):
+// those that reached their length start their run.
+void Batch::complete_done_pushoffs() {
+  std::vector<int> done;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used && info_[r].pending_pushoff > 0 && h_reps_[r].step >= info_[r].pending_pushoff)
+      done.push_back(r);
+  complete_pushoffs(done);
+}
+
+// Replicas whose push-off is done start their run: run mode, step 0, fresh
+// thermostat / barostat state, a rebuild and first forces.
+void Batch::complete_pushoffs(const std::vector<int>& pend) {
+  if (pend.empty()) return;
   for (int r : pend) {
     info_[r].pending_pushoff = 0;
     Rep& R3 = h_reps_[r];
@@ -616,8 +641,14 @@ void Batch::advance_direct(int64_t nsteps) {
   FMD_CUDA(cudaStreamSynchronize(st_));
 }
 
+static bool same_shape(const StepShape& a, const StepShape& b) {
+  return a.nchunks == b.nchunks && a.nreps == b.nreps && a.max_cells == b.max_cells && a.max_home == b.max_home &&
+         a.force_variant == b.force_variant && a.nbr_variant == b.nbr_variant;
+}
+
 void Batch::ensure_graph() {
-  if (!graph_dirty_ && graph_exec_) return;
+  const StepShape want = shape();
+  if (!graph_dirty_ && graph_exec_ && same_shape(want, graph_shape_)) return;
   if (graph_exec_) {
     cudaGraphExecDestroy(graph_exec_);
     graph_exec_ = nullptr;
@@ -626,7 +657,7 @@ void Batch::ensure_graph() {
     cudaGraph_t g;
   FMD_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   try {
-    for (int k = 0; k < graph_steps_; ++k) capture_step(d, shape(), st_, side_, branch_);
+    for (int k = 0; k < graph_steps_; ++k) capture_step(d, want, st_, side_, branch_);
   } catch (...) {
     cudaGraph_t partial = nullptr;
     cudaStreamEndCapture(st_, &partial);
@@ -637,10 +668,12 @@ void Batch::ensure_graph() {
   FMD_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
   cudaGraphDestroy(g);
   graph_dirty_ = false;
+  graph_shape_ = want;
+  ++graph_captures_;
 }
 
 void Batch::run(int64_t nsteps, bool respect_nsteps) {
-  finish_pushoffs();
+  if (!concurrent_pushoff_) finish_pushoffs();
   if (nsteps <= 0) return;
   download_reps();
   int64_t need = 0;
@@ -652,11 +685,17 @@ void Batch::run(int64_t nsteps, bool respect_nsteps) {
       continue;
     }
     int64_t stop = R.step + nsteps;
-    if (respect_nsteps && R.nsteps > 0) stop = std::min<int64_t>(stop, R.nsteps);
+    if (info_[r].pending_pushoff > 0)  // concurrent push-off: its own length
+      stop = std::min<int64_t>(stop, info_[r].pending_pushoff);
+    else if (respect_nsteps && R.nsteps > 0)
+      stop = std::min<int64_t>(stop, R.nsteps);
     R.stop_step = stop;
     need = std::max<int64_t>(need, stop - R.step);
   }
-  if (need == 0) return;
+  if (need == 0) {
+    if (concurrent_pushoff_) complete_done_pushoffs();
+    return;
+  }
   upload_reps();
   if (graph_steps_ > 0 && need >= graph_steps_) {
     ensure_graph();
@@ -666,11 +705,12 @@ void Batch::run(int64_t nsteps, bool respect_nsteps) {
   }
   if (need > 0) {
     const Dev d = dev();
-        for (int64_t k = 0; k < need; ++k) launch_step(d, shape(), &host_mode_, st_);
+    for (int64_t k = 0; k < need; ++k) launch_step(d, shape(), &host_mode_, st_);
     FMD_CUDA_LAUNCH();
   }
   FMD_CUDA(cudaStreamSynchronize(st_));
   download_reps();
+  if (concurrent_pushoff_) complete_done_pushoffs();
   // A faulted replica stops; the others continue.
   bool changed = false;
   for (int r = 0; r < max_reps_; ++r) {
@@ -702,7 +742,6 @@ void Batch::retire(int r) {
   I = ReplicaInfo{};
   upload_reps();
   FMD_CUDA(cudaStreamSynchronize(st_));
-  graph_dirty_ = true;
 }
 
 void Batch::mark(int which) {

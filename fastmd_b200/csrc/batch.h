@@ -69,6 +69,11 @@ class Batch {
   const RunConfig& cfg(int r) const { return info_[r].cfg; }
   void get_state(int r, double* xyz, double* vel, int32_t* image);
   void write_restart(int r, const std::string& path);
+  // Server mode: push-offs advance inside run() beside the running replicas
+  // instead of freezing them first.
+  void set_concurrent_pushoff(bool on) { concurrent_pushoff_ = on; }
+  int64_t pushoff_pending(int r) const { return info_[r].pending_pushoff; }
+  int64_t graph_captures() const { return graph_captures_; }
   void launch_counts(int64_t* counts, int n);
   void read_state(int r, double* xyz, double* vel, int32_t* image, bool rewrap);
   void set_state(int r, const double* xyz, const double* vel, const int32_t* image);
@@ -81,6 +86,8 @@ class Batch {
   void ensure_ev(int r);
   // Run the capped-force push-off of every replica admitted with one, batched.
   void finish_pushoffs();
+  void complete_pushoffs(const std::vector<int>& pend);
+  void complete_done_pushoffs();
   int64_t budget_bytes() const { return budget_bytes_; }
   int64_t bytes_in_use() const { return bytes_in_use_; }
   cudaStream_t stream() const { return st_; }
@@ -117,6 +124,11 @@ class Batch {
   cudaStream_t branch_ = nullptr;  // second branch of a captured step
   int graph_steps_ = 50;
   int force_variant_ = 0;
+  bool concurrent_pushoff_ = false;
+  int hw_nreps_ = 0, hw_cells_ = 0, hw_home_ = 0;  // layout high-water marks
+  int slot_cap_chunks_ = 0;                        // chunks the per-chunk arrays hold
+  StepShape graph_shape_{};
+  int64_t graph_captures_ = 0;
   int nbr_variant_ = 0;
   double nbr_ms_[kNbrVariants] = {0, 0, 0};
   int max_reps_ = 256;

@@ -729,8 +729,10 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
                 const float rz = (pi.z - jz) - shift_term(ez, kz, h, dL);
                 const float r2 = rx * rx + ry * ry + rz * rz;
                 if (r2 < rcs2) {
-                  const int ax = axis_shift_code(ex, kx), ay = axis_shift_code(ey, ky), az = axis_shift_code(ez, kz);
-                  if (ax < 0 || ay < 0 || az < 0) {
+                  const bool ok = ex >= -1 && ex <= 1 && ey >= -1 && ey <= 1 && ez >= -1 && ez <= 1 &&
+                                  kx == implied_wrap(w_cx(ui), ex, G) && ky == implied_wrap(w_cy(ui), ey, G) &&
+                                  kz == implied_wrap(w_cz(ui), ez, G);
+                  if (!ok) {
                     overflow |= kStatusCellCapacity;
                     continue;
                   }
@@ -739,7 +741,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
                   for (int b = b0; b < b1; ++b) excl |= (d.bent[R.bond_base + b].x == idj);
                   if (excl) continue;
                   if (count < M)
-                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)(ax * 25 + ay * 5 + az) << kCodeShift);
+                    out[(size_t)count * 32] = (uint32_t)j | (cell_offset_code(ex, ey, ez) << kCodeShift);
                   ++count;
                 }
               }
@@ -808,8 +810,7 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
     s_sx[t] = shift_term(dx, kx, h, dL);
     s_sy[t] = shift_term(dy, ky, h, dL);
     s_sz[t] = shift_term(dz, kz, h, dL);
-    s_code[t] = (uint32_t)(axis_shift_code(dx, kx) * 25 + axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz))
-                << kCodeShift;
+    s_code[t] = cell_offset_code(dx, dy, dz) << kCodeShift;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -929,8 +930,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
   __shared__ float4 s_c[kNbrCap];
   __shared__ int s_ns[kNbrUnion], s_off[kNbrUnion + 1];
   __shared__ float s_sx[kNbrUnion], s_sy[kNbrUnion], s_sz[kNbrUnion];
-  __shared__ int s_ax[kNbrUnion];   // wrap count kx of the union column
-  __shared__ int s_ayz[kNbrUnion];  // (axis code y) * 5 + (axis code z)
+  __shared__ uint32_t s_yz[kNbrUnion];  // y and z parts of the cell-offset code
   if (threadIdx.x < nu) {
     const int u = threadIdx.x;
     const int row = u / ux, col = u % ux;
@@ -948,8 +948,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
     s_sx[u] = shift_term(xu - hx0, kx, h, dL);
     s_sy[u] = shift_term(dy, ky, h, dL);
     s_sz[u] = shift_term(dz, kz, h, dL);
-    s_ax[u] = kx;
-    s_ayz[u] = axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz);
+    s_yz[u] = cell_offset_code(-1, dy, dz);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -996,8 +995,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
       for (int row = 0; row < 9; ++row) {
         for (int dx = -1; dx <= 1; ++dx) {
           const int u = row * ux + a + 1 + dx;
-          const uint32_t code =
-              (uint32_t)(axis_shift_code(dx, s_ax[u]) * 25 + s_ayz[u]) << kCodeShift;
+          const uint32_t code = (s_yz[u] | (uint32_t)(dx + 1)) << kCodeShift;
           const int k0 = s_off[u], k1 = s_off[u + 1];
           const float sx = s_sx[u], sy = s_sy[u], sz = s_sz[u];
           const int ns = s_ns[u];
@@ -1105,20 +1103,29 @@ __device__ __forceinline__ void block_partials(double* vals, int nv, double* out
   }
 }
 
-// LJ contribution of one listed neighbor (lj.cu:32-61 semantics).  sh is
-// the periodic shift vector named by the entry's code, so
-// r_ij = (pos_i - pos_j) - sh.  EV: also accumulate half the pair energy and
-// the virial half-pair.
+// LJ contribution of one listed neighbor (lj.cu:32-61 semantics).  t is
+// atom i's position minus the entry's cell shift, so r_ij = t - pos_j.  EV:
+// also accumulate half the pair energy and the virial half-pair.
 struct PairAcc {
   float fx, fy, fz, pe, v0, v1, v2, v3, v4, v5;
 };
 
+// Atom i's coordinates minus the cell shift for e = -1, 0, +1 per axis
+// (periodic wrap included where i sits in an edge cell); a list entry's
+// 6-bit cell-offset code picks one per axis.
+struct ShiftedPos {
+  float xm, x0, xp, ym, y0, yp, zm, z0, zp;
+  __device__ __forceinline__ float3 pick(uint32_t c) const {
+    return make_float3((c & 2u) ? xp : ((c & 1u) ? x0 : xm), (c & 8u) ? yp : ((c & 4u) ? y0 : ym),
+                       (c & 32u) ? zp : ((c & 16u) ? z0 : zm));
+  }
+};
+
 template <bool EV>
-__device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4 pj, float rc2, float e24,
-                                        float sig2) {
-  const float dx = (pi.x - pj.x) - sh.x;
-  const float dy = (pi.y - pj.y) - sh.y;
-  const float dz = (pi.z - pj.z) - sh.z;
+__device__ __forceinline__ void lj_pair(PairAcc& a, float3 t, float4 pj, float rc2, float e24, float sig2) {
+  const float dx = t.x - pj.x;
+  const float dy = t.y - pj.y;
+  const float dz = t.z - pj.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   // Branch-free: every listed pair is evaluated and pairs outside the cutoff
   // (or the r = 0 padding entries) contribute an exact zero through selects.
@@ -1151,8 +1158,8 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
 // words are loaded before this batch's gathers (software pipelining, B more
 // registers).  nn is the padded length (a multiple of B).
 template <bool EV, int B, bool PF, int KB>
-__device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
-                                        const float4* s_shift, bool one_type, int ti, int nt, const float* s_eps24,
+__device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, const ShiftedPos& sp,
+                                        bool one_type, int ti, int nt, const float* s_eps24,
                                         const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
                                         PairAcc& acc) {
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
@@ -1188,7 +1195,7 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
         e24 = s_eps24[pidx];
         sig2 = s_sig2[pidx];
       }
-      lj_pair<EV>(g, pi, s_shift[w[q] >> kCodeShift], pj[q], rc2, e24, sig2);
+      lj_pair<EV>(g, sp.pick(w[q] >> kCodeShift), pj[q], rc2, e24, sig2);
     }
     if (++kb == KB || k + B >= nn) {
       fx.add(g.fx);
@@ -1264,7 +1271,6 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
   if (!R.adv) return;
   if (need_ev(R) != EV) return;
   constexpr bool ev = EV;
-  __shared__ float4 s_shift[kShiftCodes];
   __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
   const int nt = R.ntypes;
   const int G = R.G;
@@ -1273,13 +1279,6 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
     s_eps24[k] = R.lj_eps24[k];
     s_sig2[k] = R.lj_sig2[k];
-  }
-  if (threadIdx.x < kShiftCodes) {
-    const int c = threadIdx.x;
-    const int ax = c / 25, ay = (c / 5) % 5, az = c % 5;
-    s_shift[c] = make_float4(shift_term(axis_code_e(ax), axis_code_k(ax), h, dL),
-                             shift_term(axis_code_e(ay), axis_code_k(ay), h, dL),
-                             shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
   }
   __syncthreads();
   const int local = ci.w * kChunk + threadIdx.x;
@@ -1299,7 +1298,21 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
     const bool one_type = (nt == 1);
-    lj_loop<EV, B, PF, KB>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    // pos_i - (e h + k dL) per axis for e = -1, 0, +1 (k from this atom's cell)
+    ShiftedPos sp;
+    {
+      const int cx = w_cx(ui), cy = w_cy(ui), cz = w_cz(ui);
+      sp.x0 = pi.x;
+      sp.xm = pi.x - shift_term(-1, implied_wrap(cx, -1, G), h, dL);
+      sp.xp = pi.x - shift_term(1, implied_wrap(cx, 1, G), h, dL);
+      sp.y0 = pi.y;
+      sp.ym = pi.y - shift_term(-1, implied_wrap(cy, -1, G), h, dL);
+      sp.yp = pi.y - shift_term(1, implied_wrap(cy, 1, G), h, dL);
+      sp.z0 = pi.z;
+      sp.zm = pi.z - shift_term(-1, implied_wrap(cz, -1, G), h, dL);
+      sp.zp = pi.z - shift_term(1, implied_wrap(cz, 1, G), h, dL);
+    }
+    lj_loop<EV, B, PF, KB>(lst, nn, pbase, sp, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};

@@ -1,9 +1,11 @@
 // Continuous-batching request server over one mixed-precision batch.
 //
-// A host thread owns the batch.  Each round it admits queued requests while
-// replica slots and the device-memory budget allow (generation and optional
-// push-off happen at admission), advances every resident replica by
-// steps_per_round steps in the shared CUDA-graph step loop, retires the
+// A pool of generator threads parses each submitted request and builds its
+// melt on the host; the batch thread receives them in submission order.  The batch thread owns the batch: each
+// round it admits generated requests while replica slots and the
+// device-memory budget allow, advances every resident replica by
+// steps_per_round steps in the shared CUDA-graph step loop (new replicas run
+// their capped push-off in the same steps, beside the others), retires the
 // replicas that reached their run.conf nsteps (or faulted), publishes their
 // results, and back-fills the freed slots in the next round.  A replica's
 // trajectory does not depend on what else is resident (chunk-aligned
@@ -11,7 +13,9 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <algorithm>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -29,6 +33,15 @@ struct Request {
   double submit;
 };
 
+// A request whose melt has been generated off the batch thread.
+struct Prepared {
+  Request rq;
+  fmd::RunConfig cfg;
+  fmd::Topology topo;
+  int64_t bytes = 0;
+  fmd_status error = FMD_OK;
+};
+
 struct Running {
   int64_t id;
   int slot;
@@ -36,6 +49,7 @@ struct Running {
   int64_t target;
   double submit, start;
   int64_t last_step;
+  bool pushing;  // capped push-off still running (its steps are not counted)
 };
 
 double now_s() {
@@ -50,85 +64,134 @@ struct fmd_server {
   int32_t steps_per_round = 200;
   int device = 0;
   std::mutex mu;
-  std::condition_variable cv;
-  std::deque<Request> queue;
+  std::condition_variable cv, gen_cv;
+  std::deque<Request> queue;   // submitted, not taken by a generator
+  std::deque<Prepared> ready;  // generated, in submission order, waiting for a slot and memory
+  std::map<int64_t, Prepared> out_of_order;  // generated ahead of an earlier request
+  int64_t next_ready = 1;      // id of the next request to move into ready
   std::vector<Running> running;
   std::deque<fmd_request_result> done;
   std::atomic<bool> stop{false};
   std::thread th;
+  std::vector<std::thread> gen_th;
   int64_t next_id = 1;
   int64_t finished = 0;
   double atom_steps = 0;
   double t0 = 0;
   std::string fatal;
+  // host seconds per phase of the batch thread, rounds
+  double t_admit = 0, t_run = 0, t_retire = 0;
+  int64_t rounds = 0;
+
+  void publish_error(const Request& rq, fmd_status code) {
+    fmd_request_result res{};
+    res.request_id = rq.id;
+    res.status = code;
+    res.submit_time = rq.submit - t0;
+    res.finish_time = now_s() - t0;
+    std::lock_guard<std::mutex> lk(mu);
+    done.push_back(res);
+    ++finished;
+  }
+
+  // Melt generation, parsing and sizing on a pool of host threads; results
+  // reach the batch thread in submission order, so it only uploads and steps.
+  void generate() {
+    while (!stop.load()) {
+      Request rq;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        gen_cv.wait_for(lk, std::chrono::milliseconds(20), [&] { return !queue.empty() || stop.load(); });
+        if (queue.empty()) continue;
+        rq = queue.front();
+        queue.pop_front();
+      }
+      Prepared p;
+      p.rq = rq;
+      try {
+        p.cfg = fmd::parse_run_conf(rq.conf);
+        p.topo = fmd::generate_melt(rq.gen);
+        fmd::validate(p.cfg, p.topo);
+        const auto plan = fmd::mixed::plan_replica(p.cfg, p.topo.natoms, p.topo.box_L);
+        p.bytes = fmd::mixed::estimate_bytes(plan, p.topo.nbonds(), p.topo.nangles());
+      } catch (const fmd::Error& e) {
+        p.error = e.code;
+      } catch (const std::exception&) {
+        p.error = FMD_ERR_ARG;
+      }
+      std::lock_guard<std::mutex> lk(mu);
+      out_of_order.emplace(p.rq.id, std::move(p));
+      for (auto it = out_of_order.find(next_ready); it != out_of_order.end(); it = out_of_order.find(next_ready)) {
+        ready.push_back(std::move(it->second));
+        out_of_order.erase(it);
+        ++next_ready;
+      }
+      cv.notify_one();
+    }
+  }
 
   void loop() {
     cudaSetDevice(device);
     while (!stop.load()) {
-      // ---- admission
-      std::vector<Request> admit;
       {
         std::unique_lock<std::mutex> lk(mu);
-        if (queue.empty() && running.empty()) {
+        if (ready.empty() && running.empty()) {
           cv.wait_for(lk, std::chrono::milliseconds(20));
           continue;
         }
       }
+      // ---- admission: generated requests, while slots and memory allow
+      const double ta = now_s();
       for (;;) {
-        Request rq;
+        Prepared p;
         {
           std::lock_guard<std::mutex> lk(mu);
-          if (queue.empty()) break;
-          rq = queue.front();
+          if (ready.empty()) break;
+          if (ready.front().error == FMD_OK && batch->bytes_in_use() + ready.front().bytes > batch->budget_bytes() &&
+              !running.empty())
+            break;  // wait for memory
+          p = std::move(ready.front());
+          ready.pop_front();
         }
-        fmd_request_result res{};
-        res.request_id = rq.id;
-        res.submit_time = rq.submit - t0;
+        if (p.error != FMD_OK) {
+          publish_error(p.rq, p.error);
+          continue;
+        }
         try {
-          fmd::RunConfig cfg = fmd::parse_run_conf(rq.conf);
-          const int64_t n = (int64_t)rq.gen.nchains * rq.gen.chain_length;
-          const double L = std::cbrt((double)n / rq.gen.density);
-          const auto plan = fmd::mixed::plan_replica(cfg, (int32_t)n, L);
-          const int64_t need = fmd::mixed::estimate_bytes(plan, (int32_t)n, (int32_t)n);
-          if (batch->bytes_in_use() + need > batch->budget_bytes() && !running.empty()) break;  // wait for memory
-          fmd::Topology t = fmd::generate_melt(rq.gen);
-          fmd::validate(cfg, t);
+          const int64_t natoms = p.topo.natoms;
           int slot;
           try {
-            slot = batch->add(cfg, std::move(t), &rq.gen);
+            slot = batch->add(p.cfg, p.topo, &p.rq.gen);
           } catch (const fmd::Error& e) {
-            if (e.code == FMD_ERR_CAPACITY && !running.empty()) break;  // back-fill later
+            if (e.code == FMD_ERR_CAPACITY && !running.empty()) {
+              // back-fill later, first in line
+              std::lock_guard<std::mutex> lk(mu);
+              ready.push_front(std::move(p));
+              break;
+            }
             throw;
           }
           Running r;
-          r.id = rq.id;
+          r.id = p.rq.id;
           r.slot = slot;
-          r.natoms = (int32_t)n;
-          r.target = cfg.nsteps;
-          r.submit = rq.submit;
+          r.natoms = (int32_t)natoms;
+          r.target = p.cfg.nsteps;
+          r.submit = p.rq.submit;
           r.start = now_s();
           r.last_step = 0;
+          r.pushing = batch->pushoff_pending(slot) > 0;
           std::lock_guard<std::mutex> lk(mu);
-          queue.pop_front();
           running.push_back(r);
         } catch (const fmd::Error& e) {
-          res.status = e.code;
-          res.finish_time = now_s() - t0;
-          std::lock_guard<std::mutex> lk(mu);
-          queue.pop_front();
-          done.push_back(res);
-          ++finished;
-        } catch (const std::exception& e) {
-          res.status = FMD_ERR_ARG;
-          res.finish_time = now_s() - t0;
-          std::lock_guard<std::mutex> lk(mu);
-          queue.pop_front();
-          done.push_back(res);
-          ++finished;
+          publish_error(p.rq, e.code);
+        } catch (const std::exception&) {
+          publish_error(p.rq, FMD_ERR_ARG);
         }
       }
+      t_admit += now_s() - ta;
       if (running.empty()) continue;
-      // ---- advance every resident replica
+      // ---- advance every resident replica (push-offs alongside)
+      const double tr = now_s();
       try {
         batch->run(steps_per_round, true);
       } catch (const std::exception& e) {
@@ -137,15 +200,25 @@ struct fmd_server {
         stop = true;
         break;
       }
+      t_run += now_s() - tr;
+      ++rounds;
       // ---- retire finished / faulted replicas
+      const double tt = now_s();
       std::vector<Running> keep;
       for (auto& r : running) {
         const auto& R = batch->rep(r.slot);
+        if (r.pushing) {
+          if (R.status == 0 && batch->pushoff_pending(r.slot) > 0) {
+            keep.push_back(r);
+            continue;
+          }
+          r.pushing = false;  // its run starts at step 0
+          r.last_step = 0;
+        }
         atom_steps += (double)r.natoms * (double)(R.step - r.last_step);
         r.last_step = R.step;
         const bool fault = R.status != 0;
-        if (R.step >= r.target || fault) {
-          fmd_request_result res{};
+        if (R.step >= r.target || fault) {          fmd_request_result res{};
           res.request_id = r.id;
           res.status = fault ? FMD_ERR_FAULT : FMD_OK;
           res.natoms = r.natoms;
@@ -169,6 +242,7 @@ struct fmd_server {
       }
       std::lock_guard<std::mutex> lk(mu);
       running.swap(keep);
+      t_retire += now_s() - tt;
     }
   }
 };
@@ -207,8 +281,12 @@ FMD_API fmd_status fmd_server_create(const fmd_server_opts* opts, fmd_server** o
     s->device = o.batch.device;
     s->steps_per_round = o.steps_per_round > 0 ? o.steps_per_round : 200;
     s->batch.reset(new fmd::mixed::Batch(o.batch));
+    s->batch->set_concurrent_pushoff(true);
     s->t0 = now_s();
     s->th = std::thread([p = s.get()] { p->loop(); });
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const int ngen = (int)std::min(8u, hw / 2);
+    for (int k = 0; k < ngen; ++k) s->gen_th.emplace_back([p = s.get()] { p->generate(); });
     *out = s.release();
   });
 }
@@ -222,7 +300,7 @@ FMD_API fmd_status fmd_server_submit(fmd_server* s, const char* conf, const fmd_
     Request r{s->next_id++, conf, *gen, now_s()};
     s->queue.push_back(r);
     *request_id = r.id;
-    s->cv.notify_one();
+    s->gen_cv.notify_one();
   });
 }
 
@@ -244,7 +322,7 @@ FMD_API fmd_status fmd_server_stats(fmd_server* s, int64_t* queued, int64_t* run
   return guarded([&] {
     if (!s) throw fmd::Error(FMD_ERR_ARG, "null server");
     std::lock_guard<std::mutex> lk(s->mu);
-    if (queued) *queued = (int64_t)s->queue.size();
+    if (queued) *queued = s->next_id - s->next_ready + (int64_t)s->ready.size();
     if (running) *running = (int64_t)s->running.size();
     if (finished) *finished = s->finished;
     if (atoms_resident) {
@@ -256,6 +334,19 @@ FMD_API fmd_status fmd_server_stats(fmd_server* s, int64_t* queued, int64_t* run
   });
 }
 
+FMD_API fmd_status fmd_server_timing(fmd_server* s, double* admit_s, double* run_s, double* retire_s, int64_t* rounds,
+                                     int64_t* graph_captures) {
+  return guarded([&] {
+    if (!s) throw fmd::Error(FMD_ERR_ARG, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (admit_s) *admit_s = s->t_admit;
+    if (run_s) *run_s = s->t_run;
+    if (retire_s) *retire_s = s->t_retire;
+    if (rounds) *rounds = s->rounds;
+    if (graph_captures) *graph_captures = s->batch->graph_captures();
+  });
+}
+
 FMD_API fmd_status fmd_server_drain(fmd_server* s, double timeout_s) {
   return guarded([&] {
     if (!s) throw fmd::Error(FMD_ERR_ARG, "null server");
@@ -264,7 +355,9 @@ FMD_API fmd_status fmd_server_drain(fmd_server* s, double timeout_s) {
       {
         std::lock_guard<std::mutex> lk(s->mu);
         if (!s->fatal.empty()) throw fmd::Error(FMD_ERR_STATE, "server stopped: " + s->fatal);
-        if (s->queue.empty() && s->running.empty()) return;
+        if (s->queue.empty() && s->ready.empty() && s->out_of_order.empty() && s->running.empty() &&
+            s->next_ready == s->next_id)
+          return;
       }
       if (now_s() > t_end) throw fmd::Error(FMD_ERR_TIMEOUT, "drain timed out");
       std::this_thread::sleep_for(std::chrono::milliseconds(5));
@@ -277,7 +370,10 @@ FMD_API fmd_status fmd_server_destroy(fmd_server* s) {
     if (!s) return;
     s->stop = true;
     s->cv.notify_all();
+    s->gen_cv.notify_all();
     if (s->th.joinable()) s->th.join();
+    for (auto& t : s->gen_th)
+      if (t.joinable()) t.join();
     delete s;
   });
 }

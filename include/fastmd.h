@@ -292,6 +292,10 @@ FMD_API fmd_status fmd_server_poll(fmd_server* s, fmd_request_result* out, int32
 /* queued, running, finished, atoms resident, atom-steps done. */
 FMD_API fmd_status fmd_server_stats(fmd_server* s, int64_t* queued, int64_t* running, int64_t* finished,
                                     int64_t* atoms_resident, double* atom_steps);
+/* Host seconds the batch thread spent admitting (upload, setup), stepping and
+ * retiring (readouts), rounds run, and CUDA-graph captures so far. */
+FMD_API fmd_status fmd_server_timing(fmd_server* s, double* admit_s, double* run_s, double* retire_s,
+                                     int64_t* rounds, int64_t* graph_captures);
 FMD_API fmd_status fmd_server_drain(fmd_server* s, double timeout_s);
 FMD_API fmd_status fmd_server_destroy(fmd_server* s);
 
