@@ -603,11 +603,12 @@ def main():
         line["clocks"] = clk.summary()
         launched = {k: counts1[k] - counts0[k] for k in counts0}
         line["gpu_launches"] = int(sum(launched.values()))
-        line["autotune"] = {"force_variant": variant, "neighbor_variant": int(variant_ms[10]),
-                            "ms_per_full_rebuild": {"ballot m8": round(float(variant_ms[7]), 4),
-                                                    "rows m6": round(float(variant_ms[8]), 4),
-                                                    "ballot m6": round(float(variant_ms[9]), 4)},
-                            "ms_per_variant": [round(float(x), 4) for x in variant_ms[:7]],
+        nf = 7
+        line["autotune"] = {"force_variant": variant, "neighbor_variant": int(variant_ms[nf + 3]),
+                            "ms_per_full_rebuild": {"ballot m8": round(float(variant_ms[nf]), 4),
+                                                    "rows m6": round(float(variant_ms[nf + 1]), 4),
+                                                    "ballot m6": round(float(variant_ms[nf + 2]), 4)},
+                            "ms_per_variant": [round(float(x), 4) for x in variant_ms[:nf]],
                             "variants": ["b4 m6 pipelined k1", "b4 m8 pipelined k1", "b4 m6 pipelined k2",
                                          "b4 m8 pipelined k2", "b2 m8 pipelined k4", "b4 m7 pipelined k2",
                                          "b8 m6 k1"],
@@ -615,7 +616,9 @@ def main():
                                       "list words loaded ahead, k = batches per compensated add"}
         line["launches_by_kernel"] = launched
         line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
-                                    "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0)}
+                                    "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0),
+                                    "policy": "skin/2 displacement trigger only (forced cadence lifted by the "
+                                              "autotuner; the reference forces one every 20 steps)"}
         # ---- roofline of the force kernel
         entries = C.c_int64()
         mx = C.c_int32()

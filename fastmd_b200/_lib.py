@@ -433,8 +433,16 @@ class Batch:
     LAUNCH_KINDS = ("pre", "bin", "scan", "scatter", "cellsort", "permute", "topo", "neighbors", "force",
                     "force_ev", "post", "plan", "commit")
 
+    def set_rebuild_cadence(self, slot, max_steps):
+        """Force a neighbor-list rebuild at least every max_steps steps
+        (20 by default, as the reference); max_steps <= 0 leaves rebuilds to
+        the displacement / box-shrink trigger alone."""
+        _call("fmd_batch_set_rebuild_cadence", self._h, C.c_int32(slot), C.c_int32(max_steps))
+
     def autotune(self, iters=20):
-        """Pick the fastest force-kernel variant on the current state."""
+        """Pick the fastest force-kernel and neighbor-list variants on the
+        current state and lift the forced rebuild cadence of the active
+        replicas."""
         ms = np.zeros(16)
         v = C.c_int32()
         _call("fmd_batch_autotune", self._h, C.c_int32(iters), C.byref(v), _ptr(ms), C.c_int32(len(ms)))

@@ -315,6 +315,7 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   G = std::max(1, std::min(G, G_alloc));
   R.G = G;
   R.L = L;
+  R.L_list = L;
   R.Lpos = L;
   R.h = (float)(L / G);
   R.maxdisp_bits = 0;
@@ -606,6 +607,7 @@ void Batch::setup(const std::vector<int>& rs) {
     R.adv = 1;
     R.rebuild_now = 1;
     R.since = 0;
+    R.L_list = R.L;
     R.maxdisp_bits = 0;
     R.force_ev = 1;
   }
@@ -845,6 +847,15 @@ int Batch::autotune(int iters, double* ms_out, int cap) {
   }
   if (best != force_variant_) graph_dirty_ = true;
   force_variant_ = best;
+  // Rebuild cadence: the skin/2 displacement trigger alone keeps every pair
+  // within rc listed, so a forced cadence (the reference's 20 steps) only
+  // adds rebuilds; it is lifted for the active replicas (set_max_between
+  // restores one).
+  download_reps();
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used && h_reps_[r].active) h_reps_[r].max_between = kNoForcedRebuild;
+  upload_reps();
+  FMD_CUDA(cudaStreamSynchronize(st_));
   return best;
 }
 
@@ -867,7 +878,7 @@ void Batch::list_stats(int64_t* entries, int32_t* max_per_atom) {
 
 void Batch::set_max_between(int r, int k) {
   download_reps();
-  h_reps_[r].max_between = k > 0 ? k : 20;
+  h_reps_[r].max_between = k > 0 ? k : kNoForcedRebuild;
   upload_reps();
   FMD_CUDA(cudaStreamSynchronize(st_));
 }

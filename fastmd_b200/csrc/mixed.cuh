@@ -35,26 +35,19 @@ constexpr int kTile = 32;         // slots per warp tile
 constexpr int kMaxTypes = 16;
 constexpr int kGhostType = 31;
 constexpr int kMaxG = 512;        // cells per axis (9 bits)
-// Neighbor-list entry: slot (26 bits) | cell offsets (6 bits: e + 1 per axis,
-// 2 bits each, x lowest).  The pair displacement per axis is
-// (o_i - o_j) - (e h + k dL); the periodic wrap k is not stored: it follows
-// from atom i's own cell c_i (k = -1 iff e = -1 and c_i = 0, k = +1 iff e = +1
-// and c_i = G - 1), so a thread keeps its three shifted coordinates per axis
-// in registers and picks one per pair.
-constexpr uint32_t kIdxMask = (1u << 26) - 1;
-constexpr int kCodeShift = 26;
-constexpr uint32_t kZeroShiftCode = 0x15;  // e = (0, 0, 0)
-__host__ __device__ inline uint32_t cell_offset_code(int ex, int ey, int ez) {
-  return (uint32_t)(ex + 1) | ((uint32_t)(ey + 1) << 2) | ((uint32_t)(ez + 1) << 4);
-}
-// The wrap count the force kernel infers for atom cell c and offset e.
-__host__ __device__ inline int implied_wrap(int c, int e, int G) {
-  return (e == -1 && c == 0) ? -1 : ((e == 1 && c == G - 1) ? 1 : 0);
-}
+// Neighbor-list entry: slot (25 bits) | shift code (7 bits).  The shift
+// code names one of 125 periodic shift vectors: per axis a in 0..4 for
+// e*h + k*dL with (e, k) = (-1,-1), (-1,0), (0,0), (1,0), (1,1), code =
+// 25 ax + 5 ay + az.  The vector is the same for every atom of a replica.
+constexpr uint32_t kIdxMask = (1u << 25) - 1;
+constexpr int kCodeShift = 25;
+constexpr int kShiftCodes = 125;
+constexpr uint32_t kZeroShiftCode = 62;  // (0, 0, 0): 2 * 25 + 2 * 5 + 2
 // Lists are padded to a multiple of kListPad entries with the atom's own
 // slot and the zero shift (r = 0, excluded by the r^2 > 1e-10 guard), so the
 // force loop runs whole batches.
 constexpr int kListPad = 8;
+constexpr int32_t kNoForcedRebuild = 1 << 30;  // rebuild cadence: skin trigger only
 constexpr uint32_t kSlotMask26 = (1u << 26) - 1;  // bonded-table slot field
 constexpr int kNumPartials = 14;  // pe, vir[6], ke[6], sum m v^2
 constexpr int kMaxBondsPerAtom = 4;   // per-slot bonded tables rebuilt with the list
@@ -104,7 +97,7 @@ struct Rep {
   int32_t ntypes;
   int32_t ensemble;
   int32_t chain_M;
-  int32_t max_between;           // forced rebuild cadence (steps)
+  int32_t max_between;           // forced rebuild cadence (steps; kNoForcedRebuild: skin trigger only)
   int64_t nsteps;                // run.conf nsteps (ramp denominator)
   uint64_t seed;
   double dt, rc, skin;
@@ -125,6 +118,7 @@ struct Rep {
   int32_t G;
   double L;      // box edge (barostat value)
   double Lpos;   // box the stored positions are wrapped in (last pre-force)
+  double L_list; // box the neighbor list was built in (box-shrink term of the rebuild trigger)
   float h;
   uint32_t maxdisp_bits;
   int32_t status;
@@ -191,6 +185,17 @@ struct Dev {
   int* rb;
   int rb_cap;
 };
+
+// Axis part of the shift code for cell shift e and wrap count k; -1 when
+// (e, k) is not one of the five representable cases.
+__host__ __device__ inline int axis_shift_code(int e, int k) {
+  if (e == 0) return k == 0 ? 2 : -1;
+  if (e == -1) return k == -1 ? 0 : (k == 0 ? 1 : -1);
+  if (e == 1) return k == 1 ? 4 : (k == 0 ? 3 : -1);
+  return -1;
+}
+__host__ __device__ inline int axis_code_e(int a) { return a < 2 ? -1 : (a == 2 ? 0 : 1); }
+__host__ __device__ inline int axis_code_k(int a) { return a == 0 ? -1 : (a == 4 ? 1 : 0); }
 
 __host__ __device__ inline uint32_t spread3(uint32_t v) {
   v &= 0x3FFu;

@@ -139,7 +139,74 @@ __device__ __forceinline__ void count_launch(const Dev& d, int kind) {
 }
 
 // ---------------------------------------------------------------- pre-force
-__global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
+// One atom's pre-force update on its loaded state (p, v, f, q); returns the
+// squared displacement bits since the last rebuild and a non-finite flag.
+__device__ __forceinline__ void pre_atom(const Dev& d, const Rep& R, const StepScalars& S, int s, bool deferred,
+                                         float4 p, float4 v, const float4 f, float4 q, uint32_t& d2bits, int& bad) {
+  const float hm = S.hdt * v.w;
+  if (deferred) {
+    // the previous step's post-force half kick (same step size, same
+    // operation as the post-force kernel would have done)
+    v.x = fmaf(hm, f.x, v.x);
+    v.y = fmaf(hm, f.y, v.y);
+    v.z = fmaf(hm, f.z, v.z);
+  }
+  v.x *= S.vscale;
+  v.y *= S.vscale;
+  v.z *= S.vscale;
+  if (S.ens == FMD_LANGEVIN) {
+    float n0, n1, n2;
+    normal3_f32(R.seed, S.stream, (uint64_t)S.step, (uint32_t)__float_as_int(q.w), n0, n1, n2);
+    const float ns = S.c2kT * sqrtf(v.w);
+    v.x = fmaf(hm, f.x, v.x);
+    v.y = fmaf(hm, f.y, v.y);
+    v.z = fmaf(hm, f.z, v.z);
+    p.x = fmaf(S.hdt, v.x, p.x);
+    p.y = fmaf(S.hdt, v.y, p.y);
+    p.z = fmaf(S.hdt, v.z, p.z);
+    v.x = fmaf(S.c1, v.x, ns * n0);
+    v.y = fmaf(S.c1, v.y, ns * n1);
+    v.z = fmaf(S.c1, v.z, ns * n2);
+    p.x = fmaf(S.hdt, v.x, p.x);
+    p.y = fmaf(S.hdt, v.y, p.y);
+    p.z = fmaf(S.hdt, v.z, p.z);
+  } else if (S.ens == FMD_NVT_NH) {
+    v.x = fmaf(hm, f.x, v.x);
+    v.y = fmaf(hm, f.y, v.y);
+    v.z = fmaf(hm, f.z, v.z);
+    p.x = fmaf(S.dt, v.x, p.x);
+    p.y = fmaf(S.dt, v.y, p.y);
+    p.z = fmaf(S.dt, v.z, p.z);
+  } else {
+    v.x = fmaf(hm, f.x, v.x);
+    v.y = fmaf(hm, f.y, v.y);
+    v.z = fmaf(hm, f.z, v.z);
+    const uint32_t u = w_bits(p.w);
+    const float cx = (float)w_cx(u), cy = (float)w_cy(u), cz = (float)w_cz(u);
+    const float wx = floorf(fmaf(cx, S.h_old, p.x) * S.inv_Lold);
+    const float wy = floorf(fmaf(cy, S.h_old, p.y) * S.inv_Lold);
+    const float wz = floorf(fmaf(cz, S.h_old, p.z) * S.inv_Lold);
+    p.x = fmaf(p.x, S.ev, fmaf(cx, S.dh, fmaf(wx, S.dW, v.x * S.fpos)));
+    p.y = fmaf(p.y, S.ev, fmaf(cy, S.dh, fmaf(wy, S.dW, v.y * S.fpos)));
+    p.z = fmaf(p.z, S.ev, fmaf(cz, S.dh, fmaf(wz, S.dW, v.z * S.fpos)));
+    q.x = fmaf(q.x, S.ev, cx * S.dh);
+    q.y = fmaf(q.y, S.ev, cy * S.dh);
+    q.z = fmaf(q.z, S.ev, cz * S.dh);
+    d.ref[s] = q;
+  }
+  const float ux = p.x - q.x, uy = p.y - q.y, uz = p.z - q.z;
+  const float dd = ux * ux + uy * uy + uz * uz;
+  bad |= !isfinite(dd) || !isfinite(v.x + v.y + v.z);
+  d2bits = max(d2bits, __float_as_uint(dd));
+  d.pos[s] = p;
+  d.vel[s] = v;
+}
+
+// Pre-force update of one chunk per block; each of the kChunk / APT threads
+// updates APT atoms (all loads issued before any arithmetic).
+template <int APT>
+__global__ void __launch_bounds__(kChunk / APT, APT == 1 ? 6 : 12) k_pre(Dev d, StepConds cond) {
+  constexpr int T = kChunk / APT;
   count_launch(d, kKPre);
   // the previous step's rebuild has finished: empty the work list before
   // this step's commits append to it
@@ -149,102 +216,53 @@ __global__ void __launch_bounds__(kChunk, 6) k_pre(Dev d, StepConds cond) {
   }
   const int4 ci = d.chunk_rep[blockIdx.x];
   if (ci.x < 0) return;
-  const int s = ci.y + threadIdx.x;
-  const bool have = (int)threadIdx.x < ci.z;
-  // The atom's data depends neither on the replica record nor on the step
-  // scalars: issue its loads first.
-  float4 p = make_float4(0, 0, 0, 0), v = p, f = p, q = p;
-  if (have) {
-    p = d.pos[s];
-    v = d.vel[s];
-    f = d.force[s];
-    q = d.ref[s];
+  // The atoms' data depends neither on the replica record nor on the step
+  // scalars: issue their loads first.
+  float4 p[APT], v[APT], f[APT], q[APT];
+#pragma unroll
+  for (int k = 0; k < APT; ++k) {
+    const int t = threadIdx.x + k * T;
+    p[k] = v[k] = f[k] = q[k] = make_float4(0, 0, 0, 0);
+    if (t < ci.z) {
+      p[k] = d.pos[ci.y + t];
+      v[k] = d.vel[ci.y + t];
+      f[k] = d.force[ci.y + t];
+      q[k] = d.ref[ci.y + t];
+    }
   }
   Rep& R = d.reps[ci.x];
   __shared__ StepScalars S;
-  __shared__ uint32_t wmax[kChunk / 32];
+  __shared__ uint32_t wmax[T / 32];
   if (!(R.active && R.step < R.stop_step)) return;
   const bool deferred = R.defer != 0;
   if (R.next_valid) {
     constexpr int nw = (int)(sizeof(StepScalars) / sizeof(uint32_t));
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&R.next);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&S);
-    for (int k = threadIdx.x; k < nw; k += kChunk) dst[k] = src[k];
+    for (int k = threadIdx.x; k < nw; k += T) dst[k] = src[k];
   } else if (threadIdx.x == 0) {
     compute_step_scalars(R, S);
   }
   __syncthreads();
   uint32_t d2bits = 0;
   int bad = 0;
-  if (have) {
-    const float hm = S.hdt * v.w;
-    if (deferred) {
-      // the previous step's post-force half kick (same step size, same
-      // operation as the post-force kernel would have done)
-      v.x = fmaf(hm, f.x, v.x);
-      v.y = fmaf(hm, f.y, v.y);
-      v.z = fmaf(hm, f.z, v.z);
-    }
-    v.x *= S.vscale;
-    v.y *= S.vscale;
-    v.z *= S.vscale;
-    if (S.ens == FMD_LANGEVIN) {
-      float n0, n1, n2;
-      normal3_f32(R.seed, S.stream, (uint64_t)S.step, (uint32_t)__float_as_int(q.w), n0, n1, n2);
-      const float ns = S.c2kT * sqrtf(v.w);
-      v.x = fmaf(hm, f.x, v.x);
-      v.y = fmaf(hm, f.y, v.y);
-      v.z = fmaf(hm, f.z, v.z);
-      p.x = fmaf(S.hdt, v.x, p.x);
-      p.y = fmaf(S.hdt, v.y, p.y);
-      p.z = fmaf(S.hdt, v.z, p.z);
-      v.x = fmaf(S.c1, v.x, ns * n0);
-      v.y = fmaf(S.c1, v.y, ns * n1);
-      v.z = fmaf(S.c1, v.z, ns * n2);
-      p.x = fmaf(S.hdt, v.x, p.x);
-      p.y = fmaf(S.hdt, v.y, p.y);
-      p.z = fmaf(S.hdt, v.z, p.z);
-    } else if (S.ens == FMD_NVT_NH) {
-      v.x = fmaf(hm, f.x, v.x);
-      v.y = fmaf(hm, f.y, v.y);
-      v.z = fmaf(hm, f.z, v.z);
-      p.x = fmaf(S.dt, v.x, p.x);
-      p.y = fmaf(S.dt, v.y, p.y);
-      p.z = fmaf(S.dt, v.z, p.z);
-    } else {
-      v.x = fmaf(hm, f.x, v.x);
-      v.y = fmaf(hm, f.y, v.y);
-      v.z = fmaf(hm, f.z, v.z);
-      const uint32_t u = w_bits(p.w);
-      const float cx = (float)w_cx(u), cy = (float)w_cy(u), cz = (float)w_cz(u);
-      const float wx = floorf(fmaf(cx, S.h_old, p.x) * S.inv_Lold);
-      const float wy = floorf(fmaf(cy, S.h_old, p.y) * S.inv_Lold);
-      const float wz = floorf(fmaf(cz, S.h_old, p.z) * S.inv_Lold);
-      p.x = fmaf(p.x, S.ev, fmaf(cx, S.dh, fmaf(wx, S.dW, v.x * S.fpos)));
-      p.y = fmaf(p.y, S.ev, fmaf(cy, S.dh, fmaf(wy, S.dW, v.y * S.fpos)));
-      p.z = fmaf(p.z, S.ev, fmaf(cz, S.dh, fmaf(wz, S.dW, v.z * S.fpos)));
-      q.x = fmaf(q.x, S.ev, cx * S.dh);
-      q.y = fmaf(q.y, S.ev, cy * S.dh);
-      q.z = fmaf(q.z, S.ev, cz * S.dh);
-      d.ref[s] = q;
-    }
-    const float ux = p.x - q.x, uy = p.y - q.y, uz = p.z - q.z;
-    const float dd = ux * ux + uy * uy + uz * uz;
-    bad = !isfinite(dd) || !isfinite(v.x + v.y + v.z);
-    d2bits = __float_as_uint(dd);
-    d.pos[s] = p;
-    d.vel[s] = v;
+#pragma unroll
+  for (int k = 0; k < APT; ++k) {
+    const int t = threadIdx.x + k * T;
+    if (t < ci.z) pre_atom(d, R, S, ci.y + t, deferred, p[k], v[k], f[k], q[k], d2bits, bad);
   }
   warp_max_u32(d2bits);
   if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2bits;
   bad = __syncthreads_or(bad);
   if (threadIdx.x == 0) {
     uint32_t m = 0;
-    for (int w = 0; w < kChunk / 32; ++w) m = max(m, wmax[w]);
+    for (int w = 0; w < T / 32; ++w) m = max(m, wmax[w]);
     atomicMax(&R.maxdisp_bits, m);
     if (bad) atomicOr(&R.status, kStatusNonFinite);
   }
 }
+
+constexpr int kPreAPT = 2;  // atoms per thread of the launched pre-force kernel
 
 // Per-replica commit of the pre-force update (one thread per replica, after
 // every pre-force block finished): step counter, chain / barostat state, box,
@@ -288,11 +306,18 @@ __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& con
   R.Lpos = R.L;
   R.adv = 1;
   R.since += 1;
+  // An unlisted pair was farther than rc + skin when the list was built; a
+  // box that has shrunk by s = L / L_list since brings it to s (rc + skin)
+  // less the two atoms' displacements in the co-scaled frame, so the list
+  // stays complete while each displacement is below (s (rc + skin) - rc) / 2
+  // (skin / 2 at constant box, the trigger of skin_trigger.cuh:6-33).
   const float maxd2 = __uint_as_float(R.maxdisp_bits);
-  const float hs = (float)(0.5 * R.skin);
-  const bool trig = maxd2 > hs * hs;
+  const double s = R.L / R.L_list;
+  const float hs = (float)(s < 1.0 ? 0.5 * (s * (R.rc + R.skin) - R.rc) : 0.5 * R.skin);
+  const bool trig = hs <= 0.f || maxd2 > hs * hs;
   if (trig || R.since >= R.max_between) {
     R.since = 0;
+    R.L_list = R.L;
     R.maxdisp_bits = 0u;
     R.rebuilds += 1;
     R.rebuild_now = 1;
@@ -729,10 +754,8 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
                 const float rz = (pi.z - jz) - shift_term(ez, kz, h, dL);
                 const float r2 = rx * rx + ry * ry + rz * rz;
                 if (r2 < rcs2) {
-                  const bool ok = ex >= -1 && ex <= 1 && ey >= -1 && ey <= 1 && ez >= -1 && ez <= 1 &&
-                                  kx == implied_wrap(w_cx(ui), ex, G) && ky == implied_wrap(w_cy(ui), ey, G) &&
-                                  kz == implied_wrap(w_cz(ui), ez, G);
-                  if (!ok) {
+                  const int ax = axis_shift_code(ex, kx), ay = axis_shift_code(ey, ky), az = axis_shift_code(ez, kz);
+                  if (ax < 0 || ay < 0 || az < 0) {
                     overflow |= kStatusCellCapacity;
                     continue;
                   }
@@ -741,7 +764,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
                   for (int b = b0; b < b1; ++b) excl |= (d.bent[R.bond_base + b].x == idj);
                   if (excl) continue;
                   if (count < M)
-                    out[(size_t)count * 32] = (uint32_t)j | (cell_offset_code(ex, ey, ez) << kCodeShift);
+                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)(ax * 25 + ay * 5 + az) << kCodeShift);
                   ++count;
                 }
               }
@@ -810,7 +833,8 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
     s_sx[t] = shift_term(dx, kx, h, dL);
     s_sy[t] = shift_term(dy, ky, h, dL);
     s_sz[t] = shift_term(dz, kz, h, dL);
-    s_code[t] = cell_offset_code(dx, dy, dz) << kCodeShift;
+    s_code[t] = (uint32_t)(axis_shift_code(dx, kx) * 25 + axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz))
+                << kCodeShift;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -930,7 +954,8 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
   __shared__ float4 s_c[kNbrCap];
   __shared__ int s_ns[kNbrUnion], s_off[kNbrUnion + 1];
   __shared__ float s_sx[kNbrUnion], s_sy[kNbrUnion], s_sz[kNbrUnion];
-  __shared__ uint32_t s_yz[kNbrUnion];  // y and z parts of the cell-offset code
+  __shared__ int s_ax[kNbrUnion];   // wrap count kx of the union column
+  __shared__ int s_ayz[kNbrUnion];  // (axis code y) * 5 + (axis code z)
   if (threadIdx.x < nu) {
     const int u = threadIdx.x;
     const int row = u / ux, col = u % ux;
@@ -948,7 +973,8 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
     s_sx[u] = shift_term(xu - hx0, kx, h, dL);
     s_sy[u] = shift_term(dy, ky, h, dL);
     s_sz[u] = shift_term(dz, kz, h, dL);
-    s_yz[u] = cell_offset_code(-1, dy, dz);
+    s_ax[u] = kx;
+    s_ayz[u] = axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -995,7 +1021,8 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
       for (int row = 0; row < 9; ++row) {
         for (int dx = -1; dx <= 1; ++dx) {
           const int u = row * ux + a + 1 + dx;
-          const uint32_t code = (s_yz[u] | (uint32_t)(dx + 1)) << kCodeShift;
+          const uint32_t code =
+              (uint32_t)(axis_shift_code(dx, s_ax[u]) * 25 + s_ayz[u]) << kCodeShift;
           const int k0 = s_off[u], k1 = s_off[u + 1];
           const float sx = s_sx[u], sy = s_sy[u], sz = s_sz[u];
           const int ns = s_ns[u];
@@ -1103,29 +1130,20 @@ __device__ __forceinline__ void block_partials(double* vals, int nv, double* out
   }
 }
 
-// LJ contribution of one listed neighbor (lj.cu:32-61 semantics).  t is
-// atom i's position minus the entry's cell shift, so r_ij = t - pos_j.  EV:
-// also accumulate half the pair energy and the virial half-pair.
+// LJ contribution of one listed neighbor (lj.cu:32-61 semantics).  sh is
+// the periodic shift vector named by the entry's code, so
+// r_ij = (pos_i - pos_j) - sh.  EV: also accumulate half the pair energy and
+// the virial half-pair.
 struct PairAcc {
   float fx, fy, fz, pe, v0, v1, v2, v3, v4, v5;
 };
 
-// Atom i's coordinates minus the cell shift for e = -1, 0, +1 per axis
-// (periodic wrap included where i sits in an edge cell); a list entry's
-// 6-bit cell-offset code picks one per axis.
-struct ShiftedPos {
-  float xm, x0, xp, ym, y0, yp, zm, z0, zp;
-  __device__ __forceinline__ float3 pick(uint32_t c) const {
-    return make_float3((c & 2u) ? xp : ((c & 1u) ? x0 : xm), (c & 8u) ? yp : ((c & 4u) ? y0 : ym),
-                       (c & 32u) ? zp : ((c & 16u) ? z0 : zm));
-  }
-};
-
 template <bool EV>
-__device__ __forceinline__ void lj_pair(PairAcc& a, float3 t, float4 pj, float rc2, float e24, float sig2) {
-  const float dx = t.x - pj.x;
-  const float dy = t.y - pj.y;
-  const float dz = t.z - pj.z;
+__device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4 pj, float rc2, float e24,
+                                        float sig2) {
+  const float dx = (pi.x - pj.x) - sh.x;
+  const float dy = (pi.y - pj.y) - sh.y;
+  const float dz = (pi.z - pj.z) - sh.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   // Branch-free: every listed pair is evaluated and pairs outside the cutoff
   // (or the r = 0 padding entries) contribute an exact zero through selects.
@@ -1158,8 +1176,8 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float3 t, float4 pj, float r
 // words are loaded before this batch's gathers (software pipelining, B more
 // registers).  nn is the padded length (a multiple of B).
 template <bool EV, int B, bool PF, int KB>
-__device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, const ShiftedPos& sp,
-                                        bool one_type, int ti, int nt, const float* s_eps24,
+__device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
+                                        const float4* s_shift, bool one_type, int ti, int nt, const float* s_eps24,
                                         const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
                                         PairAcc& acc) {
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
@@ -1195,7 +1213,7 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
         e24 = s_eps24[pidx];
         sig2 = s_sig2[pidx];
       }
-      lj_pair<EV>(g, sp.pick(w[q] >> kCodeShift), pj[q], rc2, e24, sig2);
+      lj_pair<EV>(g, pi, s_shift[w[q] >> kCodeShift], pj[q], rc2, e24, sig2);
     }
     if (++kb == KB || k + B >= nn) {
       fx.add(g.fx);
@@ -1271,6 +1289,7 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
   if (!R.adv) return;
   if (need_ev(R) != EV) return;
   constexpr bool ev = EV;
+  __shared__ float4 s_shift[kShiftCodes];
   __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
   const int nt = R.ntypes;
   const int G = R.G;
@@ -1279,6 +1298,13 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
     s_eps24[k] = R.lj_eps24[k];
     s_sig2[k] = R.lj_sig2[k];
+  }
+  if (threadIdx.x < kShiftCodes) {
+    const int c = threadIdx.x;
+    const int ax = c / 25, ay = (c / 5) % 5, az = c % 5;
+    s_shift[c] = make_float4(shift_term(axis_code_e(ax), axis_code_k(ax), h, dL),
+                             shift_term(axis_code_e(ay), axis_code_k(ay), h, dL),
+                             shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
   }
   __syncthreads();
   const int local = ci.w * kChunk + threadIdx.x;
@@ -1298,21 +1324,7 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
     const bool one_type = (nt == 1);
-    // pos_i - (e h + k dL) per axis for e = -1, 0, +1 (k from this atom's cell)
-    ShiftedPos sp;
-    {
-      const int cx = w_cx(ui), cy = w_cy(ui), cz = w_cz(ui);
-      sp.x0 = pi.x;
-      sp.xm = pi.x - shift_term(-1, implied_wrap(cx, -1, G), h, dL);
-      sp.xp = pi.x - shift_term(1, implied_wrap(cx, 1, G), h, dL);
-      sp.y0 = pi.y;
-      sp.ym = pi.y - shift_term(-1, implied_wrap(cy, -1, G), h, dL);
-      sp.yp = pi.y - shift_term(1, implied_wrap(cy, 1, G), h, dL);
-      sp.z0 = pi.z;
-      sp.zm = pi.z - shift_term(-1, implied_wrap(cz, -1, G), h, dL);
-      sp.zp = pi.z - shift_term(1, implied_wrap(cz, 1, G), h, dL);
-    }
-    lj_loop<EV, B, PF, KB>(lst, nn, pbase, sp, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    lj_loop<EV, B, PF, KB>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
@@ -1562,7 +1574,7 @@ int num_sms() {
 
 void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t st) {
   const StepConds none{0, 0, 0, 0, 0, 0};
-  k_pre<<<g.nchunks, kChunk, 0, st>>>(d, none);
+  k_pre<kPreAPT><<<g.nchunks, kChunk / kPreAPT, 0, st>>>(d, none);
   k_commit<<<g.nreps, 32, 0, st>>>(d, none);
   FMD_CUDA(cudaMemcpyAsync(host_mode, d.rb + kRbMode, sizeof(int), cudaMemcpyDeviceToHost, st));
   FMD_CUDA(cudaStreamSynchronize(st));
@@ -1613,7 +1625,7 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_plain, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
-  k_pre<<<nchunks, kChunk, 0, st>>>(d, c);
+  k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
   k_commit<<<nreps, 32, 0, st>>>(d, c);
   // The two rebuild forms exclude each other, and so do the replicas each
   // force flavour serves: each pair is captured as parallel branches so the

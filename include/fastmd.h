@@ -255,12 +255,16 @@ FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_
  * fastest for all following steps.  chosen = force variant index;
  * ms_per_variant (cap entries, may be NULL) = device ms per launch of each
  * force variant (7), then ms per full rebuild of each neighbor variant (3),
- * then the chosen neighbor variant. */
+ * then the chosen neighbor variant.  It also lifts the forced rebuild
+ * cadence of the active replicas (rebuilds then follow the skin/2
+ * displacement trigger alone; fmd_batch_set_rebuild_cadence restores one). */
 FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chosen, double* ms_per_variant,
                                       int32_t cap);
 /* Set the forced rebuild cadence of a replica (the reference rebuilds at
- * least every 20 steps, main.cu:401); the skin/2 displacement test still
- * triggers rebuilds in between. */
+ * least every 20 steps, main.cu:401, the default here); the skin/2
+ * displacement test still triggers rebuilds in between.  max_steps <= 0:
+ * no forced cadence (skin trigger only, which is what fmd_batch_autotune
+ * selects). */
 FMD_API fmd_status fmd_batch_set_rebuild_cadence(fmd_batch* b, int32_t slot, int32_t max_steps);
 
 /* ------------------------------------------------------------- serving */

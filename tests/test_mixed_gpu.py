@@ -123,6 +123,34 @@ def test_batch_alone_equals_in_mix():
         alone.close()
 
 
+@pytest.mark.parametrize("ens", ["nvt_langevin 1.0 1.0 1.0 7", "npt_nh 1.0 1.0 0.5 12.0 12.0 0.3 3"])
+def test_trigger_only_rebuilds_keep_list_complete(ens):
+    """With the forced cadence lifted, rebuilds follow the displacement and
+    box-shrink trigger alone, and the forces computed from the list in use
+    stay the oracle's (a missing pair would show as a large error).  The NPT
+    case drives the box down with a high target pressure."""
+    pre = fm.Simulation(run_conf(), gen=dict(nchains=20, chain_length=50, density=0.85, seed=11, pushoff_steps=2000),
+                        form=fm.FMD_FORM_MIXED)
+    x0, v0, i0 = pre.state()
+    d = _melt(20, 50, seed=11)
+    d.xyz, d.vel, d.image = x0, v0, i0
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 14)
+    s = b.add(run_conf(ensemble=ens, nsteps=600), desc=d)
+    b.set_rebuild_cadence(s, 0)
+    L0 = b.info(s).box_L
+    for _ in range(12):
+        b.run(50)
+        x, _, _ = b.state(s)
+        f, _, _ = b.forces(s)
+        info = b.info(s)
+        fo, _, _ = po.forces(oracle_system(d, xyz=x, L=info.box_L))
+        assert rel_rms(f, fo) < FORCE_RMS_TOL, (ens, info.step, rel_rms(f, fo))
+        assert info.status_word == 0
+    if ens.startswith("npt"):
+        assert b.info(s).box_L < 0.995 * L0
+    b.close()
+
+
 def test_pushoff_then_langevin_is_stable():
     conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 42", nsteps=2000)
     sim = fm.Simulation(conf, gen=dict(nchains=30, chain_length=100, density=0.85, seed=42, pushoff_steps=2000),
