@@ -420,6 +420,15 @@ class Batch:
         _call("fmd_batch_compute_forces", self._h, C.c_int32(slot), _ptr(f), _ptr(pe), _ptr(vir))
         return f, pe, vir
 
+    def force_frame(self, slot):
+        """Positions and box edge of the geometry the forces belong to (the
+        box of the last pre-force update; differs from info().box_L under NPT
+        after the barostat's post-force half step)."""
+        x = np.zeros((self._natoms[slot], 3))
+        L = C.c_double()
+        _call("fmd_batch_get_force_frame", self._h, C.c_int32(slot), _ptr(x), C.byref(L))
+        return x, L.value
+
     def totals(self):
         a = C.c_int32()
         n = C.c_int64()

@@ -316,6 +316,7 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   R.G = G;
   R.L = L;
   R.L_list = L;
+  R.list_scale = 1.0;
   R.Lpos = L;
   R.h = (float)(L / G);
   R.maxdisp_bits = 0;
@@ -608,6 +609,7 @@ void Batch::setup(const std::vector<int>& rs) {
     R.rebuild_now = 1;
     R.since = 0;
     R.L_list = R.L;
+    R.list_scale = 1.0;
     R.maxdisp_bits = 0;
     R.force_ev = 1;
   }
@@ -889,6 +891,11 @@ const Rep& Batch::rep(int r) const {
 }
 
 void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) { read_state(r, xyz, vel, image, true); }
+
+void Batch::force_frame(int r, double* xyz, double* box) {
+  read_state(r, xyz, nullptr, nullptr, false);
+  if (box) *box = rep(r).Lpos;
+}
 
 void Batch::read_state(int r, double* xyz, double* vel, int32_t* image, bool rewrap) {
   const Rep& R = rep(r);

@@ -76,6 +76,7 @@ class Batch {
   int64_t graph_captures() const { return graph_captures_; }
   void launch_counts(int64_t* counts, int n);
   void read_state(int r, double* xyz, double* vel, int32_t* image, bool rewrap);
+  void force_frame(int r, double* xyz, double* box);
   void set_state(int r, const double* xyz, const double* vel, const int32_t* image);
   void forces(int r, double* f, double* pe, double* vir);
   void thermo(int r, fmd_thermo_row* row);

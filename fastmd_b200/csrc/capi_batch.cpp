@@ -151,6 +151,14 @@ FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* 
   });
 }
 
+FMD_API fmd_status fmd_batch_get_force_frame(fmd_batch* b, int32_t slot, double* xyz, double* box_L) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    bb.force_frame(slot, xyz, box_L);
+  });
+}
+
 FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n) {
   return guarded([&] {
     auto& bb = B(b);

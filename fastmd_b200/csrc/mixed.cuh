@@ -119,6 +119,7 @@ struct Rep {
   double L;      // box edge (barostat value)
   double Lpos;   // box the stored positions are wrapped in (last pre-force)
   double L_list; // box the neighbor list was built in (box-shrink term of the rebuild trigger)
+  double list_scale;  // product of the NPT position scale factors since the list was built
   float h;
   uint32_t maxdisp_bits;
   int32_t status;

@@ -306,18 +306,22 @@ __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& con
   R.Lpos = R.L;
   R.adv = 1;
   R.since += 1;
-  // An unlisted pair was farther than rc + skin when the list was built; a
-  // box that has shrunk by s = L / L_list since brings it to s (rc + skin)
-  // less the two atoms' displacements in the co-scaled frame, so the list
-  // stays complete while each displacement is below (s (rc + skin) - rc) / 2
-  // (skin / 2 at constant box, the trigger of skin_trigger.cuh:6-33).
+  // An unlisted pair was farther than rc + skin when the list was built; an
+  // NPT contraction by s since brings it to s (rc + skin) less the two atoms'
+  // displacements in the co-scaled frame, so the list stays complete while
+  // each displacement is below (s (rc + skin) - rc) / 2 (skin / 2 at
+  // constant box, the trigger of skin_trigger.cuh:6-33).  Pairs inside the
+  // box scale with the positions' factors, pairs across a face with the box:
+  // s is the smaller of the two.
+  if (S.ens == FMD_NPT_NH) R.list_scale *= (double)S.ev;
   const float maxd2 = __uint_as_float(R.maxdisp_bits);
-  const double s = R.L / R.L_list;
+  const double s = fmin(R.L / R.L_list, R.list_scale);
   const float hs = (float)(s < 1.0 ? 0.5 * (s * (R.rc + R.skin) - R.rc) : 0.5 * R.skin);
   const bool trig = hs <= 0.f || maxd2 > hs * hs;
   if (trig || R.since >= R.max_between) {
     R.since = 0;
     R.L_list = R.L;
+    R.list_scale = 1.0;
     R.maxdisp_bits = 0u;
     R.rebuilds += 1;
     R.rebuild_now = 1;

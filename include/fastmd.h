@@ -225,6 +225,12 @@ FMD_API fmd_status fmd_batch_thermo(fmd_batch* b, int32_t slot, fmd_thermo_row* 
 FMD_API fmd_status fmd_batch_write_restart(fmd_batch* b, int32_t slot, const char* path);
 FMD_API fmd_status fmd_batch_rg(fmd_batch* b, int32_t slot, double* rg);
 FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* f, double* pe, double* virial);
+/* The geometry fmd_batch_compute_forces' forces belong to: positions (3N,
+ * atom-id order) wrapped in the box of the last pre-force update, and that
+ * box edge.  It is the current box except under NPT, whose post-force
+ * barostat half step moves box_L before the next pre-force rescales the
+ * positions (fmd_batch_get_state reports them re-wrapped into box_L). */
+FMD_API fmd_status fmd_batch_get_force_frame(fmd_batch* b, int32_t slot, double* xyz, double* box_L);
 FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n);
 /* Totals: active replicas, atoms, device bytes in use. */
 FMD_API fmd_status fmd_batch_totals(fmd_batch* b, int32_t* active, int64_t* atoms, int64_t* bytes);
