@@ -104,7 +104,12 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   FMD_CUDA(cudaSetDevice(device_));
   FMD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
   FMD_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-  FMD_CUDA(cudaStreamCreateWithFlags(&branch_, cudaStreamNonBlocking));
+  for (auto& b : branch_) FMD_CUDA(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+  {
+    int least = 0, greatest = 0;
+    FMD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    FMD_CUDA(cudaStreamCreateWithPriority(&side_hi_, cudaStreamNonBlocking, greatest));
+  }
   // graph_steps < 0: no graph (every step launched directly; for profilers
   // that cannot see into graphs with conditional nodes)
   graph_steps_ = o.graph_steps > 0 ? o.graph_steps : (o.graph_steps < 0 ? 0 : 50);
@@ -176,7 +181,9 @@ Batch::~Batch() {
     if (e) cudaEventDestroy(e);
   if (st_) cudaStreamDestroy(st_);
   if (side_) cudaStreamDestroy(side_);
-  if (branch_) cudaStreamDestroy(branch_);
+  for (auto& b : branch_)
+    if (b) cudaStreamDestroy(b);
+  if (side_hi_) cudaStreamDestroy(side_hi_);
 }
 
 Dev Batch::dev() const {
@@ -661,7 +668,7 @@ void Batch::ensure_graph() {
     cudaGraph_t g;
   FMD_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   try {
-    for (int k = 0; k < graph_steps_; ++k) capture_step(d, want, st_, side_, branch_);
+    for (int k = 0; k < graph_steps_; ++k) capture_step(d, want, st_, side_, side_hi_, branch_);
   } catch (...) {
     cudaGraph_t partial = nullptr;
     cudaStreamEndCapture(st_, &partial);
@@ -669,7 +676,9 @@ void Batch::ensure_graph() {
     throw;
   }
   FMD_CUDA(cudaStreamEndCapture(st_, &g));
-  FMD_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
+  // per-node priorities: the rebuild branch's kernels are dispatched ahead of
+  // the force kernels that run beside them
+  FMD_CUDA(cudaGraphInstantiate(&graph_exec_, g, cudaGraphInstantiateFlagUseNodePriority));
   cudaGraphDestroy(g);
   graph_dirty_ = false;
   graph_shape_ = want;
@@ -780,8 +789,8 @@ double Batch::time_force(int iters, int variant) {
   const Dev d = dev();
   const int nc = nchunks_launch();
   auto once = [&] {
-    if (any_plain) launch_force(d, nc, false, variant, st_);
-    if (any_ev) launch_force(d, nc, true, variant, st_);
+    if (any_plain) launch_force(d, nc, false, variant, st_, false);
+    if (any_ev) launch_force(d, nc, true, variant, st_, false);
   };
   once();  // warm
   FMD_CUDA_LAUNCH();

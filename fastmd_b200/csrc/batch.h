@@ -122,7 +122,8 @@ class Batch {
   int device_ = 0;
   cudaStream_t st_ = nullptr;
   cudaStream_t side_ = nullptr;    // captures conditional-node bodies
-  cudaStream_t branch_ = nullptr;  // second branch of a captured step
+  cudaStream_t side_hi_ = nullptr;  // captures the rebuild branches' bodies (high priority)
+  cudaStream_t branch_[3] = {};     // further branches of a captured step
   int graph_steps_ = 50;
   int force_variant_ = 0;
   bool concurrent_pushoff_ = false;

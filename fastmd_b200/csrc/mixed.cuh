@@ -264,9 +264,15 @@ void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t 
 // The same step recorded into the graph being captured on st, with the
 // conditional nodes; side is a second stream used to capture their bodies.
 // st2: a second capture stream for the parallel branches of a step.
-void capture_step(const Dev& d, const StepShape& g, cudaStream_t st, cudaStream_t side, cudaStream_t st2);
+// Records one step into the graph being captured on st.  side / side_hi
+// record conditional-node bodies (side_hi: high priority, for the rebuild
+// branches); br: three further streams for the parallel branches.
+void capture_step(const Dev& d, const StepShape& g, cudaStream_t st, cudaStream_t side, cudaStream_t side_hi,
+                  const cudaStream_t* br);
 void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st);
-void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st);
+void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st, bool skip_rebuilt);
+// Forces of the replicas on the rebuild work list (after their rebuild).
+void launch_force_rebuilt(const Dev& d, bool ev, int variant, cudaStream_t st);
 // Rebuild of the replicas on the work list (rb): bin, scan, scatter, cell sort,
 // permute, bonded tables, neighbor lists.
 void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st);

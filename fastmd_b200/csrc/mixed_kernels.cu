@@ -405,19 +405,23 @@ __device__ __forceinline__ int rb_find(const int* off, int n, int item) {
   return lo;
 }
 
-// Block-wide exclusive scan of v over the list (1024 threads), into off[0..n].
+// Small single-block kernels (plans, per-replica scans) run kPlanThreads
+// threads: blocks that fit beside the force kernels when they share the GPU.
+constexpr int kPlanThreads = 256;
+
+// Block-wide exclusive scan of v over the list (kPlanThreads threads), into off[0..n].
 template <typename F>
 __device__ void rb_scan(const Dev& d, int n, int* off, F value) {
-  __shared__ int sm[1024];
+  __shared__ int sm[kPlanThreads];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
-  for (int base = 0; base < n; base += 1024) {
+  for (int base = 0; base < n; base += kPlanThreads) {
     const int i = base + threadIdx.x;
     const int v = i < n ? value(rb_rep(d, i)) : 0;
     sm[threadIdx.x] = v;
     __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
+    for (int o = 1; o < kPlanThreads; o <<= 1) {
       const int t = threadIdx.x >= o ? sm[threadIdx.x - o] : 0;
       __syncthreads();
       sm[threadIdx.x] += t;
@@ -425,7 +429,7 @@ __device__ void rb_scan(const Dev& d, int n, int* off, F value) {
     }
     if (i < n) off[i] = carry + sm[threadIdx.x] - v;
     __syncthreads();
-    if (threadIdx.x == 1023) carry += sm[1023];
+    if (threadIdx.x == kPlanThreads - 1) carry += sm[kPlanThreads - 1];
     __syncthreads();
   }
   if (threadIdx.x == 0) off[n] = carry;
@@ -434,7 +438,7 @@ __device__ void rb_scan(const Dev& d, int n, int* off, F value) {
 constexpr int kCellGroup = 8;  // cells per cell-sort work item (one warp each)
 
 // Offsets of chunk items and cell-group items (P^3 Morton cells per replica).
-__global__ void __launch_bounds__(1024) k_rbplan(Dev d) {
+__global__ void __launch_bounds__(kPlanThreads) k_rbplan(Dev d) {
   count_launch(d, kKPlan);
   const int n = rb_count(d);
   rb_scan(d, n, rb_off(d, 0), [&](int r) { return d.reps[r].nchunks; });
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(1024) k_rbplan(Dev d) {
 }
 
 // Offsets of home-cell items (G^3 per replica, G as set by k_scan).
-__global__ void __launch_bounds__(1024) k_rbplan_home(Dev d, int variant) {
+__global__ void __launch_bounds__(kPlanThreads) k_rbplan_home(Dev d, int variant) {
   count_launch(d, kKPlan);
   const int n = rb_count(d);
   rb_scan(d, n, rb_off(d, 2), [&](int r) {
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(kChunk) k_bin(Dev d) {
 }
 
 // Exclusive scan of the replica's cell counts; one block per replica.
-__global__ void __launch_bounds__(1024) k_scan(Dev d) {
+__global__ void __launch_bounds__(kPlanThreads) k_scan(Dev d) {
   count_launch(d, kKScan);
   if ((int)blockIdx.x >= rb_count(d)) return;
   Rep& R = d.reps[rb_rep(d, blockIdx.x)];
@@ -550,10 +554,10 @@ __global__ void __launch_bounds__(1024) k_scan(Dev d) {
   const int b1 = min(b0 + per, ncell);
   int sum = 0;
   for (int c = b0; c < b1; ++c) sum += d.cell_cnt[R.cell_base + c];
-  __shared__ int sm[1024];
+  __shared__ int sm[kPlanThreads];
   sm[threadIdx.x] = sum;
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
+  for (int off = 1; off < kPlanThreads; off <<= 1) {
     const int t = threadIdx.x >= off ? sm[threadIdx.x - off] : 0;
     __syncthreads();
     sm[threadIdx.x] += t;
@@ -1279,19 +1283,21 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
   }
 }
 
-// Two instantiations: with energies / virial (thermo steps, NPT, host
-// requests) and without (all other steps); a block runs in the one that
-// matches its replica's need this step and the other returns at once.
-template <bool EV, int B, int MINB, bool PF, int KB>
-__global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
-  count_launch(d, EV ? kKForceEv : kKForce);
-  const int chunk = blockIdx.x;
+// Forces of one chunk (block-uniform: every thread of the block calls it
+// with the same chunk).  Two instantiations: with energies / virial (thermo
+// steps, NPT, host requests) and without (all other steps); a chunk is
+// computed by the one that matches its replica's need this step and the
+// other returns at once.  skip_rebuilt: leave replicas that rebuild their
+// list this step to the work-list launch that follows their rebuild.
+template <bool EV, int B, bool PF, int KB>
+__device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_rebuilt) {
   const int4 ci = d.chunk_rep[chunk];
   const int r = ci.x;
   if (r < 0) return;
   const Rep& R = d.reps[r];
   if (!R.adv) return;
   if (need_ev(R) != EV) return;
+  if (skip_rebuilt && R.rebuild_now) return;
   constexpr bool ev = EV;
   __shared__ float4 s_shift[kShiftCodes];
   __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
@@ -1409,6 +1415,31 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d) {
   status = __syncthreads_or(status);
   if (threadIdx.x == 0 && status) atomicOr((int*)&d.reps[r].status, status);
   if (EV) block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
+}
+
+// One block per chunk of the batch.
+template <bool EV, int B, int MINB, bool PF, int KB>
+__global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt) {
+  count_launch(d, EV ? kKForceEv : kKForce);
+  force_chunk<EV, B, PF, KB>(d, blockIdx.x, skip_rebuilt != 0);
+}
+
+// The chunks of the replicas on the rebuild work list (a resident grid
+// striding over them), launched after their rebuild while the other
+// replicas' forces run beside it.
+template <bool EV, int B, int MINB, bool PF, int KB>
+__global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
+  count_launch(d, EV ? kKForceEv : kKForce);
+  const int n = rb_count(d);
+  const int* off = rb_off(d, 0);
+  const int total = n > 0 ? off[n] : 0;
+  RbCursor cur(off, n, blockIdx.x);
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    cur.seek(item);
+    __syncthreads();  // the previous item's shared tables are no longer read
+    const Rep& R = d.reps[rb_rep(d, cur.i)];
+    force_chunk<EV, B, PF, KB>(d, R.chunk_base + (item - cur.lo), false);
+  }
 }
 
 // ---------------------------------------------------------------- post-force
@@ -1584,8 +1615,8 @@ void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t 
   FMD_CUDA(cudaStreamSynchronize(st));
   if (*host_mode == kRbList) launch_rebuild(d, g.nreps, g.nbr_variant, st);
   if (*host_mode == kRbFull) launch_rebuild_full(d, g, st);
-  launch_force(d, g.nchunks, false, g.force_variant, st);
-  launch_force(d, g.nchunks, true, g.force_variant, st);
+  launch_force(d, g.nchunks, false, g.force_variant, st, false);
+  launch_force(d, g.nchunks, true, g.force_variant, st, false);
   k_post<<<g.nchunks, kChunk, 0, st>>>(d, 1);
   k_post_commit<<<g.nreps, 32, 0, st>>>(d, 1);
 }
@@ -1617,7 +1648,8 @@ void capture_if(cudaStream_t st, cudaStream_t side, cudaGraphConditionalHandle h
 }
 }  // namespace
 
-void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStream_t side, cudaStream_t st2) {
+void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStream_t side, cudaStream_t side_hi,
+                  const cudaStream_t* br) {
   const int nchunks = shape.nchunks, nreps = shape.nreps, force_variant = shape.force_variant,
             nbr_variant = shape.nbr_variant;
   cudaStreamCaptureStatus cs;
@@ -1631,40 +1663,39 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
   k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
   k_commit<<<nreps, 32, 0, st>>>(d, c);
-  // The two rebuild forms exclude each other, and so do the replicas each
-  // force flavour serves: each pair is captured as parallel branches so the
-  // step's critical path has one conditional node per phase.
-  cudaEvent_t fork, join;
+  // Four parallel branches, each one conditional node: the two rebuild forms
+  // (they exclude each other), each followed by the forces of the replicas
+  // it rebuilt, and the two force flavours of every other replica, which so
+  // run beside the rebuild instead of after it.  The rebuild bodies are
+  // captured on a high-priority stream, so their blocks go first whenever
+  // the force kernels free a slot.
+  cudaEvent_t fork, join[3];
   FMD_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-  FMD_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
-  auto parallel = [&](auto&& a, auto&& b) {
-    FMD_CUDA(cudaEventRecord(fork, st));
-    FMD_CUDA(cudaStreamWaitEvent(st2, fork, 0));
-    a(st);
-    b(st2);
-    FMD_CUDA(cudaEventRecord(join, st2));
-    FMD_CUDA(cudaStreamWaitEvent(st, join, 0));
-  };
-  parallel(
-      [&](cudaStream_t s0) {
-        capture_if(s0, side, c.rebuild, [&](cudaStream_t s) { launch_rebuild(d, nreps, nbr_variant, s); });
-      },
-      [&](cudaStream_t s1) {
-        capture_if(s1, side, c.rebuild_full, [&](cudaStream_t s) { launch_rebuild_full(d, shape, s); });
-      });
-  parallel(
-      [&](cudaStream_t s0) {
-        capture_if(s0, side, c.force_plain, [&](cudaStream_t s) { launch_force(d, nchunks, false, force_variant, s); });
-      },
-      [&](cudaStream_t s1) {
-        capture_if(s1, side, c.force_ev, [&](cudaStream_t s) { launch_force(d, nchunks, true, force_variant, s); });
-      });
+  for (auto& e : join) FMD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  FMD_CUDA(cudaEventRecord(fork, st));
+  for (int b = 0; b < 3; ++b) FMD_CUDA(cudaStreamWaitEvent(br[b], fork, 0));
+  capture_if(st, side_hi, c.rebuild, [&](cudaStream_t s) {
+    launch_rebuild(d, nreps, nbr_variant, s);
+    launch_force_rebuilt(d, false, force_variant, s);
+    launch_force_rebuilt(d, true, force_variant, s);
+  });
+  capture_if(br[0], side_hi, c.rebuild_full, [&](cudaStream_t s) {
+    launch_rebuild_full(d, shape, s);
+    launch_force_rebuilt(d, false, force_variant, s);
+    launch_force_rebuilt(d, true, force_variant, s);
+  });
+  capture_if(br[1], side, c.force_plain, [&](cudaStream_t s) { launch_force(d, nchunks, false, force_variant, s, true); });
+  capture_if(br[2], side, c.force_ev, [&](cudaStream_t s) { launch_force(d, nchunks, true, force_variant, s, true); });
+  for (int b = 0; b < 3; ++b) {
+    FMD_CUDA(cudaEventRecord(join[b], br[b]));
+    FMD_CUDA(cudaStreamWaitEvent(st, join[b], 0));
+  }
   capture_if(st, side, c.post, [&](cudaStream_t s) {
     k_post<<<nchunks, kChunk, 0, s>>>(d, 1);
     k_post_commit<<<nreps, 32, 0, s>>>(d, 1);
   });
   FMD_CUDA(cudaEventDestroy(fork));
-  FMD_CUDA(cudaEventDestroy(join));
+  for (auto& e : join) FMD_CUDA(cudaEventDestroy(e));
 }
 
 namespace {
@@ -1676,17 +1707,45 @@ int resident_grid(K kernel, int threads) {
   FMD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
   return num_sms() * (per_sm > 0 ? per_sm : 1);
 }
+
+int rebuild_priority() {
+  static const int p = [] {
+    int least = 0, greatest = 0;
+    FMD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    return greatest;
+  }();
+  return p;
+}
+
+// Launch at the rebuild branch's priority.  Recorded in the kernel node when
+// captured, it makes the block scheduler dispatch the rebuild's blocks ahead
+// of the pending blocks of the force kernels running beside it.
+template <typename... KArgs, typename... Args>
+void launch_hi(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributePriority;
+  at[0].val.priority = rebuild_priority();
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  FMD_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
 }  // namespace
 
 void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st) {
   const int nr = g.nreps;
-  k_bin_g<<<g.nchunks, kChunk, 0, st>>>(d);
-  k_scan<<<nr, 1024, 0, st>>>(d);
-  k_scatter_g<<<g.nchunks, kChunk, 0, st>>>(d);
-  k_cellsort_g<<<dim3((g.max_cells + kCellGroup - 1) / kCellGroup, nr), 32 * kCellGroup, 0, st>>>(d);
-  k_permute_g<<<g.nchunks, kChunk, 0, st>>>(d);
-  k_topo_g<<<g.nchunks, kChunk, 0, st>>>(d);
-  k_neighbors_g<<<dim3(g.max_home, nr), kNbrThreads, 0, st>>>(d);
+  launch_hi(k_rbplan, 1, kPlanThreads, st, d);  // work-list offsets for the forces that follow
+  launch_hi(k_bin_g, g.nchunks, kChunk, st, d);
+  launch_hi(k_scan, nr, kPlanThreads, st, d);
+  launch_hi(k_scatter_g, g.nchunks, kChunk, st, d);
+  launch_hi(k_cellsort_g, dim3((g.max_cells + kCellGroup - 1) / kCellGroup, nr), 32 * kCellGroup, st, d);
+  launch_hi(k_permute_g, g.nchunks, kChunk, st, d);
+  launch_hi(k_topo_g, g.nchunks, kChunk, st, d);
+  launch_hi(k_neighbors_g, dim3(g.max_home, nr), kNbrThreads, st, d);
 }
 
 void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
@@ -1695,20 +1754,20 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
                    g_topo = resident_grid(k_topo, kChunk), g_nbr0 = resident_grid(k_neighbors<0, 8>, kNbrThreads),
                    g_nbr1 = resident_grid(k_neighbors<1, 6>, kNbrThreads),
                    g_nbr2 = resident_grid(k_neighbors<0, 6>, kNbrThreads);
-  k_rbplan<<<1, 1024, 0, st>>>(d);
-  k_bin<<<g_bin, kChunk, 0, st>>>(d);
-  k_scan<<<nreps, 1024, 0, st>>>(d);
-  k_scatter<<<g_scatter, kChunk, 0, st>>>(d);
-  k_cellsort<<<g_sort, 32 * kCellGroup, 0, st>>>(d);
-  k_permute<<<g_perm, kChunk, 0, st>>>(d);
-  k_topo<<<g_topo, kChunk, 0, st>>>(d);
-  k_rbplan_home<<<1, 1024, 0, st>>>(d, nbr_variant);
+  launch_hi(k_rbplan, 1, kPlanThreads, st, d);
+  launch_hi(k_bin, g_bin, kChunk, st, d);
+  launch_hi(k_scan, nreps, kPlanThreads, st, d);
+  launch_hi(k_scatter, g_scatter, kChunk, st, d);
+  launch_hi(k_cellsort, g_sort, 32 * kCellGroup, st, d);
+  launch_hi(k_permute, g_perm, kChunk, st, d);
+  launch_hi(k_topo, g_topo, kChunk, st, d);
+  launch_hi(k_rbplan_home, 1, kPlanThreads, st, d, nbr_variant);
   if (nbr_variant == 1)
-    k_neighbors<1, 6><<<g_nbr1, kNbrThreads, 0, st>>>(d);
+    launch_hi(k_neighbors<1, 6>, g_nbr1, kNbrThreads, st, d);
   else if (nbr_variant == 2)
-    k_neighbors<0, 6><<<g_nbr2, kNbrThreads, 0, st>>>(d);
+    launch_hi(k_neighbors<0, 6>, g_nbr2, kNbrThreads, st, d);
   else
-    k_neighbors<0, 8><<<g_nbr0, kNbrThreads, 0, st>>>(d);
+    launch_hi(k_neighbors<0, 8>, g_nbr0, kNbrThreads, st, d);
 }
 
 // Force-kernel variants (list entries per batch, blocks per SM, pipelined
@@ -1716,30 +1775,48 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
 // The energy flavour of a variant walks the list in the same batches with
 // the same compensated adds, so its forces are bit-identical: energy steps
 // and host re-evaluations do not perturb a trajectory.
+// The variant's two kernels: one block per chunk, and the work-list form.
 template <bool EV>
-void launch_force_t(const Dev& d, int nchunks, int variant, cudaStream_t st) {
+void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(Dev)) {
   constexpr int E = 5;  // blocks per SM of the energy flavours (more registers)
+#define FMD_FORCE_VARIANT(B, MINB, PF, KB)          \
+  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB>; \
+  *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB>;
   switch (variant) {
-    case 1: k_force<EV, 4, EV ? E : 8, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 2: k_force<EV, 4, EV ? E : 6, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 3: k_force<EV, 4, EV ? E : 8, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 4: k_force<EV, 2, EV ? E : 8, true, 4><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 5: k_force<EV, 4, EV ? E : 7, true, 2><<<nchunks, kChunk, 0, st>>>(d); break;
-    case 6: k_force<EV, 8, EV ? E : 6, false, 1><<<nchunks, kChunk, 0, st>>>(d); break;
-    default: k_force<EV, 4, EV ? E : 6, true, 1><<<nchunks, kChunk, 0, st>>>(d); break;
+    case 1: FMD_FORCE_VARIANT(4, 8, true, 1) break;
+    case 2: FMD_FORCE_VARIANT(4, 6, true, 2) break;
+    case 3: FMD_FORCE_VARIANT(4, 8, true, 2) break;
+    case 4: FMD_FORCE_VARIANT(2, 8, true, 4) break;
+    case 5: FMD_FORCE_VARIANT(4, 7, true, 2) break;
+    case 6: FMD_FORCE_VARIANT(8, 6, false, 1) break;
+    default: FMD_FORCE_VARIANT(4, 6, true, 1) break;
   }
+#undef FMD_FORCE_VARIANT
 }
 
-void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st) {
-  if (ev)
-    launch_force_t<true>(d, nchunks, variant, st);
-  else
-    launch_force_t<false>(d, nchunks, variant, st);
+void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st, bool skip_rebuilt) {
+  void (*per_chunk)(Dev, int) = nullptr;
+  void (*listed)(Dev) = nullptr;
+  if (ev) force_kernels<true>(variant, &per_chunk, &listed);
+  else force_kernels<false>(variant, &per_chunk, &listed);
+  per_chunk<<<nchunks, kChunk, 0, st>>>(d, skip_rebuilt ? 1 : 0);
+}
+
+void launch_force_rebuilt(const Dev& d, bool ev, int variant, cudaStream_t st) {
+  static int grid[2][kForceVariants] = {};
+  void (*per_chunk)(Dev, int) = nullptr;
+  void (*listed)(Dev) = nullptr;
+  if (ev) force_kernels<true>(variant, &per_chunk, &listed);
+  else force_kernels<false>(variant, &per_chunk, &listed);
+  const int v = variant >= 0 && variant < kForceVariants ? variant : 0;
+  int& g = grid[ev ? 1 : 0][v];
+  if (!g) g = resident_grid(listed, kChunk);
+  launch_hi(listed, g, kChunk, st, d);
 }
 
 void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st) {
-  launch_force(d, nchunks, false, variant, st);
-  launch_force(d, nchunks, true, variant, st);
+  launch_force(d, nchunks, false, variant, st, false);
+  launch_force(d, nchunks, true, variant, st, false);
 }
 void launch_reduce_only(const Dev& d, int nchunks, int nreps, cudaStream_t st, int mode) {
   k_post<<<nchunks, kChunk, 0, st>>>(d, mode);
