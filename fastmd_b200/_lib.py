@@ -84,6 +84,17 @@ class RequestResult(C.Structure):
     ]
 
 
+def _acf_rows(call):
+    cap = 16 * 16
+    lag = np.zeros(cap, np.int64)
+    val = np.zeros((cap, 6))
+    cnt = np.zeros(cap, np.int64)
+    n = C.c_int32()
+    call(_ptr(lag), _ptr(val), _ptr(cnt), C.c_int32(cap), C.byref(n))
+    k = n.value
+    return lag[:k].copy(), val[:k].copy(), cnt[:k].copy()
+
+
 def lib():
     """Load the shared library; raises if it was not built."""
     global _LIB
@@ -349,6 +360,14 @@ class Simulation:
     def write_restart(self, path):
         _call("fmd_write_restart", self._h, str(path).encode())
 
+    def stress_acf(self):
+        """Stress autocorrelation rows: (lag in steps, 6 averaged products
+        per row in thermo column order, number of products)."""
+        return _acf_rows(lambda *a: _call("fmd_stress_acf", self._h, *a))
+
+    def write_stress_acf(self, path):
+        _call("fmd_write_stress_acf", self._h, str(path).encode())
+
 
 class Batch:
     """Many replicas advanced together (the mixed form)."""
@@ -438,6 +457,13 @@ class Batch:
 
     def write_restart(self, slot, path):
         _call("fmd_batch_write_restart", self._h, C.c_int32(slot), str(path).encode())
+
+    def stress_acf(self, slot):
+        """Stress autocorrelation rows of a replica (see Simulation.stress_acf)."""
+        return _acf_rows(lambda *a: _call("fmd_batch_stress_acf", self._h, C.c_int32(slot), *a))
+
+    def write_stress_acf(self, slot, path):
+        _call("fmd_batch_write_stress_acf", self._h, C.c_int32(slot), str(path).encode())
 
     LAUNCH_KINDS = ("pre", "bin", "scan", "scatter", "cellsort", "permute", "topo", "neighbors", "force",
                     "force_ev", "post", "plan", "commit")

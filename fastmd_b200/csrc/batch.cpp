@@ -158,6 +158,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   ang_.alloc(S * kMaxAnglesPerAtom);
   part_.alloc_zero(S / kChunk * kNumPartials);
   kcount_.alloc_zero(kKernelKinds);
+  acf_.alloc_zero((size_t)max_reps_ * kAcfWords);
   rb_.alloc_zero(kRbHead + (size_t)max_reps_ + 3 * ((size_t)max_reps_ + 1));
   cell_cnt_.alloc_zero(c.cells);
   cell_start_.alloc_zero(c.cells);
@@ -216,6 +217,7 @@ Dev Batch::dev() const {
   d.ang = ang_;
   d.part = part_;
   d.kcount = kcount_;
+  d.acf = acf_;
   d.rb = rb_;
   d.rb_cap = max_reps_;
   return d;
@@ -270,6 +272,7 @@ static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
   R.chain_M = cfg.chain_length;
   R.max_between = 20;  // main.cu:401
   R.thermo_freq = cfg.thermo_on ? cfg.thermo_freq : 0;
+  R.stress_freq = cfg.stress_on ? cfg.stress_freq : 0;
   R.nsteps = cfg.nsteps;
   R.seed = cfg.seed;
   R.dt = cfg.dt;
@@ -459,6 +462,7 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
   R.angle_base = (int32_t)an;
   fill_static(R, cfg, t);
   init_dynamic(R, t.box_L, p.G_alloc, cfg.rc + cfg.skin);
+  FMD_CUDA(cudaMemsetAsync(acf_.p + (size_t)r * kAcfWords, 0, kAcfWords * sizeof(double), st_));
   // Topology CSR by atom id.
   {
     const int n = t.natoms;
@@ -1067,6 +1071,47 @@ void Batch::thermo(int r, fmd_thermo_row* row) {
   row->conserved = e / n;
 }
 
+// Rows of the stress autocorrelation in the order of the reference's output
+// file (main.cu:758-783): per level, per lag with samples, the lag in steps
+// stress_freq * kAcfPoints^level * (lag + 1), the six averages and the count.
+void Batch::stress_acf(int r, std::vector<int64_t>& lag, std::vector<double>& val, std::vector<int64_t>& cnt) {
+  const Rep& R = rep(r);
+  if (R.stress_freq <= 0) throw Error(FMD_ERR_ARG, "run.conf has no 'stress' output for this replica");
+  std::vector<double> st(kAcfWords);
+  FMD_CUDA(cudaMemcpyAsync(st.data(), acf_.p + (size_t)r * kAcfWords, kAcfWords * sizeof(double),
+                           cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  lag.clear();
+  val.clear();
+  cnt.clear();
+  int64_t lag_step = R.stress_freq;
+  for (int level = 0; level < kAcfLevels; ++level) {
+    for (int k = 0; k < kAcfPoints; ++k) {
+      const double n = st[kAcfCnt + level * kAcfPoints + k];
+      if (n == 0.0) continue;
+      lag.push_back(lag_step * (k + 1));
+      for (int c = 0; c < kAcfComps; ++c) val.push_back(st[kAcfCorr + (level * kAcfPoints + k) * kAcfComps + c] / n);
+      cnt.push_back((int64_t)n);
+    }
+    lag_step *= kAcfPoints;
+  }
+}
+
+void Batch::write_stress_acf(int r, const std::string& path) {
+  std::vector<int64_t> lag, cnt;
+  std::vector<double> val;
+  stress_acf(r, lag, val, cnt);
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) throw Error(FMD_ERR_IO, "cannot open " + path);
+  std::fprintf(f, "# lag_steps  C_xx  C_xy  C_xz  C_yy  C_yz  C_zz  count\n");
+  for (size_t i = 0; i < lag.size(); ++i) {
+    std::fprintf(f, "%lld", (long long)lag[i]);
+    for (int c = 0; c < kAcfComps; ++c) std::fprintf(f, " %.8e", val[i * kAcfComps + c]);
+    std::fprintf(f, " %lld\n", (long long)cnt[i]);
+  }
+  std::fclose(f);
+}
+
 double Batch::rg(int r) {
   const Rep& R = rep(r);
   const int n = R.natoms;
@@ -1182,6 +1227,10 @@ class MixedEngine final : public SimEngine {
   int64_t rebuilds() const override { return b_->rep(r_).rebuilds; }
   int32_t status_word() override { return b_->rep(r_).status; }
   int32_t max_neighbors() const override { return b_->rep(r_).M; }
+  void stress_acf(std::vector<int64_t>& lag, std::vector<double>& val, std::vector<int64_t>& cnt) override {
+    b_->stress_acf(r_, lag, val, cnt);
+  }
+  void write_stress_acf(const std::string& path) override { b_->write_stress_acf(r_, path); }
 
  private:
   std::unique_ptr<Batch> b_;

@@ -77,6 +77,9 @@ class Batch {
   void launch_counts(int64_t* counts, int n);
   void read_state(int r, double* xyz, double* vel, int32_t* image, bool rewrap);
   void force_frame(int r, double* xyz, double* box);
+  // Stress autocorrelation rows (lag in steps, 6 values per row, samples).
+  void stress_acf(int r, std::vector<int64_t>& lag, std::vector<double>& val, std::vector<int64_t>& cnt);
+  void write_stress_acf(int r, const std::string& path);
   void set_state(int r, const double* xyz, const double* vel, const int32_t* image);
   void forces(int r, double* f, double* pe, double* vir);
   void thermo(int r, fmd_thermo_row* row);
@@ -145,6 +148,7 @@ class Batch {
   DevBuf<uint2> ang_;
   DevBuf<double> part_;
   DevBuf<unsigned long long> kcount_;
+  DevBuf<double> acf_;  // stress autocorrelator state per replica slot
   DevBuf<int> rb_;  // rebuild work list
   std::vector<int> wl_;  // host staging of a host-written work list (kept alive for the async copy)
   int host_mode_ = 0;  // rebuild form of the current step, read back by direct-launch steps

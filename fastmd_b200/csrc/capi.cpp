@@ -245,6 +245,31 @@ FMD_API fmd_status fmd_set_state(fmd_sim* sim, const double* xyz, const double* 
   });
 }
 
+FMD_API fmd_status fmd_stress_acf(fmd_sim* sim, int64_t* lag_steps, double* values, int64_t* counts, int32_t cap,
+                                  int32_t* nrows) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (!nrows || cap < 0 || (cap > 0 && (!lag_steps || !values || !counts))) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    std::vector<int64_t> lag, cnt;
+    std::vector<double> val;
+    sim->eng->stress_acf(lag, val, cnt);
+    *nrows = (int32_t)lag.size();
+    for (int32_t i = 0; i < cap && i < (int32_t)lag.size(); ++i) {
+      lag_steps[i] = lag[i];
+      counts[i] = cnt[i];
+      for (int c = 0; c < 6; ++c) values[6 * i + c] = val[6 * (size_t)i + c];
+    }
+  });
+}
+
+FMD_API fmd_status fmd_write_stress_acf(fmd_sim* sim, const char* path) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (!path) throw fmd::Error(FMD_ERR_ARG, "null path");
+    sim->eng->write_stress_acf(path);
+  });
+}
+
 FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path) {
   return guarded([&] {
     SIM_CHECK();

@@ -159,6 +159,33 @@ FMD_API fmd_status fmd_batch_get_force_frame(fmd_batch* b, int32_t slot, double*
   });
 }
 
+FMD_API fmd_status fmd_batch_stress_acf(fmd_batch* b, int32_t slot, int64_t* lag_steps, double* values,
+                                        int64_t* counts, int32_t cap, int32_t* nrows) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!nrows || cap < 0 || (cap > 0 && (!lag_steps || !values || !counts))) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    std::vector<int64_t> lag, cnt;
+    std::vector<double> val;
+    bb.stress_acf(slot, lag, val, cnt);
+    *nrows = (int32_t)lag.size();
+    for (int32_t i = 0; i < cap && i < (int32_t)lag.size(); ++i) {
+      lag_steps[i] = lag[i];
+      counts[i] = cnt[i];
+      for (int c = 0; c < 6; ++c) values[6 * i + c] = val[6 * (size_t)i + c];
+    }
+  });
+}
+
+FMD_API fmd_status fmd_batch_write_stress_acf(fmd_batch* b, int32_t slot, const char* path) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!path) throw fmd::Error(FMD_ERR_ARG, "null path");
+    bb.write_stress_acf(slot, path);
+  });
+}
+
 FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n) {
   return guarded([&] {
     auto& bb = B(b);

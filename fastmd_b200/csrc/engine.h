@@ -1,6 +1,8 @@
 // Engine interface shared by the FP64 plain form and the mixed batched form.
 #pragma once
 #include <memory>
+#include <string>
+#include <vector>
 
 #include "host.h"
 
@@ -24,6 +26,18 @@ class SimEngine {
   virtual int64_t rebuilds() const = 0;
   virtual int32_t status_word() = 0;
   virtual int32_t max_neighbors() const = 0;
+  // Stress autocorrelation rows (run.conf 'stress'); the mixed form keeps the
+  // correlator on the device.
+  virtual void stress_acf(std::vector<int64_t>& lag, std::vector<double>& val, std::vector<int64_t>& cnt) {
+    (void)lag;
+    (void)val;
+    (void)cnt;
+    throw Error(FMD_ERR_ARG, "the stress autocorrelation is computed by the mixed form");
+  }
+  virtual void write_stress_acf(const std::string& path) {
+    (void)path;
+    throw Error(FMD_ERR_ARG, "the stress autocorrelation is computed by the mixed form");
+  }
 };
 
 // FP64 mirror of the reference step loop (one system, host-driven rebuild test).

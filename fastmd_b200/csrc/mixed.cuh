@@ -130,6 +130,7 @@ struct Rep {
   double pe, vir[6], ke[6];
   int64_t thermo_step;
   int32_t thermo_freq;           // run.conf thermo cadence (0: off); energies/virial computed on those steps
+  int32_t stress_freq;           // run.conf stress cadence (0: off); a pressure-tensor sample feeds the correlator
   int32_t force_ev;              // host request: compute energies/virial at the next force evaluation
   int64_t ev_step;               // step whose energies/virial are in pe/vir
   int32_t defer;                 // this step's post-force kick is applied by the next pre-force
@@ -139,11 +140,29 @@ struct Rep {
 
 // Energies and virial are needed on thermo steps, for NPT (the barostat uses
 // the virial every step) and when the host asks for them.
+__host__ __device__ inline bool stress_step(const Rep& R) {
+  return R.mode != kModePushoff && R.stress_freq > 0 && (R.step % R.stress_freq) == 0;
+}
+
 __host__ __device__ inline bool need_ev(const Rep& R) {
   if (R.force_ev) return true;
   if (R.mode != kModePushoff && R.ensemble == FMD_NPT_NH) return true;
+  if (stress_step(R)) return true;
   return R.thermo_freq > 0 && (R.step % R.thermo_freq) == 0;
 }
+
+// Multiple-tau stress autocorrelator per replica (analysis/correlator.cu
+// semantics: kAcfLevels levels of kAcfPoints samples of the 6 pressure
+// components, each level fed with block averages of kAcfPoints samples of
+// the level below).  FP64 state, kAcfWords doubles per replica:
+constexpr int kAcfLevels = 16, kAcfPoints = 16, kAcfComps = 6;
+constexpr int kAcfBuf = 0;                                              // [level][point][comp] samples
+constexpr int kAcfCorr = kAcfBuf + kAcfLevels * kAcfPoints * kAcfComps;  // [level][lag][comp] sums of products
+constexpr int kAcfCnt = kAcfCorr + kAcfLevels * kAcfPoints * kAcfComps;  // [level][lag] products summed
+constexpr int kAcfIdx = kAcfCnt + kAcfLevels * kAcfPoints;               // [level] insert position
+constexpr int kAcfAcc = kAcfIdx + kAcfLevels;                            // [level][comp] block accumulator
+constexpr int kAcfAccN = kAcfAcc + kAcfLevels * kAcfComps;               // [level] samples in the block
+constexpr int kAcfWords = kAcfAccN + kAcfLevels;
 
 // Device pointers of the batch arrays.
 struct Dev {
@@ -179,6 +198,7 @@ struct Dev {
   uint32_t* nbr;
   int32_t* ncnt;
   double* part;                  // [chunks][kNumPartials]
+  double* acf;                   // [replica][kAcfWords] stress autocorrelator state
   unsigned long long* kcount;    // [kKernelKinds] launches executed (block 0 of each launch counts)
   // rebuild work list: header (RbHeader), rb_cap replicas, then three
   // offset arrays of rb_cap + 1 (chunk items, cell-group items, home-cell

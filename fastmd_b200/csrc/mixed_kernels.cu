@@ -1479,6 +1479,54 @@ __global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
   block_partials<kChunk>(vals, 6, d.part + (size_t)chunk * kNumPartials + 7);
 }
 
+// One pressure-tensor sample into a replica's multiple-tau correlator, by
+// one warp (lanes = lags).  Follows correlator.cu:33-92: each level stores
+// the sample at its insert position, adds sample x (sample `lag` positions
+// back) for the lags 0 .. insert position (the reference counts lags from
+// the insert position, not from the samples held), and passes the average
+// of every kAcfPoints samples to the next level.  Products and sums are
+// rounded separately (no contraction), so the sums are reproducible by a
+// plain FP64 restatement.
+__device__ void acf_push(double* st, const double* sample_in) {
+  const int lane = threadIdx.x & 31;
+  double smp[kAcfComps];
+  for (int c = 0; c < kAcfComps; ++c) smp[c] = sample_in[c];
+  for (int level = 0; level < kAcfLevels; ++level) {
+    const int idx = (int)st[kAcfIdx + level];
+    double* buf = st + kAcfBuf + level * kAcfPoints * kAcfComps;
+    if (lane == 0)
+      for (int c = 0; c < kAcfComps; ++c) buf[idx * kAcfComps + c] = smp[c];
+    __syncwarp();
+    const int nstored = min(idx + 1, kAcfPoints);
+    if (lane < nstored) {
+      const int older = (idx - lane + kAcfPoints) % kAcfPoints;
+      double* corr = st + kAcfCorr + (level * kAcfPoints + lane) * kAcfComps;
+      for (int c = 0; c < kAcfComps; ++c) corr[c] = __dadd_rn(corr[c], __dmul_rn(smp[c], buf[older * kAcfComps + c]));
+      st[kAcfCnt + level * kAcfPoints + lane] += 1.0;
+    }
+    int carry = 0;
+    if (lane == 0) {
+      st[kAcfIdx + level] = (double)((idx + 1) % kAcfPoints);
+      double* acc = st + kAcfAcc + level * kAcfComps;
+      for (int c = 0; c < kAcfComps; ++c) acc[c] = __dadd_rn(acc[c], smp[c]);
+      const double n = st[kAcfAccN + level] + 1.0;
+      if (n >= (double)kAcfPoints) {
+        for (int c = 0; c < kAcfComps; ++c) {
+          smp[c] = acc[c] / (double)kAcfPoints;
+          acc[c] = 0.0;
+        }
+        st[kAcfAccN + level] = 0.0;
+        carry = 1;
+      } else {
+        st[kAcfAccN + level] = n;
+      }
+    }
+    __syncwarp();
+    if (!__shfl_sync(0xFFFFFFFFu, carry, 0)) break;
+    for (int c = 0; c < kAcfComps; ++c) smp[c] = __shfl_sync(0xFFFFFFFFu, smp[c], 0);
+  }
+}
+
 // Per-replica commit of the post-force update (one warp per replica, after
 // every post-force block finished): reduce the chunk partials in chunk order
 // (deterministic), store energies / virial / KE, run the post-force chain or
@@ -1537,6 +1585,17 @@ __global__ void __launch_bounds__(32) k_post_commit(Dev d, int kick) {
       // scalars of the next pre-force, computed once here for all its blocks
       compute_step_scalars(R, R.next);
       R.next_valid = 1;
+    }
+    // Stress steps: the thermo row's pressure tensor, (KE tensor (with the
+    // pending thermostat scale) + virial) / V in the current box, feeds the
+    // correlator (main.cu:632-666).
+    __syncwarp();
+    if (kick == 1 && stress_step(R)) {
+      const double s2 = __dmul_rn(R.pending_scale, R.pending_scale);
+      const double V = __dmul_rn(__dmul_rn(R.L, R.L), R.L);
+      double smp[kAcfComps];
+      for (int c = 0; c < kAcfComps; ++c) smp[c] = __dadd_rn(__dmul_rn(R.ke[c], s2), R.vir[c]) / V;
+      acf_push(d.acf + (size_t)r * kAcfWords, smp);
     }
   }
 }

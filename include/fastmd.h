@@ -177,6 +177,10 @@ FMD_API fmd_status fmd_thermo(fmd_sim* sim, fmd_thermo_row* row);
 /* Restart file of the current state (write_lammps_data, io/lammps_data.cpp:269;
  * main.cu:681-691, 738-745 call it every restart_freq steps and at the end). */
 FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path);
+/* Stress autocorrelation of a mixed-form simulation (see fmd_batch_stress_acf). */
+FMD_API fmd_status fmd_stress_acf(fmd_sim* sim, int64_t* lag_steps, double* values, int64_t* counts, int32_t cap,
+                                  int32_t* nrows);
+FMD_API fmd_status fmd_write_stress_acf(fmd_sim* sim, const char* path);
 FMD_API fmd_status fmd_rg(fmd_sim* sim, double* rg);
 /* Current Verlet pair set (unordered pairs i < j within rc + skin at the last
  * rebuild, 1-2 bonded pairs excluded), in data-file indices. */
@@ -231,6 +235,17 @@ FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* 
  * barostat half step moves box_L before the next pre-force rescales the
  * positions (fmd_batch_get_state reports them re-wrapped into box_L). */
 FMD_API fmd_status fmd_batch_get_force_frame(fmd_batch* b, int32_t slot, double* xyz, double* box_L);
+/* Stress autocorrelation of a replica with run.conf 'stress <on> <freq>
+ * <file>' (analysis/correlator.cu:33-92, output main.cu:758-783): the
+ * pressure tensor of every stress step (columns xx, xy, xz, yy, yz, zz, as
+ * in the thermo row) feeds a 16-level x 16-point multiple-tau correlator.
+ * Rows in the reference file's order: lag in steps, 6 averaged products
+ * (values[6 * row + c]) and the number of products.  *nrows = rows available
+ * (up to 256); at most cap are copied. */
+FMD_API fmd_status fmd_batch_stress_acf(fmd_batch* b, int32_t slot, int64_t* lag_steps, double* values,
+                                        int64_t* counts, int32_t cap, int32_t* nrows);
+/* The same rows as the reference's stress file ("# lag_steps  C_xx ... count"). */
+FMD_API fmd_status fmd_batch_write_stress_acf(fmd_batch* b, int32_t slot, const char* path);
 FMD_API fmd_status fmd_batch_pairs(fmd_batch* b, int32_t slot, int32_t* i, int32_t* j, int64_t cap, int64_t* n);
 /* Totals: active replicas, atoms, device bytes in use. */
 FMD_API fmd_status fmd_batch_totals(fmd_batch* b, int32_t* active, int64_t* atoms, int64_t* bytes);

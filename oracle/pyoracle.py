@@ -319,3 +319,64 @@ class Sim:
                 self._h = None
         except Exception:
             pass
+
+
+class StressACF:
+    """Multiple-tau stress autocorrelator, restated from the reference
+    (analysis/correlator.cu:33-92 for the update, main.cu:758-783 for the
+    rows): 16 levels x 16 points x 6 components; each pushed sample is stored
+    at its level's insert position and multiplied with the samples 0 ..
+    insert position back (the reference bounds the lags by the insert
+    position, not by the samples held); every 16 samples of a level pass
+    their average to the next level.  FP64, products and sums rounded
+    separately (plain Python floats)."""
+
+    LEVELS = POINTS = 16
+
+    def __init__(self, freq):
+        L, P = self.LEVELS, self.POINTS
+        self.freq = freq
+        self.buf = [[[0.0] * 6 for _ in range(P)] for _ in range(L)]
+        self.corr = [[[0.0] * 6 for _ in range(P)] for _ in range(L)]
+        self.cnt = [[0] * P for _ in range(L)]
+        self.idx = [0] * L
+        self.acc = [[0.0] * 6 for _ in range(L)]
+        self.accn = [0] * L
+
+    def push(self, sample):
+        P = self.POINTS
+        smp = [float(x) for x in sample]
+        for level in range(self.LEVELS):
+            idx = self.idx[level]
+            self.buf[level][idx] = list(smp)
+            for lag in range(min(idx + 1, P)):
+                older = self.buf[level][(idx - lag + P) % P]
+                row = self.corr[level][lag]
+                for c in range(6):
+                    row[c] = row[c] + smp[c] * older[c]
+                self.cnt[level][lag] += 1
+            self.idx[level] = (idx + 1) % P
+            acc = self.acc[level]
+            for c in range(6):
+                acc[c] = acc[c] + smp[c]
+            self.accn[level] += 1
+            if self.accn[level] >= P:
+                smp = [acc[c] / P for c in range(6)]
+                self.acc[level] = [0.0] * 6
+                self.accn[level] = 0
+            else:
+                break
+
+    def rows(self):
+        lag, val, cnt = [], [], []
+        step = self.freq
+        for level in range(self.LEVELS):
+            for k in range(self.POINTS):
+                n = self.cnt[level][k]
+                if n == 0:
+                    continue
+                lag.append(step * (k + 1))
+                val.append([self.corr[level][k][c] / n for c in range(6)])
+                cnt.append(n)
+            step *= self.POINTS
+        return np.array(lag, np.int64), np.array(val).reshape(-1, 6), np.array(cnt, np.int64)

@@ -238,3 +238,29 @@ def test_server_results_equal_alone_and_in_mix():
         assert np.array_equal(alone.thermo(s).as_array(), np.asarray(r.thermo.as_array()))
         assert alone.rg(s) == r.rg
         alone.close()
+
+
+@pytest.mark.parametrize("ens", ["nvt_langevin 1.0 1.0 1.0 5", "npt_nh 1.0 1.0 0.5 1.0 1.0 1.0 3"])
+def test_stress_acf_matches_oracle_correlator(ens, tmp_path):
+    """The device correlator equals the oracle correlator fed with the thermo
+    pressure tensor of every stress step (the same doubles), in the rows of
+    the reference's stress file."""
+    freq, nsamp = 3, 300
+    conf = run_conf(ensemble=ens, nsteps=freq * nsamp, extra=f"stress 1 {freq} acf.dat")
+    d = _melt(10, 30, seed=9)
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    s = b.add(conf, desc=d)
+    acf = po.StressACF(freq)
+    for _ in range(nsamp):
+        b.run(freq)
+        acf.push(b.thermo(s).stress)
+    lag, val, cnt = b.stress_acf(s)
+    olag, oval, ocnt = acf.rows()
+    assert np.array_equal(lag, olag) and np.array_equal(cnt, ocnt)
+    assert np.allclose(val, oval, rtol=1e-12, atol=1e-14 * np.max(np.abs(oval)))
+    p = tmp_path / "acf.dat"
+    b.write_stress_acf(s, p)
+    rows = np.loadtxt(p)
+    assert rows.shape == (len(lag), 8)
+    assert np.array_equal(rows[:, 0].astype(np.int64), lag) and np.array_equal(rows[:, 7].astype(np.int64), cnt)
+    b.close()
