@@ -26,6 +26,7 @@ from ._lib import (  # noqa: F401
     Simulation,
     SystemDesc,
     ThermoRow,
+    Trajectory,
     format_rg_row,
     format_thermo_row,
     generate_melt,
@@ -33,6 +34,9 @@ from ._lib import (  # noqa: F401
     lib_path,
     parse_run_conf,
     read_lammps_data,
+    read_pair_table,
+    run_conf_tables,
+    read_trajectory,
     write_lammps_data,
 )
 

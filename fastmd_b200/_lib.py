@@ -227,6 +227,30 @@ def parse_run_conf(text):
                 angle=angle[: 2 * iout[10]].reshape(-1, 2).copy(), seed=int(seed.value))
 
 
+def read_pair_table(path, keyword):
+    """One section of a pair_style table file: dict(rmin, rmax, dr, inv_dr,
+    r, f, e) with the grid in single precision (the force column f is
+    applied as F/r)."""
+    grid = np.zeros(4, np.float32)
+    n = C.c_int32()
+    _call("fmd_read_pair_table", str(path).encode(), keyword.encode(), _ptr(grid), C.byref(n), None, C.c_int32(0))
+    data = np.zeros((n.value, 3), np.float32)
+    _call("fmd_read_pair_table", str(path).encode(), keyword.encode(), _ptr(grid), C.byref(n), _ptr(data),
+          C.c_int32(n.value))
+    return dict(rmin=float(grid[0]), rmax=float(grid[1]), dr=float(grid[2]), inv_dr=float(grid[3]),
+                r=data[:, 0].copy(), f=data[:, 1].copy(), e=data[:, 2].copy())
+
+
+def run_conf_tables(text):
+    """(table index per type pair [ntypes, ntypes] (-1: none), number of tables) of a run.conf."""
+    cap = 16 * 16
+    t = np.full(cap, -1, np.int32)
+    n = C.c_int32()
+    _call("fmd_run_conf_tables", text.encode(), _ptr(t), C.c_int32(cap), C.byref(n))
+    nt = parse_run_conf(text)["ntypes"]
+    return t[:nt * nt].reshape(nt, nt), n.value
+
+
 def read_lammps_data(path):
     counts = np.zeros(4, np.int32)
     L = C.c_double()
@@ -466,7 +490,7 @@ class Batch:
         _call("fmd_batch_write_stress_acf", self._h, C.c_int32(slot), str(path).encode())
 
     LAUNCH_KINDS = ("pre", "bin", "scan", "scatter", "cellsort", "permute", "topo", "neighbors", "force",
-                    "force_ev", "post", "plan", "commit")
+                    "force_ev", "post", "plan", "commit", "table")
 
     def set_rebuild_cadence(self, slot, max_steps):
         """Force a neighbor-list rebuild at least every max_steps steps
@@ -488,6 +512,58 @@ class Batch:
         c = np.zeros(len(self.LAUNCH_KINDS), np.int64)
         _call("fmd_batch_launch_counts", self._h, _ptr(c), C.c_int32(len(c)))
         return dict(zip(self.LAUNCH_KINDS, c.tolist()))
+
+
+class Trajectory:
+    """Binary trajectory in the reference's dump format (io/dump.cu:12-56):
+    frames of a Simulation or of a Batch replica, written by a background
+    thread from pinned buffers."""
+
+    def __init__(self, path, natoms, ntypes=1):
+        self._h = C.c_void_p()
+        _call("fmd_traj_open", str(path).encode(), C.c_int32(natoms), C.c_int32(ntypes), C.byref(self._h))
+
+    def write(self, source, slot=None):
+        if slot is None:
+            _call("fmd_traj_write_sim", self._h, source._h)
+        else:
+            _call("fmd_traj_write_batch", self._h, source._h, C.c_int32(slot))
+
+    def close(self):
+        if self._h:
+            h, self._h = self._h, None
+            _call("fmd_traj_close", h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_trajectory(path):
+    """Parse a trajectory file: dict(natoms, ntypes, steps, box_L, xyz[frames, natoms, 3])."""
+    raw = open(path, "rb").read()
+    magic, natoms, ntypes = np.frombuffer(raw[:12], np.int32)
+    if magic != 0x4D444247:
+        raise ValueError("not a trajectory file")
+    fsz = 8 + 4 + 4 + 12 * int(natoms)
+    nf = (len(raw) - 12) // fsz
+    steps, box, xyz = [], [], []
+    for k in range(nf):
+        o = 12 + k * fsz
+        steps.append(int(np.frombuffer(raw[o:o + 8], np.int64)[0]))
+        assert int(np.frombuffer(raw[o + 8:o + 12], np.int32)[0]) == natoms
+        box.append(float(np.frombuffer(raw[o + 12:o + 16], np.float32)[0]))
+        xyz.append(np.frombuffer(raw[o + 16:o + fsz], np.float32).reshape(int(natoms), 3))
+    return dict(natoms=int(natoms), ntypes=int(ntypes), steps=np.array(steps), box_L=np.array(box, np.float32),
+                xyz=np.array(xyz).reshape(nf, int(natoms), 3))
 
 
 class Server:

@@ -218,6 +218,7 @@ Dev Batch::dev() const {
   d.part = part_;
   d.kcount = kcount_;
   d.acf = acf_;
+  d.tab = tab_.p;
   d.rb = rb_;
   d.rb_cap = max_reps_;
   return d;
@@ -258,6 +259,9 @@ StepShape Batch::shape() const {
   g.max_home = pow2_at_least(std::max(1, hw_home_));
   g.force_variant = force_variant_;
   g.nbr_variant = nbr_variant_;
+  g.has_table = 0;
+  for (int r = 0; r < max_reps_; ++r)
+    if (info_[r].used && h_reps_[r].ntables > 0) g.has_table = 1;
   return g;
 }
 int Batch::nreps_launch() const {
@@ -273,6 +277,19 @@ static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
   R.max_between = 20;  // main.cu:401
   R.thermo_freq = cfg.thermo_on ? cfg.thermo_freq : 0;
   R.stress_freq = cfg.stress_on ? cfg.stress_freq : 0;
+  R.ntables = (int32_t)cfg.tables.size();
+  for (int k = 0; k < kMaxTypes * kMaxTypes; ++k) R.table_of[k] = -1;
+  for (size_t k = 0; k < cfg.table_of.size() && k < (size_t)(kMaxTypes * kMaxTypes); ++k)
+    R.table_of[k] = (int8_t)cfg.table_of[k];
+  for (int k = 0; k < R.ntables && k < kMaxTables; ++k) {
+    const PairTable& tb = cfg.tables[k];
+    R.tab_rmin[k] = tb.rmin;
+    R.tab_rmax[k] = tb.rmax;
+    R.tab_dr[k] = tb.dr;
+    R.tab_inv_dr[k] = tb.inv_dr;
+    R.tab_n[k] = tb.npoints;
+    R.tab_off[k] = 0;  // set when the points are stored (Batch::add)
+  }
   R.nsteps = cfg.nsteps;
   R.seed = cfg.seed;
   R.dt = cfg.dt;
@@ -460,8 +477,24 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
   R.M = p.M;
   R.bond_base = (int32_t)bo;
   R.angle_base = (int32_t)an;
+  if (cfg.tables.size() > (size_t)kMaxTables) throw Error(FMD_ERR_CONFIG, "more than 8 distinct pair tables");
   fill_static(R, cfg, t);
   init_dynamic(R, t.box_L, p.G_alloc, cfg.rc + cfg.skin);
+  if (!cfg.tables.empty()) {
+    // the replica's table points, appended to the batch's table array
+    for (size_t k = 0; k < cfg.tables.size(); ++k) {
+      R.tab_off[k] = (int32_t)tab_host_.size();
+      for (int i = 0; i < cfg.tables[k].npoints; ++i)
+        tab_host_.push_back(make_float2(cfg.tables[k].f[i], cfg.tables[k].e[i]));
+    }
+    if (tab_host_.size() > tab_.n) {
+      FMD_CUDA(cudaStreamSynchronize(st_));
+      tab_.alloc(std::max<size_t>(tab_host_.size(), 2 * tab_.n));  // all points are uploaded below
+      graph_dirty_ = true;  // captured launches hold the old array
+    }
+    FMD_CUDA(cudaMemcpyAsync(tab_.p, tab_host_.data(), tab_host_.size() * sizeof(float2), cudaMemcpyHostToDevice, st_));
+    FMD_CUDA(cudaStreamSynchronize(st_));
+  }
   FMD_CUDA(cudaMemsetAsync(acf_.p + (size_t)r * kAcfWords, 0, kAcfWords * sizeof(double), st_));
   // Topology CSR by atom id.
   {
@@ -630,7 +663,7 @@ void Batch::setup(const std::vector<int>& rs) {
   const Dev d = dev();
   launch_rebuild(d, nreps_launch(), nbr_variant_, st_);
   FMD_CUDA_LAUNCH();
-  launch_forces_only(d, nchunks_launch(), force_variant_, st_);
+  launch_forces_only(d, nchunks_launch(), force_variant_, shape().has_table != 0, st_);
   FMD_CUDA_LAUNCH();
   launch_reduce_only(d, nchunks_launch(), nreps_launch(), st_, 0);
   FMD_CUDA_LAUNCH();
@@ -658,7 +691,7 @@ void Batch::advance_direct(int64_t nsteps) {
 
 static bool same_shape(const StepShape& a, const StepShape& b) {
   return a.nchunks == b.nchunks && a.nreps == b.nreps && a.max_cells == b.max_cells && a.max_home == b.max_home &&
-         a.force_variant == b.force_variant && a.nbr_variant == b.nbr_variant;
+         a.force_variant == b.force_variant && a.nbr_variant == b.nbr_variant && a.has_table == b.has_table;
 }
 
 void Batch::ensure_graph() {
@@ -905,6 +938,14 @@ const Rep& Batch::rep(int r) const {
 
 void Batch::get_state(int r, double* xyz, double* vel, int32_t* image) { read_state(r, xyz, vel, image, true); }
 
+void Batch::pack_frame(int r, float* d_xyz, float* h_xyz, cudaEvent_t ready) {
+  const Rep& R = rep(r);
+  launch_pack_frame(dev(), r, R.natoms, d_xyz, st_);
+  FMD_CUDA_LAUNCH();
+  FMD_CUDA(cudaMemcpyAsync(h_xyz, d_xyz, (size_t)R.natoms * 3 * sizeof(float), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaEventRecord(ready, st_));
+}
+
 void Batch::force_frame(int r, double* xyz, double* box) {
   read_state(r, xyz, nullptr, nullptr, false);
   if (box) *box = rep(r).Lpos;
@@ -1013,7 +1054,7 @@ void Batch::ensure_ev(int r) {
   R.rebuild_now = 0;
   upload_reps();
   const Dev d = dev();
-  launch_forces_only(d, nchunks_launch(), force_variant_, st_);
+  launch_forces_only(d, nchunks_launch(), force_variant_, shape().has_table != 0, st_);
   FMD_CUDA_LAUNCH();
   launch_reduce_only(d, nchunks_launch(), nreps_launch(), st_, 2);
   FMD_CUDA_LAUNCH();
@@ -1231,6 +1272,7 @@ class MixedEngine final : public SimEngine {
     b_->stress_acf(r_, lag, val, cnt);
   }
   void write_stress_acf(const std::string& path) override { b_->write_stress_acf(r_, path); }
+  void dump_frame(TrajWriter& w) override { w.write(*b_, r_); }
 
  private:
   std::unique_ptr<Batch> b_;

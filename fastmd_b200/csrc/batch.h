@@ -77,6 +77,10 @@ class Batch {
   void launch_counts(int64_t* counts, int n);
   void read_state(int r, double* xyz, double* vel, int32_t* image, bool rewrap);
   void force_frame(int r, double* xyz, double* box);
+  // Queue a trajectory frame of replica r on the batch stream: positions
+  // (id order, wrapped in the last pre-force box) packed into d_xyz, copied
+  // to the pinned h_xyz; ready is recorded after the copy.
+  void pack_frame(int r, float* d_xyz, float* h_xyz, cudaEvent_t ready);
   // Stress autocorrelation rows (lag in steps, 6 values per row, samples).
   void stress_acf(int r, std::vector<int64_t>& lag, std::vector<double>& val, std::vector<int64_t>& cnt);
   void write_stress_acf(int r, const std::string& path);
@@ -149,6 +153,8 @@ class Batch {
   DevBuf<double> part_;
   DevBuf<unsigned long long> kcount_;
   DevBuf<double> acf_;  // stress autocorrelator state per replica slot
+  DevBuf<float2> tab_;  // pair-table points of every replica (appended at add)
+  std::vector<float2> tab_host_;
   DevBuf<int> rb_;  // rebuild work list
   std::vector<int> wl_;  // host staging of a host-written work list (kept alive for the async copy)
   int host_mode_ = 0;  // rebuild form of the current step, read back by direct-launch steps

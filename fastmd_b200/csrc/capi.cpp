@@ -126,6 +126,34 @@ FMD_API fmd_status fmd_parse_run_conf(const char* text, int32_t* iout, double* f
   });
 }
 
+FMD_API fmd_status fmd_read_pair_table(const char* path, const char* keyword, float* grid, int32_t* npoints,
+                                       float* data, int32_t cap) {
+  return guarded([&] {
+    if (!path || !keyword || !grid || !npoints || cap < 0 || (cap > 0 && !data))
+      throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    const fmd::PairTable t = fmd::read_pair_table(path, keyword);
+    grid[0] = t.rmin;
+    grid[1] = t.rmax;
+    grid[2] = t.dr;
+    grid[3] = t.inv_dr;
+    *npoints = t.npoints;
+    for (int32_t k = 0; k < t.npoints && k < cap; ++k) {
+      data[3 * k] = t.r[k];
+      data[3 * k + 1] = t.f[k];
+      data[3 * k + 2] = t.e[k];
+    }
+  });
+}
+
+FMD_API fmd_status fmd_run_conf_tables(const char* text, int32_t* table_of, int32_t cap, int32_t* ntables) {
+  return guarded([&] {
+    if (!text || !ntables || cap < 0 || (cap > 0 && !table_of)) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    const fmd::RunConfig c = fmd::parse_run_conf(text);
+    *ntables = (int32_t)c.tables.size();
+    for (int32_t k = 0; k < (int32_t)c.table_of.size() && k < cap; ++k) table_of[k] = c.table_of[k];
+  });
+}
+
 FMD_API fmd_status fmd_read_lammps_data(const char* path, int32_t* counts, double* box_L, double* xyz,
                                         int32_t* image, int32_t* type, int32_t* mol, double* vel, int32_t* bonds,
                                         int32_t* bond_type, int32_t* angles, int32_t* angle_type, double* masses) {
@@ -267,6 +295,33 @@ FMD_API fmd_status fmd_write_stress_acf(fmd_sim* sim, const char* path) {
     SIM_CHECK();
     if (!path) throw fmd::Error(FMD_ERR_ARG, "null path");
     sim->eng->write_stress_acf(path);
+  });
+}
+
+FMD_API fmd_status fmd_traj_open(const char* path, int32_t natoms, int32_t ntypes, fmd_traj** out) {
+  return guarded([&] {
+    if (!path || !out) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::unique_ptr<fmd_traj> t(new fmd_traj());
+    t->w.reset(new fmd::TrajWriter(path, natoms, ntypes));
+    *out = t.release();
+  });
+}
+
+FMD_API fmd_status fmd_traj_write_sim(fmd_traj* t, fmd_sim* sim) {
+  return guarded([&] {
+    SIM_CHECK();
+    if (!t || !t->w) throw fmd::Error(FMD_ERR_ARG, "null trajectory");
+    if (sim->eng->natoms() != t->w->natoms()) throw fmd::Error(FMD_ERR_ARG, "natoms differs from the trajectory's");
+    sim->eng->dump_frame(*t->w);
+  });
+}
+
+FMD_API fmd_status fmd_traj_close(fmd_traj* t) {
+  return guarded([&] {
+    if (!t) return;
+    std::unique_ptr<fmd_traj> own(t);
+    if (own->w) own->w->close();
   });
 }
 

@@ -4,6 +4,7 @@
 
 #include "batch.h"
 #include "host.h"
+#include "traj.h"
 
 struct fmd_batch {
   std::unique_ptr<fmd::mixed::Batch> b;
@@ -183,6 +184,15 @@ FMD_API fmd_status fmd_batch_write_stress_acf(fmd_batch* b, int32_t slot, const 
     need_slot(bb, slot);
     if (!path) throw fmd::Error(FMD_ERR_ARG, "null path");
     bb.write_stress_acf(slot, path);
+  });
+}
+
+FMD_API fmd_status fmd_traj_write_batch(fmd_traj* t, fmd_batch* b, int32_t slot) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!t || !t->w) throw fmd::Error(FMD_ERR_ARG, "null trajectory");
+    t->w->write(bb, slot);
   });
 }
 

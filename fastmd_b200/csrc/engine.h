@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "host.h"
+#include "traj.h"
 
 namespace fmd {
 
@@ -33,6 +34,13 @@ class SimEngine {
     (void)val;
     (void)cnt;
     throw Error(FMD_ERR_ARG, "the stress autocorrelation is computed by the mixed form");
+  }
+  // One trajectory frame of the current state (positions wrapped in the box
+  // of the last pre-force update, the current box edge).
+  virtual void dump_frame(TrajWriter& w) {
+    std::vector<double> x(3 * (size_t)natoms());
+    get_state(x.data(), nullptr, nullptr);
+    w.write_host(step_count(), box_L(), x.data());
   }
   virtual void write_stress_acf(const std::string& path) {
     (void)path;

@@ -17,6 +17,19 @@ struct Error : std::runtime_error {
 
 void set_last_error(const std::string& msg);
 
+// One tabulated pair potential: a keyword section of a LAMMPS pair_style
+// table file (io/table_parser.cpp:7-87).  Grid parameters in single
+// precision exactly as the reference derives them; per point the force
+// column (applied as F/r, as force/table.cu:92-96 does) and the energy.
+struct PairTable {
+  std::string file, keyword;
+  float rmin = 0, rmax = 0, dr = 0, inv_dr = 0;
+  int32_t npoints = 0;
+  std::vector<float> r, f, e;
+};
+
+PairTable read_pair_table(const std::string& path, const std::string& keyword);
+
 // Parsed run.conf (the key set of src/io/config.cpp:32-127).
 struct RunConfig {
   int32_t natoms = 0;
@@ -41,6 +54,8 @@ struct RunConfig {
   std::vector<double> lj;                   // [ntypes*ntypes*2] (eps, sig)
   std::vector<std::array<double, 4>> bond;  // k, R0, eps, sig
   std::vector<std::array<double, 2>> angle; // k_theta, theta0 (radians)
+  std::vector<PairTable> tables;            // distinct (file, keyword) sections
+  std::vector<int32_t> table_of;            // [ntypes*ntypes]: index into tables, -1: none
 };
 
 RunConfig parse_run_conf(const std::string& text);

@@ -19,6 +19,72 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 const std::string& last_error() { return g_last_error; }
 
 // ---------------------------------------------------------------------------
+// Pair table file section (io/table_parser.cpp:7-87): skip blank and '#'
+// lines; the section starts at the line whose first word is the keyword; the
+// next line holds "N n [R rlo rhi]"; then n lines "index r energy force".
+// Without R the grid spans the first and last r.  r must increase.
+// ---------------------------------------------------------------------------
+PairTable read_pair_table(const std::string& path, const std::string& keyword) {
+  std::ifstream in(path);
+  if (!in) throw Error(FMD_ERR_IO, "cannot open table file: " + path);
+  PairTable t;
+  t.file = path;
+  t.keyword = keyword;
+  std::string line;
+  bool found = false, has_r = false;
+  int n = 0;
+  float rlo = 0, rhi = 0;
+  while (std::getline(in, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream iss(line);
+    std::string first;
+    iss >> first;
+    if (first != keyword) continue;
+    found = true;
+    while (std::getline(in, line)) {
+      if (line.empty() || line[0] == '#') continue;
+      std::istringstream hs(line);
+      std::string key, rkey;
+      hs >> key;
+      if (key == "N") {
+        hs >> n;
+        if (hs >> rkey && rkey == "R") {
+          hs >> rlo >> rhi;
+          has_r = true;
+        }
+      }
+      break;
+    }
+    break;
+  }
+  if (!found) throw Error(FMD_ERR_IO, "table keyword not found: " + keyword);
+  if (n < 2) throw Error(FMD_ERR_IO, "table section " + keyword + " needs 'N n' with n >= 2");
+  while ((int)t.r.size() < n && std::getline(in, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream iss(line);
+    int idx = 0;
+    float r = 0, e = 0, f = 0;
+    iss >> idx >> r >> e >> f;
+    t.r.push_back(r);
+    t.e.push_back(e);
+    t.f.push_back(f);
+  }
+  if ((int)t.r.size() != n) throw Error(FMD_ERR_IO, "table data line count mismatch in " + path);
+  for (int i = 1; i < n; ++i)
+    if (!(t.r[i] > t.r[i - 1])) throw Error(FMD_ERR_IO, "table r values not monotonically increasing");
+  if (!has_r) {
+    rlo = t.r.front();
+    rhi = t.r.back();
+  }
+  t.rmin = rlo;
+  t.rmax = rhi;
+  t.npoints = n;
+  t.dr = (rhi - rlo) / (float)(n - 1);
+  t.inv_dr = 1.0f / t.dr;
+  return t;
+}
+
+// ---------------------------------------------------------------------------
 // run.conf: whitespace-separated key/value lines, '#' comments, unknown keys
 // ignored, deprecated keys rejected (src/io/config.cpp:10-213).
 // ---------------------------------------------------------------------------
@@ -29,7 +95,11 @@ RunConfig parse_run_conf(const std::string& text) {
     double eps, sig;
   };
   std::vector<LJ> lj_entries;
-  bool saw_table = false;
+  struct TableLine {
+    int ti, tj;
+    std::string file, keyword;
+  };
+  std::vector<TableLine> table_entries;
   std::istringstream in(text);
   std::string line;
   auto bad = [](const std::string& m) { throw Error(FMD_ERR_CONFIG, m); };
@@ -75,7 +145,11 @@ RunConfig parse_run_conf(const std::string& text) {
       LJ e{};
       iss >> e.ti >> e.tj >> e.eps >> e.sig;
       lj_entries.push_back(e);
-    } else if (key == "table") saw_table = true;
+    } else if (key == "table") {
+      TableLine e{};
+      iss >> e.ti >> e.tj >> e.file >> e.keyword;
+      table_entries.push_back(e);
+    }
     else if (key == "bond_type") {
       int t = 0;
       double k = 0, R0 = 0, eps = 0, sig = 0;
@@ -92,7 +166,6 @@ RunConfig parse_run_conf(const std::string& text) {
       c.angle[t] = {k, th * 3.14159265358979323846 / 180.0};  // config.cpp:176
     } else if (key == "forces_dump_file") iss >> c.forces_dump_file;
   }
-  if (saw_table) bad("'table' pair potentials are not supported by this library");
   if (c.ntypes < 1 || c.ntypes > 16) bad("ntypes must be in [1, 16]");
   c.lj.assign((size_t)c.ntypes * c.ntypes * 2, 0.0);
   for (auto& e : lj_entries) {  // config.cpp:130-134 (both orders)
@@ -101,6 +174,24 @@ RunConfig parse_run_conf(const std::string& text) {
     c.lj[2 * (e.ti * c.ntypes + e.tj) + 1] = e.sig;
     c.lj[2 * (e.tj * c.ntypes + e.ti)] = e.eps;
     c.lj[2 * (e.tj * c.ntypes + e.ti) + 1] = e.sig;
+  }
+  // config.cpp:136-162: one table per distinct (file, keyword), both orders;
+  // a pair may not have both an lj and a table entry.
+  c.table_of.assign((size_t)c.ntypes * c.ntypes, -1);
+  for (auto& e : table_entries) {
+    if (e.ti < 0 || e.ti >= c.ntypes || e.tj < 0 || e.tj >= c.ntypes) bad("table type index out of range");
+    const size_t ij = (size_t)(e.ti * c.ntypes + e.tj);
+    if (c.lj[2 * ij] != 0.0 || c.lj[2 * ij + 1] != 0.0)
+      bad("Both lj and table defined for pair (" + std::to_string(e.ti) + "," + std::to_string(e.tj) + ")");
+    int idx = -1;
+    for (size_t k = 0; k < c.tables.size(); ++k)
+      if (c.tables[k].file == e.file && c.tables[k].keyword == e.keyword) idx = (int)k;
+    if (idx < 0) {
+      c.tables.push_back(read_pair_table(e.file, e.keyword));
+      idx = (int)c.tables.size() - 1;
+    }
+    c.table_of[ij] = idx;
+    c.table_of[(size_t)(e.tj * c.ntypes + e.ti)] = idx;
   }
   // config.cpp:195-210
   if (c.ensemble == FMD_LANGEVIN && c.Tdamp <= 0) bad("Tdamp must be > 0 for nvt_langevin");

@@ -33,6 +33,7 @@ namespace mixed {
 constexpr int kChunk = 128;       // slots per block / per reduction partial
 constexpr int kTile = 32;         // slots per warp tile
 constexpr int kMaxTypes = 16;
+constexpr int kMaxTables = 8;  // distinct pair tables per replica
 constexpr int kGhostType = 31;
 constexpr int kMaxG = 512;        // cells per axis (9 bits)
 // Neighbor-list entry: slot (25 bits) | shift code (7 bits).  The shift
@@ -58,7 +59,7 @@ enum Mode : int32_t { kModeRun = 0, kModePushoff = 1 };
 // Per-kernel launch counters (executed launches, graph conditionals included).
 enum KernelKind : int {
   kKPre = 0, kKBin, kKScan, kKScatter, kKCellsort, kKPermute, kKTopo, kKNeighbors, kKForce, kKForceEv, kKPost,
-  kKPlan, kKCommit, kKernelKinds
+  kKPlan, kKCommit, kKTable, kKernelKinds
 };
 
 // Per-replica record (device).  Static fields are set at admission; dynamic
@@ -109,6 +110,12 @@ struct Rep {
   float lj_sig2[kMaxTypes * kMaxTypes];   // sig^2
   float fene[4 * 4];             // up to 4 bond types: k, R0^2, eps, sig^2
   float angp[2 * 4];             // up to 4 angle types: k, theta0
+  // tabulated pair potentials (force/table.cu): table per type pair (-1:
+  // none), grid of each table, its points at Dev::tab + tab_off (force, energy)
+  int32_t ntables;
+  int8_t table_of[kMaxTypes * kMaxTypes];
+  float tab_rmin[kMaxTables], tab_rmax[kMaxTables], tab_dr[kMaxTables], tab_inv_dr[kMaxTables];
+  int32_t tab_n[kMaxTables], tab_off[kMaxTables];
   // --- dynamic
   int32_t mode;
   double fcap;                   // force cap (push-off)
@@ -199,6 +206,7 @@ struct Dev {
   int32_t* ncnt;
   double* part;                  // [chunks][kNumPartials]
   double* acf;                   // [replica][kAcfWords] stress autocorrelator state
+  const float2* tab;             // pair-table points (force, energy) of every replica's tables
   unsigned long long* kcount;    // [kKernelKinds] launches executed (block 0 of each launch counts)
   // rebuild work list: header (RbHeader), rb_cap replicas, then three
   // offset arrays of rb_cap + 1 (chunk items, cell-group items, home-cell
@@ -274,6 +282,7 @@ struct StepShape {
   int max_cells;        // largest P^3 (Morton cells) over replicas
   int max_home;         // largest G_alloc^3 (home cells) over replicas
   int force_variant, nbr_variant;
+  int has_table;        // some replica has tabulated pairs: the table pass follows the forces
 };
 using RebuildShape = StepShape;
 constexpr int kForceVariants = 7;
@@ -291,12 +300,19 @@ void capture_step(const Dev& d, const StepShape& g, cudaStream_t st, cudaStream_
                   const cudaStream_t* br);
 void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st);
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st, bool skip_rebuilt);
+// Positions (3 floats per atom, id order) of replica r, wrapped in its
+// last pre-force box, into out.
+void launch_pack_frame(const Dev& d, int r, int natoms, float* out, cudaStream_t st);
 // Forces of the replicas on the rebuild work list (after their rebuild).
 void launch_force_rebuilt(const Dev& d, bool ev, int variant, cudaStream_t st);
 // Rebuild of the replicas on the work list (rb): bin, scan, scatter, cell sort,
 // permute, bonded tables, neighbor lists.
 void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st);
-void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st);
+void launch_forces_only(const Dev& d, int nchunks, int variant, bool has_table, cudaStream_t st);
+// Tabulated pairs of the replicas that have them, added to the forces (and,
+// ev, to the energies and virial partials) the force kernel wrote.  sel: 0
+// every replica, 1 replicas not rebuilding this step, 2 rebuilding ones.
+void launch_table(const Dev& d, int nchunks, bool ev, int sel, cudaStream_t st);
 void launch_reduce_only(const Dev& d, int nchunks, int nreps, cudaStream_t st, int mode);
 // Scalars of the next pre-force for replicas whose copy a host upload made stale.
 void launch_prepare(const Dev& d, int nreps, cudaStream_t st);  // 0 setup, 2 re-evaluation

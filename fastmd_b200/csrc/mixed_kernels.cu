@@ -1442,6 +1442,112 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
   }
 }
 
+// ---------------------------------------------------------------- pair tables
+// Tabulated pair potential (force/table.cu:60-110 semantics): for listed
+// pairs within rc whose type pair has a table, r is clamped to the grid,
+// the force column (applied as F/r) and the energy are interpolated
+// linearly between the two grid points around r; half the energy and half
+// the virial per side.  A second pass over the list, run after the force
+// kernel for replicas with tables only; explicit roundings keep the energy
+// flavour's forces identical to the plain one's.
+template <bool EV>
+__global__ void __launch_bounds__(kChunk) k_table(Dev d, int sel) {
+  count_launch(d, kKTable);
+  const int chunk = blockIdx.x;
+  const int4 ci = d.chunk_rep[chunk];
+  const int r = ci.x;
+  if (r < 0) return;
+  const Rep& R = d.reps[r];
+  if (!R.adv || R.ntables == 0 || need_ev(R) != EV) return;
+  if ((sel == 1 && R.rebuild_now) || (sel == 2 && !R.rebuild_now)) return;
+  __shared__ float4 s_shift[kShiftCodes];
+  const int G = R.G;
+  const float h = R.h;
+  const float dL = (float)(R.L - (double)G * (double)h);
+  if (threadIdx.x < kShiftCodes) {
+    const int c = threadIdx.x;
+    const int ax = c / 25, ay = (c / 5) % 5, az = c % 5;
+    s_shift[c] = make_float4(shift_term(axis_code_e(ax), axis_code_k(ax), h, dL),
+                             shift_term(axis_code_e(ay), axis_code_k(ay), h, dL),
+                             shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
+  }
+  __syncthreads();
+  const int local = ci.w * kChunk + threadIdx.x;
+  const int s = ci.y + threadIdx.x;
+  const float rc2 = (float)(R.rc * R.rc);
+  const int nt = R.ntypes;
+  double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (local < R.natoms) {
+    const float4 pi = d.pos[s];
+    const int ti = w_type(w_bits(pi.w));
+    const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
+    const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+    const float4* pbase = d.pos + R.slot_base;
+    float fx = 0, fy = 0, fz = 0, pe = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+    for (int k = 0; k < nn; ++k) {
+      const uint32_t w = __ldg(lst + (size_t)k * 32);
+      const float4 pj = __ldg(pbase + (w & kIdxMask));
+      const float4 sh = s_shift[w >> kCodeShift];
+      const float dx = __fsub_rn(__fsub_rn(pi.x, pj.x), sh.x);
+      const float dy = __fsub_rn(__fsub_rn(pi.y, pj.y), sh.y);
+      const float dz = __fsub_rn(__fsub_rn(pi.z, pj.z), sh.z);
+      const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+      const int tid = R.table_of[ti * nt + w_type(w_bits(pj.w))];
+      if (!(r2 < rc2 && r2 > 1e-10f) || tid < 0) continue;
+      const float rmin = R.tab_rmin[tid], rmax = R.tab_rmax[tid], dr = R.tab_dr[tid], inv_dr = R.tab_inv_dr[tid];
+      const int np = R.tab_n[tid];
+      const float rr = fminf(fmaxf(__fsqrt_rn(r2), rmin), rmax);
+      int idx = (int)__fmul_rn(__fsub_rn(rr, rmin), inv_dr);
+      idx = max(0, min(idx, np - 2));
+      const float t = __fmul_rn(__fsub_rn(rr, __fadd_rn(rmin, __fmul_rn((float)idx, dr))), inv_dr);
+      const float2 p0 = __ldg(d.tab + R.tab_off[tid] + idx), p1 = __ldg(d.tab + R.tab_off[tid] + idx + 1);
+      const float fs = __fadd_rn(p0.x, __fmul_rn(t, __fsub_rn(p1.x, p0.x)));
+      const float fxij = __fmul_rn(fs, dx), fyij = __fmul_rn(fs, dy), fzij = __fmul_rn(fs, dz);
+      fx = __fadd_rn(fx, fxij);
+      fy = __fadd_rn(fy, fyij);
+      fz = __fadd_rn(fz, fzij);
+      if (EV) {
+        const float e = __fadd_rn(p0.y, __fmul_rn(t, __fsub_rn(p1.y, p0.y)));
+        pe += 0.5f * e;
+        v0 += 0.5f * fxij * dx;
+        v1 += 0.5f * fxij * dy;
+        v2 += 0.5f * fxij * dz;
+        v3 += 0.5f * fyij * dy;
+        v4 += 0.5f * fyij * dz;
+        v5 += 0.5f * fzij * dz;
+      }
+    }
+    float4 f = d.force[s];
+    f.x = __fadd_rn(f.x, fx);
+    f.y = __fadd_rn(f.y, fy);
+    f.z = __fadd_rn(f.z, fz);
+    if (EV) f.w += pe;
+    d.force[s] = f;
+    if (EV) {
+      vals[0] = pe;
+      vals[1] = v0;
+      vals[2] = v1;
+      vals[3] = v2;
+      vals[4] = v3;
+      vals[5] = v4;
+      vals[6] = v5;
+    }
+  }
+  if (EV) {
+    __shared__ double s_add[7];
+    block_partials<kChunk>(vals, 7, s_add);
+    __syncthreads();
+    if (threadIdx.x < 7) d.part[(size_t)chunk * kNumPartials + threadIdx.x] += s_add[threadIdx.x];
+  }
+}
+
+void launch_table(const Dev& d, int nchunks, bool ev, int sel, cudaStream_t st) {
+  if (ev)
+    k_table<true><<<nchunks, kChunk, 0, st>>>(d, sel);
+  else
+    k_table<false><<<nchunks, kChunk, 0, st>>>(d, sel);
+}
+
 // ---------------------------------------------------------------- post-force
 __global__ void __launch_bounds__(kChunk, 7) k_post(Dev d, int kick) {
   count_launch(d, kKPost);
@@ -1600,6 +1706,31 @@ __global__ void __launch_bounds__(32) k_post_commit(Dev d, int kick) {
   }
 }
 
+// One trajectory frame of a replica in atom-id order: each position wrapped
+// in the box of the last pre-force update, as the reference stores and dumps
+// them (dump.cu:5-11, main.cu:675-679), in single precision.
+__global__ void __launch_bounds__(256) k_pack_frame(Dev d, int r, float* out) {
+  const Rep& R = d.reps[r];
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= R.natoms) return;
+  const int s = d.slot_of[R.slot_base + id];
+  const float4 p = d.pos[R.slot_base + s];
+  const uint32_t u = w_bits(p.w);
+  const int c[3] = {w_cx(u), w_cy(u), w_cz(u)};
+  const float o[3] = {p.x, p.y, p.z};
+  const double h = (double)R.h, Lp = R.Lpos;
+  for (int a = 0; a < 3; ++a) {
+    // the host readout's operations, rounded one by one
+    double x = __dadd_rn(__dmul_rn((double)c[a], h), (double)o[a]);
+    x = __dsub_rn(x, __dmul_rn(floor(x / Lp), Lp));
+    out[3 * id + a] = (float)x;
+  }
+}
+
+void launch_pack_frame(const Dev& d, int r, int natoms, float* out, cudaStream_t st) {
+  k_pack_frame<<<(natoms + 255) / 256, 256, 0, st>>>(d, r, out);
+}
+
 // ---- full-grid rebuild kernels: one block per chunk / cell group / home
 // cell of every replica (blocks of replicas that do not rebuild return at
 // once).  Used when many replicas rebuild in the same step, where they beat
@@ -1676,6 +1807,10 @@ void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t 
   if (*host_mode == kRbFull) launch_rebuild_full(d, g, st);
   launch_force(d, g.nchunks, false, g.force_variant, st, false);
   launch_force(d, g.nchunks, true, g.force_variant, st, false);
+  if (g.has_table) {
+    launch_table(d, g.nchunks, false, 0, st);
+    launch_table(d, g.nchunks, true, 0, st);
+  }
   k_post<<<g.nchunks, kChunk, 0, st>>>(d, 1);
   k_post_commit<<<g.nreps, 32, 0, st>>>(d, 1);
 }
@@ -1733,18 +1868,33 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   for (auto& e : join) FMD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   FMD_CUDA(cudaEventRecord(fork, st));
   for (int b = 0; b < 3; ++b) FMD_CUDA(cudaStreamWaitEvent(br[b], fork, 0));
+  const bool tab = shape.has_table != 0;
   capture_if(st, side_hi, c.rebuild, [&](cudaStream_t s) {
     launch_rebuild(d, nreps, nbr_variant, s);
     launch_force_rebuilt(d, false, force_variant, s);
     launch_force_rebuilt(d, true, force_variant, s);
+    if (tab) {
+      launch_table(d, nchunks, false, 2, s);
+      launch_table(d, nchunks, true, 2, s);
+    }
   });
   capture_if(br[0], side_hi, c.rebuild_full, [&](cudaStream_t s) {
     launch_rebuild_full(d, shape, s);
     launch_force_rebuilt(d, false, force_variant, s);
     launch_force_rebuilt(d, true, force_variant, s);
+    if (tab) {
+      launch_table(d, nchunks, false, 2, s);
+      launch_table(d, nchunks, true, 2, s);
+    }
   });
-  capture_if(br[1], side, c.force_plain, [&](cudaStream_t s) { launch_force(d, nchunks, false, force_variant, s, true); });
-  capture_if(br[2], side, c.force_ev, [&](cudaStream_t s) { launch_force(d, nchunks, true, force_variant, s, true); });
+  capture_if(br[1], side, c.force_plain, [&](cudaStream_t s) {
+    launch_force(d, nchunks, false, force_variant, s, true);
+    if (tab) launch_table(d, nchunks, false, 1, s);
+  });
+  capture_if(br[2], side, c.force_ev, [&](cudaStream_t s) {
+    launch_force(d, nchunks, true, force_variant, s, true);
+    if (tab) launch_table(d, nchunks, true, 1, s);
+  });
   for (int b = 0; b < 3; ++b) {
     FMD_CUDA(cudaEventRecord(join[b], br[b]));
     FMD_CUDA(cudaStreamWaitEvent(st, join[b], 0));
@@ -1873,9 +2023,13 @@ void launch_force_rebuilt(const Dev& d, bool ev, int variant, cudaStream_t st) {
   launch_hi(listed, g, kChunk, st, d);
 }
 
-void launch_forces_only(const Dev& d, int nchunks, int variant, cudaStream_t st) {
+void launch_forces_only(const Dev& d, int nchunks, int variant, bool has_table, cudaStream_t st) {
   launch_force(d, nchunks, false, variant, st, false);
   launch_force(d, nchunks, true, variant, st, false);
+  if (has_table) {
+    launch_table(d, nchunks, false, 0, st);
+    launch_table(d, nchunks, true, 0, st);
+  }
 }
 void launch_reduce_only(const Dev& d, int nchunks, int nreps, cudaStream_t st, int mode) {
   k_post<<<nchunks, kChunk, 0, st>>>(d, mode);

@@ -1047,6 +1047,8 @@ class PlainEngine final : public SimEngine {
 }  // namespace plain
 
 std::unique_ptr<SimEngine> make_plain_engine(const RunConfig& cfg, Topology topo, const fmd_melt_spec* pushoff) {
+  if (!cfg.tables.empty()) throw Error(FMD_ERR_CONFIG, "tabulated pair potentials are computed by the mixed form");
+  if (cfg.stress_on) throw Error(FMD_ERR_CONFIG, "the stress autocorrelation is computed by the mixed form");
   return std::unique_ptr<SimEngine>(new plain::PlainEngine(cfg, std::move(topo), pushoff));
 }
 

@@ -140,6 +140,16 @@ FMD_API fmd_status fmd_generate_melt(const fmd_melt_spec* spec, int32_t* counts,
 FMD_API fmd_status fmd_parse_run_conf(const char* text, int32_t* iout, double* fout, double* lj,
                                       int32_t lj_cap, double* bond, int32_t bond_cap, double* angle,
                                       int32_t angle_cap, uint64_t* seed);
+/* Read one keyword section of a LAMMPS pair_style table file, as the
+ * run.conf key 'table ti tj file keyword' does (io/table_parser.cpp:7-87):
+ * grid = rmin, rmax, dr, inv_dr (single precision, as the reference derives
+ * them); data = r, force, energy per point (cap points at most).  The force
+ * column is applied as F/r, as force/table.cu:92-96 applies it. */
+FMD_API fmd_status fmd_read_pair_table(const char* path, const char* keyword, float* grid, int32_t* npoints,
+                                       float* data, int32_t cap);
+/* Type pair -> table index of a run.conf ([ntypes*ntypes], -1: no table);
+ * *ntables = distinct tables. */
+FMD_API fmd_status fmd_run_conf_tables(const char* text, int32_t* table_of, int32_t cap, int32_t* ntables);
 /* Read a LAMMPS data file (src/io/lammps_data.cpp:18-229).  First call with
  * xyz == NULL to get counts[0..3] = natoms, nbonds, nangles, ntypes. */
 FMD_API fmd_status fmd_read_lammps_data(const char* path, int32_t* counts, double* box_L, double* xyz,
@@ -177,6 +187,19 @@ FMD_API fmd_status fmd_thermo(fmd_sim* sim, fmd_thermo_row* row);
 /* Restart file of the current state (write_lammps_data, io/lammps_data.cpp:269;
  * main.cu:681-691, 738-745 call it every restart_freq steps and at the end). */
 FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path);
+/* Binary trajectory (the reference's dump format, io/dump.cu:12-56, file
+ * "traj.bin" of run.conf dump_freq): header {int32 0x4D444247, int32 natoms,
+ * int32 ntypes}, then per frame {int64 step, int32 natoms, float box_L,
+ * float xyz[3 natoms]}, positions in atom-id order wrapped in the box of the
+ * last pre-force update.  A frame of a batch replica is packed on the device
+ * and copied into one of two pinned buffers; a background thread writes it,
+ * so the call returns once the copy is queued. */
+typedef struct fmd_traj fmd_traj;
+FMD_API fmd_status fmd_traj_open(const char* path, int32_t natoms, int32_t ntypes, fmd_traj** out);
+FMD_API fmd_status fmd_traj_write_sim(fmd_traj* t, fmd_sim* sim);
+FMD_API fmd_status fmd_traj_write_batch(fmd_traj* t, fmd_batch* b, int32_t slot);
+/* Writes the queued frames, closes the file and frees the handle. */
+FMD_API fmd_status fmd_traj_close(fmd_traj* t);
 /* Stress autocorrelation of a mixed-form simulation (see fmd_batch_stress_acf). */
 FMD_API fmd_status fmd_stress_acf(fmd_sim* sim, int64_t* lag_steps, double* values, int64_t* counts, int32_t cap,
                                   int32_t* nrows);

@@ -132,6 +132,9 @@ def ref_lib():
         R.ref_parse_lammps_data.restype = C.c_int32
         R.ref_parse_lammps_data.argtypes = [C.c_char_p, i32p, C.POINTER(C.c_float)] + [C.c_void_p] * 10 + [
             C.c_char_p, C.c_int32]
+        R.ref_parse_table.restype = C.c_int32
+        R.ref_parse_table.argtypes = [C.c_char_p, C.c_char_p, f32p, C.POINTER(C.c_int32), f32p, C.c_int32,
+                                      C.c_char_p, C.c_int32]
         _REF = R
     return _REF
 
@@ -380,3 +383,42 @@ class StressACF:
                 cnt.append(n)
             step *= self.POINTS
         return np.array(lag, np.int64), np.array(val).reshape(-1, 6), np.array(cnt, np.int64)
+
+
+def table_forces(xyz, L, rc, types, table_of, tables, bonds=None):
+    """FP64 tabulated pair forces (force/table.cu:60-110 semantics): every
+    pair within rc (minimum image; 1-2 bonded pairs excluded, as from the
+    Verlet list the reference's table kernel walks) whose type pair has a
+    table; r clamped to [rmin, rmax], grid index clamped to [0, n - 2],
+    linear interpolation of the force column (applied as F/r) and of the
+    energy.  tables: list of dict(rmin, rmax, dr, inv_dr, f, e).
+    Returns (forces [N, 3], per-atom energy [N], virial [6])."""
+    xyz = np.asarray(xyz, np.float64)
+    n = len(xyz)
+    f = np.zeros((n, 3))
+    pe = np.zeros(n)
+    vir = np.zeros(6)
+    ii, jj = pairs_brute(xyz, L, rc, bonds=bonds)
+    for i, j in zip(ii, jj):
+        t = table_of[types[i]][types[j]]
+        if t < 0:
+            continue
+        tb = tables[t]
+        d = xyz[i] - xyz[j]
+        d -= L * np.round(d / L)
+        r2 = float(d @ d)
+        if not (r2 < rc * rc and r2 > 1e-10):
+            continue
+        r = min(max(np.sqrt(r2), tb["rmin"]), tb["rmax"])
+        k = int((r - tb["rmin"]) * tb["inv_dr"])
+        k = max(0, min(k, len(tb["f"]) - 2))
+        u = (r - (tb["rmin"] + k * tb["dr"])) * tb["inv_dr"]
+        fs = tb["f"][k] + u * (tb["f"][k + 1] - tb["f"][k])
+        e = tb["e"][k] + u * (tb["e"][k + 1] - tb["e"][k])
+        f[i] += fs * d
+        f[j] -= fs * d
+        pe[i] += 0.5 * e
+        pe[j] += 0.5 * e
+        fd = fs * d
+        vir += np.array([fd[0] * d[0], fd[0] * d[1], fd[0] * d[2], fd[1] * d[1], fd[1] * d[2], fd[2] * d[2]])
+    return f, pe, vir

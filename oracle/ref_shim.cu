@@ -21,6 +21,7 @@ using std::min;
 #include "reference/cpu_reference.hpp"
 #include "integrate/nose_hoover.cuh"
 #include "io/config.hpp"
+#include "io/table_parser.hpp"
 #include "io/lammps_data.hpp"
 
 namespace {
@@ -224,6 +225,32 @@ int32_t ref_parse_config(const char* path, float* fout, int32_t* iout, float* lj
       angle[2 * k + 1] = topo.angle_params[k].theta0;
     }
     *seed = p.seed;
+    return 0;
+  } catch (const std::exception& e) {
+    if (err && err_len > 0) {
+      std::strncpy(err, e.what(), err_len - 1);
+      err[err_len - 1] = 0;
+    }
+    return 1;
+  }
+}
+
+// Pair table section reader (io/table_parser.cpp:7-87).  grid: rmin, rmax,
+// dr, inv_dr; data: r, force, energy per point (cap points at most).
+int32_t ref_parse_table(const char* path, const char* keyword, float* grid, int32_t* npoints, float* data,
+                        int32_t cap, char* err, int32_t err_len) {
+  try {
+    TableFileData t = parse_table_file(path, keyword);
+    grid[0] = t.params[0].rmin;
+    grid[1] = t.params[0].rmax;
+    grid[2] = t.params[0].dr;
+    grid[3] = t.params[0].inv_dr;
+    *npoints = t.params[0].npoints;
+    for (int32_t k = 0; k < (int32_t)t.data.size() && k < cap; ++k) {
+      data[3 * k] = t.data[k].x;
+      data[3 * k + 1] = t.data[k].y;
+      data[3 * k + 2] = t.data[k].z;
+    }
     return 0;
   } catch (const std::exception& e) {
     if (err && err_len > 0) {

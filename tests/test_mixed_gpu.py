@@ -264,3 +264,119 @@ def test_stress_acf_matches_oracle_correlator(ens, tmp_path):
     assert rows.shape == (len(lag), 8)
     assert np.array_equal(rows[:, 0].astype(np.int64), lag) and np.array_equal(rows[:, 7].astype(np.int64), cnt)
     b.close()
+
+
+def test_trajectory_frames_are_the_force_frame(tmp_path):
+    """Dumped frames (reference dump format) hold the positions the forces
+    belong to, in single precision and atom-id order, with step and box."""
+    conf = run_conf(ensemble="npt_nh 1.0 1.0 0.5 2.0 2.0 1.0 3", nsteps=400)
+    d = _melt(8, 25, seed=4)
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 12)
+    s = b.add(conf, desc=d)
+    p = tmp_path / "traj.bin"
+    want = []
+    with fm.Trajectory(p, d.natoms if hasattr(d, "natoms") else len(d.type), ntypes=1) as t:
+        for _ in range(5):
+            b.run(37)
+            x, Lf = b.force_frame(s)
+            want.append((b.info(s).step, np.float32(b.info(s).box_L), x.astype(np.float32)))
+            t.write(b, s)
+    tr = fm.read_trajectory(p)
+    assert tr["natoms"] == len(d.type) and tr["ntypes"] == 1 and len(tr["steps"]) == 5
+    for k, (st, L, x) in enumerate(want):
+        assert tr["steps"][k] == st and tr["box_L"][k] == L
+        assert np.array_equal(tr["xyz"][k], x)
+    b.close()
+
+
+def test_trajectory_of_a_simulation(tmp_path):
+    d = _melt(6, 20, seed=2)
+    for form in (fm.FMD_FORM_MIXED, fm.FMD_FORM_PLAIN_FP64):
+        sim = fm.Simulation(run_conf(nsteps=100), desc=d, form=form)
+        p = tmp_path / f"traj{form}.bin"
+        with fm.Trajectory(p, sim.natoms) as t:
+            sim.step(10)
+            t.write(sim)
+            sim.step(10)
+            t.write(sim)
+        tr = fm.read_trajectory(p)
+        assert list(tr["steps"]) == [10, 20]
+        x, _, _ = sim.state()
+        assert np.max(np.abs(tr["xyz"][1] - x.astype(np.float32))) < 1e-4 * sim.box_L
+
+
+def _soft_table(path, keyword, n=2001, rlo=0.05, rhi=2.5):
+    """A smooth tabulated pair: E = A cos^2(pi r / (2 rhi)), force column
+    F/r = -dE/dr / r."""
+    r = np.linspace(rlo, rhi, n)
+    A = 5.0
+    e = A * np.cos(np.pi * r / (2 * rhi)) ** 2
+    f = A * np.pi / rhi * np.cos(np.pi * r / (2 * rhi)) * np.sin(np.pi * r / (2 * rhi)) / r
+    lines = [keyword, f"N {n} R {rlo} {rhi}", ""]
+    lines += [f"{k + 1} {a:.9g} {b:.9g} {c:.9g}" for k, (a, b, c) in enumerate(zip(r, e, f))]
+    path.write_text("\n".join(lines) + "\n")
+
+
+def test_table_forces_match_oracle(tmp_path):
+    p = tmp_path / "soft.table"
+    _soft_table(p, "SOFT")
+    d = _melt(20, 50, seed=6)
+    conf = run_conf(lj=[(0, 0, 0.0, 0.0)], extra=f"table 0 0 {p} SOFT")
+    sim = fm.Simulation(conf, desc=d, form=fm.FMD_FORM_MIXED)
+    x, _, _ = sim.state()
+    f, pe, vir = sim.forces()
+    tb = fm.read_pair_table(p, "SOFT")
+    ft, pet, virt = po.table_forces(x, d.box_L, 2.5, d.type, [[0]], [tb], bonds=d.bonds)
+    fb, peb, virb = po.forces(oracle_system(d, xyz=x, lj_table=np.zeros((1, 1, 2))))
+    fo = fb + ft
+    assert rel_rms(f, fo) < FORCE_RMS_TOL
+    assert abs(pe.sum() - (peb.sum() + pet.sum())) < 1e-5 * abs(peb.sum() + pet.sum())
+    assert np.max(np.abs(vir - (virb + virt))) < 1e-5 * np.max(np.abs(virb + virt))
+
+
+def test_lj_shaped_table_reproduces_lj(tmp_path):
+    # force/table.cu's own check (tests/test_table.cu:7-104): a 10,000-point
+    # table of the clamped LJ force and energy matches the LJ kernel.
+    n, rlo, rc = 10000, 0.01, 2.5
+    r = np.linspace(rlo, rc, n)
+    sr6 = (1.0 / r ** 2) ** 3
+    fcol = np.clip(24.0 / r ** 2 * (2 * sr6 * sr6 - sr6), -1000, 1000)
+    ecol = 4.0 * (sr6 * sr6 - sr6)
+    p = tmp_path / "lj.table"
+    p.write_text("LJT\n" + f"N {n} R {rlo} {rc}\n\n" +
+                 "\n".join(f"{k + 1} {a:.9g} {b:.9g} {c:.9g}" for k, (a, b, c) in enumerate(zip(r, ecol, fcol))) + "\n")
+    d = _melt(20, 50, seed=8)
+    pre = fm.Simulation(run_conf(), gen=dict(nchains=20, chain_length=50, density=0.85, seed=8, pushoff_steps=2000),
+                        form=fm.FMD_FORM_MIXED)
+    x0, v0, i0 = pre.state()
+    d.xyz, d.vel, d.image = x0, v0, i0
+    lj_sim = fm.Simulation(run_conf(), desc=d, form=fm.FMD_FORM_MIXED)
+    tb_sim = fm.Simulation(run_conf(lj=[(0, 0, 0.0, 0.0)], extra=f"table 0 0 {p} LJT"), desc=d,
+                           form=fm.FMD_FORM_MIXED)
+    f1, pe1, _ = lj_sim.forces()
+    f2, pe2, _ = tb_sim.forces()
+    assert np.max(np.abs(f1 - f2)) < 1e-2 * max(1.0, np.max(np.abs(f1)))
+    assert abs(pe1.sum() - pe2.sum()) < 1e-3 * abs(pe1.sum())
+
+
+def test_table_replica_alone_equals_in_mix(tmp_path):
+    p = tmp_path / "soft.table"
+    _soft_table(p, "SOFT")
+    tconf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 3", nsteps=200, lj=[(0, 0, 0.0, 0.0)],
+                     extra=f"table 0 0 {p} SOFT\nthermo 1 7 th.dat")
+    lconf = run_conf(ensemble="nvt_nh 1.0 1.0 0.5 3", nsteps=200)
+    mt, ml = _melt(12, 30, seed=1), _melt(9, 40, seed=2)
+    mix = fm.Batch(max_replicas=4, max_atoms=1 << 13)
+    st = mix.add(tconf, desc=mt)
+    mix.add(lconf, desc=ml)
+    mix.run(80)
+    alone = fm.Batch(max_replicas=1, max_atoms=1 << 12)
+    a = alone.add(tconf, desc=mt)
+    alone.run(80)
+    xa, va, _ = alone.state(a)
+    xm, vm, _ = mix.state(st)
+    assert np.array_equal(xa, xm) and np.array_equal(va, vm)
+    assert np.array_equal(alone.thermo(a).as_array(), mix.thermo(st).as_array())
+    assert np.all(np.isfinite(xa)) and alone.info(a).status_word == 0
+    alone.close()
+    mix.close()
