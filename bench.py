@@ -516,6 +516,55 @@ def wl_c4(args, fm):
 WORKLOADS = {"c0": wl_c0, "c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c4": wl_c4}
 
 
+def kernel_timeline(b, steps, path):
+    """Kernel timeline of `steps` graph steps, from the CUDA activity records
+    the torch profiler collects over CUPTI (kernels inside the step graph's
+    conditional nodes included): per-kernel totals, step durations (k_pre to
+    k_pre) and the kernels of the first step with a rebuild.  Written to path
+    as text; the run's timing is not taken from it."""
+    import collections
+    import tempfile
+
+    import numpy as np
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        b.run(steps)
+        torch.cuda.synchronize()
+    with tempfile.TemporaryDirectory() as td:
+        tp = os.path.join(td, "trace.json")
+        prof.export_chrome_trace(tp)
+        with open(tp) as f:
+            ev = [e for e in json.load(f)["traceEvents"] if e.get("cat") == "kernel"]
+    ev.sort(key=lambda e: e["ts"])
+
+    def short(n):
+        return n.replace("void fmd::mixed::", "").replace("fmd::mixed::", "").split("(")[0]
+
+    tot, cnt = collections.defaultdict(float), collections.Counter()
+    for e in ev:
+        tot[short(e["name"])] += e["dur"]
+        cnt[short(e["name"])] += 1
+    pre = [e for e in ev if short(e["name"]).startswith("k_pre")]
+    dur = np.array([pre[i + 1]["ts"] - pre[i]["ts"] for i in range(len(pre) - 1)])
+    out = [f"kernels {len(ev)}, steps {len(dur)}: step us mean {dur.mean():.1f}, median {np.median(dur):.1f}, "
+           f"p90 {np.percentile(dur, 90):.1f}, max {dur.max():.1f}", "",
+           "| kernel | launches | total us | mean us |", "|---|---|---|---|"]
+    for k, v in sorted(tot.items(), key=lambda x: -x[1]):
+        out.append(f"| `{k}` | {cnt[k]} | {v:.1f} | {v / cnt[k]:.2f} |")
+    for i in range(len(pre) - 1):
+        a, z = pre[i]["ts"], pre[i + 1]["ts"]
+        win = [e for e in ev if a <= e["ts"] < z]
+        if any("k_neighbors" in e["name"] for e in win):
+            out += ["", f"first step with a rebuild ({z - a:.1f} us; start offset, duration, stream, kernel):", ""]
+            out += [f"    {e['ts'] - a:8.1f} +{e['dur']:7.1f}  s{e['args'].get('stream')}  {short(e['name'])}"
+                    for e in win]
+            break
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -529,6 +578,9 @@ def main():
                     help="steps per CUDA graph launch; < 0 launches every step directly (for kernel profilers)")
     ap.add_argument("--workload", default="headline", choices=["headline"] + sorted(WORKLOADS),
                     help="headline = the 64 x 30K benchmark; c0..c4 = the reported cases (one GPU)")
+    ap.add_argument("--timeline", default="", help="after the timed run, write a kernel timeline of "
+                    "--timeline-steps graph steps (torch profiler / CUPTI) to this file")
+    ap.add_argument("--timeline-steps", type=int, default=200)
     ap.add_argument("--drift-chunks", type=int, default=20, help="c1 / c2: conserved-quantity samples")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="c4: arrival window")
     ap.add_argument("--serve-step-scale", type=float, default=0.25, help="c4: scale of the requests' nsteps")
@@ -635,6 +687,8 @@ def main():
                             "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                             "ms_per_launch": fms.value, "mean_neighbors": entries.value / natoms,
                             "max_neighbors": mx.value}
+        if args.timeline:
+            kernel_timeline(b, args.timeline_steps, args.timeline)
         if not args.no_extras:
             # ---- end to end through the public C API: run in thermo-sized
             # chunks (100 steps) and read every replica's thermo row.
