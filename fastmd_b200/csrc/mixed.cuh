@@ -45,8 +45,12 @@ constexpr int kCodeShift = 25;
 constexpr int kShiftCodes = 125;
 constexpr uint32_t kZeroShiftCode = 62;  // (0, 0, 0): 2 * 25 + 2 * 5 + 2
 // Lists are padded to a multiple of kListPad entries with the atom's own
-// slot and the zero shift (r = 0, excluded by the r^2 > 1e-10 guard), so the
-// force loop runs whole batches.
+// slot and the shift (h + dL) on every axis (code 124: (e, k) = (1, 1)), so
+// the force loop runs whole batches and a padding entry lies sqrt(3) (h + dL)
+// > rc away: the cutoff test alone gives it an exact zero.  (The cell edge h
+// is at least rc + skin at a rebuild; an NPT contraction shrinks it by at
+// most rc / (rc + skin) before the rebuild trigger fires, so h >= rc.)
+constexpr uint32_t kPadCode = 124;
 constexpr int kListPad = 8;
 constexpr int32_t kNoForcedRebuild = 1 << 30;  // rebuild cadence: skin trigger only
 constexpr uint32_t kSlotMask26 = (1u << 26) - 1;  // bonded-table slot field

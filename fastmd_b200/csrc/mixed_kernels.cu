@@ -782,7 +782,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
         d.ncnt[base + il] = min(count, M);
         if (count > M) overflow |= kStatusOverflow;
         for (int k = count; k < ((count + kListPad - 1) & ~(kListPad - 1)) && k < M; ++k)
-          out[(size_t)k * 32] = (uint32_t)il | (kZeroShiftCode << kCodeShift);
+          out[(size_t)k * 32] = (uint32_t)il | (kPadCode << kCodeShift);
       }
     }
   }
@@ -907,7 +907,7 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
           if (count <= M) {
             const int padded = (count + kListPad - 1) & ~(kListPad - 1);
             if (lane < padded - count)
-              __stcg(out + (size_t)(count + lane) * 32, (uint32_t)i | (kZeroShiftCode << kCodeShift));
+              __stcg(out + (size_t)(count + lane) * 32, (uint32_t)i | (kPadCode << kCodeShift));
           }
           if (lane == 0) {
             d.ncnt[base + i] = min(count, M);
@@ -1059,7 +1059,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
           overflow |= kStatusOverflow;
         } else {
           for (int k = count; k < ((count + kListPad - 1) & ~(kListPad - 1)); ++k)
-            __stcg(out + (size_t)k * 32, (uint32_t)i | (kZeroShiftCode << kCodeShift));
+            __stcg(out + (size_t)k * 32, (uint32_t)i | (kPadCode << kCodeShift));
         }
       }
     }
@@ -1154,8 +1154,11 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
   const float dz = (pi.z - pj.z) - sh.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   // Branch-free: every listed pair is evaluated and pairs outside the cutoff
-  // (or the r = 0 padding entries) contribute an exact zero through selects.
-  const bool in = r2 < rc2 && r2 > 1e-10f;
+  // (padding entries included) contribute an exact zero through selects.
+  // The reference also skips r^2 <= 1e-10 (coincident atoms); here such a
+  // pair's F/r clamps to +-1000 times a separation below 1e-5, and only its
+  // energy is left out.
+  const bool in = r2 < rc2;
   const float r2inv = __fdividef(1.0f, r2);
   const float sr2 = sig2 * r2inv;
   const float sr6 = sr2 * sr2 * sr2;
@@ -1168,7 +1171,7 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
   a.fz = fmaf(fr, dz, a.fz);
   if (EV) {
     const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
-    const float e = in ? e24 * (1.0f / 12.0f) * (sr6 * (sr6 - 1.0f)) : 0.0f;  // 1/2 * 4 eps (sr12 - sr6)
+    const float e = in && r2 > 1e-10f ? e24 * (1.0f / 12.0f) * (sr6 * (sr6 - 1.0f)) : 0.0f;  // 1/2 * 4 eps (sr12 - sr6)
     a.pe += e;
     a.v0 = fmaf(fxij, dx, a.v0);
     a.v1 = fmaf(fxij, dy, a.v1);
@@ -1183,9 +1186,9 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
 // then all position gathers, then the arithmetic.  PF: the next batch's list
 // words are loaded before this batch's gathers (software pipelining, B more
 // registers).  nn is the padded length (a multiple of B).
-template <bool EV, int B, bool PF, int KB>
+template <bool EV, int B, bool PF, int KB, bool ONE>
 __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
-                                        const float4* s_shift, bool one_type, int ti, int nt, const float* s_eps24,
+                                        const float4* s_shift, int ti, int nt, const float* s_eps24,
                                         const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
                                         PairAcc& acc) {
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
@@ -1216,7 +1219,7 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
 #pragma unroll
     for (int q = 0; q < B; ++q) {
       float e24 = e24_0, sig2 = sig2_0;
-      if (!one_type) {
+      if (!ONE) {
         const int pidx = ti * nt + w_type(w_bits(pj[q].w));
         e24 = s_eps24[pidx];
         sig2 = s_sig2[pidx];
@@ -1333,8 +1336,11 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
     const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
-    const bool one_type = (nt == 1);
-    lj_loop<EV, B, PF, KB>(lst, nn, pbase, pi, s_shift, one_type, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    // one type (the Kremer-Grest melt): the pair parameters are loop constants
+    if (nt == 1)
+      lj_loop<EV, B, PF, KB, true>(lst, nn, pbase, pi, s_shift, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    else
+      lj_loop<EV, B, PF, KB, false>(lst, nn, pbase, pi, s_shift, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
@@ -1984,6 +1990,8 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
 // The energy flavour of a variant walks the list in the same batches with
 // the same compensated adds, so its forces are bit-identical: energy steps
 // and host re-evaluations do not perturb a trajectory.
+constexpr int kForceCarveoutPct = 16;  // percent of the SM's shared-memory maximum
+
 // The variant's two kernels: one block per chunk, and the work-list form.
 template <bool EV>
 void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(Dev)) {
@@ -2003,11 +2011,26 @@ void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(De
 #undef FMD_FORCE_VARIANT
 }
 
+// The force kernels use 4 KB of shared memory per block: ask for the
+// smallest shared-memory carve-out, leaving the rest of the SM's unified
+// L1 / shared array to cache the neighbor-position gathers.
+template <typename K>
+void prefer_l1(K kernel) {
+  FMD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, kForceCarveoutPct));
+}
+
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st, bool skip_rebuilt) {
   void (*per_chunk)(Dev, int) = nullptr;
   void (*listed)(Dev) = nullptr;
   if (ev) force_kernels<true>(variant, &per_chunk, &listed);
   else force_kernels<false>(variant, &per_chunk, &listed);
+  static bool set[2][kForceVariants] = {};
+  bool& done = set[ev ? 1 : 0][variant >= 0 && variant < kForceVariants ? variant : 0];
+  if (!done) {
+    prefer_l1(per_chunk);
+    prefer_l1(listed);
+    done = true;
+  }
   per_chunk<<<nchunks, kChunk, 0, st>>>(d, skip_rebuilt ? 1 : 0);
 }
 
