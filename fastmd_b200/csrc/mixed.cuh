@@ -272,7 +272,7 @@ __host__ __device__ inline int w_type(uint32_t u) { return (int)(u >> 27); }
 // of replicas that need no work return at once).
 struct StepConds {
   int use;
-  cudaGraphConditionalHandle rebuild, rebuild_full, force_plain, force_ev, post;
+  cudaGraphConditionalHandle rebuild, rebuild_full, force_plain, force_ev, post;  // force_plain: unused (plain node)
 };
 
 // Rebuild work list header (ints at the front of Dev::rb).

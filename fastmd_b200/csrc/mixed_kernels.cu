@@ -338,7 +338,7 @@ __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& con
   R.defer = post ? 0 : 1;
   if (cond.use) {
     // any replica that needs a force variant / a post switches it on
-    cudaGraphSetConditional(need_ev(R) ? cond.force_ev : cond.force_plain, 1u);
+    if (need_ev(R)) cudaGraphSetConditional(cond.force_ev, 1u);  // the plain flavour is an unconditional node
     if (post) cudaGraphSetConditional(cond.post, 1u);
   }
   if (!post) {
@@ -1858,7 +1858,6 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   StepConds c{1, 0, 0, 0, 0, 0};
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild_full, g, 0u, cudaGraphCondAssignDefault));
-  FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_plain, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
   k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
@@ -1893,10 +1892,11 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
       launch_table(d, nchunks, true, 2, s);
     }
   });
-  capture_if(br[1], side, c.force_plain, [&](cudaStream_t s) {
-    launch_force(d, nchunks, false, force_variant, s, true);
-    if (tab) launch_table(d, nchunks, false, 1, s);
-  });
+  // The plain flavour runs on nearly every step: a plain kernel node (its
+  // blocks return at once for replicas that need the energy flavour) saves
+  // the conditional node's latency.
+  launch_force(d, nchunks, false, force_variant, br[1], true);
+  if (tab) launch_table(d, nchunks, false, 1, br[1]);
   capture_if(br[2], side, c.force_ev, [&](cudaStream_t s) {
     launch_force(d, nchunks, true, force_variant, s, true);
     if (tab) launch_table(d, nchunks, true, 1, s);
