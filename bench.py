@@ -662,8 +662,8 @@ def main():
                                                     "ballot m6": round(float(variant_ms[nf + 2]), 4)},
                             "ms_per_variant": [round(float(x), 4) for x in variant_ms[:nf]],
                             "variants": ["b4 m6 pipelined k1", "b4 m8 pipelined k1", "b4 m6 pipelined k2",
-                                         "b4 m8 pipelined k2", "b2 m8 pipelined k4", "b4 m7 pipelined k2",
-                                         "b8 m6 k1"],
+                                         "b4 m8 pipelined k2", "b4 m9 pipelined k1", "b4 m7 pipelined k2",
+                                         "b4 m10 pipelined k1"],
                             "legend": "b = list entries per batch, m = min blocks per SM, pipelined = next batch's "
                                       "list words loaded ahead, k = batches per compensated add"}
         line["launches_by_kernel"] = launched

@@ -2003,9 +2003,9 @@ void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(De
     case 1: FMD_FORCE_VARIANT(4, 8, true, 1) break;
     case 2: FMD_FORCE_VARIANT(4, 6, true, 2) break;
     case 3: FMD_FORCE_VARIANT(4, 8, true, 2) break;
-    case 4: FMD_FORCE_VARIANT(2, 8, true, 4) break;
+    case 4: FMD_FORCE_VARIANT(4, 9, true, 1) break;
     case 5: FMD_FORCE_VARIANT(4, 7, true, 2) break;
-    case 6: FMD_FORCE_VARIANT(8, 6, false, 1) break;
+    case 6: FMD_FORCE_VARIANT(4, 10, true, 1) break;
     default: FMD_FORCE_VARIANT(4, 6, true, 1) break;
   }
 #undef FMD_FORCE_VARIANT
