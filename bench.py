@@ -47,8 +47,10 @@ PUSHOFF = 2000
 
 
 def run_conf(seed, nsteps=10_000_000):
+    # thermo every 100 steps, as the reference's runs of this melt print it:
+    # energies and virial come from the step itself on those steps
     return (f"ntypes 1\nrc 2.5\nskin 0.3\ndt 0.001\nnsteps {nsteps}\nnvt_langevin 1.0 1.0 1.0 {seed}\n"
-            "lj 0 0 1.0 1.0\nbond_type 0 30.0 1.5 1.0 1.0\nangle_type 0 5.0 180.0\n")
+            "lj 0 0 1.0 1.0\nbond_type 0 30.0 1.5 1.0 1.0\nangle_type 0 5.0 180.0\nthermo 1 100 thermo.dat\n")
 
 
 def measured_peaks():
