@@ -696,6 +696,10 @@ def main():
             # chunks (100 steps) and read every replica's thermo row.
             chunk = 100
             nchunks = max(1, args.steps // chunk)
+            # start on a thermo step, as a run printing every 100 steps does
+            lead = (-b.info(slots[0]).step) % chunk
+            if lead:
+                b.run(lead)
             t0 = time.perf_counter()
             lib.fmd_batch_mark(b._h, 0)
             rows = 0

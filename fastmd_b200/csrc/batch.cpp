@@ -1043,15 +1043,26 @@ void Batch::set_state(int r, const double* xyz, const double* vel, const int32_t
 // Energies and virial of the current state for replica r: steps between
 // thermo steps skip them, so a readout re-evaluates the forces (same
 // positions, same list, same result) with energies on.
+// Energies and virial of the current state of replica r, re-evaluated when
+// the last step did not compute them.  Every other running replica whose
+// energies are stale is re-evaluated in the same pass: reading the thermo
+// rows of a whole batch after a run costs one force pass, not one per
+// replica (the forces are bit-identical to the step's, so this perturbs no
+// trajectory).
 void Batch::ensure_ev(int r) {
   rep(r);
   if (h_reps_[r].ev_step == h_reps_[r].step) return;
   for (int k = 0; k < max_reps_; ++k)
     if (info_[k].used) h_reps_[k].stop_step = h_reps_[k].step;
-  Rep& R = h_reps_[r];
-  R.adv = 1;
-  R.force_ev = 1;
-  R.rebuild_now = 0;
+  for (int k = 0; k < max_reps_; ++k) {
+    Rep& K = h_reps_[k];
+    const bool stale = info_[k].used && K.active && K.mode == kModeRun && K.ev_step != K.step;
+    if (k == r || stale) {
+      K.adv = 1;
+      K.force_ev = 1;
+      K.rebuild_now = 0;
+    }
+  }
   upload_reps();
   const Dev d = dev();
   launch_forces_only(d, nchunks_launch(), force_variant_, shape().has_table != 0, st_);

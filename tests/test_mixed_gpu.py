@@ -380,3 +380,35 @@ def test_table_replica_alone_equals_in_mix(tmp_path):
     assert np.all(np.isfinite(xa)) and alone.info(a).status_word == 0
     alone.close()
     mix.close()
+
+
+def test_thermo_rows_of_a_batch_in_any_order():
+    """Reading one replica's thermo row re-evaluates every stale replica in
+    one pass; the rows and the trajectories that follow do not depend on the
+    order or number of rows read."""
+    confs = [run_conf(ensemble=f"nvt_langevin 1.0 1.0 1.0 {s}", nsteps=500) for s in (5, 6)]
+    confs.append(run_conf(ensemble="nvt_nh 1.0 1.0 0.5 3", nsteps=500))
+    melts = [_melt(8, 25, seed=11), _melt(6, 30, seed=12), _melt(10, 20, seed=13)]
+
+    def make():
+        b = fm.Batch(max_replicas=4, max_atoms=1 << 13)
+        return b, [b.add(c, desc=m) for c, m in zip(confs, melts)]
+
+    a, sa = make()
+    b, sb = make()
+    a.run(37)
+    b.run(37)
+    ra = [a.thermo(s).as_array() for s in sa]
+    rb = {s: b.thermo(s).as_array() for s in reversed(sb)}
+    for s1, s2, row in zip(sa, sb, ra):
+        assert np.array_equal(row, rb[s2])
+    a.run(20)
+    b.run(20)
+    b.thermo(sb[1])  # read one row only
+    for s1, s2 in zip(sa, sb):
+        xa, va, _ = a.state(s1)
+        xb, vb, _ = b.state(s2)
+        assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+        assert np.array_equal(a.thermo(s1).as_array(), b.thermo(s2).as_array())
+    a.close()
+    b.close()
