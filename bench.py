@@ -423,18 +423,25 @@ def wl_c2(args, fm):
                              type_block=50))
     b.run(GRAPH_CAPTURE_STEPS)  # settles the push-off and captures the step graph
     setup = time.perf_counter() - t0
-    e, ms_total = [], 0.0
+    # the configured 20,000 steps, sampled every 1,000 (--drift-chunks of them)
+    e, L, ms_total = [], [], 0.0
     for _ in range(args.drift_chunks):
-        ms_total += _dev_run(fm, b, 200)
-        e.append(b.thermo(s).conserved)
+        ms_total += _dev_run(fm, b, 1000)
+        row = b.thermo(s)
+        e.append(row.conserved)
+        L.append(row.box_L)
     e = np.array(e)
-    steps = np.arange(1, len(e) + 1) * 200.0
+    steps = np.arange(1, len(e) + 1) * 1000.0
     slope = float(np.polyfit(steps, e, 1)[0]) if len(e) > 1 else 0.0
+    h = len(e) // 2
+    slope2 = float(np.polyfit(steps[h:], e[h:], 1)[0]) if len(e) - h > 1 else 0.0
     n = 1_000_000
     return {"workload": "c2_1m_npt_two_types", "value": n * steps[-1] / (ms_total * 1e-3), "unit": "atom-steps/s",
-            "steps": int(steps[-1]), "setup_s": setup, "box_L_final": b.info(s).box_L,
+            "steps": int(steps[-1]), "setup_s": setup, "box_L": [round(x, 4) for x in L],
             "conserved_drift": {"E0": float(e[0]), "slope_per_step": slope,
-                                "relative_per_1e6_steps": slope * 1e6 / abs(e[0])}}
+                                "relative_per_1e6_steps": slope * 1e6 / abs(e[0]),
+                                "second_half_relative_per_1e6_steps": slope2 * 1e6 / abs(e[h]),
+                                "samples": [round(float(x), 7) for x in e]}}
 
 
 def wl_c3(args, fm):
