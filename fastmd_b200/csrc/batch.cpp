@@ -811,7 +811,7 @@ double Batch::elapsed_ms() {
 // Device time per launch of the force kernel on the current state (the
 // evaluation is idempotent); variant < 0: the batch's current variant.  Only
 // the kernel flavour the replicas need (with or without energies) is timed.
-double Batch::time_force(int iters, int variant) {
+double Batch::time_force(int iters, int variant, bool steady) {
   if (variant < 0) variant = force_variant_;
   download_reps();
   // mark every replica as advancing for the force kernel only
@@ -820,6 +820,11 @@ double Batch::time_force(int iters, int variant) {
   for (int r = 0; r < max_reps_; ++r)
     if (info_[r].used && h_reps_[r].active) {
       h_reps_[r].adv = 1;
+      if (steady) {
+        h_reps_[r].force_ev = 0;
+        h_reps_[r].thermo_freq = 0;
+        h_reps_[r].stress_freq = 0;
+      }
       (need_ev(h_reps_[r]) ? any_ev : any_plain) = true;
     }
   upload_reps();
@@ -886,7 +891,7 @@ int Batch::autotune(int iters, double* ms_out, int cap) {
   int best = 0;
   double best_ms = 0;
   for (int v = 0; v < kForceVariants; ++v) {
-    const double ms = time_force(iters, v);
+    const double ms = time_force(iters, v, true);
     if (ms_out && v < cap) ms_out[v] = ms;
     if (v == 0 || ms < best_ms) {
       best = v;

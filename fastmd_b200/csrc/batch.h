@@ -108,7 +108,9 @@ class Batch {
   void set_max_between(int r, int k);
   void mark(int which);
   double elapsed_ms();
-  double time_force(int iters, int variant = -1);
+  // steady: time the flavour each replica needs on ordinary steps (energies
+  // only for NPT), not the one its current step needs (a thermo step).
+  double time_force(int iters, int variant = -1, bool steady = false);
   int autotune(int iters, double* ms_out, int cap);
   double time_rebuild(int iters, int variant);
   int nbr_variant() const { return nbr_variant_; }
