@@ -50,9 +50,13 @@ def test_run_conf_rejects_like_reference(name):
     assert e.value.code == 2
 
 
-def test_run_conf_rejects_table_potential():
-    with pytest.raises(FastMDError):
-        fm.parse_run_conf("ntypes 1\nrc 2.5\nskin 0.3\ndt 0.001\nnvt_langevin 1 1 1\ntable 0 0 f.txt KW\n")
+def test_run_conf_table_file_must_exist(tmp_path):
+    # config.cpp:152 reads the table file while parsing; a missing file is an
+    # I/O error, not a silently ignored key
+    missing = tmp_path / "absent.table"
+    with pytest.raises(FastMDError) as e:
+        fm.parse_run_conf(f"ntypes 1\nrc 2.5\nskin 0.3\ndt 0.001\nnvt_langevin 1 1 1\ntable 0 0 {missing} KW\n")
+    assert e.value.code == 3 and "absent.table" in str(e.value)
 
 
 @pytest.mark.parametrize("name", ["full_style", "molecular_images", "atomic_velocities"])
