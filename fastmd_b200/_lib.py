@@ -492,6 +492,11 @@ class Batch:
     LAUNCH_KINDS = ("pre", "bin", "scan", "scatter", "cellsort", "permute", "topo", "neighbors", "force",
                     "force_ev", "post", "plan", "commit", "table")
 
+    def set_list_prune(self, slot, delta):
+        """Pruned pair list at rc + delta walked by the force kernels (on by
+        default with delta = 0.15 outside NPT); delta <= 0 turns it off."""
+        _call("fmd_batch_set_list_prune", self._h, C.c_int32(slot), C.c_double(delta))
+
     def set_rebuild_cadence(self, slot, max_steps):
         """Force a neighbor-list rebuild at least every max_steps steps
         (20 by default, as the reference); max_steps <= 0 leaves rebuilds to

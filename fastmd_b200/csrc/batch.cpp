@@ -60,6 +60,12 @@ void SegAlloc::release(int64_t at) {
   for (auto& kv : used_) hwm_ = std::max(hwm_, kv.first + kv.second);
 }
 
+static float uint_as_float_host(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, sizeof f);
+  return f;
+}
+
 // ------------------------------------------------------------- sizing
 static int next_pow2(int v) {
   int p = 1;
@@ -89,12 +95,12 @@ ReplicaPlan plan_replica(const RunConfig& cfg, int32_t natoms, double L) {
 }
 
 int64_t bytes_per_slot() {
-  return 6 * 16 + 2 * 16 + 8 * 4 + kMaxBondsPerAtom * 4 + kMaxAnglesPerAtom * 8 +
+  return 6 * 16 + 2 * 16 + 9 * 4 + kMaxBondsPerAtom * 4 + kMaxAnglesPerAtom * 8 +
          (int64_t)(kNumPartials * 8) / kChunk + 1;
 }
 
 int64_t estimate_bytes(const ReplicaPlan& p, int32_t nbonds, int32_t nangles) {
-  return p.slot_cap * bytes_per_slot() + p.nbr_entries * 4 + p.ncell * 12 + (int64_t)2 * nbonds * 8 +
+  return p.slot_cap * bytes_per_slot() + p.nbr_entries * 8 + p.ncell * 12 + (int64_t)2 * nbonds * 8 +
          (int64_t)3 * nangles * 16 + (int64_t)sizeof(Rep);
 }
 
@@ -121,7 +127,7 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
     const double budget = (o.hbm_budget_gb > 0 ? o.hbm_budget_gb : 150.0) * 1e9;
     int64_t slots = o.max_atoms > 0 ? o.max_atoms : (int64_t)4 << 20;
     // list entries at ~160 per atom, cells at ~4 per atom (Morton padding), topology at ~3 per atom
-    int64_t per = bytes_per_slot() + 160 * 4 + 4 * 12 + 3 * 16;
+    int64_t per = bytes_per_slot() + 2 * 160 * 4 + 4 * 12 + 3 * 16;  // full and pruned lists
     slots = std::min<int64_t>(slots, (int64_t)(budget / per));
     slots = ((slots + kChunk - 1) / kChunk) * kChunk;
     c.slots = slots;
@@ -153,19 +159,21 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   boff_.alloc_zero(S);
   aoff_.alloc_zero(S);
   ncnt_.alloc_zero(S);
+  pcnt_.alloc_zero(S);
   tcnt_.alloc_zero(S);
   bnd_.alloc(S * kMaxBondsPerAtom);
   ang_.alloc(S * kMaxAnglesPerAtom);
   part_.alloc_zero(S / kChunk * kNumPartials);
   kcount_.alloc_zero(kKernelKinds);
   acf_.alloc_zero((size_t)max_reps_ * kAcfWords);
-  rb_.alloc_zero(kRbHead + (size_t)max_reps_ + 3 * ((size_t)max_reps_ + 1));
+  rb_.alloc_zero(kRbHead + (size_t)max_reps_ + kRbOffArrays * ((size_t)max_reps_ + 1));
   cell_cnt_.alloc_zero(c.cells);
   cell_start_.alloc_zero(c.cells);
   cell_fill_.alloc_zero(c.cells);
   bent_.alloc(std::max<int64_t>(1, c.bonds));
   aent_.alloc(std::max<int64_t>(1, c.angles));
   nbr_.alloc(c.nbr);
+  pnbr_.alloc(c.nbr);
   reps_.alloc_zero(max_reps_);
   chunk_rep_.alloc(S / kChunk);
   slot_cap_chunks_ = (int)(S / kChunk);
@@ -212,6 +220,8 @@ Dev Batch::dev() const {
   d.aent = aent_;
   d.nbr = nbr_;
   d.ncnt = ncnt_;
+  d.pnbr = pnbr_;
+  d.pcnt = pcnt_;
   d.tcnt = tcnt_;
   d.bnd = bnd_;
   d.ang = ang_;
@@ -277,6 +287,9 @@ static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
   R.max_between = 20;  // main.cu:401
   R.thermo_freq = cfg.thermo_on ? cfg.thermo_freq : 0;
   R.stress_freq = cfg.stress_on ? cfg.stress_freq : 0;
+  // pruned list at rc + kPruneDelta: walked by the force kernels between
+  // filters (not under NPT, nor with a skin no wider than the margin)
+  R.prune_delta = (cfg.ensemble != FMD_NPT_NH && cfg.skin > kPruneDelta) ? (float)kPruneDelta : 0.f;
   R.ntables = (int32_t)cfg.tables.size();
   for (int k = 0; k < kMaxTypes * kMaxTypes; ++k) R.table_of[k] = -1;
   for (size_t k = 0; k < cfg.table_of.size() && k < (size_t)(kMaxTypes * kMaxTypes); ++k)
@@ -347,6 +360,7 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   R.Lpos = L;
   R.h = (float)(L / G);
   R.maxdisp_bits = 0;
+  R.disp_acc = 0.f;
   R.status = 0;
   R.rebuilds = 0;
   std::memset(&R.nh, 0, sizeof(R.nh));
@@ -655,6 +669,7 @@ void Batch::setup(const std::vector<int>& rs) {
     R.L_list = R.L;
     R.list_scale = 1.0;
     R.maxdisp_bits = 0;
+    R.disp_acc = 0.f;
     R.force_ev = 1;
   }
   upload_reps();
@@ -856,6 +871,12 @@ double Batch::time_rebuild(int iters, int v) {
   for (int r = 0; r < max_reps_; ++r)
     if (info_[r].used && h_reps_[r].active) rs.push_back(r);
   if (rs.empty()) return 0.0;
+  for (int r : rs) {
+    h_reps_[r].rebuild_now = 1;  // the rebuild kernels act on replicas marked so
+    h_reps_[r].maxdisp_bits = 0;
+    h_reps_[r].disp_acc = 0.f;
+  }
+  upload_reps();
   const Dev d = dev();
   auto once = [&] {
     write_rebuild_list(rs);
@@ -919,7 +940,9 @@ void Batch::list_stats(int64_t* entries, int32_t* max_per_atom) {
     if (!info_[r].used || !h_reps_[r].active) continue;
     const Rep& R = h_reps_[r];
     std::vector<int32_t> c(R.natoms);
-    FMD_CUDA(cudaMemcpy(c.data(), ncnt_.p + R.slot_base, R.natoms * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    // the list the force kernel walks: the pruned one where the replica keeps it
+    const int32_t* src = (R.prune_delta > 0.f ? pcnt_.p : ncnt_.p) + R.slot_base;
+    FMD_CUDA(cudaMemcpy(c.data(), src, R.natoms * sizeof(int32_t), cudaMemcpyDeviceToHost));
     for (int32_t v : c) {
       tot += v;
       mx = std::max(mx, v);
@@ -927,6 +950,29 @@ void Batch::list_stats(int64_t* entries, int32_t* max_per_atom) {
   }
   if (entries) *entries = tot;
   if (max_per_atom) *max_per_atom = mx;
+}
+
+// Turn a replica's pruned list on (margin delta beyond rc) or off (delta <=
+// 0).  Turning it on filters the list at once; under NPT it stays off.
+void Batch::set_list_prune(int r, double delta) {
+  download_reps();
+  Rep& R = h_reps_[r];
+  const bool on = delta > 0.0 && R.ensemble != FMD_NPT_NH;
+  R.prune_delta = on ? (float)delta : 0.f;
+  if (on) {
+    // a filter now: the displacement since the last reference joins the
+    // accumulated bound and the current positions become the reference
+    R.disp_acc += std::sqrt(uint_as_float_host(R.maxdisp_bits));
+    R.maxdisp_bits = 0;
+    R.rebuild_now = 2;
+    upload_reps();
+    write_rebuild_list(std::vector<int>{r}, 0);
+    launch_rebuild(dev(), nreps_launch(), nbr_variant_, st_);
+    FMD_CUDA_LAUNCH();
+    R.rebuild_now = 0;
+  }
+  upload_reps();
+  FMD_CUDA(cudaStreamSynchronize(st_));
 }
 
 void Batch::set_max_between(int r, int k) {
@@ -998,9 +1044,10 @@ void Batch::read_state(int r, double* xyz, double* vel, int32_t* image, bool rew
 }
 
 // The rebuild work list holds exactly these replicas (a host-driven rebuild).
-void Batch::write_rebuild_list(const std::vector<int>& rs) {
+void Batch::write_rebuild_list(const std::vector<int>& rs, int rebuilds) {
   wl_.assign(kRbHead + rs.size(), 0);
   wl_[kRbCount] = (int)rs.size();
+  wl_[kRbRebuilds] = rebuilds < 0 ? (int)rs.size() : rebuilds;
   wl_[kRbMode] = kRbList;
   std::copy(rs.begin(), rs.end(), wl_.begin() + kRbHead);
   FMD_CUDA(cudaMemcpyAsync(rb_.p, wl_.data(), wl_.size() * sizeof(int), cudaMemcpyHostToDevice, st_));

@@ -103,9 +103,10 @@ class Batch {
   int nchunks_launch() const;
   int nreps_launch() const;
   StepShape shape() const;
-  void write_rebuild_list(const std::vector<int>& rs);
+  void write_rebuild_list(const std::vector<int>& rs, int rebuilds = -1);  // rebuilds < 0: all listed
   int graph_steps() const { return graph_steps_; }
   void set_max_between(int r, int k);
+  void set_list_prune(int r, double delta);
   void mark(int which);
   double elapsed_ms();
   // steady: time the flavour each replica needs on ordinary steps (energies
@@ -132,7 +133,7 @@ class Batch {
   cudaStream_t st_ = nullptr;
   cudaStream_t side_ = nullptr;    // captures conditional-node bodies
   cudaStream_t side_hi_ = nullptr;  // captures the rebuild branches' bodies (high priority)
-  cudaStream_t branch_[3] = {};     // further branches of a captured step
+  cudaStream_t branch_[4] = {};     // further branches of a captured step
   int graph_steps_ = 50;
   int force_variant_ = 0;
   bool concurrent_pushoff_ = false;
@@ -149,7 +150,7 @@ class Batch {
   DevBuf<float4> pos_, vel_, force_, ref_, tpos_, tvel_;
   DevBuf<int4> img_, timg_;
   DevBuf<uint32_t> key_;
-  DevBuf<int32_t> perm_, bucket_, slot_of_, boff_, aoff_, ncnt_, tcnt_;
+  DevBuf<int32_t> perm_, bucket_, slot_of_, boff_, aoff_, ncnt_, tcnt_, pcnt_;
   DevBuf<uint32_t> bnd_;
   DevBuf<uint2> ang_;
   DevBuf<double> part_;
@@ -163,7 +164,7 @@ class Batch {
   DevBuf<int32_t> cell_cnt_, cell_start_, cell_fill_;
   DevBuf<int2> bent_;
   DevBuf<int4> aent_;
-  DevBuf<uint32_t> nbr_;
+  DevBuf<uint32_t> nbr_, pnbr_;  // full (rc + skin) and pruned (rc + prune_delta) lists
   DevBuf<Rep> reps_;
   DevBuf<int4> chunk_rep_;
   std::vector<int4> h_chunk_rep_;

@@ -265,6 +265,14 @@ FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_
   });
 }
 
+FMD_API fmd_status fmd_batch_set_list_prune(fmd_batch* b, int32_t slot, double delta) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    bb.set_list_prune(slot, delta);
+  });
+}
+
 FMD_API fmd_status fmd_batch_set_rebuild_cadence(fmd_batch* b, int32_t slot, int32_t max_steps) {
   return guarded([&] {
     auto& bb = B(b);

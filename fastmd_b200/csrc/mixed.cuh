@@ -52,6 +52,7 @@ constexpr uint32_t kZeroShiftCode = 62;  // (0, 0, 0): 2 * 25 + 2 * 5 + 2
 // most rc / (rc + skin) before the rebuild trigger fires, so h >= rc.)
 constexpr uint32_t kPadCode = 124;
 constexpr int kListPad = 8;
+constexpr double kPruneDelta = 0.15;  // pruned-list margin beyond rc (sigma)
 constexpr int32_t kNoForcedRebuild = 1 << 30;  // rebuild cadence: skin trigger only
 constexpr uint32_t kSlotMask26 = (1u << 26) - 1;  // bonded-table slot field
 constexpr int kNumPartials = 14;  // pe, vir[6], ke[6], sum m v^2
@@ -133,6 +134,17 @@ struct Rep {
   double list_scale;  // product of the NPT position scale factors since the list was built
   float h;
   uint32_t maxdisp_bits;
+  // Pruned list: the pairs of the rc + skin list within rc + prune_delta,
+  // walked by the force kernels instead of the full list.  It is re-filtered
+  // when a displacement since the last filter exceeds prune_delta / 2; ref
+  // then holds the positions of the last filter (or rebuild), and disp_acc
+  // the sum of the largest displacements of the filters since the rebuild,
+  // so that largest displacement since the last filter + disp_acc bounds
+  // every displacement since the rebuild (the full list's trigger).
+  // prune_delta = 0: no pruned list (also under NPT, whose co-scaled frame
+  // can stretch past displacements).
+  float prune_delta;
+  float disp_acc;
   int32_t status;
   int64_t rebuilds;
   NHScalars nh;
@@ -208,6 +220,8 @@ struct Dev {
   // neighbor list
   uint32_t* nbr;
   int32_t* ncnt;
+  uint32_t* pnbr;                // pruned list (same layout and bases as nbr)
+  int32_t* pcnt;
   double* part;                  // [chunks][kNumPartials]
   double* acf;                   // [replica][kAcfWords] stress autocorrelator state
   const float2* tab;             // pair-table points (force, energy) of every replica's tables
@@ -272,12 +286,16 @@ __host__ __device__ inline int w_type(uint32_t u) { return (int)(u >> 27); }
 // of replicas that need no work return at once).
 struct StepConds {
   int use;
-  cudaGraphConditionalHandle rebuild, rebuild_full, force_plain, force_ev, post;  // force_plain: unused (plain node)
+  cudaGraphConditionalHandle rebuild, rebuild_full, force_plain, force_ev, post, prune;  // force_plain: unused (plain node)
 };
 
 // Rebuild work list header (ints at the front of Dev::rb).
-enum RbHeader : int { kRbCount = 0, kRbCommits = 1, kRbMode = 2, kRbHead = 4 };
-enum RbMode : int { kRbNone = 0, kRbList = 1, kRbFull = 2 };
+// The work list holds the replicas that rebuild this step (rebuild_now = 1)
+// and those that only re-filter their pruned list (rebuild_now = 2);
+// kRbRebuilds counts the former.
+enum RbHeader : int { kRbCount = 0, kRbCommits = 1, kRbMode = 2, kRbRebuilds = 3, kRbHead = 4 };
+constexpr int kRbOffArrays = 4;  // chunk items (rebuilding), cell groups, home cells, chunk items (all listed)
+enum RbMode : int { kRbNone = 0, kRbList = 1, kRbFull = 2, kRbPrune = 3 };  // kRbPrune: list filters only
 constexpr int kRbFullMin = 8;  // replicas rebuilding in one step before full grids pay
 
 // Launch geometry of a step for the current batch layout.
@@ -299,7 +317,7 @@ void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t 
 // st2: a second capture stream for the parallel branches of a step.
 // Records one step into the graph being captured on st.  side / side_hi
 // record conditional-node bodies (side_hi: high priority, for the rebuild
-// branches); br: three further streams for the parallel branches.
+// branches); br: four further streams for the parallel branches.
 void capture_step(const Dev& d, const StepShape& g, cudaStream_t st, cudaStream_t side, cudaStream_t side_hi,
                   const cudaStream_t* br);
 void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st);
@@ -307,6 +325,9 @@ void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t 
 // Positions (3 floats per atom, id order) of replica r, wrapped in its
 // last pre-force box, into out.
 void launch_pack_frame(const Dev& d, int r, int natoms, float* out, cudaStream_t st);
+// Filters of the listed replicas' pruned lists after their plan (a step
+// where no replica rebuilds).
+void launch_prune_only(const Dev& d, cudaStream_t st);
 // Forces of the replicas on the rebuild work list (after their rebuild).
 void launch_force_rebuilt(const Dev& d, bool ev, int variant, cudaStream_t st);
 // Rebuild of the replicas on the work list (rb): bin, scan, scatter, cell sort,

@@ -212,6 +212,7 @@ __global__ void __launch_bounds__(kChunk / APT, APT == 1 ? 6 : 12) k_pre(Dev d, 
   // this step's commits append to it
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     d.rb[kRbCount] = 0;
+    d.rb[kRbRebuilds] = 0;
     d.rb[kRbMode] = kRbNone;
   }
   const int4 ci = d.chunk_rep[blockIdx.x];
@@ -284,11 +285,13 @@ __global__ void __launch_bounds__(32) k_commit(Dev d, StepConds cond) {
   if (atomicAdd(d.rb + kRbCommits, 1) != (int)gridDim.x - 1) return;
   __threadfence();
   d.rb[kRbCommits] = 0;
-  const int n = d.rb[kRbCount];
-  const int mode = n == 0 ? kRbNone : (n >= kRbFullMin && 4 * n >= (int)gridDim.x ? kRbFull : kRbList);
+  const int n = d.rb[kRbCount], nr = d.rb[kRbRebuilds];
+  const int mode = n == 0 ? kRbNone
+                 : (nr == 0 ? kRbPrune : (nr >= kRbFullMin && 4 * nr >= (int)gridDim.x ? kRbFull : kRbList));
   d.rb[kRbMode] = mode;
   if (cond.use && mode == kRbList) cudaGraphSetConditional(cond.rebuild, 1u);
   if (cond.use && mode == kRbFull) cudaGraphSetConditional(cond.rebuild_full, 1u);
+  if (cond.use && mode == kRbPrune) cudaGraphSetConditional(cond.prune, 1u);
 }
 
 __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& cond) {
@@ -318,13 +321,29 @@ __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& con
   const double s = fmin(R.L / R.L_list, R.list_scale);
   const float hs = (float)(s < 1.0 ? 0.5 * (s * (R.rc + R.skin) - R.rc) : 0.5 * R.skin);
   const bool trig = hs <= 0.f || maxd2 > hs * hs;
-  if (trig || R.since >= R.max_between) {
+  // With a pruned list (pairs within rc + prune_delta, no NPT), maxd2 is the
+  // displacement since the last filter and disp_acc adds those of the earlier
+  // filters: the full list's bound is their sum; the pruned list holds while
+  // the displacement since its filter stays below prune_delta / 2.  A
+  // rebuild filters its new list too.
+  bool rtrig = trig;
+  const float dmax = sqrtf(maxd2);
+  if (R.disp_acc > 0.f) rtrig = hs <= 0.f || dmax + R.disp_acc > hs;
+  const bool ptrig = R.prune_delta > 0.f && dmax > 0.5f * R.prune_delta;
+  if (rtrig || R.since >= R.max_between) {
     R.since = 0;
     R.L_list = R.L;
     R.list_scale = 1.0;
     R.maxdisp_bits = 0u;
+    R.disp_acc = 0.f;
     R.rebuilds += 1;
     R.rebuild_now = 1;
+    atomicAdd(d.rb + kRbRebuilds, 1);
+    d.rb[kRbHead + atomicAdd(d.rb + kRbCount, 1)] = r;
+  } else if (ptrig) {
+    R.disp_acc += dmax;
+    R.maxdisp_bits = 0u;
+    R.rebuild_now = 2;
     d.rb[kRbHead + atomicAdd(d.rb + kRbCount, 1)] = r;
   } else {
     R.rebuild_now = 0;
@@ -441,11 +460,14 @@ constexpr int kCellGroup = 8;  // cells per cell-sort work item (one warp each)
 __global__ void __launch_bounds__(kPlanThreads) k_rbplan(Dev d) {
   count_launch(d, kKPlan);
   const int n = rb_count(d);
-  rb_scan(d, n, rb_off(d, 0), [&](int r) { return d.reps[r].nchunks; });
+  // rebuild items count the rebuilding replicas only; the forces and the
+  // list filter run over the chunks of every listed replica
+  rb_scan(d, n, rb_off(d, 0), [&](int r) { return d.reps[r].rebuild_now == 1 ? d.reps[r].nchunks : 0; });
   rb_scan(d, n, rb_off(d, 1), [&](int r) {
     const int P = d.reps[r].P;
-    return (P * P * P + kCellGroup - 1) / kCellGroup;
+    return d.reps[r].rebuild_now == 1 ? (P * P * P + kCellGroup - 1) / kCellGroup : 0;
   });
+  rb_scan(d, n, rb_off(d, 3), [&](int r) { return d.reps[r].nchunks; });
 }
 
 // Offsets of home-cell items (G^3 per replica, G as set by k_scan).
@@ -454,6 +476,7 @@ __global__ void __launch_bounds__(kPlanThreads) k_rbplan_home(Dev d, int variant
   const int n = rb_count(d);
   rb_scan(d, n, rb_off(d, 2), [&](int r) {
     const int G = d.reps[r].G;
+    if (d.reps[r].rebuild_now != 1) return 0;
     return variant == 1 ? nbr_items(G) : G * G * G;
   });
 }
@@ -548,6 +571,7 @@ __global__ void __launch_bounds__(kPlanThreads) k_scan(Dev d) {
   count_launch(d, kKScan);
   if ((int)blockIdx.x >= rb_count(d)) return;
   Rep& R = d.reps[rb_rep(d, blockIdx.x)];
+  if (R.rebuild_now != 1) return;  // re-filters its pruned list only
   const int ncell = R.P * R.P * R.P;
   const int per = (ncell + blockDim.x - 1) / blockDim.x;
   const int b0 = threadIdx.x * per;
@@ -1333,8 +1357,10 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
     PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     static_assert(kListPad % B == 0, "list padding must cover whole batches");
-    const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
-    const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+    // the pruned list when the replica keeps one (same layout and bases)
+    const bool pruned = R.prune_delta > 0.f;
+    const int nn = ((pruned ? d.pcnt[s] : d.ncnt[s]) + kListPad - 1) & ~(kListPad - 1);
+    const uint32_t* lst = (pruned ? d.pnbr : d.nbr) + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + base;
     // one type (the Kremer-Grest melt): the pair parameters are loop constants
     if (nt == 1)
@@ -1437,7 +1463,7 @@ template <bool EV, int B, int MINB, bool PF, int KB>
 __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
   count_launch(d, EV ? kKForceEv : kKForce);
   const int n = rb_count(d);
-  const int* off = rb_off(d, 0);
+  const int* off = rb_off(d, 3);
   const int total = n > 0 ? off[n] : 0;
   RbCursor cur(off, n, blockIdx.x);
   for (int item = blockIdx.x; item < total; item += gridDim.x) {
@@ -1447,6 +1473,65 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
     force_chunk<EV, B, PF, KB>(d, R.chunk_base + (item - cur.lo), false);
   }
 }
+
+// ---------------------------------------------------------------- pruned list
+// Filter of the listed replicas' lists (after a rebuild, or when the
+// displacement since the last filter reached prune_delta / 2): the entries
+// of the rc + skin list within rc + prune_delta at the current positions, in
+// list order, padded like the full list; the positions become the new
+// displacement reference.  Replicas without a pruned list are skipped.
+__global__ void __launch_bounds__(kChunk) k_prune(Dev d) {
+  count_launch(d, kKPlan);
+  const int n = rb_count(d);
+  const int* off = rb_off(d, 3);
+  const int total = n > 0 ? off[n] : 0;
+  __shared__ float4 s_shift[kShiftCodes];
+  RbCursor cur(off, n, blockIdx.x);
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    cur.seek(item);
+    __syncthreads();  // the previous item's shift table is no longer read
+    const Rep& R = d.reps[rb_rep(d, cur.i)];
+    if (R.prune_delta <= 0.f) continue;  // block-uniform
+    const int G = R.G;
+    const float h = R.h;
+    const float dL = (float)(R.L - (double)G * (double)h);
+    if (threadIdx.x < kShiftCodes) {
+      const int c = threadIdx.x;
+      const int ax = c / 25, ay = (c / 5) % 5, az = c % 5;
+      s_shift[c] = make_float4(shift_term(axis_code_e(ax), axis_code_k(ax), h, dL),
+                               shift_term(axis_code_e(ay), axis_code_k(ay), h, dL),
+                               shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
+    }
+    __syncthreads();
+    const int local = (item - cur.lo) * kChunk + threadIdx.x;
+    if (local >= R.natoms) continue;
+    const int base = R.slot_base, s = base + local;
+    const float4 pi = d.pos[s];
+    const float rcd = (float)(R.rc + (double)R.prune_delta);
+    const float rcd2 = rcd * rcd;
+    const size_t row0 = (size_t)R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+    const uint32_t* in = d.nbr + row0;
+    uint32_t* out = d.pnbr + row0;
+    const float4* pbase = d.pos + base;
+    const int nn = d.ncnt[s];
+    int cnt = 0;
+    for (int k = 0; k < nn; ++k) {
+      const uint32_t w = __ldg(in + (size_t)k * 32);
+      const float4 pj = __ldg(pbase + (w & kIdxMask));
+      const float4 sh = s_shift[w >> kCodeShift];
+      const float dx = (pi.x - pj.x) - sh.x, dy = (pi.y - pj.y) - sh.y, dz = (pi.z - pj.z) - sh.z;
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < rcd2) out[(size_t)(cnt++) * 32] = w;
+    }
+    const int padded = (cnt + kListPad - 1) & ~(kListPad - 1);
+    for (int k = cnt; k < padded; ++k) out[(size_t)k * 32] = (uint32_t)local | (kPadCode << kCodeShift);
+    d.pcnt[s] = cnt;
+    const float4 q = d.ref[s];
+    d.ref[s] = make_float4(pi.x, pi.y, pi.z, q.w);
+  }
+}
+
+void launch_prune(const Dev& d, cudaStream_t st);
 
 // ---------------------------------------------------------------- pair tables
 // Tabulated pair potential (force/table.cu:60-110 semantics): for listed
@@ -1486,8 +1571,10 @@ __global__ void __launch_bounds__(kChunk) k_table(Dev d, int sel) {
   if (local < R.natoms) {
     const float4 pi = d.pos[s];
     const int ti = w_type(w_bits(pi.w));
-    const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
-    const uint32_t* lst = d.nbr + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+    // the pruned list when the replica keeps one (same layout and bases)
+    const bool pruned = R.prune_delta > 0.f;
+    const int nn = ((pruned ? d.pcnt[s] : d.ncnt[s]) + kListPad - 1) & ~(kListPad - 1);
+    const uint32_t* lst = (pruned ? d.pnbr : d.nbr) + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + R.slot_base;
     float fx = 0, fy = 0, fz = 0, pe = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
     for (int k = 0; k < nn; ++k) {
@@ -1744,14 +1831,14 @@ void launch_pack_frame(const Dev& d, int r, int natoms, float* out, cudaStream_t
 __global__ void __launch_bounds__(kChunk) k_bin_g(Dev d) {
   count_launch(d, kKBin);
   const int4 ci = d.chunk_rep[blockIdx.x];
-  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  if (ci.x < 0 || d.reps[ci.x].rebuild_now != 1) return;
   bin_chunk(d, d.reps[ci.x], ci.w);
 }
 
 __global__ void __launch_bounds__(kChunk) k_scatter_g(Dev d) {
   count_launch(d, kKScatter);
   const int4 ci = d.chunk_rep[blockIdx.x];
-  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  if (ci.x < 0 || d.reps[ci.x].rebuild_now != 1) return;
   const Rep& R = d.reps[ci.x];
   const int local = ci.w * kChunk + threadIdx.x;
   if (local >= R.natoms) return;
@@ -1764,6 +1851,7 @@ __global__ void __launch_bounds__(32 * kCellGroup) k_cellsort_g(Dev d) {
   count_launch(d, kKCellsort);
   if ((int)blockIdx.y >= rb_count(d)) return;
   const Rep& R = d.reps[rb_rep(d, blockIdx.y)];
+  if (R.rebuild_now != 1) return;
   const int c = blockIdx.x * kCellGroup + (threadIdx.x >> 5);
   if (c < R.P * R.P * R.P) cellsort_cell(d, R, c, threadIdx.x & 31);
 }
@@ -1771,14 +1859,14 @@ __global__ void __launch_bounds__(32 * kCellGroup) k_cellsort_g(Dev d) {
 __global__ void __launch_bounds__(kChunk) k_permute_g(Dev d) {
   count_launch(d, kKPermute);
   const int4 ci = d.chunk_rep[blockIdx.x];
-  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  if (ci.x < 0 || d.reps[ci.x].rebuild_now != 1) return;
   permute_chunk(d, d.reps[ci.x], ci.w);
 }
 
 __global__ void __launch_bounds__(kChunk) k_topo_g(Dev d) {
   count_launch(d, kKTopo);
   const int4 ci = d.chunk_rep[blockIdx.x];
-  if (ci.x < 0 || !d.reps[ci.x].rebuild_now) return;
+  if (ci.x < 0 || d.reps[ci.x].rebuild_now != 1) return;
   topo_chunk(d, d.reps[ci.x], ci.w);
 }
 
@@ -1786,6 +1874,7 @@ __global__ void __launch_bounds__(kNbrThreads) k_neighbors_g(Dev d) {
   count_launch(d, kKNeighbors);
   if ((int)blockIdx.y >= rb_count(d)) return;
   Rep& R = d.reps[rb_rep(d, blockIdx.y)];
+  if (R.rebuild_now != 1) return;
   const int G = R.G;
   if ((int)blockIdx.x >= G * G * G) return;
   neighbors_cell_ballot(d, R, blockIdx.x);
@@ -1804,13 +1893,14 @@ int num_sms() {
 }  // namespace
 
 void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t st) {
-  const StepConds none{0, 0, 0, 0, 0, 0};
+  const StepConds none{0, 0, 0, 0, 0, 0, 0};
   k_pre<kPreAPT><<<g.nchunks, kChunk / kPreAPT, 0, st>>>(d, none);
   k_commit<<<g.nreps, 32, 0, st>>>(d, none);
   FMD_CUDA(cudaMemcpyAsync(host_mode, d.rb + kRbMode, sizeof(int), cudaMemcpyDeviceToHost, st));
   FMD_CUDA(cudaStreamSynchronize(st));
   if (*host_mode == kRbList) launch_rebuild(d, g.nreps, g.nbr_variant, st);
   if (*host_mode == kRbFull) launch_rebuild_full(d, g, st);
+  if (*host_mode == kRbPrune) launch_prune_only(d, st);
   launch_force(d, g.nchunks, false, g.force_variant, st, false);
   launch_force(d, g.nchunks, true, g.force_variant, st, false);
   if (g.has_table) {
@@ -1855,11 +1945,12 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   cudaStreamCaptureStatus cs;
   cudaGraph_t g;
   FMD_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
-  StepConds c{1, 0, 0, 0, 0, 0};
+  StepConds c{1, 0, 0, 0, 0, 0, 0};
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.rebuild_full, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
+  FMD_CUDA(cudaGraphConditionalHandleCreate(&c.prune, g, 0u, cudaGraphCondAssignDefault));
   k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
   k_commit<<<nreps, 32, 0, st>>>(d, c);
   // Four parallel branches, each one conditional node: the two rebuild forms
@@ -1868,11 +1959,11 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   // run beside the rebuild instead of after it.  The rebuild bodies are
   // captured on a high-priority stream, so their blocks go first whenever
   // the force kernels free a slot.
-  cudaEvent_t fork, join[3];
+  cudaEvent_t fork, join[4];
   FMD_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   for (auto& e : join) FMD_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   FMD_CUDA(cudaEventRecord(fork, st));
-  for (int b = 0; b < 3; ++b) FMD_CUDA(cudaStreamWaitEvent(br[b], fork, 0));
+  for (int b = 0; b < 4; ++b) FMD_CUDA(cudaStreamWaitEvent(br[b], fork, 0));
   const bool tab = shape.has_table != 0;
   capture_if(st, side_hi, c.rebuild, [&](cudaStream_t s) {
     launch_rebuild(d, nreps, nbr_variant, s);
@@ -1901,7 +1992,18 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
     launch_force(d, nchunks, true, force_variant, s, true);
     if (tab) launch_table(d, nchunks, true, 1, s);
   });
-  for (int b = 0; b < 3; ++b) {
+  // steps where replicas only re-filter their pruned lists skip the rebuild
+  // chain
+  capture_if(br[3], side_hi, c.prune, [&](cudaStream_t s) {
+    launch_prune_only(d, s);
+    launch_force_rebuilt(d, false, force_variant, s);
+    launch_force_rebuilt(d, true, force_variant, s);
+    if (tab) {
+      launch_table(d, nchunks, false, 2, s);
+      launch_table(d, nchunks, true, 2, s);
+    }
+  });
+  for (int b = 0; b < 4; ++b) {
     FMD_CUDA(cudaEventRecord(join[b], br[b]));
     FMD_CUDA(cudaStreamWaitEvent(st, join[b], 0));
   }
@@ -1951,6 +2053,16 @@ void launch_hi(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
 }
 }  // namespace
 
+void launch_prune(const Dev& d, cudaStream_t st) {
+  static const int g_prune = resident_grid(k_prune, kChunk);
+  launch_hi(k_prune, g_prune, kChunk, st, d);
+}
+
+void launch_prune_only(const Dev& d, cudaStream_t st) {
+  launch_hi(k_rbplan, 1, kPlanThreads, st, d);
+  launch_prune(d, st);
+}
+
 void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st) {
   const int nr = g.nreps;
   launch_hi(k_rbplan, 1, kPlanThreads, st, d);  // work-list offsets for the forces that follow
@@ -1961,6 +2073,7 @@ void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st) {
   launch_hi(k_permute_g, g.nchunks, kChunk, st, d);
   launch_hi(k_topo_g, g.nchunks, kChunk, st, d);
   launch_hi(k_neighbors_g, dim3(g.max_home, nr), kNbrThreads, st, d);
+  launch_prune(d, st);
 }
 
 void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
@@ -1983,6 +2096,7 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
     launch_hi(k_neighbors<0, 6>, g_nbr2, kNbrThreads, st, d);
   else
     launch_hi(k_neighbors<0, 8>, g_nbr0, kNbrThreads, st, d);
+  launch_prune(d, st);
 }
 
 // Force-kernel variants (list entries per batch, blocks per SM, pipelined

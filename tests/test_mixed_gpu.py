@@ -412,3 +412,39 @@ def test_thermo_rows_of_a_batch_in_any_order():
         assert np.array_equal(a.thermo(s1).as_array(), b.thermo(s2).as_array())
     a.close()
     b.close()
+
+
+def test_pruned_list_forces_equal_full_list():
+    """The pruned list (pairs within rc + 0.15, the default outside NPT) gives
+    the full list's forces up to summation order, at the start and after
+    many filters; switching it off and on keeps the forces."""
+    pre = fm.Simulation(run_conf(), gen=dict(nchains=20, chain_length=50, density=0.85, seed=21, pushoff_steps=2000),
+                        form=fm.FMD_FORM_MIXED)
+    x0, v0, i0 = pre.state()
+    d = _melt(20, 50, seed=21)
+    d.xyz, d.vel, d.image = x0, v0, i0
+    conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 9", nsteps=2000)
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    sp = b.add(conf, desc=d)   # pruned (default)
+    sf = b.add(conf, desc=d)
+    b.set_list_prune(sf, 0.0)  # full list
+    fp, pep, _ = b.forces(sp)
+    ff, pef, _ = b.forces(sf)
+    assert rel_rms(fp, ff) < 1e-6 and abs(pep.sum() - pef.sum()) < 1e-6 * abs(pef.sum())
+    for _ in range(6):
+        b.run(100)
+        x, _, _ = b.state(sp)
+        f, _, _ = b.forces(sp)
+        fo, _, _ = po.forces(oracle_system(d, xyz=x))
+        assert rel_rms(f, fo) < FORCE_RMS_TOL
+        assert b.info(sp).status_word == 0
+    # off mid-interval (the rebuild bound keeps the filters' displacements),
+    # then on again (filtered at once)
+    for delta in (0.0, 0.15):
+        b.set_list_prune(sp, delta)
+        for _ in range(2):
+            b.run(100)
+            x, _, _ = b.state(sp)
+            f, _, _ = b.forces(sp)
+            assert rel_rms(f, po.forces(oracle_system(d, xyz=x))[0]) < FORCE_RMS_TOL
+    b.close()
