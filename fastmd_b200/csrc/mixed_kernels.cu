@@ -1513,15 +1513,25 @@ __global__ void __launch_bounds__(kChunk) k_prune(Dev d) {
     const uint32_t* in = d.nbr + row0;
     uint32_t* out = d.pnbr + row0;
     const float4* pbase = d.pos + base;
-    const int nn = d.ncnt[s];
+    // batches of kListPad entries (the full list's padding lies beyond
+    // rc + prune_delta and drops out): all words, then all gathers, then
+    // the tests, so the loads of a batch are in flight together
+    const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
     int cnt = 0;
-    for (int k = 0; k < nn; ++k) {
-      const uint32_t w = __ldg(in + (size_t)k * 32);
-      const float4 pj = __ldg(pbase + (w & kIdxMask));
-      const float4 sh = s_shift[w >> kCodeShift];
-      const float dx = (pi.x - pj.x) - sh.x, dy = (pi.y - pj.y) - sh.y, dz = (pi.z - pj.z) - sh.z;
-      const float r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < rcd2) out[(size_t)(cnt++) * 32] = w;
+    for (int k = 0; k < nn; k += kListPad) {
+      uint32_t w[kListPad];
+      float4 pj[kListPad];
+#pragma unroll
+      for (int q = 0; q < kListPad; ++q) w[q] = __ldg(in + (size_t)(k + q) * 32);
+#pragma unroll
+      for (int q = 0; q < kListPad; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+#pragma unroll
+      for (int q = 0; q < kListPad; ++q) {
+        const float4 sh = s_shift[w[q] >> kCodeShift];
+        const float dx = (pi.x - pj[q].x) - sh.x, dy = (pi.y - pj[q].y) - sh.y, dz = (pi.z - pj[q].z) - sh.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < rcd2) out[(size_t)(cnt++) * 32] = w[q];
+      }
     }
     const int padded = (cnt + kListPad - 1) & ~(kListPad - 1);
     for (int k = cnt; k < padded; ++k) out[(size_t)k * 32] = (uint32_t)local | (kPadCode << kCodeShift);
