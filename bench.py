@@ -569,6 +569,20 @@ def kernel_timeline(b, steps, path):
            "| kernel | launches | total us | mean us |", "|---|---|---|---|"]
     for k, v in sorted(tot.items(), key=lambda x: -x[1]):
         out.append(f"| `{k}` | {cnt[k]} | {v:.1f} | {v / cnt[k]:.2f} |")
+    # steps by what ran beside the force kernel: a rebuild, a list filter only, nothing
+    cls = collections.defaultdict(list)
+    for i in range(len(pre) - 1):
+        a, z = pre[i]["ts"], pre[i + 1]["ts"]
+        names = [short(e["name"]) for e in ev if a <= e["ts"] < z]
+        force = sum(e["dur"] for e in ev if a <= e["ts"] < z and short(e["name"]).startswith("k_force<"))
+        kind = ("rebuild" if any(n.startswith("k_neighbors") for n in names)
+                else "filter only" if "k_prune" in names else "neither")
+        cls[kind].append((z - a, force))
+    out += ["", "| step kind | steps | step us mean | step us median | k_force us mean |", "|---|---|---|---|---|"]
+    for kind in ("neither", "filter only", "rebuild"):
+        if cls[kind]:
+            v = np.array(cls[kind])
+            out.append(f"| {kind} | {len(v)} | {v[:, 0].mean():.1f} | {np.median(v[:, 0]):.1f} | {v[:, 1].mean():.1f} |")
     for i in range(len(pre) - 1):
         a, z = pre[i]["ts"], pre[i + 1]["ts"]
         win = [e for e in ev if a <= e["ts"] < z]

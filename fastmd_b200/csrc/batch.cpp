@@ -967,7 +967,7 @@ void Batch::set_list_prune(int r, double delta) {
     R.rebuild_now = 2;
     upload_reps();
     write_rebuild_list(std::vector<int>{r}, 0);
-    launch_rebuild(dev(), nreps_launch(), nbr_variant_, st_);
+    launch_prune_only(dev(), st_);
     FMD_CUDA_LAUNCH();
     R.rebuild_now = 0;
   }

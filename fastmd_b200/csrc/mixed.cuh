@@ -320,19 +320,24 @@ void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t 
 // branches); br: four further streams for the parallel branches.
 void capture_step(const Dev& d, const StepShape& g, cudaStream_t st, cudaStream_t side, cudaStream_t side_hi,
                   const cudaStream_t* br);
-void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st);
+// filter: also filter the rebuilt replicas' pruned lists (k_prune); the step
+// leaves that to the work-list force launch that follows.
+void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st, bool filter = true);
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st, bool skip_rebuilt);
 // Positions (3 floats per atom, id order) of replica r, wrapped in its
 // last pre-force box, into out.
 void launch_pack_frame(const Dev& d, int r, int natoms, float* out, cudaStream_t st);
-// Filters of the listed replicas' pruned lists after their plan (a step
-// where no replica rebuilds).
+// Work-list offsets of the listed replicas (a step where none rebuilds).
+void launch_rb_plan(const Dev& d, cudaStream_t st);
+// Filters of the listed replicas' pruned lists after their plan, without a
+// force evaluation (host calls).
 void launch_prune_only(const Dev& d, cudaStream_t st);
-// Forces of the replicas on the rebuild work list (after their rebuild).
+// Forces of the replicas on the rebuild work list (after their rebuild),
+// with the filter of their pruned lists.
 void launch_force_rebuilt(const Dev& d, bool ev, int variant, cudaStream_t st);
 // Rebuild of the replicas on the work list (rb): bin, scan, scatter, cell sort,
-// permute, bonded tables, neighbor lists.
-void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st);
+// permute, bonded tables, neighbor lists (and, filter, their pruned lists).
+void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st, bool filter = true);
 void launch_forces_only(const Dev& d, int nchunks, int variant, bool has_table, cudaStream_t st);
 // Tabulated pairs of the replicas that have them, added to the forces (and,
 // ev, to the energies and virial partials) the force kernel wrote.  sel: 0

@@ -1267,6 +1267,86 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
   acc.v5 = g.v5;
 }
 
+// The LJ loop of a replica whose pruned list is due (rebuilt or filtered this
+// step), fused with the filter: it walks the rc + skin list, evaluates the
+// entries within rc + prune_delta (the others lie beyond rc and contribute
+// nothing) and writes them, in list order and padded, as the new pruned list.
+// The compensated adds follow the pruned list's batches (one per B * KB kept
+// entries, then those of its padding), so the forces are bit-identical to a
+// walk of the list it writes: a later re-evaluation at these positions (an
+// energy request) reproduces them.
+template <bool EV, int B, bool PF, int KB, bool ONE>
+__device__ __forceinline__ int lj_loop_filter(const uint32_t* lst, int nn, uint32_t* pout, float rcd2,
+                                              const float4* pbase, float4 pi, const float4* s_shift, int ti, int nt,
+                                              const float* s_eps24, const float* s_sig2, float rc2, KahanF& fx,
+                                              KahanF& fy, KahanF& fz, PairAcc& acc, uint32_t pad) {
+  constexpr int P = B * KB;  // kept entries per compensated add
+  const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
+  uint32_t wn[B];
+  if (PF) {
+#pragma unroll
+    for (int q = 0; q < B; ++q) wn[q] = nn > 0 ? __ldg(lst + (size_t)q * 32) : 0u;
+  }
+  PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
+  int pc = 0;
+  for (int k = 0; k < nn; k += B) {
+    uint32_t w[B];
+    if (PF) {
+#pragma unroll
+      for (int q = 0; q < B; ++q) w[q] = wn[q];
+      if (k + B < nn) {
+#pragma unroll
+        for (int q = 0; q < B; ++q) wn[q] = __ldg(lst + (size_t)(k + B + q) * 32);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < B; ++q) w[q] = __ldg(lst + (size_t)(k + q) * 32);
+    }
+    float4 pj[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const float4 sh = s_shift[w[q] >> kCodeShift];
+      const float dx = (pi.x - pj[q].x) - sh.x, dy = (pi.y - pj[q].y) - sh.y, dz = (pi.z - pj[q].z) - sh.z;
+      if (dx * dx + dy * dy + dz * dz < rcd2) {
+        float e24 = e24_0, sig2 = sig2_0;
+        if (!ONE) {
+          const int pidx = ti * nt + w_type(w_bits(pj[q].w));
+          e24 = s_eps24[pidx];
+          sig2 = s_sig2[pidx];
+        }
+        lj_pair<EV>(g, pi, sh, pj[q], rc2, e24, sig2);
+        pout[(size_t)pc * 32] = w[q];
+        if (++pc % P == 0) {
+          fx.add(g.fx);
+          fy.add(g.fy);
+          fz.add(g.fz);
+          g.fx = g.fy = g.fz = 0.0f;
+        }
+      }
+    }
+  }
+  // the pruned list's padding: its entries, and the compensated adds of the
+  // batches they complete
+  const int padded = (pc + kListPad - 1) & ~(kListPad - 1);
+  for (int k = pc; k < padded; ++k) pout[(size_t)k * 32] = pad;
+  for (int f = pc / P; f < (padded + P - 1) / P; ++f) {
+    fx.add(g.fx);
+    fy.add(g.fy);
+    fz.add(g.fz);
+    g.fx = g.fy = g.fz = 0.0f;
+  }
+  acc.pe = g.pe;
+  acc.v0 = g.v0;
+  acc.v1 = g.v1;
+  acc.v2 = g.v2;
+  acc.v3 = g.v3;
+  acc.v4 = g.v4;
+  acc.v5 = g.v5;
+  return pc;
+}
+
 // Harmonic angle (angle.cu:17-80) on (ri, rj = vertex, rk): force on the
 // member `role` (0: i, 1: j, 2: k), selected without branching so that lanes
 // in different roles follow one path.  EV: a third of the energy per member,
@@ -1316,7 +1396,10 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
 // computed by the one that matches its replica's need this step and the
 // other returns at once.  skip_rebuilt: leave replicas that rebuild their
 // list this step to the work-list launch that follows their rebuild.
-template <bool EV, int B, bool PF, int KB>
+// LISTED: the work-list launch itself (replicas rebuilt or re-filtered this
+// step), which walks the rc + skin list and, where the replica keeps a
+// pruned list, writes it (the filter) and its displacement reference.
+template <bool EV, int B, bool PF, int KB, bool LISTED>
 __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_rebuilt) {
   const int4 ci = d.chunk_rep[chunk];
   const int r = ci.x;
@@ -1358,15 +1441,29 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     static_assert(kListPad % B == 0, "list padding must cover whole batches");
     // the pruned list when the replica keeps one (same layout and bases)
-    const bool pruned = R.prune_delta > 0.f;
+    const bool keeps = R.prune_delta > 0.f;
+    const bool pruned = keeps && !LISTED;
+    const size_t row = (size_t)R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const int nn = ((pruned ? d.pcnt[s] : d.ncnt[s]) + kListPad - 1) & ~(kListPad - 1);
-    const uint32_t* lst = (pruned ? d.pnbr : d.nbr) + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+    const uint32_t* lst = (pruned ? d.pnbr : d.nbr) + row;
     const float4* pbase = d.pos + base;
-    // one type (the Kremer-Grest melt): the pair parameters are loop constants
-    if (nt == 1)
+    if (LISTED && keeps) {
+      const float rcd = (float)(R.rc + (double)R.prune_delta);
+      const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
+      const int pc =
+          nt == 1 ? lj_loop_filter<EV, B, PF, KB, true>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi, s_shift, ti, nt,
+                                                        s_eps24, s_sig2, rc2, fx, fy, fz, acc, pad)
+                  : lj_loop_filter<EV, B, PF, KB, false>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi, s_shift, ti, nt,
+                                                         s_eps24, s_sig2, rc2, fx, fy, fz, acc, pad);
+      d.pcnt[s] = pc;
+      const float4 q = d.ref[s];
+      d.ref[s] = make_float4(pi.x, pi.y, pi.z, q.w);
+    } else if (nt == 1) {
+      // one type (the Kremer-Grest melt): the pair parameters are loop constants
       lj_loop<EV, B, PF, KB, true>(lst, nn, pbase, pi, s_shift, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
-    else
+    } else {
       lj_loop<EV, B, PF, KB, false>(lst, nn, pbase, pi, s_shift, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+    }
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
     float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
@@ -1453,12 +1550,12 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
 template <bool EV, int B, int MINB, bool PF, int KB>
 __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt) {
   count_launch(d, EV ? kKForceEv : kKForce);
-  force_chunk<EV, B, PF, KB>(d, blockIdx.x, skip_rebuilt != 0);
+  force_chunk<EV, B, PF, KB, false>(d, blockIdx.x, skip_rebuilt != 0);
 }
 
 // The chunks of the replicas on the rebuild work list (a resident grid
 // striding over them), launched after their rebuild while the other
-// replicas' forces run beside it.
+// replicas' forces run beside it; it also writes their pruned lists.
 template <bool EV, int B, int MINB, bool PF, int KB>
 __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
   count_launch(d, EV ? kKForceEv : kKForce);
@@ -1470,7 +1567,7 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
     cur.seek(item);
     __syncthreads();  // the previous item's shared tables are no longer read
     const Rep& R = d.reps[rb_rep(d, cur.i)];
-    force_chunk<EV, B, PF, KB>(d, R.chunk_base + (item - cur.lo), false);
+    force_chunk<EV, B, PF, KB, true>(d, R.chunk_base + (item - cur.lo), false);
   }
 }
 
@@ -1908,14 +2005,25 @@ void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t 
   k_commit<<<g.nreps, 32, 0, st>>>(d, none);
   FMD_CUDA(cudaMemcpyAsync(host_mode, d.rb + kRbMode, sizeof(int), cudaMemcpyDeviceToHost, st));
   FMD_CUDA(cudaStreamSynchronize(st));
-  if (*host_mode == kRbList) launch_rebuild(d, g.nreps, g.nbr_variant, st);
-  if (*host_mode == kRbFull) launch_rebuild_full(d, g, st);
-  if (*host_mode == kRbPrune) launch_prune_only(d, st);
-  launch_force(d, g.nchunks, false, g.force_variant, st, false);
-  launch_force(d, g.nchunks, true, g.force_variant, st, false);
+  // the graph's kernels in one stream: the listed replicas' forces (and
+  // pruned-list filters) from the work-list launch after their rebuild
+  const int mode = *host_mode;
+  if (mode == kRbList) launch_rebuild(d, g.nreps, g.nbr_variant, st, false);
+  if (mode == kRbFull) launch_rebuild_full(d, g, st, false);
+  if (mode == kRbPrune) launch_rb_plan(d, st);
+  if (mode != kRbNone) {
+    launch_force_rebuilt(d, false, g.force_variant, st);
+    launch_force_rebuilt(d, true, g.force_variant, st);
+    if (g.has_table) {
+      launch_table(d, g.nchunks, false, 2, st);
+      launch_table(d, g.nchunks, true, 2, st);
+    }
+  }
+  launch_force(d, g.nchunks, false, g.force_variant, st, true);
+  launch_force(d, g.nchunks, true, g.force_variant, st, true);
   if (g.has_table) {
-    launch_table(d, g.nchunks, false, 0, st);
-    launch_table(d, g.nchunks, true, 0, st);
+    launch_table(d, g.nchunks, false, 1, st);
+    launch_table(d, g.nchunks, true, 1, st);
   }
   k_post<<<g.nchunks, kChunk, 0, st>>>(d, 1);
   k_post_commit<<<g.nreps, 32, 0, st>>>(d, 1);
@@ -1976,7 +2084,7 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   for (int b = 0; b < 4; ++b) FMD_CUDA(cudaStreamWaitEvent(br[b], fork, 0));
   const bool tab = shape.has_table != 0;
   capture_if(st, side_hi, c.rebuild, [&](cudaStream_t s) {
-    launch_rebuild(d, nreps, nbr_variant, s);
+    launch_rebuild(d, nreps, nbr_variant, s, false);
     launch_force_rebuilt(d, false, force_variant, s);
     launch_force_rebuilt(d, true, force_variant, s);
     if (tab) {
@@ -1985,7 +2093,7 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
     }
   });
   capture_if(br[0], side_hi, c.rebuild_full, [&](cudaStream_t s) {
-    launch_rebuild_full(d, shape, s);
+    launch_rebuild_full(d, shape, s, false);
     launch_force_rebuilt(d, false, force_variant, s);
     launch_force_rebuilt(d, true, force_variant, s);
     if (tab) {
@@ -2003,9 +2111,9 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
     if (tab) launch_table(d, nchunks, true, 1, s);
   });
   // steps where replicas only re-filter their pruned lists skip the rebuild
-  // chain
+  // chain: the work-list force launch filters
   capture_if(br[3], side_hi, c.prune, [&](cudaStream_t s) {
-    launch_prune_only(d, s);
+    launch_rb_plan(d, s);
     launch_force_rebuilt(d, false, force_variant, s);
     launch_force_rebuilt(d, true, force_variant, s);
     if (tab) {
@@ -2068,12 +2176,14 @@ void launch_prune(const Dev& d, cudaStream_t st) {
   launch_hi(k_prune, g_prune, kChunk, st, d);
 }
 
+void launch_rb_plan(const Dev& d, cudaStream_t st) { launch_hi(k_rbplan, 1, kPlanThreads, st, d); }
+
 void launch_prune_only(const Dev& d, cudaStream_t st) {
-  launch_hi(k_rbplan, 1, kPlanThreads, st, d);
+  launch_rb_plan(d, st);
   launch_prune(d, st);
 }
 
-void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st) {
+void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st, bool filter) {
   const int nr = g.nreps;
   launch_hi(k_rbplan, 1, kPlanThreads, st, d);  // work-list offsets for the forces that follow
   launch_hi(k_bin_g, g.nchunks, kChunk, st, d);
@@ -2083,10 +2193,10 @@ void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st) {
   launch_hi(k_permute_g, g.nchunks, kChunk, st, d);
   launch_hi(k_topo_g, g.nchunks, kChunk, st, d);
   launch_hi(k_neighbors_g, dim3(g.max_home, nr), kNbrThreads, st, d);
-  launch_prune(d, st);
+  if (filter) launch_prune(d, st);
 }
 
-void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
+void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st, bool filter) {
   static const int g_bin = resident_grid(k_bin, kChunk), g_scatter = resident_grid(k_scatter, kChunk),
                    g_sort = resident_grid(k_cellsort, 32 * kCellGroup), g_perm = resident_grid(k_permute, kChunk),
                    g_topo = resident_grid(k_topo, kChunk), g_nbr0 = resident_grid(k_neighbors<0, 8>, kNbrThreads),
@@ -2106,7 +2216,7 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st) {
     launch_hi(k_neighbors<0, 6>, g_nbr2, kNbrThreads, st, d);
   else
     launch_hi(k_neighbors<0, 8>, g_nbr0, kNbrThreads, st, d);
-  launch_prune(d, st);
+  if (filter) launch_prune(d, st);
 }
 
 // Force-kernel variants (list entries per batch, blocks per SM, pipelined

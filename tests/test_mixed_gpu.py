@@ -210,6 +210,33 @@ def test_observing_does_not_perturb(ens):
     b.close()
 
 
+def test_observing_every_step_does_not_perturb():
+    """Forces read after every step, so also right after the steps whose
+    work-list force launch rebuilt or re-filtered the pruned list while
+    evaluating the forces: the re-evaluation over the pruned list it wrote
+    reproduces those forces bit for bit, and the trajectory stays identical
+    to an unobserved one."""
+    conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 9", nsteps=10_000)
+    m = _melt(15, 40, seed=33)
+    a = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    sa = a.add(conf, desc=m)
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    sb = b.add(conf, desc=m)
+    for _ in range(150):
+        a.run(1)
+    r0 = b.info(sb).rebuilds
+    for _ in range(150):
+        b.run(1)
+        f, _, _ = b.forces(sb)
+        assert np.all(np.isfinite(f))
+    assert b.info(sb).rebuilds - r0 >= 2
+    for x, y in zip(a.state(sa), b.state(sb)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.thermo(sa).as_array(), b.thermo(sb).as_array())
+    a.close()
+    b.close()
+
+
 def test_server_results_equal_alone_and_in_mix():
     """Continuous batching: requests admitted while others run, retired and
     back-filled, give the same final thermo row and Rg as the same request
