@@ -576,7 +576,7 @@ def kernel_timeline(b, steps, path):
         names = [short(e["name"]) for e in ev if a <= e["ts"] < z]
         force = sum(e["dur"] for e in ev if a <= e["ts"] < z and short(e["name"]).startswith("k_force<"))
         kind = ("rebuild" if any(n.startswith("k_neighbors") for n in names)
-                else "filter only" if "k_prune" in names else "neither")
+                else "filter only" if any(n.startswith(("k_prune", "k_force_rb")) for n in names) else "neither")
         cls[kind].append((z - a, force))
     out += ["", "| step kind | steps | step us mean | step us median | k_force us mean |", "|---|---|---|---|---|"]
     for kind in ("neither", "filter only", "rebuild"):

@@ -822,6 +822,14 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
 // is deterministic.  Pairs within rc + skin, 1-2 bonded pairs excluded
 // (verlet_list.cu:108-335 semantics), exclusions compared as slots from the
 // per-slot bond table.
+// 16-byte asynchronous global -> shared copy (cp.async, L1-cached) and the
+// wait for all of this thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 constexpr int kNbrWarps = kNbrThreads / 32;
 constexpr int kNbrWin = 1024;     // staged candidates per window
 constexpr int kNbrGroup = 64;     // home atoms per pass
@@ -849,29 +857,41 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
   __shared__ int s_ns[27], s_off[28], s_cnt[kNbrGroup];
   __shared__ float s_sx[27], s_sy[27], s_sz[27];
   __shared__ uint32_t s_code[27];
+  constexpr int kExcl = 1 + kMaxBondsPerAtom;  // the atom itself and its bonded partners
+  __shared__ float4 s_hp[kNbrGroup];            // home atoms' positions
+  __shared__ int s_xk[kNbrGroup][kExcl];        // and their excluded candidates (index, or -1)
+  __shared__ uint32_t s_xm[kNbrWarps][kNbrWin / 32];  // per warp: excluded candidates of the window
+  for (int k = threadIdx.x; k < kNbrWarps * (kNbrWin / 32); k += blockDim.x) (&s_xm[0][0])[k] = 0u;
   const int hx = lc % G, hy = (lc / G) % G, hz = lc / (G * G);
-  if (threadIdx.x < 27) {
-    const int t = threadIdx.x;
-    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-    const int nx = (hx + dx + G) % G, ny = (hy + dy + G) % G, nz = (hz + dz + G) % G;
-    const uint32_t nkey = cell_key(nx, ny, nz);
-    const int ns = d.cell_start[cell_base + nkey];
-    s_ns[t] = ns;
-    s_off[t + 1] = d.cell_fill[cell_base + nkey] - ns;
-    // a candidate's position relative to the home cell: offset + shift
-    const int kx = (hx + dx < 0) ? -1 : (hx + dx >= G ? 1 : 0);
-    const int ky = (hy + dy < 0) ? -1 : (hy + dy >= G ? 1 : 0);
-    const int kz = (hz + dz < 0) ? -1 : (hz + dz >= G ? 1 : 0);
-    s_sx[t] = shift_term(dx, kx, h, dL);
-    s_sy[t] = shift_term(dy, ky, h, dL);
-    s_sz[t] = shift_term(dz, kz, h, dL);
-    s_code[t] = (uint32_t)(axis_shift_code(dx, kx) * 25 + axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz))
-                << kCodeShift;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_off[0] = 0;
-    for (int t = 0; t < 27; ++t) s_off[t + 1] += s_off[t];
+  if (warp == 0) {
+    // the 27 cells (one lane each) and their candidate offsets (warp scan)
+    int cnt = 0;
+    if (lane < 27) {
+      const int t = lane;
+      const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+      const int nx = (hx + dx + G) % G, ny = (hy + dy + G) % G, nz = (hz + dz + G) % G;
+      const uint32_t nkey = cell_key(nx, ny, nz);
+      const int ns = d.cell_start[cell_base + nkey];
+      s_ns[t] = ns;
+      cnt = d.cell_fill[cell_base + nkey] - ns;
+      // a candidate's position relative to the home cell: offset + shift
+      const int kx = (hx + dx < 0) ? -1 : (hx + dx >= G ? 1 : 0);
+      const int ky = (hy + dy < 0) ? -1 : (hy + dy >= G ? 1 : 0);
+      const int kz = (hz + dz < 0) ? -1 : (hz + dz >= G ? 1 : 0);
+      s_sx[t] = shift_term(dx, kx, h, dL);
+      s_sy[t] = shift_term(dy, ky, h, dL);
+      s_sz[t] = shift_term(dz, kz, h, dL);
+      s_code[t] = (uint32_t)(axis_shift_code(dx, kx) * 25 + axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz))
+                  << kCodeShift;
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane < 27) s_off[lane + 1] = incl;
+    if (lane == 0) s_off[0] = 0;
   }
   __syncthreads();
   const int total = s_off[27];
@@ -882,51 +902,92 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
   const uint32_t lt = (1u << lane) - 1u;
   for (int hg = 0; hg < nh; hg += kNbrGroup) {
     const int gn = min(kNbrGroup, nh - hg);
+    __syncthreads();  // the previous group's home data and window are no longer read
+    // home atoms, one thread each (their loads in flight together): the
+    // position, and the candidate indices of the atom itself and of its
+    // bonded partners, whose cells (within one cell of the home cell: a bond
+    // is shorter than a cell edge) the partners' cell fields give
+    for (int a = threadIdx.x; a < gn; a += blockDim.x) {
+      const int s = base + hs + hg + a;
+      s_hp[a] = d.pos[s];
+      s_xk[a][0] = s_off[13] + hg + a;
+      const int nb = d.tcnt[s] & 0xFF;
+#pragma unroll
+      for (int b = 0; b < kMaxBondsPerAtom; ++b) {
+        int k = -1;
+        if (b < nb) {
+          const int v = (int)(d.bnd[(size_t)s * kMaxBondsPerAtom + b] & kSlotMask26);
+          const uint32_t u = w_bits(d.pos[base + v].w);
+          int ex = w_cx(u) - hx, ey = w_cy(u) - hy, ez = w_cz(u) - hz;
+          ex += ex > 1 ? -G : (ex < -1 ? G : 0);
+          ey += ey > 1 ? -G : (ey < -1 ? G : 0);
+          ez += ez > 1 ? -G : (ez < -1 ? G : 0);
+          if (ex >= -1 && ex <= 1 && ey >= -1 && ey <= 1 && ez >= -1 && ez <= 1) {
+            const int t = (ez + 1) * 9 + (ey + 1) * 3 + (ex + 1);
+            if ((unsigned)(v - s_ns[t]) < (unsigned)(s_off[t + 1] - s_off[t])) k = s_off[t] + (v - s_ns[t]);
+          }
+        }
+        s_xk[a][1 + b] = k;
+      }
+    }
     for (int w0 = 0; w0 < total; w0 += kNbrWin) {
       const int wn = min(kNbrWin, total - w0);
       if (hg == 0 || total > kNbrWin) {
-        __syncthreads();
+        if (w0 > 0) __syncthreads();  // the previous window is no longer read
+        // candidates of the window, each warp taking cells warp, warp + 4, ...:
+        // asynchronous copies first (all in flight together), then each
+        // thread adds the cell shifts to the candidates it copied
+        for (int t = warp; t < 27; t += kNbrWarps) {
+          const int o0 = s_off[t], o1 = s_off[t + 1];
+          const int lo = max(o0, w0), hi = min(o1, w0 + wn);
+          const float4* src = d.pos + base + s_ns[t] - o0;
+          for (int k = lo + lane; k < hi; k += 32) cp_async16(&s_c[k - w0], src + k);
+        }
+        cp_async_wait_all();
         for (int t = warp; t < 27; t += kNbrWarps) {
           const int o0 = s_off[t], o1 = s_off[t + 1];
           const int lo = max(o0, w0), hi = min(o1, w0 + wn);
           const float sx = s_sx[t], sy = s_sy[t], sz = s_sz[t];
-          const uint32_t code = s_code[t];
           const int ns = s_ns[t];
+          const uint32_t code = s_code[t];
           for (int k = lo + lane; k < hi; k += 32) {
-            const int j = ns + (k - o0);
-            const float4 p = d.pos[base + j];
-            s_c[k - w0] = make_float4(p.x + sx, p.y + sy, p.z + sz, __uint_as_float((uint32_t)j | code));
+            const float4 p = s_c[k - w0];
+            s_c[k - w0] = make_float4(p.x + sx, p.y + sy, p.z + sz, __uint_as_float((uint32_t)(ns + (k - o0)) | code));
           }
         }
-        __syncthreads();
       }
+      // the window padded to whole pairs of 32 with candidates far away
+      const int wnp = (wn + 63) & ~63;
+      for (int k = wn + threadIdx.x; k < wnp; k += blockDim.x) s_c[k] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+      __syncthreads();  // window (and home data) staged
       for (int a = warp; a < gn; a += kNbrWarps) {
         const int i = hs + hg + a;
-        const float4 pi = d.pos[base + i];
-        const int nb = d.tcnt[base + i] & 0xFF;
-        uint32_t ex[kMaxBondsPerAtom];
-#pragma unroll
-        for (int b = 0; b < kMaxBondsPerAtom; ++b)
-          ex[b] = b < nb ? (d.bnd[(size_t)(base + i) * kMaxBondsPerAtom + b] & kSlotMask26) : 0xFFFFFFFFu;
+        const float4 pi = s_hp[a];
+        // this atom's excluded candidates in the window, as bits
+        int xk = -1;
+        if (lane < kExcl) {
+          const int k = s_xk[a][lane] - w0;
+          if (k >= 0 && k < wn) {
+            xk = k;
+            atomicOr(&s_xm[warp][k >> 5], 1u << (k & 31));
+          }
+        }
+        __syncwarp();
         int count = w0 == 0 ? 0 : s_cnt[a];
         uint32_t* out = list + ((size_t)(i >> 5) * M) * 32 + (i & 31);
-        for (int c0 = 0; c0 < wn; c0 += 32) {
-          const int k = c0 + lane;
-          bool acc = false;
-          uint32_t e = 0;
-          if (k < wn) {
-            const float4 c = s_c[k];
-            const float rx = pi.x - c.x, ry = pi.y - c.y, rz = pi.z - c.z;
-            const float r2 = rx * rx + ry * ry + rz * rz;
-            e = __float_as_uint(c.w);
-            const uint32_t j = e & kIdxMask;
-            acc = r2 < rcs2 && j != (uint32_t)i && j != ex[0] && j != ex[1] && j != ex[2] && j != ex[3];
-          }
-          const uint32_t m = __ballot_sync(0xFFFFFFFFu, acc);
+#pragma unroll 2
+        for (int c0 = 0; c0 < wnp; c0 += 32) {
+          const float4 c = s_c[c0 + lane];
+          const float rx = pi.x - c.x, ry = pi.y - c.y, rz = pi.z - c.z;
+          const float r2 = rx * rx + ry * ry + rz * rz;
+          const uint32_t m = __ballot_sync(0xFFFFFFFFu, r2 < rcs2) & ~s_xm[warp][c0 >> 5];
           const int at = count + __popc(m & lt);
-          if (acc && at < M) __stcg(out + (size_t)at * 32, e);
+          if (((m >> lane) & 1u) && at < M) __stcg(out + (size_t)at * 32, __float_as_uint(c.w));
           count += __popc(m);
         }
+        __syncwarp();
+        if (xk >= 0) s_xm[warp][xk >> 5] = 0u;
+        __syncwarp();
         if (w0 + kNbrWin >= total) {
           if (count <= M) {
             const int padded = (count + kListPad - 1) & ~(kListPad - 1);
