@@ -702,8 +702,12 @@ def main():
         line["launches_by_kernel"] = launched
         line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
                                     "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0),
-                                    "policy": "skin/2 displacement trigger only (forced cadence lifted by the "
-                                              "autotuner; the reference forces one every 20 steps)"}
+                                    "policy": "displacement trigger only (forced cadence lifted by the "
+                                              "autotuner; the reference forces one every 20 steps)",
+                                    "list_buffer": round(b.list_buffer(slots[0]), 4),
+                                    "list_buffer_policy": "run.conf skin 0.3 widened by the autotuner to the "
+                                                          "cell edge minus rc (replicas with a pruned list; the "
+                                                          "forces walk the pairs within rc + 0.15 either way)"}
         # ---- roofline of the force kernel
         entries = C.c_int64()
         mx = C.c_int32()

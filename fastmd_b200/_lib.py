@@ -497,6 +497,17 @@ class Batch:
         default with delta = 0.15 outside NPT); delta <= 0 turns it off."""
         _call("fmd_batch_set_list_prune", self._h, C.c_int32(slot), C.c_double(delta))
 
+    def set_list_buffer(self, slot, skin):
+        """Verlet-list margin beyond rc (the run.conf skin by default; the
+        autotuner widens it for replicas with a pruned list); rebuilds the
+        replica's list at once."""
+        _call("fmd_batch_set_list_buffer", self._h, C.c_int32(slot), C.c_double(skin))
+
+    def list_buffer(self, slot):
+        v = C.c_double()
+        _call("fmd_batch_get_list_buffer", self._h, C.c_int32(slot), C.byref(v))
+        return v.value
+
     def set_rebuild_cadence(self, slot, max_steps):
         """Force a neighbor-list rebuild at least every max_steps steps
         (20 by default, as the reference); max_steps <= 0 leaves rebuilds to

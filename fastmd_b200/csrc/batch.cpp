@@ -930,6 +930,19 @@ int Batch::autotune(int iters, double* ms_out, int cap) {
     if (info_[r].used && h_reps_[r].active) h_reps_[r].max_between = kNoForcedRebuild;
   upload_reps();
   FMD_CUDA(cudaStreamSynchronize(st_));
+  // List buffer: where a replica keeps a pruned list, the force kernels walk
+  // that list whatever the Verlet list's margin, so the margin is widened to
+  // the cell edge (the widest the cell grid allows unchanged): the list
+  // build, per atom the costliest work of a step, then runs less often.
+  for (int r = 0; r < max_reps_; ++r) {
+    if (!info_[r].used || !h_reps_[r].active) continue;
+    const Rep& R = h_reps_[r];
+    if (!(R.prune_delta > 0.f) || R.G < 3) continue;
+    const double wide = R.L / (1.0002 * R.G) - R.rc;
+    const double rcs = R.rc + wide;
+    const double expect = R.natoms / (R.L * R.L * R.L) * (4.0 / 3.0) * 3.14159265358979323846 * rcs * rcs * rcs;
+    if (wide > R.skin + 0.02 && 1.3 * expect + 16.0 <= R.M) set_list_buffer(r, wide);
+  }
   return best;
 }
 
@@ -971,6 +984,30 @@ void Batch::set_list_prune(int r, double delta) {
     FMD_CUDA_LAUNCH();
     R.rebuild_now = 0;
   }
+  upload_reps();
+  FMD_CUDA(cudaStreamSynchronize(st_));
+}
+
+// The Verlet list's margin beyond rc (the run.conf skin until changed): the
+// list holds the pairs within rc + skin and a rebuild follows a displacement
+// of skin / 2.  Changing it rebuilds the replica's list at once.
+void Batch::set_list_buffer(int r, double skin) {
+  download_reps();
+  Rep& R = h_reps_[r];
+  if (!(skin > 0.0) || !std::isfinite(skin)) throw Error(FMD_ERR_ARG, "list buffer must be positive");
+  const double rcs = R.rc + skin;
+  const double rho = R.natoms / (R.L * R.L * R.L);
+  const double expect = rho * (4.0 / 3.0) * 3.14159265358979323846 * rcs * rcs * rcs;
+  if (1.3 * expect + 16.0 > R.M) throw Error(FMD_ERR_ARG, "list buffer too wide for the replica's list capacity");
+  R.skin = skin;
+  R.rebuild_now = 1;
+  R.maxdisp_bits = 0;
+  R.disp_acc = 0.f;
+  upload_reps();
+  write_rebuild_list(std::vector<int>{r});
+  launch_rebuild(dev(), nreps_launch(), nbr_variant_, st_);
+  FMD_CUDA_LAUNCH();
+  R.rebuild_now = 0;
   upload_reps();
   FMD_CUDA(cudaStreamSynchronize(st_));
 }

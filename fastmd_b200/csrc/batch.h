@@ -107,6 +107,7 @@ class Batch {
   int graph_steps() const { return graph_steps_; }
   void set_max_between(int r, int k);
   void set_list_prune(int r, double delta);
+  void set_list_buffer(int r, double skin);
   void mark(int which);
   double elapsed_ms();
   // steady: time the flavour each replica needs on ordinary steps (energies

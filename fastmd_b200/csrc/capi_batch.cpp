@@ -273,6 +273,23 @@ FMD_API fmd_status fmd_batch_set_list_prune(fmd_batch* b, int32_t slot, double d
   });
 }
 
+FMD_API fmd_status fmd_batch_set_list_buffer(fmd_batch* b, int32_t slot, double skin) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    bb.set_list_buffer(slot, skin);
+  });
+}
+
+FMD_API fmd_status fmd_batch_get_list_buffer(fmd_batch* b, int32_t slot, double* skin) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!skin) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    *skin = bb.rep(slot).skin;
+  });
+}
+
 FMD_API fmd_status fmd_batch_set_rebuild_cadence(fmd_batch* b, int32_t slot, int32_t max_steps) {
   return guarded([&] {
     auto& bb = B(b);

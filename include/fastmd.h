@@ -301,6 +301,16 @@ FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_
  * under NPT; delta <= 0 turns it off.  A refinement of the reference's single list
  * (neighbor/verlet_list.cu), same forces up to summation order. */
 FMD_API fmd_status fmd_batch_set_list_prune(fmd_batch* b, int32_t slot, double delta);
+/* List buffer of a replica: the Verlet list holds the pairs within rc + skin
+ * and is rebuilt after a displacement of skin / 2 (neighbor/verlet_list.cu,
+ * neighbor/skin_trigger.cuh with the run.conf `skin`, its default).  Setting
+ * it rebuilds the list at once; FMD_ERR_ARG when the list capacity sized at
+ * fmd_batch_add cannot hold it.  fmd_batch_autotune widens it to the cell
+ * edge for replicas with a pruned list (their forces walk the pruned list,
+ * so a wider buffer only makes rebuilds rarer).  The forces do not depend on
+ * it beyond summation order. */
+FMD_API fmd_status fmd_batch_set_list_buffer(fmd_batch* b, int32_t slot, double skin);
+FMD_API fmd_status fmd_batch_get_list_buffer(fmd_batch* b, int32_t slot, double* skin);
 /* Autotuner: time each force-kernel variant (list entries per batch, blocks
  * per SM, pipelined list loads) `iters` times on the current state and each
  * neighbor-list variant on a full rebuild (ballot form with 8 or 6 blocks
@@ -310,7 +320,9 @@ FMD_API fmd_status fmd_batch_set_list_prune(fmd_batch* b, int32_t slot, double d
  * force variant (7), then ms per full rebuild of each neighbor variant (3),
  * then the chosen neighbor variant.  It also lifts the forced rebuild
  * cadence of the active replicas (rebuilds then follow the skin/2
- * displacement trigger alone; fmd_batch_set_rebuild_cadence restores one). */
+ * displacement trigger alone; fmd_batch_set_rebuild_cadence restores one)
+ * and widens the list buffer of replicas with a pruned list to the cell
+ * edge (fmd_batch_set_list_buffer restores the run.conf skin). */
 FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chosen, double* ms_per_variant,
                                       int32_t cap);
 /* Set the forced rebuild cadence of a replica (the reference rebuilds at

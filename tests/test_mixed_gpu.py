@@ -475,3 +475,38 @@ def test_pruned_list_forces_equal_full_list():
             f, _, _ = b.forces(sp)
             assert rel_rms(f, po.forces(oracle_system(d, xyz=x))[0]) < FORCE_RMS_TOL
     b.close()
+
+
+def test_list_buffer_widened_by_autotune_keeps_forces():
+    """The autotuner widens the Verlet-list margin of a replica with a pruned
+    list to the cell edge; rebuilds come further apart and the forces stay
+    the oracle's.  The run.conf skin can be restored, and a margin the list
+    capacity cannot hold is refused."""
+    pre = fm.Simulation(run_conf(), gen=dict(nchains=30, chain_length=100, density=0.85, seed=41, pushoff_steps=2000),
+                        form=fm.FMD_FORM_MIXED)
+    x0, v0, i0 = pre.state()
+    d = _melt(30, 100, seed=41)
+    d.xyz, d.vel, d.image = x0, v0, i0
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    s = b.add(run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 5", nsteps=10_000), desc=d)
+    assert b.list_buffer(s) == pytest.approx(0.3)
+    b.autotune(3)
+    wide = b.list_buffer(s)
+    assert wide > 0.45, wide
+    r0 = b.info(s).rebuilds
+    for _ in range(8):
+        b.run(50)
+        f, _, _ = b.forces(s)
+        x, Lf = b.force_frame(s)
+        assert rel_rms(f, po.forces(oracle_system(d, xyz=x, L=Lf))[0]) < FORCE_RMS_TOL
+        assert b.info(s).status_word == 0
+    assert b.info(s).rebuilds - r0 >= 2
+    b.set_list_buffer(s, 0.3)
+    assert b.list_buffer(s) == pytest.approx(0.3)
+    b.run(50)
+    f, _, _ = b.forces(s)
+    x, Lf = b.force_frame(s)
+    assert rel_rms(f, po.forces(oracle_system(d, xyz=x, L=Lf))[0]) < FORCE_RMS_TOL
+    with pytest.raises(fm.FastMDError):
+        b.set_list_buffer(s, 3.0)
+    b.close()
