@@ -707,7 +707,7 @@ def main():
                                     "list_buffer": round(b.list_buffer(slots[0]), 4),
                                     "list_buffer_policy": "run.conf skin 0.3 widened by the autotuner to the "
                                                           "cell edge minus rc (replicas with a pruned list; the "
-                                                          "forces walk the pairs within rc + 0.15 either way)"}
+                                                          "forces walk the pairs within rc + 0.12 either way)"}
         # ---- roofline of the force kernel
         entries = C.c_int64()
         mx = C.c_int32()

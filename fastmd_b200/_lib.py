@@ -494,7 +494,7 @@ class Batch:
 
     def set_list_prune(self, slot, delta):
         """Pruned pair list at rc + delta walked by the force kernels (on by
-        default with delta = 0.15 outside NPT); delta <= 0 turns it off."""
+        default with delta = 0.12 outside NPT); delta <= 0 turns it off."""
         _call("fmd_batch_set_list_prune", self._h, C.c_int32(slot), C.c_double(delta))
 
     def set_list_buffer(self, slot, skin):

@@ -297,7 +297,7 @@ FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_
  * filter exceeds delta / 2, are what the force kernels walk (fewer entries
  * than the full list; a rebuild then waits for the displacement since the
  * rebuild, bounded by the filters' displacements, to reach skin / 2).  On by
- * default with delta = 0.15 in the mixed form when the skin is wider, except
+ * default with delta = 0.12 in the mixed form when the skin is wider, except
  * under NPT; delta <= 0 turns it off.  A refinement of the reference's single list
  * (neighbor/verlet_list.cu), same forces up to summation order. */
 FMD_API fmd_status fmd_batch_set_list_prune(fmd_batch* b, int32_t slot, double delta);

@@ -442,7 +442,7 @@ def test_thermo_rows_of_a_batch_in_any_order():
 
 
 def test_pruned_list_forces_equal_full_list():
-    """The pruned list (pairs within rc + 0.15, the default outside NPT) gives
+    """The pruned list (pairs within rc + 0.12, the default outside NPT) gives
     the full list's forces up to summation order, at the start and after
     many filters; switching it off and on keeps the forces."""
     pre = fm.Simulation(run_conf(), gen=dict(nchains=20, chain_length=50, density=0.85, seed=21, pushoff_steps=2000),
@@ -467,7 +467,7 @@ def test_pruned_list_forces_equal_full_list():
         assert b.info(sp).status_word == 0
     # off mid-interval (the rebuild bound keeps the filters' displacements),
     # then on again (filtered at once)
-    for delta in (0.0, 0.15):
+    for delta in (0.0, 0.12):
         b.set_list_prune(sp, delta)
         for _ in range(2):
             b.run(100)
