@@ -52,6 +52,7 @@ constexpr uint32_t kZeroShiftCode = 62;  // (0, 0, 0): 2 * 25 + 2 * 5 + 2
 // most rc / (rc + skin) before the rebuild trigger fires, so h >= rc.)
 constexpr uint32_t kPadCode = 124;
 constexpr int kListPad = 8;
+constexpr int kPrunePad = 4;  // the pruned list: padded to whole force batches only
 constexpr double kPruneDelta = 0.12;  // pruned-list margin beyond rc (sigma)
 constexpr int32_t kNoForcedRebuild = 1 << 30;  // rebuild cadence: skin trigger only
 constexpr uint32_t kSlotMask26 = (1u << 26) - 1;  // bonded-table slot field

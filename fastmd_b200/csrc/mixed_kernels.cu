@@ -1390,7 +1390,7 @@ __device__ __forceinline__ int lj_loop_filter(const uint32_t* lst, int nn, uint3
   }
   // the pruned list's padding: its entries, and the compensated adds of the
   // batches they complete
-  const int padded = (pc + kListPad - 1) & ~(kListPad - 1);
+  const int padded = (pc + kPrunePad - 1) & ~(kPrunePad - 1);
   for (int k = pc; k < padded; ++k) pout[(size_t)k * 32] = pad;
   for (int f = pc / P; f < (padded + P - 1) / P; ++f) {
     fx.add(g.fx);
@@ -1500,12 +1500,12 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     const int ti = w_type(ui);
     KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
     PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    static_assert(kListPad % B == 0, "list padding must cover whole batches");
+    static_assert(kListPad % B == 0 && kPrunePad % B == 0, "list padding must cover whole batches");
     // the pruned list when the replica keeps one (same layout and bases)
     const bool keeps = R.prune_delta > 0.f;
     const bool pruned = keeps && !LISTED;
     const size_t row = (size_t)R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
-    const int nn = ((pruned ? d.pcnt[s] : d.ncnt[s]) + kListPad - 1) & ~(kListPad - 1);
+    const int nn = pruned ? (d.pcnt[s] + kPrunePad - 1) & ~(kPrunePad - 1) : (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
     const uint32_t* lst = (pruned ? d.pnbr : d.nbr) + row;
     const float4* pbase = d.pos + base;
     if (LISTED && keeps) {
@@ -1691,7 +1691,7 @@ __global__ void __launch_bounds__(kChunk) k_prune(Dev d) {
         if (r2 < rcd2) out[(size_t)(cnt++) * 32] = w[q];
       }
     }
-    const int padded = (cnt + kListPad - 1) & ~(kListPad - 1);
+    const int padded = (cnt + kPrunePad - 1) & ~(kPrunePad - 1);
     for (int k = cnt; k < padded; ++k) out[(size_t)k * 32] = (uint32_t)local | (kPadCode << kCodeShift);
     d.pcnt[s] = cnt;
     const float4 q = d.ref[s];
@@ -1741,7 +1741,7 @@ __global__ void __launch_bounds__(kChunk) k_table(Dev d, int sel) {
     const int ti = w_type(w_bits(pi.w));
     // the pruned list when the replica keeps one (same layout and bases)
     const bool pruned = R.prune_delta > 0.f;
-    const int nn = ((pruned ? d.pcnt[s] : d.ncnt[s]) + kListPad - 1) & ~(kListPad - 1);
+    const int nn = pruned ? (d.pcnt[s] + kPrunePad - 1) & ~(kPrunePad - 1) : (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
     const uint32_t* lst = (pruned ? d.pnbr : d.nbr) + R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
     const float4* pbase = d.pos + R.slot_base;
     float fx = 0, fy = 0, fz = 0, pe = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
