@@ -396,12 +396,16 @@ def wl_c1(args, fm):
     b2 = fm.Batch(max_replicas=1, max_atoms=65536, device=0)
     s2 = b2.add(cn, desc=d)
     b2.run(10)
+    # 100 samples over c1_drift_steps: the conserved quantity's step-to-step
+    # fluctuation (FP32 forces, dt = 0.001) swamps a slope fitted over a
+    # short run
     e = []
-    for _ in range(args.drift_chunks):
-        b2.run(1000)
+    chunk = max(1, args.c1_drift_steps // 100)
+    for _ in range(100):
+        b2.run(chunk)
         e.append(b2.thermo(s2).conserved)
     e = np.array(e)
-    steps = np.arange(1, len(e) + 1) * 1000.0
+    steps = np.arange(1, len(e) + 1) * float(chunk)
     slope = float(np.polyfit(steps, e, 1)[0]) if len(e) > 1 else 0.0
     rel_per_1e6 = slope * 1e6 / abs(e[0]) if len(e) else 0.0
     return {"workload": "c1_30k", "force_rel_rms_vs_fp64_oracle": {"max": max(errs), "mean": float(np.mean(errs)),
@@ -611,7 +615,8 @@ def main():
     ap.add_argument("--timeline", default="", help="after the timed run, write a kernel timeline of "
                     "--timeline-steps graph steps (torch profiler / CUPTI) to this file")
     ap.add_argument("--timeline-steps", type=int, default=200)
-    ap.add_argument("--drift-chunks", type=int, default=20, help="c1 / c2: conserved-quantity samples")
+    ap.add_argument("--drift-chunks", type=int, default=20, help="c2: conserved-quantity samples")
+    ap.add_argument("--c1-drift-steps", type=int, default=200_000, help="c1: NVT steps of the drift fit")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="c4: arrival window")
     ap.add_argument("--serve-step-scale", type=float, default=0.25, help="c4: scale of the requests' nsteps")
     args = ap.parse_args()
