@@ -582,11 +582,26 @@ def kernel_timeline(b, steps, path):
         kind = ("rebuild" if any(n.startswith("k_neighbors") for n in names)
                 else "filter only" if any(n.startswith(("k_prune", "k_force_rb")) for n in names) else "neither")
         cls[kind].append((z - a, force))
+    # rebuild steps by the list kernel's duration (grows with the atoms rebuilt)
+    rb = []
+    for i in range(len(pre) - 1):
+        a, z = pre[i]["ts"], pre[i + 1]["ts"]
+        nb = sum(e["dur"] for e in ev if a <= e["ts"] < z and short(e["name"]).startswith("k_neighbors"))
+        if nb > 0:
+            rb.append((nb, z - a))
+    rb_lines = []
+    if len(rb) >= 8:
+        rb = np.array(sorted(rb))
+        rb_lines = ["", "| rebuild steps by list-kernel time | steps | list kernel us mean | step us mean |",
+                    "|---|---|---|---|"]
+        for q, part in enumerate(np.array_split(rb, 4)):
+            rb_lines.append(f"| quartile {q + 1} | {len(part)} | {part[:, 0].mean():.1f} | {part[:, 1].mean():.1f} |")
     out += ["", "| step kind | steps | step us mean | step us median | k_force us mean |", "|---|---|---|---|---|"]
     for kind in ("neither", "filter only", "rebuild"):
         if cls[kind]:
             v = np.array(cls[kind])
             out.append(f"| {kind} | {len(v)} | {v[:, 0].mean():.1f} | {np.median(v[:, 0]):.1f} | {v[:, 1].mean():.1f} |")
+    out += rb_lines
     for i in range(len(pre) - 1):
         a, z = pre[i]["ts"], pre[i + 1]["ts"]
         win = [e for e in ev if a <= e["ts"] < z]
