@@ -510,3 +510,30 @@ def test_list_buffer_widened_by_autotune_keeps_forces():
     with pytest.raises(fm.FastMDError):
         b.set_list_buffer(s, 3.0)
     b.close()
+
+
+def test_table_replica_over_rebuilds_and_filters(tmp_path):
+    """A tabulated-pair replica stepped through rebuilds and pruned-list
+    filters (the table pass then walks the pruned list the work-list force
+    launch wrote), with the list buffer widened by the autotuner: the forces
+    stay the oracle's."""
+    p = tmp_path / "soft.table"
+    _soft_table(p, "SOFT")
+    d = _melt(30, 100, seed=12)
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    s = b.add(run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 4", nsteps=10_000, lj=[(0, 0, 0.0, 0.0)],
+                       extra=f"table 0 0 {p} SOFT"), desc=d)
+    b.autotune(3)
+    assert b.list_buffer(s) > 0.45
+    tb = fm.read_pair_table(p, "SOFT")
+    r0 = b.info(s).rebuilds
+    for _ in range(6):
+        b.run(50)
+        f, _, _ = b.forces(s)
+        x, Lf = b.force_frame(s)
+        ft, _, _ = po.table_forces(x, Lf, 2.5, d.type, [[0]], [tb], bonds=d.bonds)
+        fb, _, _ = po.forces(oracle_system(d, xyz=x, L=Lf, lj_table=np.zeros((1, 1, 2))))
+        assert rel_rms(f, fb + ft) < FORCE_RMS_TOL
+        assert b.info(s).status_word == 0
+    assert b.info(s).rebuilds - r0 >= 1
+    b.close()
