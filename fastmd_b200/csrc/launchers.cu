@@ -11,6 +11,7 @@
 // raises a flag instead of truncating silently; the caller owns all memory.
 #include <cub/cub.cuh>
 
+#include <cmath>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -30,12 +31,25 @@ struct VerletGeom {
   float cell, inv_cell;
 };
 
+// Cells per axis above which the cubed cell count no longer fits an int
+// (1290^3 > 2^31); larger grids are refused before any size is computed.
+constexpr int kMaxCellsPerAxis = 1290;
+
 // verlet_list.cu:3-13 (grid from the box) with the same FP32 arithmetic.
+// Refuses a box or cutoff that is not finite and positive, and a grid whose
+// cell count would overflow (the reference computes nx^3 in int).
 inline VerletGeom verlet_geom(float L, float rcs) {
+  if (!(std::isfinite(L) && std::isfinite(rcs) && L > 0.0f && rcs > 0.0f))
+    throw Error(FMD_ERR_ARG, "box_L and rc_skin must be finite and positive");
+  const float per_axis = L / rcs;
+  if (!std::isfinite(per_axis) || per_axis >= (float)kMaxCellsPerAxis)
+    throw Error(FMD_ERR_CAPACITY, "cell grid too large: box_L / rc_skin must stay below " +
+                                      std::to_string(kMaxCellsPerAxis));
   VerletGeom g;
-  g.nx = (int)(L / rcs);
+  g.nx = (int)per_axis;
   if (g.nx < 1) g.nx = 1;
-  g.ncell = g.nx * g.nx * g.nx;
+  const int64_t ncell = (int64_t)g.nx * g.nx * g.nx;
+  g.ncell = (int)ncell;
   g.cell = L / (float)g.nx;
   g.inv_cell = 1.0f / g.cell;
   return g;
@@ -278,6 +292,7 @@ MortonScratch morton_carve(void* base, int n) {
 constexpr size_t kStaticScratchBytes = (size_t)8 << 20;  // 8 MiB
 constexpr int kStaticMaxAtoms = 1 << 17;                  // 131072 atoms
 constexpr int kStaticMaxCells = 1 << 16;                  // 65536 cells
+constexpr int kStaticMaxCellsPerAxis = 40;                // 40^3 = 64000 cells
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_verlet_static_scratch[kStaticScratchBytes];
@@ -286,7 +301,9 @@ static std::mutex g_static_mu;
 static void* g_static_ptr[kMaxDevices] = {};
 
 // Device address of the static scratch for the current device (looked up on
-// the first call for that device, with that device current).
+// the first call for that device, with that device current, and kept for the
+// life of the process: a cudaDeviceReset on that device invalidates it, and
+// calls after such a reset are not supported).
 void* static_scratch_for_current_device() {
   int dev = 0;
   FMD_CUDA(cudaGetDevice(&dev));
@@ -331,7 +348,7 @@ extern "C" {
 
 FMD_API fmd_status fmd_verlet_scratch_bytes(int32_t natoms, float rc_skin, float box_L, size_t* bytes) {
   return guarded([&] {
-    if (!bytes || natoms <= 0 || rc_skin <= 0 || box_L <= 0) throw Error(FMD_ERR_ARG, "bad argument");
+    if (!bytes || natoms <= 0) throw Error(FMD_ERR_ARG, "bad argument");
     const VerletGeom g = verlet_geom(box_L, rc_skin);
     *bytes = verlet_carve(nullptr, natoms, g.ncell).total;
   });
@@ -389,6 +406,13 @@ FMD_API fmd_status fmd_launch_verlet_build_static(const void* pos, int32_t natom
       throw Error(FMD_ERR_ARG, "bad argument");
     if (natoms > kStaticMaxAtoms)
       throw Error(FMD_ERR_CAPACITY, "natoms exceeds the static-scratch limit of " + std::to_string(kStaticMaxAtoms));
+    if (!(std::isfinite(box_L) && std::isfinite(rc_skin) && box_L > 0.0f && rc_skin > 0.0f))
+      throw Error(FMD_ERR_ARG, "box_L and rc_skin must be finite and positive");
+    // at most 40 cells per axis (40^3 = 64000 <= kStaticMaxCells), checked
+    // before the cell count is formed
+    if (box_L / rc_skin >= (float)(kStaticMaxCellsPerAxis + 1))
+      throw Error(FMD_ERR_CAPACITY, "cell grid exceeds the static-scratch limit of " +
+                                        std::to_string(kStaticMaxCellsPerAxis) + " cells per axis");
     const VerletGeom g = verlet_geom(box_L, rc_skin);
     if (g.ncell > kStaticMaxCells)
       throw Error(FMD_ERR_CAPACITY, "cell grid exceeds the static-scratch limit of " + std::to_string(kStaticMaxCells) +

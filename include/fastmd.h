@@ -391,9 +391,13 @@ FMD_API fmd_status fmd_launch_verlet_build(const void* pos, int32_t natoms, floa
  * buffers; the cell-list scratch lives in one static device array inside the
  * library (8 MiB, held by every GPU that loads the library until the process
  * exits).  Limits: natoms <= 131072 and at most 65536 cells (box_L / rc_skin
- * <= 40 per axis); larger inputs return FMD_ERR_CAPACITY.  The first call on a
- * device looks the array's address up for that device (cudaGetSymbolAddress),
- * so make that first call before any stream capture.  Every call on a device
+ * <= 40 per axis); larger inputs return FMD_ERR_CAPACITY, and a box_L or
+ * rc_skin that is not finite and positive returns FMD_ERR_ARG, both before
+ * anything is launched.  The first call on a device looks the array's address
+ * up for that device (cudaGetSymbolAddress) and keeps it for the life of the
+ * process, so make that first call before any stream capture; a
+ * cudaDeviceReset of that device invalidates the kept address, and calls
+ * after one are not supported.  Every call on a device
  * shares the one array and each call re-initialises what must start at zero,
  * so calls whose kernels overlap on the GPU (different streams, no ordering)
  * race; order them on one stream.  No cudaMalloc / cudaFree is called. */

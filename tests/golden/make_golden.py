@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this directory from the reference's own CPU
 code (oracle/_ref/libfmdref.so, compiled from the reference sources by
-`make -C oracle ref`).
+`make -C oracle ref REF=<reference checkout>`).
 
 Run in a container that has the reference tree; the outputs are committed and
 the tests read only the committed files.  Inputs follow the reference's unit
@@ -44,7 +44,7 @@ def crand_f32():
 def main():
     R = po.ref_lib()
     if R is None:
-        raise SystemExit("oracle/_ref/libfmdref.so missing: run `make -C oracle ref` with the reference present")
+        raise SystemExit("oracle/_ref/libfmdref.so missing: run `make -C oracle ref REF=<reference checkout>`")
     out = {}
 
     # --- PBC minimum image (test_pbc.cu:29-41)

@@ -16,7 +16,6 @@ import pytest
 
 import fastmd_b200 as fm
 
-pytestmark = pytest.mark.gpu
 G = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden.npz"))
 
 
@@ -66,6 +65,7 @@ def _build(static, pos, eo, el, n, L, rcs, max_nbr=256):
     return c, lists, int(flag.item())
 
 
+@pytest.mark.gpu
 def test_static_scratch_build_matches_caller_scratch_build_twice():
     cases = [
         (G["melt_pos"], G["melt_bonds"], float(G["melt_L"][0]), np.float32(2.8)),
@@ -81,6 +81,7 @@ def test_static_scratch_build_matches_caller_scratch_build_twice():
         assert all(np.array_equal(a, b) for a, b in zip(l_ref, l_st))
 
 
+@pytest.mark.gpu
 def test_static_scratch_rejects_oversized_input():
     import torch
     lib = fm.lib()
@@ -93,3 +94,44 @@ def test_static_scratch_rejects_oversized_input():
     st = fn(C.c_void_p(pos.data_ptr()), C.c_int32(n), C.c_float(100.0), None, None, C.c_float(2.8), C.c_int32(4),
             C.c_void_p(nbr.data_ptr()), C.c_void_p(cnt.data_ptr()), None, None)
     assert st == 8   # FMD_ERR_CAPACITY, nothing launched
+
+
+def _no_device():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except Exception:
+        return True
+
+
+# Argument checks that return before anything is launched.  The pointers
+# below are never dereferenced: each call must fail on the host, so these run
+# on a machine without a GPU only.
+@pytest.mark.skipif(not _no_device(), reason="host-side argument checks; run where no GPU is visible")
+@pytest.mark.parametrize("L,rcs,code", [
+    (200.0, 2.8, 8),        # 71 cells per axis: beyond the 40-per-axis (65,536-cell) limit
+    (5735.0, 2.8, 8),       # 2048 per axis: 2048^3 wraps a 32-bit cell count to 0
+    (1.0e30, 2.8, 8),       # per-axis count beyond int
+    (float("inf"), 2.8, 1),
+    (float("nan"), 2.8, 1),
+    (30.0, 0.0, 1),
+    (30.0, -2.8, 1),
+    (-30.0, 2.8, 1),
+])
+def test_static_scratch_rejects_bad_geometry_before_launch(L, rcs, code):
+    lib = fm.lib()
+    fn = lib.fmd_launch_verlet_build_static
+    fn.restype = C.c_int32
+    dummy = C.c_void_p(256)
+    st = fn(dummy, C.c_int32(64), C.c_float(L), None, None, C.c_float(rcs), C.c_int32(4), dummy, dummy, None, None)
+    assert st == code
+
+
+@pytest.mark.skipif(not _no_device(), reason="host-side argument checks; run where no GPU is visible")
+@pytest.mark.parametrize("L,rcs,code", [(5735.0, 2.8, 8), (1.0e30, 2.8, 8), (float("nan"), 2.8, 1), (30.0, 0.0, 1)])
+def test_caller_scratch_sizing_rejects_bad_geometry(L, rcs, code):
+    lib = fm.lib()
+    sb = C.c_size_t(123)
+    fn = lib.fmd_verlet_scratch_bytes
+    fn.restype = C.c_int32
+    assert fn(C.c_int32(64), C.c_float(rcs), C.c_float(L), C.byref(sb)) == code
