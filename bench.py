@@ -182,45 +182,65 @@ def cpu_oracle_rate(desc, seconds=12.0, threads=None):
                                     f"{threads} OpenMP threads, {dt:.1f} s"
 
 
-def cpu_state_from_generator(seed):
-    import fastmd_b200 as fm
-    d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=seed)
-    return dict(xyz=d.xyz, L=d.box_L, type=d.type, bonds=d.bonds, angles=d.angles, mol=d.mol,
-                vel=np.zeros_like(d.xyz), image=d.image)
+def bench_replica_state():
+    """Replica 0 of the workload after its push-off, from the committed
+    fixture (tests/golden/make_bench_replica.py made it on a GPU), with the
+    implied topology: linear chains of CHAIN_LEN beads in atom order."""
+    p = os.path.join(ROOT, "tests", "golden", "kg30k_replica0.npz")
+    z = np.load(p)
+    n = len(z["xyz"])
+    nch, cl = int(z["nchains"][0]), int(z["chain_length"][0])
+    ids = np.arange(n, dtype=np.int32).reshape(nch, cl)
+    bonds = np.stack([ids[:, :-1].ravel(), ids[:, 1:].ravel()], axis=1).astype(np.int32)
+    angles = np.stack([ids[:, :-2].ravel(), ids[:, 1:-1].ravel(), ids[:, 2:].ravel()], axis=1).astype(np.int32)
+    mol = np.repeat(np.arange(1, nch + 1, dtype=np.int32), cl)
+    return dict(xyz=z["xyz"].astype(np.float64), L=float(z["box_L"][0]), type=np.zeros(n, np.int32), bonds=bonds,
+                angles=angles, mol=mol, vel=z["vel"].astype(np.float64), image=z["image"].astype(np.int32),
+                seed=int(z["seed"][0]))
+
+
+def headline_config(world, graph_steps, replicas):
+    return {"workload": "kg_melt_64x30k_langevin_batched", "replicas_per_gpu": replicas,
+            "beads_per_replica": NCHAINS * CHAIN_LEN, "chains": NCHAINS, "chain_length": CHAIN_LEN,
+            "density": DENSITY, "rc": 2.5, "skin": 0.3, "dt": 0.001, "ensemble": "nvt_langevin T=1 Tdamp=1",
+            "l2": "working set > L2 (no flush needed)", "parallelism": f"replicas x{world} (no collective)"}
 
 
 def run_reference(args, rank, world, local, dist):
-    """--impl reference: the FP64 CPU oracle port stepping the workload's
-    replica on the host cores (the reference has no CPU stepping path)."""
+    """--impl reference: the reference has no CPU stepping path, so its CPU
+    arm is the FP64 oracle port (OpenMP over the host cores) stepping replica
+    0 of the same workload (the pushed-off state from the committed fixture,
+    the same Langevin settings and seed, no force cap): one replica per step
+    is the bounded sample.  Loads no library of this repository."""
     if rank != 0:
         return
     from oracle import pyoracle as po
-    desc = cpu_state_from_generator(0)
+    desc = bench_replica_state()
     threads = os.cpu_count() or 1
     s = po.System(xyz=desc["xyz"], L=desc["L"], type=desc["type"], mass=np.ones(1), lj=np.ones((1, 1, 2)),
                   bonds=desc["bonds"], bond_type=np.zeros(len(desc["bonds"]), np.int32),
                   fene=np.array([[30.0, 1.5, 1.0, 1.0]]), angles=desc["angles"],
                   angle_type=np.zeros(len(desc["angles"]), np.int32), angle_p=np.array([[5.0, np.pi]]),
                   mol=desc["mol"], vel=desc["vel"], image=desc["image"])
-    sim = po.Sim(s, ensemble="langevin", T=(1.0, 1.0, 1.0), seed=1, nsteps=10**7, nthreads=threads,
-                 force_cap=50.0)
+    sim = po.Sim(s, ensemble="langevin", T=(1.0, 1.0, 1.0), seed=desc["seed"], nsteps=10**7, nthreads=threads)
     sim.step(args.warmup)
     t0 = time.perf_counter()
     sim.step(args.steps)
     dt = time.perf_counter() - t0
     n = len(desc["type"])
     v = n * args.steps / dt
+    sample = (f"replica 0 of the workload ({n} beads, pushed off), {args.steps} steps (+{args.warmup} warm-up), "
+              "FP64 oracle port (the reference has no CPU stepping path)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "atom-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random-walk melt)",
-        "config": {"workload": "kg_melt_30k_langevin (one replica of the 64x30K workload per step)",
-                   "beads_per_replica": n, "density": DENSITY, "rc": 2.5, "skin": 0.3, "dt": 0.001},
-        "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"one {n}-bead replica, {args.steps} steps (+{args.warmup} warm-up), "
-                                   "FP64 oracle port (the reference has no CPU stepping path)"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random-walk melt, "
+        "2,000-step capped push-off; replica 0 from tests/golden/kg30k_replica0.npz)",
+        "config": headline_config(world, None, args.replicas),
+        "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    assert "fastmd_b200" not in sys.modules, "the reference arm must not load this repository's library"
     print(json.dumps(line), flush=True)
 
 
@@ -614,6 +634,74 @@ def kernel_timeline(b, steps, path):
         f.write("\n".join(out) + "\n")
 
 
+def graph_steps_for(steps, requested):
+    """Steps per CUDA-graph launch: the largest divisor of the timed steps not
+    above the requested length, so every timed step is a graph replay
+    (requested < 0: direct launches, for kernel profilers)."""
+    if requested < 0:
+        return requested
+    cap = max(1, min(requested or 50, steps))
+    return max(d for d in range(1, cap + 1) if steps % d == 0)
+
+
+def _kg_oracle_system(po, x, L, natoms):
+    nch = natoms // CHAIN_LEN
+    ids = np.arange(natoms, dtype=np.int32).reshape(nch, CHAIN_LEN)
+    bonds = np.stack([ids[:, :-1].ravel(), ids[:, 1:].ravel()], axis=1).astype(np.int32)
+    angles = np.stack([ids[:, :-2].ravel(), ids[:, 1:-1].ravel(), ids[:, 2:].ravel()], axis=1).astype(np.int32)
+    return po.System(xyz=x, L=L, type=np.zeros(natoms, np.int32), mass=np.ones(1), lj=np.ones((1, 1, 2)),
+                     bonds=bonds, bond_type=np.zeros(len(bonds), np.int32), fene=np.array([[30.0, 1.5, 1.0, 1.0]]),
+                     angles=angles, angle_type=np.zeros(len(angles), np.int32), angle_p=np.array([[5.0, np.pi]]),
+                     mol=np.repeat(np.arange(1, nch + 1, dtype=np.int32), CHAIN_LEN))
+
+
+def force_rms_vs_oracle(fm, b, slots):
+    """Force RMS error relative to the FP64 oracle of the benchmarked
+    replicas at the end of the timed run (the forces the kernels produce
+    for the current positions, read in FP64)."""
+    from oracle import pyoracle as po
+    errs = []
+    for s in slots:
+        x, _, _ = b.state(s)
+        f, _, _ = b.forces(s)
+        fo, _, _ = po.forces(_kg_oracle_system(po, x, b.info(s).box_L, len(x)))
+        errs.append(float(np.sqrt(np.mean((f - fo) ** 2)) / np.sqrt(np.mean(fo ** 2))))
+    return {"max": max(errs), "per_replica": errs, "replicas": len(errs), "tolerance": 1e-5,
+            "how": "mixed-form forces of the timed replicas' final states vs the FP64 oracle on the same positions"}
+
+
+def nvt_drift(fm, b, slots, steps, device):
+    """Nose-Hoover NVT conserved-quantity drift (extended energy per atom,
+    thermostat terms included) of the benchmarked replicas' final states run
+    under nvt_nh T = 1, Tdamp = 0.5, chain 3 for `steps` steps: a line fitted
+    per replica, relative slope per 10^6 steps, mean and standard error over
+    the replicas."""
+    conf = ("ntypes 1\nrc 2.5\nskin 0.3\ndt 0.001\nnsteps 100000000\nnvt_nh 1.0 1.0 0.5 3\n"
+            "lj 0 0 1.0 1.0\nbond_type 0 30.0 1.5 1.0 1.0\nangle_type 0 5.0 180.0\n")
+    nb = fm.Batch(max_replicas=len(slots), max_atoms=len(slots) * 30080 + 4096, device=device)
+    ns = []
+    for s in slots:
+        x, v, img = b.state(s)
+        d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0)
+        d.xyz, d.vel, d.image = x, v, img
+        ns.append(nb.add(conf, desc=d))
+    nb.run(50)
+    samples = 50
+    chunk = max(50, steps // samples // 50 * 50)
+    e = np.zeros((samples, len(ns)))
+    for k in range(samples):
+        nb.run(chunk)
+        for j, s in enumerate(ns):
+            e[k, j] = nb.thermo(s).conserved
+    nb.close()
+    t = np.arange(1, samples + 1) * float(chunk)
+    rel = np.array([np.polyfit(t, e[:, j], 1)[0] * 1e6 / abs(e[0, j]) for j in range(len(ns))])
+    return {"relative_per_1e6_steps": float(rel.mean()),
+            "stderr": float(rel.std(ddof=1) / np.sqrt(len(rel))) if len(rel) > 1 else None,
+            "per_replica": rel.tolist(), "steps": int(t[-1]), "replicas": len(ns), "target": 1e-4,
+            "ensemble": "nvt_nh T=1 Tdamp=0.5 chain 3, from the timed replicas' final states"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -624,7 +712,10 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip e2e / plain / CPU / reference-GPU legs")
     ap.add_argument("--ref-gpu-steps", type=int, default=5000, help="steps of the reference GPU datapoint")
     ap.add_argument("--graph-steps", type=int, default=50,
-                    help="steps per CUDA graph launch; < 0 launches every step directly (for kernel profilers)")
+                    help="longest CUDA graph (steps per launch; the largest divisor of --steps not above it is "
+                         "used); < 0 launches every step directly (for kernel profilers)")
+    ap.add_argument("--drift-steps", type=int, default=100_000,
+                    help="NVT conserved-quantity drift leg: steps (0 skips it)")
     ap.add_argument("--workload", default="headline", choices=["headline"] + sorted(WORKLOADS),
                     help="headline = the 64 x 30K benchmark; c0..c4 = the reported cases (one GPU)")
     ap.add_argument("--timeline", default="", help="after the timed run, write a kernel timeline of "
@@ -650,7 +741,8 @@ def main():
     import fastmd_b200 as fm
 
     R = args.replicas
-    b = fm.Batch(max_replicas=R, max_atoms=R * 30080 + 4096, hbm_budget_gb=150.0, graph_steps=args.graph_steps,
+    gsteps = graph_steps_for(args.steps, args.graph_steps)
+    b = fm.Batch(max_replicas=R, max_atoms=R * 30080 + 4096, hbm_budget_gb=150.0, graph_steps=gsteps,
                  device=local)
     t_setup = time.perf_counter()
     slots = []
@@ -667,8 +759,9 @@ def main():
     variant, variant_ms = b.autotune(20)
     # The autotuner's choices invalidate the step graph: replay one graph's
     # worth of steps untimed so that its capture (host work while the device
-    # idles) is not inside the timed region.
-    b.run(max(3, args.graph_steps))
+    # idles) is not inside the timed region.  The graph length divides the
+    # timed steps, so every timed step is a graph replay.
+    b.run(max(3, gsteps))
     barrier(dist, local)
     counts0 = b.launch_counts()
     rebuilds0 = sum(b.info(s).rebuilds for s in slots)
@@ -697,11 +790,10 @@ def main():
         "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 forces / f64 reductions",
         "data": "synthetic (seeded random-walk melts, 2,000-step capped push-off)",
-        "config": {"workload": "kg_melt_64x30k_langevin_batched", "replicas_per_gpu": R,
-                   "beads_per_replica": NCHAINS * CHAIN_LEN, "chains": NCHAINS, "chain_length": CHAIN_LEN,
-                   "density": DENSITY, "rc": 2.5, "skin": 0.3, "dt": 0.001, "ensemble": "nvt_langevin T=1 Tdamp=1",
-                   "form": "mixed (FP32 cell-offset forces, FP64 reductions)", "graph_steps": args.graph_steps,
-                   "l2": "working set > L2 (no flush needed)", "parallelism": f"replicas x{world} (no collective)"},
+        "config": headline_config(world, gsteps, R),
+        "form": "mixed (FP32 cell-offset forces, FP64 reductions)",
+        "path": "graph" if gsteps > 0 else "direct launches",
+        "graph_steps": gsteps,
     }
 
     if rank == 0:
@@ -749,7 +841,7 @@ def main():
         if not args.no_extras:
             # ---- end to end through the public C API: run in thermo-sized
             # chunks (100 steps) and read every replica's thermo row.
-            chunk = 100
+            chunk = 100 if gsteps <= 0 or 100 % gsteps == 0 else gsteps * -(-100 // gsteps)
             nchunks = max(1, args.steps // chunk)
             # start on a thermo step, as a run printing every 100 steps does
             lead = (-b.info(slots[0]).step) % chunk
@@ -806,6 +898,17 @@ def main():
                                         "sample": sample}
             except Exception as e:
                 line["cpu_baseline"] = {"error": str(e)}
+            # ---- force RMS error of the timed state against the FP64 oracle
+            try:
+                line["force_rms_vs_oracle"] = force_rms_vs_oracle(fm, b, slots[:2])
+            except Exception as e:
+                line["force_rms_vs_oracle"] = {"error": str(e)}
+            # ---- Nose-Hoover conserved-quantity drift from the timed states
+            if args.drift_steps > 0:
+                try:
+                    line["nvt_drift"] = nvt_drift(fm, b, slots[:8], args.drift_steps, local)
+                except Exception as e:
+                    line["nvt_drift"] = {"error": str(e)}
         line["setup_s"] = t_setup
         print(json.dumps(line), flush=True)
     b.close()

@@ -472,6 +472,15 @@ class Batch:
         _call("fmd_batch_get_force_frame", self._h, C.c_int32(slot), _ptr(x), C.byref(L))
         return x, L.value
 
+    def pairs(self, slot):
+        """The replica's Verlet pair set (i < j, data-file indices)."""
+        n = C.c_int64()
+        _call("fmd_batch_pairs", self._h, C.c_int32(slot), None, None, C.c_int64(0), C.byref(n))
+        i = np.zeros(n.value, np.int32)
+        j = np.zeros(n.value, np.int32)
+        _call("fmd_batch_pairs", self._h, C.c_int32(slot), _ptr(i), _ptr(j), C.c_int64(n.value), C.byref(n))
+        return i[: n.value], j[: n.value]
+
     def totals(self):
         a = C.c_int32()
         n = C.c_int64()
@@ -522,6 +531,22 @@ class Batch:
         v = C.c_int32()
         _call("fmd_batch_autotune", self._h, C.c_int32(iters), C.byref(v), _ptr(ms), C.c_int32(len(ms)))
         return v.value, ms
+
+    def set_variants(self, force_variant=-1, nbr_variant=-1):
+        """Pin the force-kernel and neighbor-list variants (< 0 keeps one)."""
+        _call("fmd_batch_set_variants", self._h, C.c_int32(force_variant), C.c_int32(nbr_variant))
+
+    def variants(self):
+        """(force variant, neighbor variant, number of force variants, number of neighbor variants)."""
+        a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        _call("fmd_batch_get_variants", self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
+        return a.value, b.value, c.value, d.value
+
+    def last_forces(self, slot):
+        """Forces of the last evaluation as stored (FP32 values, id order), not re-evaluated."""
+        f = np.zeros((self._natoms[slot], 3))
+        _call("fmd_batch_last_forces", self._h, C.c_int32(slot), _ptr(f))
+        return f
 
     def launch_counts(self):
         """Kernel launches executed so far, per kernel (counted on the device)."""

@@ -946,6 +946,34 @@ int Batch::autotune(int iters, double* ms_out, int cap) {
   return best;
 }
 
+void Batch::set_variants(int fv, int nv) {
+  if (fv >= kForceVariants || nv >= kNbrVariants) throw Error(FMD_ERR_ARG, "no such kernel variant");
+  if (fv >= 0 && fv != force_variant_) {
+    force_variant_ = fv;
+    graph_dirty_ = true;
+  }
+  if (nv >= 0 && nv != nbr_variant_) {
+    nbr_variant_ = nv;
+    graph_dirty_ = true;
+  }
+}
+
+void Batch::last_forces(int r, double* f) {
+  const Rep& R = rep(r);
+  const int n = R.natoms;
+  std::vector<float4> hf(n);
+  std::vector<int4> hi(n);
+  FMD_CUDA(cudaMemcpyAsync(hf.data(), force_.p + R.slot_base, n * sizeof(float4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaMemcpyAsync(hi.data(), img_.p + R.slot_base, n * sizeof(int4), cudaMemcpyDeviceToHost, st_));
+  FMD_CUDA(cudaStreamSynchronize(st_));
+  for (int s = 0; s < n; ++s) {
+    const int id = hi[s].w;
+    f[3 * id] = hf[s].x;
+    f[3 * id + 1] = hf[s].y;
+    f[3 * id + 2] = hf[s].z;
+  }
+}
+
 void Batch::list_stats(int64_t* entries, int32_t* max_per_atom) {
   int64_t tot = 0;
   int32_t mx = 0;

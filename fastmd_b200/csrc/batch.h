@@ -118,6 +118,10 @@ class Batch {
   int nbr_variant() const { return nbr_variant_; }
   const double* nbr_variant_ms() const { return nbr_ms_; }
   int force_variant() const { return force_variant_; }
+  // Force / neighbor-list kernel variants for the following steps (< 0: keep).
+  void set_variants(int force_variant, int nbr_variant);
+  // Forces of the last evaluation as stored (no re-evaluation), id order.
+  void last_forces(int r, double* f);
   void list_stats(int64_t* entries, int32_t* max_per_atom);
 
  private:

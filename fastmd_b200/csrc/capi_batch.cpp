@@ -298,4 +298,28 @@ FMD_API fmd_status fmd_batch_set_rebuild_cadence(fmd_batch* b, int32_t slot, int
   });
 }
 
+FMD_API fmd_status fmd_batch_set_variants(fmd_batch* b, int32_t force_variant, int32_t nbr_variant) {
+  return guarded([&] { B(b).set_variants(force_variant, nbr_variant); });
+}
+
+FMD_API fmd_status fmd_batch_get_variants(fmd_batch* b, int32_t* force_variant, int32_t* nbr_variant,
+                                          int32_t* n_force, int32_t* n_nbr) {
+  return guarded([&] {
+    auto& bb = B(b);
+    if (force_variant) *force_variant = bb.force_variant();
+    if (nbr_variant) *nbr_variant = bb.nbr_variant();
+    if (n_force) *n_force = fmd::mixed::kForceVariants;
+    if (n_nbr) *n_nbr = fmd::mixed::kNbrVariants;
+  });
+}
+
+FMD_API fmd_status fmd_batch_last_forces(fmd_batch* b, int32_t slot, double* f) {
+  return guarded([&] {
+    auto& bb = B(b);
+    need_slot(bb, slot);
+    if (!f) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    bb.last_forces(slot, f);
+  });
+}
+
 }  // extern "C"

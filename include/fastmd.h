@@ -332,6 +332,20 @@ FMD_API fmd_status fmd_batch_autotune(fmd_batch* b, int32_t iters, int32_t* chos
  * selects). */
 FMD_API fmd_status fmd_batch_set_rebuild_cadence(fmd_batch* b, int32_t slot, int32_t max_steps);
 
+/* Kernel variants (the autotuner's choices), for tests and for pinning a
+ * choice: force_variant in [0, n_force), nbr_variant in [0, n_nbr); a value
+ * < 0 keeps the current one.  Variants round the force sums differently in
+ * the last bits (different batch and compensation groupings); each is
+ * bit-reproducible.  No counterpart in the reference (one kernel each). */
+FMD_API fmd_status fmd_batch_set_variants(fmd_batch* b, int32_t force_variant, int32_t nbr_variant);
+FMD_API fmd_status fmd_batch_get_variants(fmd_batch* b, int32_t* force_variant, int32_t* nbr_variant,
+                                          int32_t* n_force, int32_t* n_nbr);
+/* Forces of the replica's last force evaluation as stored on the device (FP32
+ * values, id order), without re-evaluating them: after a step these are the
+ * forces the kernel flavour of that step produced at the positions of
+ * fmd_batch_get_force_frame. */
+FMD_API fmd_status fmd_batch_last_forces(fmd_batch* b, int32_t slot, double* f);
+
 /* ------------------------------------------------------------- serving */
 /* A request loop on its own host thread: submitted requests are admitted as
  * slots and the device-memory budget allow, advanced together in the batch,
