@@ -1126,15 +1126,90 @@ void Batch::launch_counts(int64_t* counts, int n) {
 }
 
 void Batch::write_restart(int r, const std::string& path) {
-  const Rep& R = rep(r);
   Topology t = info_[r].topo;
-  const size_t n = (size_t)R.natoms;
+  StateFile st;
+  checkpoint(r, t, st);
+  write_lammps_data(path, t, rep(r).step);
+  write_state_file(state_path(path), st);
+}
+
+namespace {
+// Sidecar values of a replica's dynamic state (what a data file lacks).
+void put_nh(StateFile& s, const NHScalars& nh) {
+  s.put("nh_xi", std::vector<double>(nh.xi, nh.xi + 10));
+  s.put("nh_vxi", std::vector<double>(nh.vxi, nh.vxi + 10));
+  s.put("nh_scalars", {nh.eps, nh.veps, nh.carry, nh.scale, nh.L, nh.inv_L, nh.V, nh.bscale, nh.exp_vW, nh.vWdt,
+                       nh.fpos, nh.ke_raw, nh.vir_tr});
+}
+void get_nh(const StateFile& s, NHScalars& nh) {
+  const auto& xi = s.get("nh_xi");
+  const auto& vxi = s.get("nh_vxi");
+  const auto& c = s.get("nh_scalars");
+  if (xi.size() != 10 || vxi.size() != 10 || c.size() != 13) throw Error(FMD_ERR_IO, "bad chain state in sidecar");
+  for (int k = 0; k < 10; ++k) {
+    nh.xi[k] = xi[k];
+    nh.vxi[k] = vxi[k];
+  }
+  nh.eps = c[0];
+  nh.veps = c[1];
+  nh.carry = c[2];
+  nh.scale = c[3];
+  nh.L = c[4];
+  nh.inv_L = c[5];
+  nh.V = c[6];
+  nh.bscale = c[7];
+  nh.exp_vW = c[8];
+  nh.vWdt = c[9];
+  nh.fpos = c[10];
+  nh.ke_raw = c[11];
+  nh.vir_tr = c[12];
+}
+}  // namespace
+
+void Batch::checkpoint(int r, Topology& t, StateFile& s) {
+  rep(r);
+  const size_t n = (size_t)h_reps_[r].natoms;
   t.xyz.resize(3 * n);
   t.vel.resize(3 * n);
   t.image.resize(3 * n);
   get_state(r, t.xyz.data(), t.vel.data(), t.image.data());
-  t.box_L = rep(r).L;
-  write_lammps_data(path, t, rep(r).step);
+  download_reps();
+  const Rep& R = h_reps_[r];
+  t.box_L = R.L;
+  s.put("form", {1.0});
+  s.put("natoms", {(double)R.natoms});
+  s.put("ensemble", {(double)R.ensemble});
+  s.put("step", {(double)R.step});
+  s.put("box_L", {R.L});
+  s.put("V0", {R.V0});
+  s.put("rebuilds", {(double)R.rebuilds});
+  s.put("list_buffer", {R.skin});
+  s.put("rebuild_cadence", {(double)R.max_between});
+  s.put("prune_delta", {(double)R.prune_delta});
+  put_nh(s, R.nh);
+  // continue from exactly what a resumed run starts from
+  restore(r, t, s);
+}
+
+void Batch::restore(int r, const Topology& t, const StateFile& s) {
+  rep(r);
+  download_reps();
+  Rep& R = h_reps_[r];
+  if ((int)s.get1("natoms") != R.natoms) throw Error(FMD_ERR_IO, "restart state is for another atom count");
+  if ((int)s.get1("ensemble") != R.ensemble) throw Error(FMD_ERR_IO, "restart state is for another ensemble");
+  R.step = (int64_t)s.get1("step");
+  R.L = s.get1("box_L");
+  R.V0 = s.get1("V0");
+  if (s.has("rebuilds")) R.rebuilds = (int64_t)s.get1("rebuilds");
+  if (s.has("list_buffer")) R.skin = s.get1("list_buffer");
+  if (s.has("rebuild_cadence")) R.max_between = (int32_t)s.get1("rebuild_cadence");
+  if (s.has("prune_delta")) R.prune_delta = R.ensemble == FMD_NPT_NH ? 0.f : (float)s.get1("prune_delta");
+  get_nh(s, R.nh);
+  // the cell grid of the box, as a fresh replica derives it
+  int G = (int)std::floor(R.L / ((R.rc + R.skin) * 1.0001));
+  R.G = std::max(1, std::min(G, R.G_alloc));
+  upload_reps();
+  set_state(r, t.xyz.data(), t.vel.data(), t.image.data());
 }
 
 void Batch::set_state(int r, const double* xyz, const double* vel, const int32_t* image) {
@@ -1385,6 +1460,8 @@ class MixedEngine final : public SimEngine {
   void compute_forces(double* f, double* pe, double* vir) override { b_->forces(r_, f, pe, vir); }
   void get_state(double* x, double* v, int32_t* i) override { b_->get_state(r_, x, v, i); }
   void set_state(const double* x, const double* v, const int32_t* i) override { b_->set_state(r_, x, v, i); }
+  void checkpoint(Topology& t, StateFile& s) override { b_->checkpoint(r_, t, s); }
+  void restore(const Topology& t, const StateFile& s) override { b_->restore(r_, t, s); }
   void thermo(fmd_thermo_row* row) override { b_->thermo(r_, row); }
   double rg() override { return b_->rg(r_); }
   int64_t pairs(int32_t* pi, int32_t* pj, int64_t cap) override { return b_->pairs(r_, pi, pj, cap); }

@@ -69,6 +69,9 @@ class Batch {
   const RunConfig& cfg(int r) const { return info_[r].cfg; }
   void get_state(int r, double* xyz, double* vel, int32_t* image);
   void write_restart(int r, const std::string& path);
+  // Restart checkpoint / resume of replica r (see SimEngine::checkpoint).
+  void checkpoint(int r, Topology& t, StateFile& s);
+  void restore(int r, const Topology& t, const StateFile& s);
   // Server mode: push-offs advance inside run() beside the running replicas
   // instead of freezing them first.
   void set_concurrent_pushoff(bool on) { concurrent_pushoff_ = on; }

@@ -126,6 +126,46 @@ FMD_API fmd_status fmd_parse_run_conf(const char* text, int32_t* iout, double* f
   });
 }
 
+FMD_API fmd_status fmd_run_conf_outputs(const char* text, fmd_output_spec* out) {
+  return guarded([&] {
+    if (!text || !out) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    const fmd::RunConfig c = fmd::parse_run_conf(text);
+    fmd_output_spec o{};
+    o.nsteps = c.nsteps;
+    o.ensemble = c.ensemble;
+    o.thermo_on = c.thermo_on;
+    o.thermo_freq = c.thermo_freq;
+    o.rg_on = c.rg_on;
+    o.rg_freq = c.rg_freq;
+    o.stress_on = c.stress_on;
+    o.stress_freq = c.stress_freq;
+    o.dump_freq = c.dump_freq;
+    o.restart_freq = c.restart_freq;
+    auto put = [](char* dst, const std::string& v) {
+      std::snprintf(dst, 256, "%s", v.c_str());
+    };
+    put(o.thermo_file, c.thermo_file);
+    put(o.rg_file, c.rg_file);
+    put(o.stress_file, c.stress_file);
+    put(o.restart_file, c.restart_file);
+    put(o.data_file, c.data_file);
+    put(o.forces_dump_file, c.forces_dump_file);
+    *out = o;
+  });
+}
+
+FMD_API fmd_status fmd_restart_filename(const char* base, int64_t step, char* buf, size_t len) {
+  return guarded([&] {
+    if (!base || !buf || len == 0) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    const std::string b(base);
+    const std::string tag = step >= 0 ? "_" + std::to_string(step) : std::string("_final");
+    const size_t dot = b.rfind('.');
+    const std::string name = dot != std::string::npos ? b.substr(0, dot) + tag + b.substr(dot) : b + tag;
+    if (name.size() + 1 > len) throw fmd::Error(FMD_ERR_ARG, "buffer too small");
+    std::memcpy(buf, name.c_str(), name.size() + 1);
+  });
+}
+
 FMD_API fmd_status fmd_read_pair_table(const char* path, const char* keyword, float* grid, int32_t* npoints,
                                        float* data, int32_t cap) {
   return guarded([&] {
@@ -215,12 +255,19 @@ FMD_API fmd_status fmd_sim_create(const char* conf, const char* data_path, const
     s->topo.xyz.clear();
     s->topo.vel.clear();
     s->topo.image.clear();
+    // a data file written by fmd_write_restart carries a state sidecar: resume from it
+    const std::string data = data_path ? std::string(data_path) : (desc || gen ? std::string() : cfg.data_file);
+    fmd::StateFile st;
+    const bool resume = !data.empty() && fmd::read_state_file(fmd::state_path(data), st);
+    fmd::Topology saved;
+    if (resume) saved = t;
     if (form == FMD_FORM_PLAIN_FP64)
       s->eng = fmd::make_plain_engine(cfg, std::move(t), gen);
     else if (form == FMD_FORM_MIXED)
       s->eng = fmd::make_mixed_engine(cfg, std::move(t), gen);
     else
       throw fmd::Error(FMD_ERR_ARG, "unknown form");
+    if (resume) s->eng->restore(saved, st);
     *out = s.release();
   });
 }
@@ -330,13 +377,10 @@ FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path) {
     SIM_CHECK();
     if (!path) throw fmd::Error(FMD_ERR_ARG, "null path");
     fmd::Topology t = sim->topo;
-    const int n = sim->eng->natoms();
-    t.xyz.resize(3 * (size_t)n);
-    t.vel.resize(3 * (size_t)n);
-    t.image.resize(3 * (size_t)n);
-    sim->eng->get_state(t.xyz.data(), t.vel.data(), t.image.data());
-    t.box_L = sim->eng->box_L();
+    fmd::StateFile st;
+    sim->eng->checkpoint(t, st);
     fmd::write_lammps_data(path, t, sim->eng->step_count());
+    fmd::write_state_file(fmd::state_path(path), st);
   });
 }
 

@@ -1,6 +1,7 @@
 // extern "C" entry points for batches of replicas (include/fastmd.h).
 #include <cstring>
 #include <memory>
+#include <string>
 
 #include "batch.h"
 #include "host.h"
@@ -68,7 +69,14 @@ FMD_API fmd_status fmd_batch_add_replica(fmd_batch* b, const char* conf, const c
     if (!conf || !slot) throw fmd::Error(FMD_ERR_ARG, "null argument");
     fmd::RunConfig cfg = fmd::parse_run_conf(conf);
     fmd::Topology t = fmd::load_atoms(cfg, data_path, desc, gen);
+    // a data file written by fmd_batch_write_restart carries a state sidecar: resume from it
+    const std::string data = data_path ? std::string(data_path) : (desc || gen ? std::string() : cfg.data_file);
+    fmd::StateFile st;
+    const bool resume = !data.empty() && fmd::read_state_file(fmd::state_path(data), st);
+    fmd::Topology saved;
+    if (resume) saved = t;
     *slot = B(b).add(cfg, std::move(t), gen);
+    if (resume) B(b).restore(*slot, saved, st);
   });
 }
 

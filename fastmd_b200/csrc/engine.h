@@ -42,6 +42,14 @@ class SimEngine {
     get_state(x.data(), nullptr, nullptr);
     w.write_host(step_count(), box_L(), x.data());
   }
+  // Restart checkpoint: fills t's positions, velocities, image flags and box
+  // (data-file order) and the sidecar values; the engine then continues from
+  // exactly the state restore() gives a resumed run (positions re-loaded from
+  // those FP64 values, list rebuilt, forces re-evaluated), so the run after a
+  // checkpoint is the same whether the process continues or resumes.
+  virtual void checkpoint(Topology& t, StateFile& s) = 0;
+  // Resume: the state of a data file (t) and its sidecar.
+  virtual void restore(const Topology& t, const StateFile& s) = 0;
   virtual void write_stress_acf(const std::string& path) {
     (void)path;
     throw Error(FMD_ERR_ARG, "the stress autocorrelation is computed by the mixed form");

@@ -92,6 +92,21 @@ Topology generate_melt(const fmd_melt_spec& spec);
 // defaults for masses.  Throws Error(FMD_ERR_CONFIG) on mismatch.
 void validate(const RunConfig& cfg, Topology& topo);
 
+// Restart state sidecar ("<data file>.state"): the run state a LAMMPS data
+// file does not carry (step counter, thermostat / barostat chain, box and
+// reference volume, list settings), as "key v1 v2 ..." text lines with
+// doubles written to 17 significant digits (exact round trip).
+struct StateFile {
+  std::vector<std::pair<std::string, std::vector<double>>> entries;
+  void put(const std::string& key, std::vector<double> v) { entries.emplace_back(key, std::move(v)); }
+  bool has(const std::string& key) const;
+  const std::vector<double>& get(const std::string& key) const;  // throws Error(FMD_ERR_IO) when missing
+  double get1(const std::string& key) const { return get(key).at(0); }
+};
+std::string state_path(const std::string& data_path);
+void write_state_file(const std::string& path, const StateFile& s);
+bool read_state_file(const std::string& path, StateFile& s);  // false when the file does not exist
+
 // Load the atoms for a simulation from one of the sources.
 Topology load_atoms(const RunConfig& cfg, const char* data_path, const fmd_system_desc* desc,
                     const fmd_melt_spec* gen);

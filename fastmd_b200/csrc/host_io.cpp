@@ -668,4 +668,58 @@ int32_t reference_max_neighbors(int32_t natoms, double box_L, double rcs) {
   return std::max(256, est);
 }
 
+// ---------------------------------------------------------------------------
+// Restart state sidecar.
+// ---------------------------------------------------------------------------
+bool StateFile::has(const std::string& key) const {
+  for (const auto& e : entries)
+    if (e.first == key) return true;
+  return false;
+}
+
+const std::vector<double>& StateFile::get(const std::string& key) const {
+  for (const auto& e : entries)
+    if (e.first == key) return e.second;
+  throw Error(FMD_ERR_IO, "restart state file lacks '" + key + "'");
+}
+
+std::string state_path(const std::string& data_path) { return data_path + ".state"; }
+
+void write_state_file(const std::string& path, const StateFile& s) {
+  FILE* fp = std::fopen(path.c_str(), "w");
+  if (!fp) throw Error(FMD_ERR_IO, "cannot write " + path);
+  std::fprintf(fp, "# fastmd_b200 restart state v1\n");
+  for (const auto& e : s.entries) {
+    std::fprintf(fp, "%s", e.first.c_str());
+    for (double v : e.second) std::fprintf(fp, " %.17g", v);
+    std::fprintf(fp, "\n");
+  }
+  const bool ok = std::fflush(fp) == 0;
+  std::fclose(fp);
+  if (!ok) throw Error(FMD_ERR_IO, "cannot write " + path);
+}
+
+bool read_state_file(const std::string& path, StateFile& s) {
+  std::ifstream in(path);
+  if (!in) return false;
+  std::string line;
+  s.entries.clear();
+  while (std::getline(in, line)) {
+    if (line.empty() || line[0] == '#') continue;
+    std::istringstream iss(line);
+    std::string key;
+    iss >> key;
+    std::vector<double> v;
+    std::string tok;
+    while (iss >> tok) {
+      char* end = nullptr;
+      const double x = std::strtod(tok.c_str(), &end);
+      if (!end || *end) throw Error(FMD_ERR_IO, "bad value in " + path + ": " + tok);
+      v.push_back(x);
+    }
+    s.put(key, std::move(v));
+  }
+  return true;
+}
+
 }  // namespace fmd

@@ -784,6 +784,62 @@ class PlainEngine final : public SimEngine {
     init_carry();
   }
 
+  void checkpoint(Topology& t, StateFile& s) override {
+    t.xyz.resize(3 * (size_t)n_);
+    t.vel.resize(3 * (size_t)n_);
+    t.image.resize(3 * (size_t)n_);
+    get_state(t.xyz.data(), t.vel.data(), t.image.data());
+    t.box_L = L_;
+    NHScalars nh;
+    FMD_CUDA(cudaMemcpy(&nh, nh_, sizeof(nh), cudaMemcpyDeviceToHost));
+    s.put("form", {0.0});
+    s.put("natoms", {(double)n_});
+    s.put("ensemble", {(double)cfg_.ensemble});
+    s.put("step", {(double)step_});
+    s.put("box_L", {L_});
+    s.put("V0", {V0_});
+    s.put("rebuilds", {(double)rebuilds_});
+    s.put("nh_xi", std::vector<double>(nh.xi, nh.xi + 10));
+    s.put("nh_vxi", std::vector<double>(nh.vxi, nh.vxi + 10));
+    s.put("nh_scalars", {nh.eps, nh.veps, nh.carry, nh.scale, nh.L, nh.inv_L, nh.V, nh.bscale, nh.exp_vW, nh.vWdt,
+                         nh.fpos, nh.ke_raw, nh.vir_tr});
+    restore(t, s);
+  }
+
+  void restore(const Topology& t, const StateFile& s) override {
+    if ((int)s.get1("natoms") != n_) throw Error(FMD_ERR_IO, "restart state is for another atom count");
+    if ((int)s.get1("ensemble") != cfg_.ensemble) throw Error(FMD_ERR_IO, "restart state is for another ensemble");
+    step_ = (int64_t)s.get1("step");
+    L_ = s.get1("box_L");
+    V0_ = s.get1("V0");
+    set_state(t.xyz.data(), t.vel.data(), t.image.data());
+    if (s.has("rebuilds")) rebuilds_ = (int64_t)s.get1("rebuilds");
+    NHScalars nh;
+    FMD_CUDA(cudaMemcpy(&nh, nh_, sizeof(nh), cudaMemcpyDeviceToHost));
+    const auto& xi = s.get("nh_xi");
+    const auto& vxi = s.get("nh_vxi");
+    const auto& c = s.get("nh_scalars");
+    if (xi.size() != 10 || vxi.size() != 10 || c.size() != 13) throw Error(FMD_ERR_IO, "bad chain state in sidecar");
+    for (int k = 0; k < 10; ++k) {
+      nh.xi[k] = xi[k];
+      nh.vxi[k] = vxi[k];
+    }
+    nh.eps = c[0];
+    nh.veps = c[1];
+    nh.carry = c[2];
+    nh.scale = c[3];
+    nh.L = c[4];
+    nh.inv_L = c[5];
+    nh.V = c[6];
+    nh.bscale = c[7];
+    nh.exp_vW = c[8];
+    nh.vWdt = c[9];
+    nh.fpos = c[10];
+    nh.ke_raw = c[11];
+    nh.vir_tr = c[12];
+    FMD_CUDA(cudaMemcpy(nh_, &nh, sizeof(nh), cudaMemcpyHostToDevice));
+  }
+
   void thermo(fmd_thermo_row* row) override {
     FMD_CUDA(cudaMemsetAsync(red_, 0, 8 * sizeof(double), st_));
     k_thermo<<<div_up(n_, kBlock), kBlock, 0, st_>>>(vel_, pos_, force_, params(), red_, status_);

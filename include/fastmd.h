@@ -140,6 +140,31 @@ FMD_API fmd_status fmd_generate_melt(const fmd_melt_spec* spec, int32_t* counts,
 FMD_API fmd_status fmd_parse_run_conf(const char* text, int32_t* iout, double* fout, double* lj,
                                       int32_t lj_cap, double* bond, int32_t bond_cap, double* angle,
                                       int32_t angle_cap, uint64_t* seed);
+/* Output and run-control keys of a run.conf (src/io/config.cpp:32-127; acted
+ * on by src/main.cu:632-691, 738-783): what the `fastmd <run.conf>` program
+ * writes and when.  restart_freq: -1 no restart files (the key absent), 0 the
+ * final file only, > 0 also every restart_freq steps.  Strings are
+ * NUL-terminated and truncated to their buffers. */
+typedef struct fmd_output_spec {
+  int64_t nsteps;
+  int32_t ensemble;
+  int32_t thermo_on, thermo_freq;
+  int32_t rg_on, rg_freq;
+  int32_t stress_on, stress_freq;
+  int32_t dump_freq;
+  int32_t restart_freq;
+  char thermo_file[256];
+  char rg_file[256];
+  char stress_file[256];
+  char restart_file[256];
+  char data_file[256];
+  char forces_dump_file[256];
+} fmd_output_spec;
+FMD_API fmd_status fmd_run_conf_outputs(const char* text, fmd_output_spec* out);
+/* Restart file names of the reference (io/lammps_data.cpp:255-267): base
+ * "restart.data" -> "restart_<step>.data" (step >= 0) or "restart_final.data"
+ * (step < 0); without an extension the suffix is appended. */
+FMD_API fmd_status fmd_restart_filename(const char* base, int64_t step, char* buf, size_t len);
 /* Read one keyword section of a LAMMPS pair_style table file, as the
  * run.conf key 'table ti tj file keyword' does (io/table_parser.cpp:7-87):
  * grid = rmin, rmax, dr, inv_dr (single precision, as the reference derives
@@ -185,7 +210,17 @@ FMD_API fmd_status fmd_get_state(fmd_sim* sim, double* xyz, double* vel, int32_t
 FMD_API fmd_status fmd_set_state(fmd_sim* sim, const double* xyz, const double* vel, const int32_t* image);
 FMD_API fmd_status fmd_thermo(fmd_sim* sim, fmd_thermo_row* row);
 /* Restart file of the current state (write_lammps_data, io/lammps_data.cpp:269;
- * main.cu:681-691, 738-745 call it every restart_freq steps and at the end). */
+ * main.cu:681-691, 738-745 call it every restart_freq steps and at the end),
+ * plus a sidecar "<path>.state" with what the data file lacks: the step
+ * counter (the Langevin noise is keyed on it), the Nose-Hoover chain and
+ * barostat state, box edge and reference volume, and the list settings
+ * (text, 17 significant digits).  Creating a simulation or a batch replica
+ * from a data file that has a sidecar resumes from it.  A restart is a
+ * checkpoint: the simulation continues from the state as written and
+ * re-loaded (list rebuilt, forces re-evaluated), which is exactly what a
+ * resumed run starts from, so run N + M equals run N, restart, run M bit
+ * for bit in either form and every ensemble (the stress autocorrelator is not
+ * carried over).  The reference writes only the data file. */
 FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path);
 /* Binary trajectory (the reference's dump format, io/dump.cu:12-56, file
  * "traj.bin" of run.conf dump_freq): header {int32 0x4D444247, int32 natoms,
@@ -249,6 +284,9 @@ FMD_API fmd_status fmd_batch_retire(fmd_batch* b, int32_t slot);
 FMD_API fmd_status fmd_batch_replica_info(fmd_batch* b, int32_t slot, fmd_replica_info* info);
 FMD_API fmd_status fmd_batch_get_state(fmd_batch* b, int32_t slot, double* xyz, double* vel, int32_t* image);
 FMD_API fmd_status fmd_batch_thermo(fmd_batch* b, int32_t slot, fmd_thermo_row* row);
+/* Restart data file and state sidecar of a replica (see fmd_write_restart);
+ * fmd_batch_add_replica with that data file resumes from it.  Exact resume
+ * also needs the same kernel variants (fmd_batch_set_variants). */
 FMD_API fmd_status fmd_batch_write_restart(fmd_batch* b, int32_t slot, const char* path);
 FMD_API fmd_status fmd_batch_rg(fmd_batch* b, int32_t slot, double* rg);
 FMD_API fmd_status fmd_batch_compute_forces(fmd_batch* b, int32_t slot, double* f, double* pe, double* virial);
