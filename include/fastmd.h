@@ -218,9 +218,11 @@ FMD_API fmd_status fmd_thermo(fmd_sim* sim, fmd_thermo_row* row);
  * from a data file that has a sidecar resumes from it.  A restart is a
  * checkpoint: the simulation continues from the state as written and
  * re-loaded (list rebuilt, forces re-evaluated), which is exactly what a
- * resumed run starts from, so run N + M equals run N, restart, run M bit
- * for bit in either form and every ensemble (the stress autocorrelator is not
- * carried over).  The reference writes only the data file. */
+ * resumed run starts from, so run N + M equals run N, restart, run M: bit
+ * for bit in the mixed form, to FP64 round-off in the plain form (whose
+ * bonded forces are scattered with atomics, as the reference's are), in
+ * every ensemble (the stress autocorrelator is not carried over).  The
+ * reference writes only the data file. */
 FMD_API fmd_status fmd_write_restart(fmd_sim* sim, const char* path);
 /* Binary trajectory (the reference's dump format, io/dump.cu:12-56, file
  * "traj.bin" of run.conf dump_freq): header {int32 0x4D444247, int32 natoms,
