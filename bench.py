@@ -304,6 +304,9 @@ def _conf(ens, nsteps, ntypes=1, lj=((0, 0, 1.0, 1.0),), thermo=0):
 
 
 GRAPH_CAPTURE_STEPS = 50  # one replay of a batch's default step graph
+# force-kernel variants, in the library's order (fastmd_b200/csrc/mixed_kernels.cu, force_kernels)
+FORCE_VARIANTS = ["m8 k1 t3", "m8 k2 t3", "m8 k1 a5", "m8 k2 a5", "m8 k1 a5 x2", "m8 k2 a5 x2", "m7 k1 a5 x2",
+                  "m9 k1 a5 x2", "m6 k1 a5"]
 
 
 def _dev_run(fm, b, nsteps):
@@ -800,17 +803,17 @@ def main():
         line["clocks"] = clk.summary()
         launched = {k: counts1[k] - counts0[k] for k in counts0}
         line["gpu_launches"] = int(sum(launched.values()))
-        nf = 7
+        nf = b.variants()[2]
         line["autotune"] = {"force_variant": variant, "neighbor_variant": int(variant_ms[nf + 3]),
                             "ms_per_full_rebuild": {"ballot m8": round(float(variant_ms[nf]), 4),
                                                     "rows m6": round(float(variant_ms[nf + 1]), 4),
                                                     "ballot m6": round(float(variant_ms[nf + 2]), 4)},
                             "ms_per_variant": [round(float(x), 4) for x in variant_ms[:nf]],
-                            "variants": ["b4 m6 pipelined k1", "b4 m8 pipelined k1", "b4 m6 pipelined k2",
-                                         "b4 m8 pipelined k2", "b4 m9 pipelined k1", "b4 m7 pipelined k2",
-                                         "b4 m10 pipelined k1"],
-                            "legend": "b = list entries per batch, m = min blocks per SM, pipelined = next batch's "
-                                      "list words loaded ahead, k = batches per compensated add"}
+                            "variants": FORCE_VARIANTS[:nf],
+                            "legend": "m = min blocks per SM, k = batches of 4 list entries per compensated add, "
+                                      "t3 = shift from the 125-entry 3D table, a5 = per-axis 5-value table, "
+                                      "x2 = pairs two at a time in packed FP32x2 arithmetic (all: next batch's "
+                                      "list words loaded ahead)"}
         line["launches_by_kernel"] = launched
         line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
                                     "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0),

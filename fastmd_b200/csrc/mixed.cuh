@@ -13,9 +13,9 @@
 //   force[s] float4 {fx, fy, fz, pe_i}
 //   ref[s]   float4 offsets at the last rebuild (displacement test); .w = atom id
 //   img[s]   int4   {ix, iy, iz, atom id}  image flags + replica-local atom id
-//   nbr      uint32 per (tile, k, lane): replica-local slot of j (27 bits) and
-//            the cell shift of j relative to i as one code
-//            (ex + 1) * 9 + (ey + 1) * 3 + (ez + 1) in the top 5 bits
+//   nbr      uint32 per (tile, k, lane): replica-local slot of j (25 bits) and
+//            the periodic shift of j relative to i as one of 125 codes in the
+//            top 7 bits (see kCodeShift below)
 //
 // A position is r = (c + 0) * h + o with h = L / G the cell edge; pair
 // displacements are formed as (o_i - o_j) - e * h, so their precision is set by
@@ -308,7 +308,7 @@ struct StepShape {
   int has_table;        // some replica has tabulated pairs: the table pass follows the forces
 };
 using RebuildShape = StepShape;
-constexpr int kForceVariants = 7;
+constexpr int kForceVariants = 9;
 constexpr int kNbrVariants = 3;
 // One step with direct launches.  The rebuild form is read back from the
 // device after the per-replica commits (one small host read per step).

@@ -1231,31 +1231,43 @@ struct PairAcc {
   float fx, fy, fz, pe, v0, v1, v2, v3, v4, v5;
 };
 
+// Every force path evaluates a pair with the same sequence of correctly
+// rounded operations (explicit intrinsics, no contraction left to the
+// compiler), so the packed two-pair form below, the scalar form, the energy
+// flavour and the list filter give bit-identical forces for one variant.
+__device__ __forceinline__ float pair_r2(float4 pi, float3 sh, float4 pj, float& dx, float& dy, float& dz) {
+  dx = __fsub_rn(__fsub_rn(pi.x, pj.x), sh.x);
+  dy = __fsub_rn(__fsub_rn(pi.y, pj.y), sh.y);
+  dz = __fsub_rn(__fsub_rn(pi.z, pj.z), sh.z);
+  return __fmaf_rn(dz, dz, __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+}
+
+// F/r of a pair at r2 (lj.cu:32-61: 24 eps r^-2 (2 (s/r)^12 - (s/r)^6), clamped
+// to +-1000 as lj.cu:48 does); pairs at or beyond the cutoff (padding entries
+// included) give an exact zero.  The reference also skips r^2 <= 1e-10
+// (coincident atoms); here such a pair's F/r clamps to +-1000 times a
+// separation below 1e-5, and only its energy is left out.
+__device__ __forceinline__ float lj_fr(float r2, float rc2, float e24, float sig2, float& inv, float& sr6) {
+  inv = __fdividef(1.0f, r2);
+  const float sr2 = __fmul_rn(sig2, inv);
+  sr6 = __fmul_rn(__fmul_rn(sr2, sr2), sr2);
+  const float t = __fmaf_rn(sr6, 2.0f, -1.0f);
+  const float fr = __fmul_rn(__fmul_rn(__fmul_rn(e24, inv), sr6), t);
+  return r2 < rc2 ? fminf(fmaxf(fr, -1000.0f), 1000.0f) : 0.0f;
+}
+
 template <bool EV>
-__device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4 pj, float rc2, float e24,
+__device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float3 sh, float4 pj, float rc2, float e24,
                                         float sig2) {
-  const float dx = (pi.x - pj.x) - sh.x;
-  const float dy = (pi.y - pj.y) - sh.y;
-  const float dz = (pi.z - pj.z) - sh.z;
-  const float r2 = dx * dx + dy * dy + dz * dz;
-  // Branch-free: every listed pair is evaluated and pairs outside the cutoff
-  // (padding entries included) contribute an exact zero through selects.
-  // The reference also skips r^2 <= 1e-10 (coincident atoms); here such a
-  // pair's F/r clamps to +-1000 times a separation below 1e-5, and only its
-  // energy is left out.
-  const bool in = r2 < rc2;
-  const float r2inv = __fdividef(1.0f, r2);
-  const float sr2 = sig2 * r2inv;
-  const float sr6 = sr2 * sr2 * sr2;
-  float fr = e24 * r2inv * sr6 * (2.0f * sr6 - 1.0f);
-  fr = in ? fminf(fmaxf(fr, -1000.0f), 1000.0f) : 0.0f;  // lj.cu:48
-  // The force sums are written as explicit FMAs, so both flavours (with and
-  // without energies) round them identically.
-  a.fx = fmaf(fr, dx, a.fx);
-  a.fy = fmaf(fr, dy, a.fy);
-  a.fz = fmaf(fr, dz, a.fz);
+  float dx, dy, dz, inv, sr6;
+  const float r2 = pair_r2(pi, sh, pj, dx, dy, dz);
+  const float fr = lj_fr(r2, rc2, e24, sig2, inv, sr6);
+  a.fx = __fmaf_rn(fr, dx, a.fx);
+  a.fy = __fmaf_rn(fr, dy, a.fy);
+  a.fz = __fmaf_rn(fr, dz, a.fz);
   if (EV) {
     const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
+    const bool in = r2 < rc2;
     const float e = in && r2 > 1e-10f ? e24 * (1.0f / 12.0f) * (sr6 * (sr6 - 1.0f)) : 0.0f;  // 1/2 * 4 eps (sr12 - sr6)
     a.pe += e;
     a.v0 = fmaf(fxij, dx, a.v0);
@@ -1267,15 +1279,73 @@ __device__ __forceinline__ void lj_pair(PairAcc& a, float4 pi, float4 sh, float4
   }
 }
 
+// Packed FP32x2 arithmetic (sm_100): two independent IEEE operations per
+// instruction, each lane rounded exactly as the scalar operation.
+__device__ __forceinline__ float2 sub_f32x2(float2 a, float2 b) {
+  float2 r;
+  asm("{.reg .b64 ra, rb, rr;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "sub.rn.f32x2 rr, ra, rb;\n\tmov.b64 {%0, %1}, rr;}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
+// Forces of two list entries in packed FP32x2 form: the (x, y) components of
+// a pair together, then the two pairs' scalar factors together.  Bitwise the
+// same as two lj_pair<false> calls in entry order.
+__device__ __forceinline__ void lj_pair2(PairAcc& a, float4 pi, float3 sha, float4 pja, float3 shb, float4 pjb,
+                                         float rc2, float e24, float sig2) {
+  const float2 pxy = make_float2(pi.x, pi.y);
+  const float2 dxya = sub_f32x2(sub_f32x2(pxy, make_float2(pja.x, pja.y)), make_float2(sha.x, sha.y));
+  const float2 dxyb = sub_f32x2(sub_f32x2(pxy, make_float2(pjb.x, pjb.y)), make_float2(shb.x, shb.y));
+  const float dza = __fsub_rn(__fsub_rn(pi.z, pja.z), sha.z);
+  const float dzb = __fsub_rn(__fsub_rn(pi.z, pjb.z), shb.z);
+  const float2 ma = __fmul2_rn(dxya, dxya), mb = __fmul2_rn(dxyb, dxyb);
+  const float2 r2 = make_float2(__fmaf_rn(dza, dza, __fadd_rn(ma.x, ma.y)), __fmaf_rn(dzb, dzb, __fadd_rn(mb.x, mb.y)));
+  const float2 inv = make_float2(__fdividef(1.0f, r2.x), __fdividef(1.0f, r2.y));
+  const float2 sr2 = __fmul2_rn(make_float2(sig2, sig2), inv);
+  const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
+  const float2 t = __ffma2_rn(sr6, make_float2(2.0f, 2.0f), make_float2(-1.0f, -1.0f));
+  const float2 fr2 = __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(e24, e24), inv), sr6), t);
+  const float fa = r2.x < rc2 ? fminf(fmaxf(fr2.x, -1000.0f), 1000.0f) : 0.0f;
+  const float fb = r2.y < rc2 ? fminf(fmaxf(fr2.y, -1000.0f), 1000.0f) : 0.0f;
+  float2 g = __ffma2_rn(make_float2(fa, fa), dxya, make_float2(a.fx, a.fy));
+  a.fz = __fmaf_rn(fa, dza, a.fz);
+  g = __ffma2_rn(make_float2(fb, fb), dxyb, g);
+  a.fz = __fmaf_rn(fb, dzb, a.fz);
+  a.fx = g.x;
+  a.fy = g.y;
+}
+
+// Periodic shift vector of a list entry.  SH = 0: the entry's 3D vector from
+// the 125-entry table (one 16-byte shared load, whose lanes conflict across
+// banks).  SH = 1: the code's three axis codes (code = 25 ax + 5 ay + az)
+// and each axis value from the 5-value table (three 4-byte shared loads that
+// never conflict: the table spans 5 banks).  The same values either way.
+template <int SH>
+__device__ __forceinline__ float3 entry_shift(uint32_t w, const float4* s_shift, const float* s_axis) {
+  const uint32_t c = w >> kCodeShift;
+  if (SH == 0) {
+    const float4 v = s_shift[c];
+    return make_float3(v.x, v.y, v.z);
+  }
+  const uint32_t ax = (c * 41u) >> 10;  // c / 25 for c < 125
+  const uint32_t rem = c - 25u * ax;
+  const uint32_t ay = (rem * 13u) >> 6;  // rem / 5 for rem < 25
+  const uint32_t az = rem - 5u * ay;
+  return make_float3(s_axis[ax], s_axis[ay], s_axis[az]);
+}
+
 // The LJ loop over one atom's list in batches of B entries: all list loads,
 // then all position gathers, then the arithmetic.  PF: the next batch's list
 // words are loaded before this batch's gathers (software pipelining, B more
 // registers).  nn is the padded length (a multiple of B).
-template <bool EV, int B, bool PF, int KB, bool ONE>
+template <bool EV, int B, bool PF, int KB, bool ONE, int SH, bool P2>
 __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
-                                        const float4* s_shift, int ti, int nt, const float* s_eps24,
-                                        const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
-                                        PairAcc& acc) {
+                                        const float4* s_shift, const float* s_axis, int ti, int nt,
+                                        const float* s_eps24, const float* s_sig2, float rc2, KahanF& fx, KahanF& fy,
+                                        KahanF& fz, PairAcc& acc) {
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
   uint32_t wn[B];
   if (PF) {
@@ -1301,15 +1371,22 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
     float4 pj[B];
 #pragma unroll
     for (int q = 0; q < B; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+    if (P2 && ONE && !EV) {
 #pragma unroll
-    for (int q = 0; q < B; ++q) {
-      float e24 = e24_0, sig2 = sig2_0;
-      if (!ONE) {
-        const int pidx = ti * nt + w_type(w_bits(pj[q].w));
-        e24 = s_eps24[pidx];
-        sig2 = s_sig2[pidx];
+      for (int q = 0; q < B; q += 2)
+        lj_pair2(g, pi, entry_shift<SH>(w[q], s_shift, s_axis), pj[q], entry_shift<SH>(w[q + 1], s_shift, s_axis),
+                 pj[q + 1], rc2, e24_0, sig2_0);
+    } else {
+#pragma unroll
+      for (int q = 0; q < B; ++q) {
+        float e24 = e24_0, sig2 = sig2_0;
+        if (!ONE) {
+          const int pidx = ti * nt + w_type(w_bits(pj[q].w));
+          e24 = s_eps24[pidx];
+          sig2 = s_sig2[pidx];
+        }
+        lj_pair<EV>(g, pi, entry_shift<SH>(w[q], s_shift, s_axis), pj[q], rc2, e24, sig2);
       }
-      lj_pair<EV>(g, pi, s_shift[w[q] >> kCodeShift], pj[q], rc2, e24, sig2);
     }
     if (++kb == KB || k + B >= nn) {
       fx.add(g.fx);
@@ -1336,11 +1413,12 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
 // entries, then those of its padding), so the forces are bit-identical to a
 // walk of the list it writes: a later re-evaluation at these positions (an
 // energy request) reproduces them.
-template <bool EV, int B, bool PF, int KB, bool ONE>
+template <bool EV, int B, bool PF, int KB, bool ONE, int SH>
 __device__ __forceinline__ int lj_loop_filter(const uint32_t* lst, int nn, uint32_t* pout, float rcd2,
-                                              const float4* pbase, float4 pi, const float4* s_shift, int ti, int nt,
-                                              const float* s_eps24, const float* s_sig2, float rc2, KahanF& fx,
-                                              KahanF& fy, KahanF& fz, PairAcc& acc, uint32_t pad) {
+                                              const float4* pbase, float4 pi, const float4* s_shift,
+                                              const float* s_axis, int ti, int nt, const float* s_eps24,
+                                              const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
+                                              PairAcc& acc, uint32_t pad) {
   constexpr int P = B * KB;  // kept entries per compensated add
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
   uint32_t wn[B];
@@ -1368,9 +1446,9 @@ __device__ __forceinline__ int lj_loop_filter(const uint32_t* lst, int nn, uint3
     for (int q = 0; q < B; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
 #pragma unroll
     for (int q = 0; q < B; ++q) {
-      const float4 sh = s_shift[w[q] >> kCodeShift];
-      const float dx = (pi.x - pj[q].x) - sh.x, dy = (pi.y - pj[q].y) - sh.y, dz = (pi.z - pj[q].z) - sh.z;
-      if (dx * dx + dy * dy + dz * dz < rcd2) {
+      const float3 sh = entry_shift<SH>(w[q], s_shift, s_axis);
+      float dx, dy, dz;
+      if (pair_r2(pi, sh, pj[q], dx, dy, dz) < rcd2) {
         float e24 = e24_0, sig2 = sig2_0;
         if (!ONE) {
           const int pidx = ti * nt + w_type(w_bits(pj[q].w));
@@ -1460,7 +1538,7 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
 // LISTED: the work-list launch itself (replicas rebuilt or re-filtered this
 // step), which walks the rc + skin list and, where the replica keeps a
 // pruned list, writes it (the filter) and its displacement reference.
-template <bool EV, int B, bool PF, int KB, bool LISTED>
+template <bool EV, int B, bool PF, int KB, bool LISTED, int SH, bool P2>
 __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_rebuilt) {
   const int4 ci = d.chunk_rep[chunk];
   const int r = ci.x;
@@ -1470,7 +1548,8 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
   if (need_ev(R) != EV) return;
   if (skip_rebuilt && R.rebuild_now) return;
   constexpr bool ev = EV;
-  __shared__ float4 s_shift[kShiftCodes];
+  __shared__ float4 s_shift[SH == 0 ? kShiftCodes : 1];
+  __shared__ float s_axis[5];
   __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
   const int nt = R.ntypes;
   const int G = R.G;
@@ -1480,13 +1559,15 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     s_eps24[k] = R.lj_eps24[k];
     s_sig2[k] = R.lj_sig2[k];
   }
-  if (threadIdx.x < kShiftCodes) {
+  if (SH == 0 && threadIdx.x < kShiftCodes) {
     const int c = threadIdx.x;
     const int ax = c / 25, ay = (c / 5) % 5, az = c % 5;
     s_shift[c] = make_float4(shift_term(axis_code_e(ax), axis_code_k(ax), h, dL),
                              shift_term(axis_code_e(ay), axis_code_k(ay), h, dL),
                              shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
   }
+  if (SH == 1 && threadIdx.x < 5)
+    s_axis[threadIdx.x] = shift_term(axis_code_e(threadIdx.x), axis_code_k(threadIdx.x), h, dL);
   __syncthreads();
   const int local = ci.w * kChunk + threadIdx.x;
   const int base = R.slot_base;
@@ -1511,19 +1592,22 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     if (LISTED && keeps) {
       const float rcd = (float)(R.rc + (double)R.prune_delta);
       const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
-      const int pc =
-          nt == 1 ? lj_loop_filter<EV, B, PF, KB, true>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi, s_shift, ti, nt,
-                                                        s_eps24, s_sig2, rc2, fx, fy, fz, acc, pad)
-                  : lj_loop_filter<EV, B, PF, KB, false>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi, s_shift, ti, nt,
-                                                         s_eps24, s_sig2, rc2, fx, fy, fz, acc, pad);
+      const int pc = nt == 1 ? lj_loop_filter<EV, B, PF, KB, true, SH>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi,
+                                                                        s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2,
+                                                                        fx, fy, fz, acc, pad)
+                             : lj_loop_filter<EV, B, PF, KB, false, SH>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi,
+                                                                         s_shift, s_axis, ti, nt, s_eps24, s_sig2,
+                                                                         rc2, fx, fy, fz, acc, pad);
       d.pcnt[s] = pc;
       const float4 q = d.ref[s];
       d.ref[s] = make_float4(pi.x, pi.y, pi.z, q.w);
     } else if (nt == 1) {
       // one type (the Kremer-Grest melt): the pair parameters are loop constants
-      lj_loop<EV, B, PF, KB, true>(lst, nn, pbase, pi, s_shift, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+      lj_loop<EV, B, PF, KB, true, SH, P2>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2, fx,
+                                            fy, fz, acc);
     } else {
-      lj_loop<EV, B, PF, KB, false>(lst, nn, pbase, pi, s_shift, ti, nt, s_eps24, s_sig2, rc2, fx, fy, fz, acc);
+      lj_loop<EV, B, PF, KB, false, SH, P2>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2, fx,
+                                             fy, fz, acc);
     }
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
@@ -1608,16 +1692,16 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
 }
 
 // One block per chunk of the batch.
-template <bool EV, int B, int MINB, bool PF, int KB>
+template <bool EV, int B, int MINB, bool PF, int KB, int SH, bool P2>
 __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt) {
   count_launch(d, EV ? kKForceEv : kKForce);
-  force_chunk<EV, B, PF, KB, false>(d, blockIdx.x, skip_rebuilt != 0);
+  force_chunk<EV, B, PF, KB, false, SH, P2>(d, blockIdx.x, skip_rebuilt != 0);
 }
 
 // The chunks of the replicas on the rebuild work list (a resident grid
 // striding over them), launched after their rebuild while the other
 // replicas' forces run beside it; it also writes their pruned lists.
-template <bool EV, int B, int MINB, bool PF, int KB>
+template <bool EV, int B, int MINB, bool PF, int KB, int SH, bool P2>
 __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
   count_launch(d, EV ? kKForceEv : kKForce);
   const int n = rb_count(d);
@@ -1628,7 +1712,7 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
     cur.seek(item);
     __syncthreads();  // the previous item's shared tables are no longer read
     const Rep& R = d.reps[rb_rep(d, cur.i)];
-    force_chunk<EV, B, PF, KB, true>(d, R.chunk_base + (item - cur.lo), false);
+    force_chunk<EV, B, PF, KB, true, SH, P2>(d, R.chunk_base + (item - cur.lo), false);
   }
 }
 
@@ -1685,7 +1769,7 @@ __global__ void __launch_bounds__(kChunk) k_prune(Dev d) {
       for (int q = 0; q < kListPad; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
 #pragma unroll
       for (int q = 0; q < kListPad; ++q) {
-        const float4 sh = s_shift[w[q] >> kCodeShift];
+        const float3 sh = entry_shift<0>(w[q], s_shift, nullptr);
         const float dx = (pi.x - pj[q].x) - sh.x, dy = (pi.y - pj[q].y) - sh.y, dz = (pi.z - pj[q].z) - sh.z;
         const float r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < rcd2) out[(size_t)(cnt++) * 32] = w[q];
@@ -1748,7 +1832,7 @@ __global__ void __launch_bounds__(kChunk) k_table(Dev d, int sel) {
     for (int k = 0; k < nn; ++k) {
       const uint32_t w = __ldg(lst + (size_t)k * 32);
       const float4 pj = __ldg(pbase + (w & kIdxMask));
-      const float4 sh = s_shift[w >> kCodeShift];
+      const float3 sh = entry_shift<0>(w, s_shift, nullptr);
       const float dx = __fsub_rn(__fsub_rn(pi.x, pj.x), sh.x);
       const float dy = __fsub_rn(__fsub_rn(pi.y, pj.y), sh.y);
       const float dz = __fsub_rn(__fsub_rn(pi.z, pj.z), sh.z);
@@ -2288,20 +2372,26 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st, b
 constexpr int kForceCarveoutPct = 16;  // percent of the SM's shared-memory maximum
 
 // The variant's two kernels: one block per chunk, and the work-list form.
+// Parameters: list entries per batch, blocks per SM, next batch's list words
+// loaded ahead, batches per compensated add, shift lookup (0: 125-entry 3D
+// table, 1: per-axis 5-value table), pairs evaluated two at a time in packed
+// FP32x2 arithmetic.
 template <bool EV>
 void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(Dev)) {
   constexpr int E = 5;  // blocks per SM of the energy flavours (more registers)
-#define FMD_FORCE_VARIANT(B, MINB, PF, KB)          \
-  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB>; \
-  *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB>;
+#define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2)          \
+  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2>; \
+  *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB, SH, P2>;
   switch (variant) {
-    case 1: FMD_FORCE_VARIANT(4, 8, true, 1) break;
-    case 2: FMD_FORCE_VARIANT(4, 6, true, 2) break;
-    case 3: FMD_FORCE_VARIANT(4, 8, true, 2) break;
-    case 4: FMD_FORCE_VARIANT(4, 9, true, 1) break;
-    case 5: FMD_FORCE_VARIANT(4, 7, true, 2) break;
-    case 6: FMD_FORCE_VARIANT(4, 10, true, 1) break;
-    default: FMD_FORCE_VARIANT(4, 6, true, 1) break;
+    case 1: FMD_FORCE_VARIANT(4, 8, true, 2, 0, false) break;
+    case 2: FMD_FORCE_VARIANT(4, 8, true, 1, 1, false) break;
+    case 3: FMD_FORCE_VARIANT(4, 8, true, 2, 1, false) break;
+    case 4: FMD_FORCE_VARIANT(4, 8, true, 1, 1, true) break;
+    case 5: FMD_FORCE_VARIANT(4, 8, true, 2, 1, true) break;
+    case 6: FMD_FORCE_VARIANT(4, 7, true, 1, 1, true) break;
+    case 7: FMD_FORCE_VARIANT(4, 9, true, 1, 1, true) break;
+    case 8: FMD_FORCE_VARIANT(4, 6, true, 1, 1, false) break;
+    default: FMD_FORCE_VARIANT(4, 8, true, 1, 0, false) break;
   }
 #undef FMD_FORCE_VARIANT
 }

@@ -89,10 +89,10 @@ def test_headline_replica_settings(headline):
     assert b.list_buffer(s) > 0.4
 
 
-@pytest.mark.parametrize("fv", range(7))
+@pytest.mark.parametrize("fv", range(9))
 def test_headline_replica_forces_every_force_variant(headline, fv):
     b, s, d = headline
-    assert b.variants()[2] == 7
+    assert b.variants()[2] == 9
     b.set_variants(fv, -1)
     b.run(23)   # direct steps with this variant's plain flavour (and its filter walk)
     assert b.variants()[0] == fv
