@@ -471,7 +471,8 @@ def wl_c2(args, fm):
                                 "samples": [round(float(x), 7) for x in e]}}
 
 
-def wl_c3(args, fm):
+def c3_replicas():
+    """The 256 uneven replicas of the batched case: (chains, chain length, T, seed)."""
     rng = np.random.default_rng(3)
     reps = []
     for i in range(256):
@@ -480,7 +481,23 @@ def wl_c3(args, fm):
         nc = max(1, int(round(beads / cl)))
         T = float(rng.uniform(0.5, 1.5))
         reps.append((nc, cl, T, i))
-    b = fm.Batch(max_replicas=256, max_atoms=sum(nc * cl + 128 for nc, cl, _, _ in reps) + 4096, device=0)
+    return reps
+
+
+def c3_assignment(fm, world):
+    """Replicas of the batched case placed on `world` GPUs by atom count
+    (greedy longest-processing-time bin-pack, the same on every rank)."""
+    reps = c3_replicas()
+    part, load = fm.partition_replicas([nc * cl for nc, cl, _, _ in reps], world)
+    return reps, part, load
+
+
+def wl_c3(args, fm, rank=0, world=1, local=0, dist=None):
+    reps_all, part, load = c3_assignment(fm, world)
+    mine = [k for k in range(len(reps_all)) if part[k] == rank]
+    reps = [reps_all[k] for k in mine]
+    b = fm.Batch(max_replicas=max(1, len(reps)), max_atoms=sum(nc * cl + 128 for nc, cl, _, _ in reps) + 4096,
+                 device=local)
     slots = [b.add(_conf(f"nvt_langevin {T} {T} 1.0 {i}", 10 ** 7),
                    gen=dict(nchains=nc, chain_length=cl, density=DENSITY, seed=i, pushoff_steps=PUSHOFF))
              for nc, cl, T, i in reps]
@@ -488,11 +505,20 @@ def wl_c3(args, fm):
     b.autotune(10)
     b.run(GRAPH_CAPTURE_STEPS)  # the autotuner's choices invalidate the step graph: capture it untimed
     k = 1000
-    ms = _dev_run(fm, b, k)
-    natoms = [nc * cl for nc, cl, _, _ in reps]
-    batched = sum(natoms) * k / (ms * 1e-3)
+    barrier(dist, local)
+    ms = allmax(dist, _dev_run(fm, b, k), local)
+    natoms_all = [nc * cl for nc, cl, _, _ in reps_all]
+    batched = sum(natoms_all) * k / (ms * 1e-3)
+    out = {"workload": "c3_256_uneven_replicas", "value": batched, "unit": "atom-steps/s", "steps": k,
+           "total_atoms": int(sum(natoms_all)), "n_gpus": world,
+           "placement": {"rule": "greedy longest-processing-time by atom count", "atoms_per_gpu": load.tolist(),
+                         "replicas_per_gpu": np.bincount(part, minlength=world).tolist()}}
+    if rank != 0:
+        b.close()
+        return out
     # plain FP64, one replica at a time: timed on 8 replicas spread over the
     # sizes, per-step cost interpolated in size for all 256
+    natoms = [nc * cl for nc, cl, _, _ in reps]
     order = np.argsort(natoms)
     pick = [int(order[j]) for j in np.linspace(0, len(order) - 1, 8).astype(int)]
     sizes, per_step = [], []
@@ -508,11 +534,12 @@ def wl_c3(args, fm):
         per_step.append((time.perf_counter() - t0) / 200)
         sizes.append(natoms[j])
         ps.close()
-    est = float(np.sum(np.interp(natoms, sizes, per_step))) * k
-    plain = sum(natoms) * k / est
-    return {"workload": "c3_256_uneven_replicas", "value": batched, "unit": "atom-steps/s", "steps": k,
-            "total_atoms": int(sum(natoms)), "plain_fp64_one_at_a_time": plain, "speedup": batched / plain,
-            "plain_sample": {"sizes": sizes, "s_per_step": per_step}}
+    b.close()
+    est = float(np.sum(np.interp(natoms_all, sizes, per_step))) * k
+    plain = sum(natoms_all) * k / est
+    out.update({"plain_fp64_one_at_a_time": plain, "speedup": batched / plain,
+                "plain_sample": {"sizes": sizes, "s_per_step": per_step}})
+    return out
 
 
 def wl_c4(args, fm):
@@ -730,11 +757,21 @@ def main():
     ap.add_argument("--serve-step-scale", type=float, default=0.25, help="c4: scale of the requests' nsteps")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    rank, world, local, dist = dist_setup(args.gpus)
     if args.workload != "headline" and args.impl == "ours":
         import fastmd_b200 as fm
-        print(json.dumps(WORKLOADS[args.workload](args, fm)), flush=True)
+        if args.workload == "c3":
+            res = wl_c3(args, fm, rank, world, local, dist)
+        elif rank == 0:
+            res = WORKLOADS[args.workload](args, fm)
+        else:
+            res = None
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        if dist is not None:
+            barrier(dist, local)
+            dist.destroy_process_group()
         return
-    rank, world, local, dist = dist_setup(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world, local, dist)
         if dist is not None:

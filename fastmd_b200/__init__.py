@@ -23,6 +23,7 @@ from ._lib import (  # noqa: F401
     FastMDError,
     MeltSpec,
     Server,
+    ServerPool,
     Simulation,
     SystemDesc,
     ThermoRow,
@@ -33,6 +34,7 @@ from ._lib import (  # noqa: F401
     lib,
     lib_path,
     parse_run_conf,
+    partition_replicas,
     read_lammps_data,
     read_pair_table,
     run_conf_tables,

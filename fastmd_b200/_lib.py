@@ -655,3 +655,62 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def partition_replicas(costs, nparts):
+    """Greedy longest-processing-time placement of replicas on nparts GPUs
+    (fmd_partition_replicas): returns (part of each replica, total cost per
+    part).  Costs are atom counts or atoms x steps."""
+    c = np.ascontiguousarray(costs, dtype=np.int64)
+    part = np.zeros(len(c), np.int32)
+    load = np.zeros(nparts, np.int64)
+    _call("fmd_partition_replicas", _ptr(c), C.c_int32(len(c)), C.c_int32(nparts), _ptr(part), _ptr(load))
+    return part, load
+
+
+class ServerPool:
+    """One continuous-batching server per listed device (a device may be
+    listed twice); each request goes to the server with the least outstanding
+    work (atoms x steps)."""
+
+    def __init__(self, devices, max_replicas=256, hbm_budget_gb=150.0, steps_per_round=0, graph_steps=0):
+        self._h = C.c_void_p()
+        dev = np.ascontiguousarray(devices, dtype=np.int32)
+        o = ServerOpts(batch=BatchOpts(device=0, max_replicas=max_replicas, max_atoms=0,
+                                       hbm_budget_gb=hbm_budget_gb, graph_steps=graph_steps),
+                       steps_per_round=steps_per_round)
+        _call("fmd_server_pool_create", C.byref(o), _ptr(dev), C.c_int32(len(dev)), C.byref(self._h))
+
+    def submit(self, run_conf, gen):
+        """Returns (request id, index of the server it was placed on)."""
+        rid = C.c_int64()
+        srv = C.c_int32()
+        spec = _melt_spec(gen)
+        _call("fmd_server_pool_submit", self._h, run_conf.encode(), C.byref(spec), C.byref(rid), C.byref(srv))
+        return rid.value, srv.value
+
+    def poll(self, cap=256):
+        out = (RequestResult * cap)()
+        n = C.c_int32()
+        _call("fmd_server_pool_poll", self._h, out, C.c_int32(cap), C.byref(n))
+        return [out[k] for k in range(n.value)]
+
+    def stats(self):
+        q, r, f, a = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        s = C.c_double()
+        _call("fmd_server_pool_stats", self._h, C.byref(q), C.byref(r), C.byref(f), C.byref(a), C.byref(s))
+        return dict(queued=q.value, running=r.value, finished=f.value, atoms_resident=a.value, atom_steps=s.value)
+
+    def drain(self, timeout_s=600.0):
+        _call("fmd_server_pool_drain", self._h, C.c_double(timeout_s))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().fmd_server_pool_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -378,4 +378,168 @@ FMD_API fmd_status fmd_server_destroy(fmd_server* s) {
   });
 }
 
+// ------------------------------------------------------------ several GPUs
+// Greedy longest-processing-time placement: items in decreasing cost (ties:
+// lower index first), each to the part with the least total cost so far
+// (ties: lower part index).  Deterministic, so every rank of a multi-process
+// run computes the same assignment.
+FMD_API fmd_status fmd_partition_replicas(const int64_t* cost, int32_t n, int32_t nparts, int32_t* part_of,
+                                          int64_t* part_cost) {
+  return guarded([&] {
+    if (n < 0 || nparts <= 0 || (n > 0 && (!cost || !part_of))) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    std::vector<int32_t> order(n);
+    for (int32_t i = 0; i < n; ++i) {
+      if (cost[i] < 0) throw fmd::Error(FMD_ERR_ARG, "negative cost");
+      order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+    std::vector<int64_t> load(nparts, 0);
+    for (int32_t i : order) {
+      int32_t best = 0;
+      for (int32_t p = 1; p < nparts; ++p)
+        if (load[p] < load[best]) best = p;
+      part_of[i] = best;
+      load[best] += cost[i];
+    }
+    if (part_cost)
+      for (int32_t p = 0; p < nparts; ++p) part_cost[p] = load[p];
+  });
+}
+
+}  // extern "C"
+
+// A request server per device; requests go to the server with the least
+// outstanding work (atoms x steps submitted and not yet polled).
+struct fmd_server_pool {
+  std::vector<fmd_server*> servers;
+  std::vector<int32_t> devices;
+  std::vector<int64_t> work;  // outstanding atoms x steps per server
+  std::mutex mu;
+  int64_t next_id = 1;
+  std::map<std::pair<int, int64_t>, std::pair<int64_t, int64_t>> ids;  // (server, local id) -> (pool id, work)
+};
+
+extern "C" {
+
+FMD_API fmd_status fmd_server_pool_create(const fmd_server_opts* opts, const int32_t* devices, int32_t ndevices,
+                                          fmd_server_pool** out) {
+  return guarded([&] {
+    if (!out || !devices || ndevices <= 0) throw fmd::Error(FMD_ERR_ARG, "bad argument");
+    *out = nullptr;
+    std::unique_ptr<fmd_server_pool> p(new fmd_server_pool());
+    try {
+      for (int32_t k = 0; k < ndevices; ++k) {
+        fmd_server_opts o{};
+        if (opts) o = *opts;
+        o.batch.device = devices[k];
+        fmd_server* s = nullptr;
+        const fmd_status st = fmd_server_create(&o, &s);
+        if (st != FMD_OK) throw fmd::Error(st, "server on device " + std::to_string(devices[k]) + " failed");
+        p->servers.push_back(s);
+        p->devices.push_back(devices[k]);
+        p->work.push_back(0);
+      }
+    } catch (...) {
+      for (fmd_server* s : p->servers) fmd_server_destroy(s);
+      throw;
+    }
+    *out = p.release();
+  });
+}
+
+FMD_API fmd_status fmd_server_pool_submit(fmd_server_pool* p, const char* conf, const fmd_melt_spec* gen,
+                                          int64_t* request_id, int32_t* server) {
+  return guarded([&] {
+    if (!p || !conf || !gen || !request_id) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    const fmd::RunConfig cfg = fmd::parse_run_conf(conf);
+    const int64_t w = (int64_t)gen->nchains * gen->chain_length * std::max<int64_t>(1, cfg.nsteps);
+    std::lock_guard<std::mutex> lk(p->mu);
+    int best = 0;
+    for (int k = 1; k < (int)p->servers.size(); ++k)
+      if (p->work[k] < p->work[best]) best = k;
+    int64_t local = 0;
+    const fmd_status st = fmd_server_submit(p->servers[best], conf, gen, &local);
+    if (st != FMD_OK) {
+      char buf[512] = {0};
+      fmd_last_error(buf, sizeof(buf));
+      throw fmd::Error(st, buf);
+    }
+    const int64_t id = p->next_id++;
+    p->ids[{best, local}] = {id, w};
+    p->work[best] += w;
+    *request_id = id;
+    if (server) *server = best;
+  });
+}
+
+FMD_API fmd_status fmd_server_pool_poll(fmd_server_pool* p, fmd_request_result* out, int32_t cap, int32_t* n) {
+  return guarded([&] {
+    if (!p || !n || (cap > 0 && !out)) throw fmd::Error(FMD_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(p->mu);
+    int32_t got = 0;
+    for (int k = 0; k < (int)p->servers.size() && got < cap; ++k) {
+      int32_t m = 0;
+      const fmd_status st = fmd_server_poll(p->servers[k], out + got, cap - got, &m);
+      if (st != FMD_OK) throw fmd::Error(st, "poll failed");
+      for (int32_t q = got; q < got + m; ++q) {
+        auto it = p->ids.find({k, out[q].request_id});
+        if (it == p->ids.end()) throw fmd::Error(FMD_ERR_STATE, "unknown request in a pooled server");
+        out[q].request_id = it->second.first;
+        p->work[k] -= it->second.second;
+        p->ids.erase(it);
+      }
+      got += m;
+    }
+    *n = got;
+  });
+}
+
+FMD_API fmd_status fmd_server_pool_stats(fmd_server_pool* p, int64_t* queued, int64_t* running, int64_t* finished,
+                                         int64_t* atoms_resident, double* atom_steps) {
+  return guarded([&] {
+    if (!p) throw fmd::Error(FMD_ERR_ARG, "null pool");
+    int64_t q = 0, r = 0, f = 0, a = 0;
+    double s = 0;
+    for (fmd_server* sv : p->servers) {
+      int64_t q1 = 0, r1 = 0, f1 = 0, a1 = 0;
+      double s1 = 0;
+      const fmd_status st = fmd_server_stats(sv, &q1, &r1, &f1, &a1, &s1);
+      if (st != FMD_OK) throw fmd::Error(st, "stats failed");
+      q += q1;
+      r += r1;
+      f += f1;
+      a += a1;
+      s += s1;
+    }
+    if (queued) *queued = q;
+    if (running) *running = r;
+    if (finished) *finished = f;
+    if (atoms_resident) *atoms_resident = a;
+    if (atom_steps) *atom_steps = s;
+  });
+}
+
+FMD_API fmd_status fmd_server_pool_drain(fmd_server_pool* p, double timeout_s) {
+  return guarded([&] {
+    if (!p) throw fmd::Error(FMD_ERR_ARG, "null pool");
+    const double t_end = now_s() + timeout_s;
+    for (fmd_server* sv : p->servers) {
+      const fmd_status st = fmd_server_drain(sv, std::max(0.0, t_end - now_s()));
+      if (st != FMD_OK) {
+        char buf[512] = {0};
+        fmd_last_error(buf, sizeof(buf));
+        throw fmd::Error(st, buf);
+      }
+    }
+  });
+}
+
+FMD_API fmd_status fmd_server_pool_destroy(fmd_server_pool* p) {
+  return guarded([&] {
+    if (!p) return;
+    for (fmd_server* s : p->servers) fmd_server_destroy(s);
+    delete p;
+  });
+}
+
 }  // extern "C"

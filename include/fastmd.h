@@ -422,6 +422,35 @@ FMD_API fmd_status fmd_server_timing(fmd_server* s, double* admit_s, double* run
 FMD_API fmd_status fmd_server_drain(fmd_server* s, double timeout_s);
 FMD_API fmd_status fmd_server_destroy(fmd_server* s);
 
+/* ---------------------------------------------------------- several GPUs */
+/* The reference runs one system on one GPU; these spread independent
+ * replicas over several (no data-path exchange between them).
+ * fmd_partition_replicas: greedy longest-processing-time placement of n
+ * replicas with the given costs (atom counts, or atoms x steps) on nparts
+ * GPUs: replicas in decreasing cost (ties: lower index first), each to the
+ * part with the least total cost so far (ties: lower part).  Deterministic,
+ * so every process of a multi-process run computes the same placement.
+ * part_of[n] receives each replica's part; part_cost[nparts] (may be NULL)
+ * the total per part. */
+FMD_API fmd_status fmd_partition_replicas(const int64_t* cost, int32_t n, int32_t nparts, int32_t* part_of,
+                                          int64_t* part_cost);
+/* A pool of request servers, one per listed device (each with its own host
+ * thread, batch and CUDA-graph step loop; a device may be listed twice).  A
+ * submitted request goes to the server with the least outstanding work
+ * (atoms x run.conf nsteps of its requests not yet polled; ties: lowest
+ * index); *server (may be NULL) receives that server's index in devices[].
+ * Request ids are pool-wide; poll, stats and drain cover every server. */
+typedef struct fmd_server_pool fmd_server_pool;
+FMD_API fmd_status fmd_server_pool_create(const fmd_server_opts* opts, const int32_t* devices, int32_t ndevices,
+                                          fmd_server_pool** out);
+FMD_API fmd_status fmd_server_pool_submit(fmd_server_pool* p, const char* run_conf_text, const fmd_melt_spec* gen,
+                                          int64_t* request_id, int32_t* server);
+FMD_API fmd_status fmd_server_pool_poll(fmd_server_pool* p, fmd_request_result* out, int32_t cap, int32_t* n);
+FMD_API fmd_status fmd_server_pool_stats(fmd_server_pool* p, int64_t* queued, int64_t* running, int64_t* finished,
+                                         int64_t* atoms_resident, double* atom_steps);
+FMD_API fmd_status fmd_server_pool_drain(fmd_server_pool* p, double timeout_s);
+FMD_API fmd_status fmd_server_pool_destroy(fmd_server_pool* p);
+
 /* ------------------------------------------- reference-layout launchers */
 /* Cell list + full Verlet list, replacing VerletList::build
  * (neighbor/verlet_list.cuh:28-30, verlet_list.cu:337-376).  pos is float4
