@@ -382,38 +382,55 @@ def wl_c1(args, fm):
                          angle_p=np.array([[5.0, np.pi]]), mol=d.mol)
         fo, _, _ = po.forces(osys)
         errs.append(float(np.sqrt(np.mean((f - fo) ** 2)) / np.sqrt(np.mean(fo ** 2))))
-    # <T>, <P>, Rg: mixed and plain FP64 from the same state, 2,000 steps sampled every 20
+    # <T>, <P>, Rg: mixed, plain FP64 and the FP64 oracle from the same state,
+    # c1_stat_steps steps sampled every 100
     x, v, img = b.state(s)
     d.xyz, d.vel, d.image = x, v, img
+    nsamp = max(10, args.c1_stat_steps // 100)
+
+    def p_of(st):
+        return (st[0] + st[3] + st[5]) / 3.0
 
     def sample_batch():
         out = []
-        for _ in range(100):
-            b.run(20)
+        for _ in range(nsamp):
+            b.run(100)
             t = b.thermo(s)
-            p = (t.stress[0] + t.stress[3] + t.stress[5]) / 3.0
-            out.append((t.temp, p, b.rg(s)))
+            out.append((t.temp, p_of(t.stress), b.rg(s)))
         return np.array(out)
 
     def sample_plain():
         ps = fm.Simulation(conf, desc=d, form=fm.FMD_FORM_PLAIN_FP64)
         out = []
-        for _ in range(100):
-            ps.step(20)
+        for _ in range(nsamp):
+            ps.step(100)
             t = ps.thermo()
-            p = (t.stress[0] + t.stress[3] + t.stress[5]) / 3.0
-            out.append((t.temp, p, ps.rg()))
+            out.append((t.temp, p_of(t.stress), ps.rg()))
         ps.close()
         return np.array(out)
 
-    mb, pl = sample_batch(), sample_plain()
+    def sample_oracle():
+        osys = po.System(xyz=x, L=d.box_L, type=d.type, mass=np.ones(1), lj=np.ones((1, 1, 2)), bonds=d.bonds,
+                         bond_type=np.zeros(len(d.bonds), np.int32), fene=np.array([[30.0, 1.5, 1.0, 1.0]]),
+                         angles=d.angles, angle_type=np.zeros(len(d.angles), np.int32),
+                         angle_p=np.array([[5.0, np.pi]]), mol=d.mol, vel=v, image=img)
+        osim = po.Sim(osys, ensemble="langevin", T=(1.0, 1.0, 1.0), seed=7, nsteps=10 ** 7)
+        out = []
+        for _ in range(nsamp):
+            osim.step(100)
+            o = osim.thermo()
+            out.append((o[2], (o[3] + o[6] + o[8]) / 3.0, osim.rg()))
+        return np.array(out)
+
+    mb, pl, orc = sample_batch(), sample_plain(), sample_oracle()
 
     def ms(a):
-        # mean and standard error with blocks of 10 samples (correlated series)
-        blocks = a[: len(a) // 10 * 10].reshape(10, -1, a.shape[1]).mean(axis=1)
+        # mean and standard error with 10 blocks (correlated series)
+        blocks = np.array([blk.mean(axis=0) for blk in np.array_split(a, 10)])
         return a.mean(axis=0).tolist(), (blocks.std(axis=0, ddof=1) / np.sqrt(len(blocks))).tolist()
 
-    (m_mean, m_err), (p_mean, p_err) = ms(mb), ms(pl)
+    (m_mean, m_err), (p_mean, p_err), (o_mean, o_err) = ms(mb), ms(pl), ms(orc)
+    sigma = [abs(a - c) / max(np.hypot(ea, ec), 1e-300) for a, ea, c, ec in zip(m_mean, m_err, o_mean, o_err)]
     # NVT conserved-quantity drift (nose_hoover test definition), mixed form
     cn = _conf("nvt_nh 1.0 1.0 0.5 3", 10 ** 7, thermo=0)
     b2 = fm.Batch(max_replicas=1, max_atoms=65536, device=0)
@@ -435,7 +452,10 @@ def wl_c1(args, fm):
                                                                    "snapshots": len(errs), "target": 1e-5},
             "langevin_T_P_Rg": {"mixed": {"mean": m_mean, "stderr": m_err},
                                 "plain_fp64": {"mean": p_mean, "stderr": p_err},
-                                "samples": "100 per form, every 20 steps, 2,000 steps from the same state"},
+                                "fp64_oracle": {"mean": o_mean, "stderr": o_err},
+                                "mixed_vs_oracle_sigmas": sigma,
+                                "samples": f"{nsamp} per form, every 100 steps, {nsamp * 100} steps from the same "
+                                           "state; standard errors from 10 block averages"},
             "nvt_conserved_drift": {"steps": int(steps[-1]) if len(e) else 0, "E0": float(e[0]) if len(e) else 0.0,
                                     "slope_per_step": slope, "relative_per_1e6_steps": rel_per_1e6,
                                     "target_relative_per_1e6": 1e-4}}
@@ -583,7 +603,135 @@ def wl_c4(args, fm):
             "offered_atom_steps_per_s": sum(work.values()) / dur, "server_thread": timing}
 
 
-WORKLOADS = {"c0": wl_c0, "c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c4": wl_c4}
+def wl_npt_drift(args, fm):
+    """Nose-Hoover NPT conserved-quantity drift on a box already at P = 0:
+    the C0 melt (3,000 beads, two types as in C2, npt_nh T = 1 Tdamp = 0.1,
+    P = 0 Pdamp = 1.0, chain 3) relaxed for --npt-equil steps in the mixed
+    form, then the same simulated time (--npt-time tau) at dt and dt / 2 in
+    the mixed form, the plain FP64 form and the FP64 oracle, each from the
+    relaxed state with a fresh chain and barostat.  Extended energy: KE + PE
+    + chain terms + v_eps^2 / (2 W) + P V (P = 0).  A slope fitted to 100
+    samples; reported per unit time and relative per 10^6 steps."""
+    from oracle import pyoracle as po
+    lj = ((0, 0, 1.0, 1.0), (1, 1, 1.0, 1.0), (0, 1, 0.9, 1.0))
+    ens = "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3"
+    pre = fm.Batch(max_replicas=1, max_atoms=8192, device=0)
+    s0 = pre.add(_conf(ens, 10 ** 8, ntypes=2, lj=lj),
+                 gen=dict(nchains=30, chain_length=100, density=DENSITY, seed=42, pushoff_steps=PUSHOFF,
+                          type_block=50))
+    pre.run(args.npt_equil)
+    x0, v0, i0 = pre.state(s0)
+    L0 = pre.info(s0).box_L
+    pre.close()
+    d = fm.generate_melt(30, 100, density=DENSITY, seed=42, type_block=50)
+    d.xyz, d.vel, d.image, d.box_L = x0, v0, i0, L0
+    tab = np.ones((2, 2, 2))
+    tab[0, 1, 0] = tab[1, 0, 0] = 0.9
+    out = {"workload": "npt_drift_c0_two_types", "relaxed_box_L": L0, "equil_steps": args.npt_equil,
+           "sim_time_tau": args.npt_time, "runs": []}
+    n = len(d.type)
+    for dt in (0.001, 0.0005):
+        nsteps = int(round(args.npt_time / dt))
+        every = max(1, nsteps // 100)
+        conf = (f"ntypes 2\nrc 2.5\nskin 0.3\ndt {dt}\nnsteps {10 ** 8}\n{ens}\n"
+                "bond_type 0 30.0 1.5 1.0 1.0\nangle_type 0 5.0 180.0\n"
+                + "".join(f"lj {a} {b} {e} {g}\n" for a, b, e, g in lj))
+        series = {}
+        for form, name in ((fm.FMD_FORM_MIXED, "mixed"), (fm.FMD_FORM_PLAIN_FP64, "plain_fp64")):
+            sim = fm.Simulation(conf, desc=d, form=form)
+            e = []
+            for _ in range(nsteps // every):
+                sim.step(every)
+                e.append(sim.thermo().conserved)
+            sim.close()
+            series[name] = np.array(e)
+        osys = po.System(xyz=x0, L=L0, type=d.type, mass=np.ones(2), lj=tab, bonds=d.bonds,
+                         bond_type=np.zeros(len(d.bonds), np.int32), fene=np.array([[30.0, 1.5, 1.0, 1.0]]),
+                         angles=d.angles, angle_type=np.zeros(len(d.angles), np.int32),
+                         angle_p=np.array([[5.0, np.pi]]), mol=d.mol, vel=v0, image=i0)
+        osim = po.Sim(osys, ensemble="npt_nh", dt=dt, T=(1.0, 1.0, 0.1), P=(0.0, 0.0, 1.0), chain=3, nsteps=10 ** 8)
+        e = []
+        for _ in range(nsteps // every):
+            osim.step(every)
+            e.append(osim.conserved() / n)
+        series["fp64_oracle"] = np.array(e)
+        t = np.arange(1, nsteps // every + 1) * every * dt
+        row = {"dt": dt, "steps": nsteps}
+        for name, e in series.items():
+            slope = float(np.polyfit(t, e, 1)[0])  # per atom per tau
+            row[name] = {"E0": float(e[0]), "slope_per_tau": slope,
+                         "relative_per_1e6_steps": slope * dt * 1e6 / abs(e[0]),
+                         "rms_fluctuation": float(np.std(e - np.polyval(np.polyfit(t, e, 1), t)))}
+        out["runs"].append(row)
+    return out
+
+
+def wl_drift(args, fm):
+    """Conserved-quantity drift of the Nose-Hoover ensembles, batched for
+    statistics: --drift-reps replicas of 30,000 beads each (seeded melts,
+    pushed off, relaxed --drift-relax steps in the same ensemble), then
+    --drift-run steps sampled 100 times; a line per replica, relative slope
+    per 10^6 steps, mean and standard error over the replicas.  NVT (nvt_nh
+    T = 1, Tdamp = 0.5) at dt and dt / 2 (the same simulated time), NPT
+    (two types as C2, npt_nh T = 1 Tdamp = 0.1, P = 0 Pdamp = 1, chain 3) at
+    dt, and the plain FP64 form on two NVT replicas for comparison."""
+    lj2 = ((0, 0, 1.0, 1.0), (1, 1, 1.0, 1.0), (0, 1, 0.9, 1.0))
+    cases = [("nvt", "nvt_nh 1.0 1.0 0.5 3", 1, ((0, 0, 1.0, 1.0),), 0, 0.001),
+             ("nvt", "nvt_nh 1.0 1.0 0.5 3", 1, ((0, 0, 1.0, 1.0),), 0, 0.0005),
+             ("npt", "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3", 2, lj2, 50, 0.001)]
+    out = {"workload": "nh_drift_batched", "replicas": args.drift_reps, "beads_per_replica": NCHAINS * CHAIN_LEN,
+           "cases": []}
+
+    def conf_for(ens, nt, lj, dt):
+        return (f"ntypes {nt}\nrc 2.5\nskin 0.3\ndt {dt}\nnsteps {10 ** 9}\n{ens}\n"
+                "bond_type 0 30.0 1.5 1.0 1.0\nangle_type 0 5.0 180.0\n"
+                + "".join(f"lj {a} {b_} {e} {g}\n" for a, b_, e, g in lj))
+
+    def slopes(series, t):
+        rel = [np.polyfit(t, e, 1)[0] / abs(e[0]) for e in series.T]
+        return np.array(rel)
+
+    for name, ens, nt, lj, tb, dt in cases:
+        b = fm.Batch(max_replicas=args.drift_reps, max_atoms=args.drift_reps * 30080 + 4096, device=0)
+        slots = [b.add(conf_for(ens, nt, lj, dt), gen=dict(nchains=NCHAINS, chain_length=CHAIN_LEN, density=DENSITY,
+                                                           seed=500 + r, pushoff_steps=PUSHOFF, type_block=tb))
+                 for r in range(args.drift_reps)]
+        b.run(int(args.drift_relax * 0.001 / dt))
+        nrun = int(args.drift_run * 0.001 / dt)
+        every = max(1, nrun // 100)
+        e = np.zeros((nrun // every, len(slots)))
+        for k in range(nrun // every):
+            b.run(every)
+            for j, s in enumerate(slots):
+                e[k, j] = b.thermo(s).conserved
+        t = np.arange(1, nrun // every + 1) * float(every)
+        rel = slopes(e, t) * 1e6
+        row = {"ensemble": ens, "dt": dt, "steps": nrun, "relative_per_1e6_steps": float(rel.mean()),
+               "stderr": float(rel.std(ddof=1) / np.sqrt(len(rel))), "per_replica": rel.tolist(),
+               "relative_per_tau": float(rel.mean() / (1e6 * dt))}
+        if name == "nvt" and dt == 0.001:
+            # the plain FP64 form from the relaxed states of the first two replicas
+            pl = []
+            for s in slots[:2]:
+                x, v, img = b.state(s)
+                d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0)
+                d.xyz, d.vel, d.image = x, v, img
+                ps = fm.Simulation(conf_for(ens, nt, lj, dt), desc=d, form=fm.FMD_FORM_PLAIN_FP64)
+                ee = []
+                for _ in range(nrun // every):
+                    ps.step(every)
+                    ee.append(ps.thermo().conserved)
+                ps.close()
+                pl.append(ee)
+            prel = slopes(np.array(pl).T, t) * 1e6
+            row["plain_fp64_two_replicas"] = {"relative_per_1e6_steps": prel.tolist()}
+        b.close()
+        out["cases"].append(row)
+    return out
+
+
+WORKLOADS = {"c0": wl_c0, "c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c4": wl_c4, "npt_drift": wl_npt_drift,
+             "drift": wl_drift}
 
 
 def kernel_timeline(b, steps, path):
@@ -753,6 +901,12 @@ def main():
     ap.add_argument("--timeline-steps", type=int, default=200)
     ap.add_argument("--drift-chunks", type=int, default=20, help="c2: conserved-quantity samples")
     ap.add_argument("--c1-drift-steps", type=int, default=200_000, help="c1: NVT steps of the drift fit")
+    ap.add_argument("--c1-stat-steps", type=int, default=20_000, help="c1: steps of the <T>, <P>, Rg comparison")
+    ap.add_argument("--npt-equil", type=int, default=20_000, help="npt_drift: relaxation steps at P = 0")
+    ap.add_argument("--drift-reps", type=int, default=16, help="drift: replicas per case")
+    ap.add_argument("--drift-relax", type=int, default=20_000, help="drift: relaxation steps (at dt = 0.001)")
+    ap.add_argument("--drift-run", type=int, default=200_000, help="drift: measured steps (at dt = 0.001)")
+    ap.add_argument("--npt-time", type=float, default=20.0, help="npt_drift: simulated time per run (tau)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="c4: arrival window")
     ap.add_argument("--serve-step-scale", type=float, default=0.25, help="c4: scale of the requests' nsteps")
     args = ap.parse_args()
