@@ -3,6 +3,7 @@
 //   fmd_launch_verlet_build  <- VerletList::build   (neighbor/verlet_list.cu:337-376)
 //   fmd_launch_lj            <- launch_lj_kernel    (force/lj.cu:109-122)
 //   fmd_launch_morton_sort   <- MortonSorter::sort_and_permute (core/morton.cu:65-85)
+//   fmd_launch_tile_list     <- TileList::build     (neighbor/tile_list.cu:143-171)
 // Buffers keep the reference's layout: float4 positions with the type id
 // bit-cast into .w, the transposed list neighbors[k * natoms + i].
 // FP32 throughout, as the reference; this file is compiled with -fmad=false so
@@ -281,6 +282,105 @@ MortonScratch morton_carve(void* base, int n) {
 }
 
 // ---------------------------------------------------------------------------
+// Tile list (neighbor/tile_list.cu:5-171): tile pairs of 32-atom tiles whose
+// axis-aligned boxes lie within rc_skin (minimum image between box centres),
+// as CSR in increasing partner order.  The reference writes ntiles^2 flags
+// and scans them (3.9 GB at 10^6 atoms); here one warp per tile tests 32
+// partners per ballot, once to count and once to write, with O(ntiles)
+// memory.  The predicate keeps the reference's statement order; this file
+// is compiled without contraction, so it is exact against the FP32 oracle.
+__global__ void k_tile_bbox(const float4* pos, float4* tmin, float4* tmax, int natoms) {
+  const int t = blockIdx.x, lane = threadIdx.x;
+  const int a = t * 32 + lane;
+  float3 lo = make_float3(1e30f, 1e30f, 1e30f), hi = make_float3(-1e30f, -1e30f, -1e30f);
+  if (a < natoms) {
+    const float4 r = pos[a];
+    lo = hi = make_float3(r.x, r.y, r.z);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = fminf(lo.x, __shfl_down_sync(0xffffffffu, lo.x, o));
+    lo.y = fminf(lo.y, __shfl_down_sync(0xffffffffu, lo.y, o));
+    lo.z = fminf(lo.z, __shfl_down_sync(0xffffffffu, lo.z, o));
+    hi.x = fmaxf(hi.x, __shfl_down_sync(0xffffffffu, hi.x, o));
+    hi.y = fmaxf(hi.y, __shfl_down_sync(0xffffffffu, hi.y, o));
+    hi.z = fmaxf(hi.z, __shfl_down_sync(0xffffffffu, hi.z, o));
+  }
+  if (lane == 0) {
+    tmin[t] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    tmax[t] = make_float4(hi.x, hi.y, hi.z, 0.f);
+  }
+}
+
+// tile_list.cu:63-99: distance between the two boxes' surfaces below rc_skin.
+__device__ __forceinline__ bool tiles_near(float4 amin, float4 amax, float4 bmin, float4 bmax, float L,
+                                           float inv_L, float rc2) {
+  const float cax = 0.5f * (amin.x + amax.x), cay = 0.5f * (amin.y + amax.y), caz = 0.5f * (amin.z + amax.z);
+  const float cbx = 0.5f * (bmin.x + bmax.x), cby = 0.5f * (bmin.y + bmax.y), cbz = 0.5f * (bmin.z + bmax.z);
+  const float eax = 0.5f * (amax.x - amin.x), eay = 0.5f * (amax.y - amin.y), eaz = 0.5f * (amax.z - amin.z);
+  const float ebx = 0.5f * (bmax.x - bmin.x), eby = 0.5f * (bmax.y - bmin.y), ebz = 0.5f * (bmax.z - bmin.z);
+  float dx = fabsf(min_image_f(cax - cbx, L, inv_L)) - eax - ebx;
+  float dy = fabsf(min_image_f(cay - cby, L, inv_L)) - eay - eby;
+  float dz = fabsf(min_image_f(caz - cbz, L, inv_L)) - eaz - ebz;
+  dx = fmaxf(dx, 0.0f);
+  dy = fmaxf(dy, 0.0f);
+  dz = fmaxf(dz, 0.0f);
+  return dx * dx + dy * dy + dz * dz < rc2;
+}
+
+// WRITE = false: per-tile pair counts (into cnt, entry ntiles set to 0 for the
+// scan); WRITE = true: the partners at off[a], at most cap in all.
+template <bool WRITE>
+__global__ void k_tile_pairs(const float4* tmin, const float4* tmax, int ntiles, float L, float inv_L, float rc2,
+                             int* cnt, const int* off, int* nbr, int cap) {
+  const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (!WRITE && blockIdx.x == 0 && threadIdx.x == 0) cnt[ntiles] = 0;
+  if (a >= ntiles) return;
+  const float4 amin = tmin[a], amax = tmax[a];
+  int run = WRITE ? off[a] : 0;
+  for (int b0 = 0; b0 < ntiles; b0 += 32) {
+    const int b = b0 + lane;
+    const bool hit = b < ntiles && tiles_near(amin, amax, tmin[b], tmax[b], L, inv_L, rc2);
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (WRITE && hit) {
+      const int at = run + __popc(m & ((1u << lane) - 1u));
+      if (at < cap) nbr[at] = b;
+    }
+    run += __popc(m);
+  }
+  if (!WRITE && lane == 0) cnt[a] = run;
+}
+
+struct TileScratch {
+  float4* tmin;
+  float4* tmax;
+  int* cnt;
+  void* cub;
+  size_t cub_bytes;
+  size_t total;
+};
+
+TileScratch tile_carve(void* base, int ntiles) {
+  TileScratch s{};
+  size_t cub_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (int*)nullptr, (int*)nullptr, ntiles + 1);
+  char* p = (char*)base;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* q = p ? p + off : nullptr;
+    off += align256(bytes);
+    return q;
+  };
+  s.tmin = (float4*)take(sizeof(float4) * ntiles);
+  s.tmax = (float4*)take(sizeof(float4) * ntiles);
+  s.cnt = (int*)take(sizeof(int) * (ntiles + 1));
+  s.cub = take(cub_bytes);
+  s.cub_bytes = cub_bytes;
+  s.total = off;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free Verlet build.  Some callers cannot allocate device memory:
 // code running inside another framework's memory pool or a stream-capture
 // region, or a host process that must not grow its device footprint after
@@ -435,6 +535,44 @@ FMD_API fmd_status fmd_launch_lj(const void* pos, void* force, float* virial, co
         (const float4*)pos, (float4*)force, virial, (const float2*)lj_params, neighbors, num_neighbors, natoms,
         ntypes, rc2, box_L, inv_L);
     FMD_CUDA_LAUNCH();
+  });
+}
+
+FMD_API fmd_status fmd_tile_list_scratch_bytes(int32_t natoms, size_t* bytes) {
+  return guarded([&] {
+    if (!bytes || natoms <= 0) throw Error(FMD_ERR_ARG, "bad argument");
+    *bytes = tile_carve(nullptr, (natoms + 31) / 32).total;
+  });
+}
+
+FMD_API fmd_status fmd_launch_tile_list(const void* pos, int32_t natoms, float box_L, float rc_skin, int32_t* offsets,
+                                        int32_t* neighbors, int32_t capacity, int32_t* npairs, void* scratch,
+                                        size_t scratch_bytes, void* stream) {
+  return guarded([&] {
+    if (!pos || natoms <= 0 || !offsets || capacity < 0 || (capacity > 0 && !neighbors) || !scratch)
+      throw Error(FMD_ERR_ARG, "bad argument");
+    if (!(std::isfinite(box_L) && std::isfinite(rc_skin) && box_L > 0.0f && rc_skin > 0.0f))
+      throw Error(FMD_ERR_ARG, "box_L and rc_skin must be finite and positive");
+    const int T = (natoms + 31) / 32;
+    const TileScratch s = tile_carve(scratch, T);
+    if (s.total > scratch_bytes) throw Error(FMD_ERR_ARG, "scratch buffer too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    const float inv_L = 1.0f / box_L, rc2 = rc_skin * rc_skin;
+    k_tile_bbox<<<T, 32, 0, st>>>((const float4*)pos, s.tmin, s.tmax, natoms);
+    FMD_CUDA_LAUNCH();
+    const int wpb = 4, gr = div_up(T, wpb);
+    k_tile_pairs<false><<<gr, 32 * wpb, 0, st>>>(s.tmin, s.tmax, T, box_L, inv_L, rc2, s.cnt, nullptr, nullptr, 0);
+    FMD_CUDA_LAUNCH();
+    size_t cb = s.cub_bytes;
+    FMD_CUDA(cub::DeviceScan::ExclusiveSum(s.cub, cb, s.cnt, offsets, T + 1, st));
+    k_tile_pairs<true><<<gr, 32 * wpb, 0, st>>>(s.tmin, s.tmax, T, box_L, inv_L, rc2, nullptr, offsets, neighbors,
+                                                capacity);
+    FMD_CUDA_LAUNCH();
+    if (npairs) {
+      FMD_CUDA(cudaMemcpyAsync(npairs, offsets + T, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      FMD_CUDA(cudaStreamSynchronize(st));
+      if (*npairs > capacity) throw Error(FMD_ERR_OVERFLOW, "tile pairs exceed the capacity");
+    }
   });
 }
 

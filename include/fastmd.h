@@ -494,6 +494,20 @@ FMD_API fmd_status fmd_launch_verlet_build_static(const void* pos, int32_t natom
 FMD_API fmd_status fmd_launch_lj(const void* pos, void* force, float* virial, const void* lj_params,
                                  const int32_t* neighbors, const int32_t* num_neighbors, int32_t natoms,
                                  int32_t ntypes, float rc2, float box_L, float inv_L, void* stream);
+/* Tile list of 32-atom tiles, replacing TileList::build
+ * (neighbor/tile_list.cuh:3-23, tile_list.cu:143-171): pairs of tiles (a, b),
+ * ntiles = ceil(natoms / 32), whose axis-aligned boxes over the tiles'
+ * positions lie within rc_skin (minimum image between the box centres,
+ * tile_list.cu:63-99), as CSR: offsets[ntiles + 1] (device) and neighbors
+ * (device, at most capacity) in increasing b for each a.  The reference
+ * materialises ntiles^2 flags; this build uses O(ntiles) scratch
+ * (fmd_tile_list_scratch_bytes).  npairs (host, may be NULL): the stream is
+ * synchronised and the pair count returned; more pairs than capacity gives
+ * FMD_ERR_OVERFLOW (the first capacity are written). */
+FMD_API fmd_status fmd_tile_list_scratch_bytes(int32_t natoms, size_t* bytes);
+FMD_API fmd_status fmd_launch_tile_list(const void* pos, int32_t natoms, float box_L, float rc_skin,
+                                        int32_t* offsets, int32_t* neighbors, int32_t capacity, int32_t* npairs,
+                                        void* scratch, size_t scratch_bytes, void* stream);
 /* 30-bit Morton sort of pos and vel, replacing MortonSorter::sort_and_permute
  * (core/morton.cuh:17-18; morton.cu:65-85); the permutation is bit-exact with
  * a stable sort of (key, index).  perm (device, [padded natoms]) receives the

@@ -615,6 +615,53 @@ int64_t orc_pairs_brute_f32(const float* xyz, int32_t n, float L, float rcs, con
   return np;
 }
 
+// Tile list of 32-atom tiles (neighbor/tile_list.cu:5-171), FP32, statement
+// order of the reference with every operation rounded on its own (no
+// contraction): per tile the axis-aligned box of its positions (padding slots
+// beyond natoms contribute +1e30 to the minimum and -1e30 to the maximum),
+// then for every ordered tile pair the distance between the boxes' surfaces
+// with the minimum image of the centre offset (tile_list.cu:63-99); pairs
+// closer than rc_skin listed per tile a in increasing b (CSR).  Returns the
+// pair count; at most cap neighbors are written.
+int64_t orc_tile_list_aabb(const float* pos4, int32_t natoms, float L, float rc_skin, int32_t* offsets,
+                           int32_t* neighbors, int64_t cap) {
+  const int32_t T = (natoms + 31) / 32;
+  const float inv_L = 1.0f / L;
+  std::vector<float> mn(3 * (size_t)T), mx(3 * (size_t)T);
+  for (int32_t t = 0; t < T; ++t)
+    for (int d = 0; d < 3; ++d) {
+      float lo = 1e30f, hi = -1e30f;
+      for (int32_t a = t * 32; a < t * 32 + 32; ++a) {
+        const float v = a < natoms ? pos4[4 * (size_t)a + d] : 1e30f;
+        lo = std::min(lo, v);
+        if (a < natoms) hi = std::max(hi, v);
+      }
+      mn[3 * t + d] = lo;
+      mx[3 * t + d] = hi;
+    }
+  const float rc2 = rc_skin * rc_skin;
+  int64_t np = 0;
+  for (int32_t a = 0; a < T; ++a) {
+    offsets[a] = (int32_t)np;
+    for (int32_t b = 0; b < T; ++b) {
+      float s2 = 0.0f;
+      for (int d = 0; d < 3; ++d) {
+        const float ca = 0.5f * (mn[3 * a + d] + mx[3 * a + d]), cb = 0.5f * (mn[3 * b + d] + mx[3 * b + d]);
+        const float ea = 0.5f * (mx[3 * a + d] - mn[3 * a + d]), eb = 0.5f * (mx[3 * b + d] - mn[3 * b + d]);
+        float g = std::fabs(orc_min_image_f32(ca - cb, L, inv_L)) - ea - eb;
+        g = std::max(g, 0.0f);
+        s2 = s2 + g * g;
+      }
+      if (s2 < rc2) {
+        if (np < cap) neighbors[np] = b;
+        ++np;
+      }
+    }
+  }
+  offsets[T] = (int32_t)np;
+  return np;
+}
+
 int32_t orc_verlet_lists(const double* xyz, int32_t n, double L, double rcs, const int32_t* bonds,
                          int32_t nbonds, int32_t max_nbr, int32_t* nbr, int32_t* counts) {
   Excl ex;

@@ -78,6 +78,8 @@ void orc_morton_sort_f32(const float* xyz, int32_t n, float inv_L, int32_t* perm
 int64_t orc_pairs_brute(const double* xyz, int32_t n, double L, double rcs,
                         const int32_t* bonds, int32_t nbonds,
                         int32_t* pi, int32_t* pj, int64_t cap);
+int64_t orc_tile_list_aabb(const float* pos4, int32_t natoms, float L, float rc_skin, int32_t* offsets,
+                           int32_t* neighbors, int64_t cap);
 int64_t orc_pairs_brute_f32(const float* xyz, int32_t n, float L, float rcs,
                             const int32_t* bonds, int32_t nbonds,
                             int32_t* pi, int32_t* pj, int64_t cap);

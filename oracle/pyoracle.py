@@ -67,6 +67,8 @@ def lib():
         L.orc_pairs_brute.restype = C.c_int64
         L.orc_pairs_brute.argtypes = [f64p, C.c_int32, C.c_double, C.c_double, C.c_void_p, C.c_int32,
                                       i32p, i32p, C.c_int64]
+        L.orc_tile_list_aabb.restype = C.c_int64
+        L.orc_tile_list_aabb.argtypes = [f32p, C.c_int32, C.c_float, C.c_float, i32p, i32p, C.c_int64]
         L.orc_pairs_brute_f32.restype = C.c_int64
         L.orc_pairs_brute_f32.argtypes = [f32p, C.c_int32, C.c_float, C.c_float, C.c_void_p, C.c_int32,
                                           i32p, i32p, C.c_int64]
@@ -227,6 +229,21 @@ def pairs_brute(xyz, L, rcs, bonds=None, f32=False):
         m = lb.orc_pairs_brute(x, n, L, rcs, b.ctypes.data if b.size else None, len(b), pi, pj, cap)
     assert m <= cap
     return pi[:m].copy(), pj[:m].copy()
+
+
+def tile_list_aabb(pos4, L, rc_skin):
+    """Tile list of 32-atom tiles (neighbor/tile_list.cu semantics, FP32):
+    CSR (offsets[ntiles + 1], neighbors) of tile pairs whose boxes lie within
+    rc_skin.  pos4: (N, 4) float32."""
+    lb = lib()
+    p = np.ascontiguousarray(pos4, dtype=np.float32)
+    n = len(p)
+    T = (n + 31) // 32
+    off = np.zeros(T + 1, np.int32)
+    cap = T * T
+    nb = np.zeros(max(cap, 1), np.int32)
+    m = lb.orc_tile_list_aabb(p.reshape(-1), n, np.float32(L), np.float32(rc_skin), off, nb, cap)
+    return off, nb[:m].copy()
 
 
 def verlet_lists(xyz, L, rcs, bonds=None, max_nbr=256):

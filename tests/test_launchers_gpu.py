@@ -162,3 +162,69 @@ def test_morton_launcher_bit_exact(pos_key, perm_key, inv):
     assert np.array_equal(p, G[perm_key])
     assert np.array_equal(pos.cpu().numpy()[:, :3], xyz[p])
     assert np.array_equal(vel.cpu().numpy()[:, 0], p.astype(np.float32))  # test_morton.cu:48
+
+
+def tile_list(pos4, L, rcs, cap=None):
+    torch = _torch()
+    lib = fm.lib()
+    n = len(pos4)
+    T = (n + 31) // 32
+    cap = T * T if cap is None else cap
+    pos = torch.from_numpy(np.ascontiguousarray(pos4, np.float32)).cuda()
+    off = torch.full((T + 1,), -1, dtype=torch.int32, device="cuda")
+    nbr = torch.full((max(cap, 1),), -1, dtype=torch.int32, device="cuda")
+    sb = C.c_size_t()
+    lib.fmd_tile_list_scratch_bytes.restype = C.c_int32
+    assert lib.fmd_tile_list_scratch_bytes(C.c_int32(n), C.byref(sb)) == 0
+    scratch = torch.empty(sb.value, dtype=torch.uint8, device="cuda")
+    npairs = C.c_int32()
+    lib.fmd_launch_tile_list.restype = C.c_int32
+    st = lib.fmd_launch_tile_list(C.c_void_p(pos.data_ptr()), C.c_int32(n), C.c_float(L), C.c_float(rcs),
+                                  C.c_void_p(off.data_ptr()), C.c_void_p(nbr.data_ptr()), C.c_int32(cap),
+                                  C.byref(npairs), C.c_void_p(scratch.data_ptr()), C.c_size_t(sb.value), None)
+    return st, off.cpu().numpy(), nbr.cpu().numpy()[: min(npairs.value, cap)], npairs.value
+
+
+def _compact(xyz, L, bits=10):
+    """Atoms ordered by a 30-bit Morton key of their positions, so that the
+    32-atom tiles are spatially compact (as a cell-sorted system's are)."""
+    q = np.clip((xyz / L * (1 << bits)).astype(np.int64), 0, (1 << bits) - 1)
+    key = np.zeros(len(xyz), np.int64)
+    for b in range(bits):
+        for d in range(3):
+            key |= ((q[:, d] >> b) & 1) << (3 * b + d)
+    return xyz[np.argsort(key, kind="stable")]
+
+
+@pytest.mark.parametrize("case", ["golden128", "melt3000", "uniform100k"])
+def test_tile_list_launcher_exact_against_oracle(case):
+    from oracle import pyoracle as po
+    if case == "golden128":
+        xyz, L, rcs = G["tile_pos"], 10.0, 3.0
+    elif case == "melt3000":
+        d = fm.generate_melt(30, 100, density=0.85, seed=3)
+        xyz, L, rcs = _compact(d.xyz, d.box_L), d.box_L, 2.8
+    else:
+        L = 49.0
+        xyz, rcs = _compact(np.random.default_rng(8).uniform(0, L, (100_000, 3)), L), 2.8
+    p4 = _pos4(xyz)
+    st, off, nbr, npairs = tile_list(p4, L, rcs)
+    assert st == 0
+    ooff, onbr = po.tile_list_aabb(p4, L, rcs)
+    assert np.array_equal(off, ooff) and np.array_equal(nbr, onbr) and npairs == len(onbr)
+    T = len(off) - 1
+    got = {(a, int(b)) for a in range(T) for b in nbr[off[a]:off[a + 1]]}
+    if case == "golden128":
+        # tests/test_tile_list.cu: every tile pair of the reference's brute force is listed
+        assert {tuple(x) for x in G["tile_pairs"]} <= got
+    elif case == "melt3000":
+        # every atom pair within rc_skin lies in a listed tile pair (both orders)
+        pi, pj = po.pairs_brute(xyz, L, rcs, f32=True)
+        assert {(int(a) // 32, int(b) // 32) for a, b in zip(pi, pj)} <= got
+        assert {(int(b) // 32, int(a) // 32) for a, b in zip(pi, pj)} <= got
+
+
+def test_tile_list_launcher_reports_overflow():
+    d = fm.generate_melt(30, 100, density=0.85, seed=3)
+    st, off, nbr, npairs = tile_list(_pos4(_compact(d.xyz, d.box_L)), d.box_L, 2.8, cap=10)
+    assert st == 5 and npairs > 10 and len(nbr) == 10   # FMD_ERR_OVERFLOW, the first 10 written
