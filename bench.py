@@ -678,7 +678,10 @@ def wl_drift(args, fm):
     lj2 = ((0, 0, 1.0, 1.0), (1, 1, 1.0, 1.0), (0, 1, 0.9, 1.0))
     cases = [("nvt", "nvt_nh 1.0 1.0 0.5 3", 1, ((0, 0, 1.0, 1.0),), 0, 0.001),
              ("nvt", "nvt_nh 1.0 1.0 0.5 3", 1, ((0, 0, 1.0, 1.0),), 0, 0.0005),
-             ("npt", "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3", 2, lj2, 50, 0.001)]
+             ("npt", "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3", 2, lj2, 50, 0.001),
+             ("npt", "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3", 2, lj2, 50, 0.0005)]
+    wanted = set(args.drift_cases.split(","))
+    cases = [c for c in cases if f"{c[0]}{c[5]}" in wanted or c[0] in wanted]
     out = {"workload": "nh_drift_batched", "replicas": args.drift_reps, "beads_per_replica": NCHAINS * CHAIN_LEN,
            "cases": []}
 
@@ -709,13 +712,13 @@ def wl_drift(args, fm):
         row = {"ensemble": ens, "dt": dt, "steps": nrun, "relative_per_1e6_steps": float(rel.mean()),
                "stderr": float(rel.std(ddof=1) / np.sqrt(len(rel))), "per_replica": rel.tolist(),
                "relative_per_tau": float(rel.mean() / (1e6 * dt))}
-        if name == "nvt" and dt == 0.001:
-            # the plain FP64 form from the relaxed states of the first two replicas
+        if dt == 0.001 and args.drift_plain > 0:
+            # the plain FP64 form from the relaxed states of the first replicas
             pl = []
-            for s in slots[:2]:
+            for s in slots[:args.drift_plain]:
                 x, v, img = b.state(s)
-                d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0)
-                d.xyz, d.vel, d.image = x, v, img
+                d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0, type_block=tb)
+                d.xyz, d.vel, d.image, d.box_L = x, v, img, b.info(s).box_L
                 ps = fm.Simulation(conf_for(ens, nt, lj, dt), desc=d, form=fm.FMD_FORM_PLAIN_FP64)
                 ee = []
                 for _ in range(nrun // every):
@@ -724,7 +727,8 @@ def wl_drift(args, fm):
                 ps.close()
                 pl.append(ee)
             prel = slopes(np.array(pl).T, t) * 1e6
-            row["plain_fp64_two_replicas"] = {"relative_per_1e6_steps": prel.tolist()}
+            row["plain_fp64"] = {"relative_per_1e6_steps": prel.tolist(), "replicas": len(pl),
+                                 "note": "from the mixed replicas' relaxed states"}
         b.close()
         out["cases"].append(row)
     return out
@@ -904,6 +908,8 @@ def main():
     ap.add_argument("--c1-stat-steps", type=int, default=20_000, help="c1: steps of the <T>, <P>, Rg comparison")
     ap.add_argument("--npt-equil", type=int, default=20_000, help="npt_drift: relaxation steps at P = 0")
     ap.add_argument("--drift-reps", type=int, default=16, help="drift: replicas per case")
+    ap.add_argument("--drift-cases", default="nvt,npt", help="drift: nvt, npt, or nvt0.001 / npt0.0005 ...")
+    ap.add_argument("--drift-plain", type=int, default=2, help="drift: plain FP64 replicas at dt = 0.001")
     ap.add_argument("--drift-relax", type=int, default=20_000, help="drift: relaxation steps (at dt = 0.001)")
     ap.add_argument("--drift-run", type=int, default=200_000, help="drift: measured steps (at dt = 0.001)")
     ap.add_argument("--npt-time", type=float, default=20.0, help="npt_drift: simulated time per run (tau)")
