@@ -306,7 +306,8 @@ def _conf(ens, nsteps, ntypes=1, lj=((0, 0, 1.0, 1.0),), thermo=0):
 GRAPH_CAPTURE_STEPS = 50  # one replay of a batch's default step graph
 # force-kernel variants, in the library's order (fastmd_b200/csrc/mixed_kernels.cu, force_kernels)
 FORCE_VARIANTS = ["m8 k1 t3", "m8 k2 t3", "m8 k1 a5", "m8 k2 a5", "m8 k1 a5 x2", "m8 k2 a5 x2", "m7 k1 a5 x2",
-                  "m9 k1 a5 x2", "m6 k1 a5"]
+                  "m9 k1 a5 x2", "m6 k1 a5", "m8 k1 a5 x2 l2", "m8 k1 a5 x2 l4",
+                  "m8 k1 a5 x2 r3", "m8 k1 a5 x2 r4"]
 
 
 def _dev_run(fm, b, nsteps):
@@ -491,6 +492,119 @@ def wl_c2(args, fm):
                                 "samples": [round(float(x), 7) for x in e]}}
 
 
+def wl_tiles(args, fm):
+    """The warp-per-tile LJ (fmd_launch_lj_tiles over fmd_launch_tile_list's
+    32-atom tile pairs at rc) against the per-atom Verlet-list LJ
+    (fmd_launch_lj over fmd_launch_verlet_build's list at rc + skin), both in
+    the reference's layout, on the same pushed-off one-type melt of
+    --tiles-chains x 100 beads with atoms in 30-bit Morton order (compact
+    tiles) and the 1-2 bonds excluded; each LJ pass timed alone with CUDA
+    events over 20 launches after 3.  Pair work per atom: tile pairs x 32
+    evaluated, against the list entries and the pairs inside rc."""
+    import ctypes as C
+    import torch
+    lib = fm.lib()
+    nch = args.tiles_chains
+    b = fm.Batch(max_replicas=1, max_atoms=nch * 100 + 4096, device=0)
+    s = b.add(_conf("nvt_langevin 1.0 1.0 1.0 7", 10 ** 7), gen=dict(nchains=nch, chain_length=100, density=DENSITY,
+                                                                     seed=5, pushoff_steps=PUSHOFF))
+    b.run(100)
+    x, _, _ = b.state(s)
+    L = b.info(s).box_L
+    b.close()
+    n = len(x)
+    q = np.clip((x / L * 1024).astype(np.int64), 0, 1023)
+    key = np.zeros(n, np.int64)
+    for bit in range(10):
+        for d in range(3):
+            key |= ((q[:, d] >> bit) & 1) << (3 * bit + d)
+    order = np.argsort(key, kind="stable")
+    rank = np.empty_like(order)
+    rank[order] = np.arange(n)
+    x = x[order]
+    k = np.arange(n) % 100
+    first = np.nonzero(k < 99)[0]
+    bonds = np.sort(rank[np.stack([first, first + 1], axis=1)], axis=1)
+    per = [[] for _ in range(n)]
+    for a_, c_ in bonds:
+        per[a_].append(c_)
+        per[c_].append(a_)
+    xo = np.zeros(n + 1, np.int32)
+    xo[1:] = np.cumsum([len(p_) for p_ in per])
+    xl = np.array([j for p_ in per for j in sorted(p_)], np.int32)
+    p4 = np.zeros((n, 4), np.float32)
+    p4[:, :3] = x
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    pos, eo, el = dev(p4), dev(xo), dev(xl)
+    rc, rcs = 2.5, 2.8
+    Lf, invL = C.c_float(L), C.c_float(1.0 / L)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    # tile list at rc
+    T = (n + 31) // 32
+    sb = C.c_size_t()
+    lib.fmd_tile_list_scratch_bytes(C.c_int32(n), C.byref(sb))
+    tscr = torch.empty(sb.value, dtype=torch.uint8, device="cuda")
+    toff = torch.zeros(T + 1, dtype=torch.int32, device="cuda")
+    cap = T * 64
+    tnbr = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    npairs = C.c_int32()
+    assert lib.fmd_launch_tile_list(ptr(pos), C.c_int32(n), Lf, C.c_float(rc), ptr(toff), ptr(tnbr), C.c_int32(cap),
+                                    C.byref(npairs), ptr(tscr), C.c_size_t(sb.value), None) == 0
+    # Verlet list at rc + skin
+    vs = C.c_size_t()
+    lib.fmd_verlet_scratch_bytes(C.c_int32(n), C.c_float(rcs), Lf, C.byref(vs))
+    vscr = torch.empty(vs.value, dtype=torch.uint8, device="cuda")
+    M = 128
+    nbr = torch.zeros(M * n, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert lib.fmd_launch_verlet_build(ptr(pos), C.c_int32(n), Lf, ptr(eo), ptr(el), C.c_float(rcs), C.c_int32(M),
+                                       ptr(nbr), ptr(cnt), ptr(vscr), C.c_size_t(vs.value), ptr(flag), None) == 0
+    torch.cuda.synchronize()
+    assert int(flag.item()) == 0
+    ljp = torch.tensor([1.0, 1.0], dtype=torch.float32, device="cuda")
+    f_t = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    f_v = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6, dtype=torch.float32, device="cuda")
+    rc2 = C.c_float(rc * rc)
+
+    def tiles():
+        return lib.fmd_launch_lj_tiles(ptr(pos), ptr(f_t), ptr(vir), ptr(ljp), ptr(toff), ptr(tnbr), ptr(eo), ptr(el),
+                                       C.c_int32(n), C.c_int32(1), rc2, Lf, invL, None)
+
+    def verlet():
+        return lib.fmd_launch_lj(ptr(pos), ptr(f_v), ptr(vir), ptr(ljp), ptr(nbr), ptr(cnt), C.c_int32(n),
+                                 C.c_int32(1), rc2, Lf, invL, None)
+
+    def timed(fn):
+        for _ in range(3):
+            assert fn() == 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(20):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 20
+
+    ms_t, ms_v = timed(tiles), timed(verlet)
+    ft, fv = f_t.cpu().numpy()[:, :3], f_v.cpu().numpy()[:, :3]
+    diff = float(np.sqrt(np.mean(np.sum((ft - fv) ** 2, 1)) / np.mean(np.sum(fv ** 2, 1))))
+    entries = float(cnt.float().mean().item())
+    from oracle import pyoracle as po
+    inside = 2.0 * len(po.pairs_brute(x, L, rc, bonds=bonds)[0]) / n if n <= 100_000 else None
+    return {"workload": "lj_tiles_vs_verlet", "natoms": n, "box_L": L,
+            "tile_pairs": int(npairs.value), "tile_pairs_per_tile": npairs.value / T,
+            "pairs_evaluated_per_atom": {"tiles": 32.0 * npairs.value / T, "verlet_list_entries": entries,
+                                         "inside_rc": inside},
+            "ms_per_launch": {"lj_tiles": ms_t, "lj_verlet": ms_v}, "ns_per_atom": {"lj_tiles": ms_t * 1e6 / n,
+                                                                                   "lj_verlet": ms_v * 1e6 / n},
+            "force_rel_rms_tiles_vs_verlet": diff,
+            "note": "reference layout (absolute FP32 positions, one thread per atom for the list form); the product "
+                    "force kernel k_force works on the cell-offset layout and also evaluates the bonded terms"}
+
+
 def c3_replicas():
     """The 256 uneven replicas of the batched case: (chains, chain length, T, seed)."""
     rng = np.random.default_rng(3)
@@ -650,11 +764,15 @@ def wl_npt_drift(args, fm):
                          angles=d.angles, angle_type=np.zeros(len(d.angles), np.int32),
                          angle_p=np.array([[5.0, np.pi]]), mol=d.mol, vel=v0, image=i0)
         osim = po.Sim(osys, ensemble="npt_nh", dt=dt, T=(1.0, 1.0, 0.1), P=(0.0, 0.0, 1.0), chain=3, nsteps=10 ** 8)
-        e = []
+        e, em = [], []
         for _ in range(nsteps // every):
             osim.step(every)
             e.append(osim.conserved() / n)
+            em.append(osim.conserved_mtk() / n)
         series["fp64_oracle"] = np.array(e)
+        # the same run's extended energy with the work of the barostat force's
+        # kinetic term (3 / N_f) 2 KE, which the reference's barostat omits
+        series["fp64_oracle_with_mtk_term"] = np.array(em)
         t = np.arange(1, nsteps // every + 1) * every * dt
         row = {"dt": dt, "steps": nsteps}
         for name, e in series.items():
@@ -664,6 +782,28 @@ def wl_npt_drift(args, fm):
                          "rms_fluctuation": float(np.std(e - np.polyval(np.polyfit(t, e, 1), t)))}
         out["runs"].append(row)
     return out
+
+
+def cutoff_jump_energy(x, L, lj, tb, rc=2.5):
+    """-sum over non-bonded pairs within rc of U(rc) (the LJ energy at the
+    cutoff, per pair type) at positions x in a box of edge L (chains of
+    CHAIN_LEN beads, types in blocks of tb along each chain): what shifting
+    the truncated LJ to zero at rc would add to the potential energy."""
+    from oracle import pyoracle as po
+    n = len(x)
+    k = np.arange(n) % CHAIN_LEN
+    first = np.nonzero(k < CHAIN_LEN - 1)[0]
+    bonds = np.stack([first, first + 1], axis=1)
+    nbr, cnt, _ = po.verlet_lists(x, L, rc, bonds=bonds, max_nbr=256)
+    typ = (k // tb) % 2 if tb > 0 else np.zeros(n, np.int64)
+    eps = np.ones((2, 2))
+    for a, c, e, _ in lj:
+        eps[a, c] = eps[c, a] = e
+    src = np.repeat(np.arange(n), cnt)
+    dst = np.concatenate([nbr[i, :cnt[i]] for i in range(n)]) if n else np.zeros(0, np.int64)
+    sr6 = (1.0 / rc) ** 6
+    u_rc = 4.0 * eps[typ[src], typ[dst]] * (sr6 * sr6 - sr6)
+    return -0.5 * float(np.sum(u_rc))   # each pair listed from both ends
 
 
 def wl_drift(args, fm):
@@ -703,39 +843,66 @@ def wl_drift(args, fm):
         nrun = int(args.drift_run * 0.001 / dt)
         every = max(1, nrun // 100)
         e = np.zeros((nrun // every, len(slots)))
+        nshift = min(args.drift_shift_check, len(slots)) if name == "npt" else 0
+        es = np.zeros((nrun // every, nshift))
+        vol = np.zeros((nrun // every, len(slots)))
         for k in range(nrun // every):
             b.run(every)
             for j, s in enumerate(slots):
                 e[k, j] = b.thermo(s).conserved
+                vol[k, j] = b.info(s).box_L ** 3
+            for j in range(nshift):
+                es[k, j] = e[k, j] + cutoff_jump_energy(*b.force_frame(slots[j]), lj, tb) / (NCHAINS * CHAIN_LEN)
         t = np.arange(1, nrun // every + 1) * float(every)
         rel = slopes(e, t) * 1e6
         row = {"ensemble": ens, "dt": dt, "steps": nrun, "relative_per_1e6_steps": float(rel.mean()),
                "stderr": float(rel.std(ddof=1) / np.sqrt(len(rel))), "per_replica": rel.tolist(),
                "relative_per_tau": float(rel.mean() / (1e6 * dt))}
+        if name == "npt":
+            vrel = slopes(vol, t) * 1e6
+            row["volume_relative_per_1e6_steps"] = {"mean": float(vrel.mean()),
+                                                    "stderr": float(vrel.std(ddof=1) / np.sqrt(len(vrel)))}
+        if nshift:
+            rs = slopes(es, t) * 1e6
+            row["with_shifted_lj_energy"] = {
+                "relative_per_1e6_steps": rs.tolist(), "same_replicas_unshifted": rel[:nshift].tolist(),
+                "how": "extended energy with the LJ energy of every pair within rc shifted by -U(rc) (the "
+                       "forces are unchanged): the jump U(rc) a pair carries across the cutoff, which the "
+                       "instantaneous virial (hence the barostat) does not see, is taken out"}
         if dt == 0.001 and args.drift_plain > 0:
             # the plain FP64 form from the relaxed states of the first replicas
-            pl = []
+            pl, pls, plv = [], [], []
             for s in slots[:args.drift_plain]:
                 x, v, img = b.state(s)
                 d = fm.generate_melt(NCHAINS, CHAIN_LEN, density=DENSITY, seed=0, type_block=tb)
                 d.xyz, d.vel, d.image, d.box_L = x, v, img, b.info(s).box_L
                 ps = fm.Simulation(conf_for(ens, nt, lj, dt), desc=d, form=fm.FMD_FORM_PLAIN_FP64)
-                ee = []
+                ee, es_, vv = [], [], []
                 for _ in range(nrun // every):
                     ps.step(every)
-                    ee.append(ps.thermo().conserved)
+                    th = ps.thermo()
+                    ee.append(th.conserved)
+                    vv.append(th.box_L ** 3)
+                    if name == "npt":
+                        es_.append(th.conserved + cutoff_jump_energy(ps.state()[0], th.box_L, lj, tb)
+                                   / (NCHAINS * CHAIN_LEN))
                 ps.close()
                 pl.append(ee)
+                pls.append(es_)
+                plv.append(vv)
             prel = slopes(np.array(pl).T, t) * 1e6
             row["plain_fp64"] = {"relative_per_1e6_steps": prel.tolist(), "replicas": len(pl),
+                                 "volume_relative_per_1e6_steps": (slopes(np.array(plv).T, t) * 1e6).tolist(),
                                  "note": "from the mixed replicas' relaxed states"}
+            if name == "npt":
+                row["plain_fp64"]["with_shifted_lj_energy"] = (slopes(np.array(pls).T, t) * 1e6).tolist()
         b.close()
         out["cases"].append(row)
     return out
 
 
 WORKLOADS = {"c0": wl_c0, "c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c4": wl_c4, "npt_drift": wl_npt_drift,
-             "drift": wl_drift}
+             "drift": wl_drift, "tiles": wl_tiles}
 
 
 def kernel_timeline(b, steps, path):
@@ -910,7 +1077,10 @@ def main():
     ap.add_argument("--drift-reps", type=int, default=16, help="drift: replicas per case")
     ap.add_argument("--drift-cases", default="nvt,npt", help="drift: nvt, npt, or nvt0.001 / npt0.0005 ...")
     ap.add_argument("--drift-plain", type=int, default=2, help="drift: plain FP64 replicas at dt = 0.001")
+    ap.add_argument("--drift-shift-check", type=int, default=4,
+                    help="drift: NPT replicas whose extended energy is also reported with the LJ shifted at rc")
     ap.add_argument("--drift-relax", type=int, default=20_000, help="drift: relaxation steps (at dt = 0.001)")
+    ap.add_argument("--tiles-chains", type=int, default=300, help="tiles: chains of 100 beads in the melt")
     ap.add_argument("--drift-run", type=int, default=200_000, help="drift: measured steps (at dt = 0.001)")
     ap.add_argument("--npt-time", type=float, default=20.0, help="npt_drift: simulated time per run (tau)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="c4: arrival window")
@@ -1009,8 +1179,10 @@ def main():
                             "variants": FORCE_VARIANTS[:nf],
                             "legend": "m = min blocks per SM, k = batches of 4 list entries per compensated add, "
                                       "t3 = shift from the 125-entry 3D table, a5 = per-axis 5-value table, "
-                                      "x2 = pairs two at a time in packed FP32x2 arithmetic (all: next batch's "
-                                      "list words loaded ahead)"}
+                                      "x2 = pairs two at a time in packed FP32x2 arithmetic, l2 / l4 = two / "
+                                      "four lanes per atom (one otherwise), r3 / r4 = list rows staged through a "
+                                      "shared-memory ring 2 / 3 batches ahead by asynchronous copies (otherwise "
+                                      "the next batch's list words are loaded ahead into registers)"}
         line["launches_by_kernel"] = launched
         line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
                                     "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0),

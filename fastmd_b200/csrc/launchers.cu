@@ -4,6 +4,7 @@
 //   fmd_launch_lj            <- launch_lj_kernel    (force/lj.cu:109-122)
 //   fmd_launch_morton_sort   <- MortonSorter::sort_and_permute (core/morton.cu:65-85)
 //   fmd_launch_tile_list     <- TileList::build     (neighbor/tile_list.cu:143-171)
+//   fmd_launch_lj_tiles      <- the LJ pass over TileList's pairs (warp per tile)
 // Buffers keep the reference's layout: float4 positions with the type id
 // bit-cast into .w, the transposed list neighbors[k * natoms + i].
 // FP32 throughout, as the reference; this file is compiled with -fmad=false so
@@ -171,6 +172,30 @@ __global__ void k_build(const float4* pos, const int* sorted, const int* scid, c
 }
 
 // lj.cu:4-107 semantics: force[i] = (F, pe_i) overwritten, virial accumulated.
+// One pair's force on i, half its energy and half its virial (lj.cu:32-61):
+// F/r clamped to +-1000 (lj.cu:48).  p = (eps, sigma) of the type pair.
+__device__ __forceinline__ void lj_ref_pair(float2 p, float dx, float dy, float dz, float r2, float& fx, float& fy,
+                                            float& fz, float& pe, float* v) {
+  const float sig2 = p.y * p.y;
+  const float r2inv = __fdividef(1.0f, r2);
+  const float sr2 = sig2 * r2inv;
+  const float sr6 = sr2 * sr2 * sr2;
+  const float sr12 = sr6 * sr6;
+  float fr = 24.0f * p.x * r2inv * (2.0f * sr12 - sr6);
+  fr = fminf(fmaxf(fr, -1000.0f), 1000.0f);
+  const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
+  fx += fxij;
+  fy += fyij;
+  fz += fzij;
+  pe += 0.5f * 4.0f * p.x * (sr12 - sr6);
+  v[0] += 0.5f * fxij * dx;
+  v[1] += 0.5f * fxij * dy;
+  v[2] += 0.5f * fxij * dz;
+  v[3] += 0.5f * fyij * dy;
+  v[4] += 0.5f * fyij * dz;
+  v[5] += 0.5f * fzij * dz;
+}
+
 __global__ void k_lj(const float4* __restrict__ pos, float4* __restrict__ force, float* __restrict__ virial,
                      const float2* __restrict__ lj, const int* __restrict__ nbr, const int* __restrict__ cnt, int n,
                      int ntypes, float rc2, float L, float inv_L) {
@@ -188,27 +213,8 @@ __global__ void k_lj(const float4* __restrict__ pos, float4* __restrict__ force,
       const float dy = min_image_f(pi.y - pj.y, L, inv_L);
       const float dz = min_image_f(pi.z - pj.z, L, inv_L);
       const float r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < rc2 && r2 > 1e-10f) {
-        const float2 p = __ldg(&lj[ti * ntypes + __float_as_int(pj.w)]);
-        const float sig2 = p.y * p.y;
-        const float r2inv = __fdividef(1.0f, r2);
-        const float sr2 = sig2 * r2inv;
-        const float sr6 = sr2 * sr2 * sr2;
-        const float sr12 = sr6 * sr6;
-        float fr = 24.0f * p.x * r2inv * (2.0f * sr12 - sr6);
-        fr = fminf(fmaxf(fr, -1000.0f), 1000.0f);
-        const float fxij = fr * dx, fyij = fr * dy, fzij = fr * dz;
-        fx += fxij;
-        fy += fyij;
-        fz += fzij;
-        pe += 0.5f * 4.0f * p.x * (sr12 - sr6);
-        v[0] += 0.5f * fxij * dx;
-        v[1] += 0.5f * fxij * dy;
-        v[2] += 0.5f * fxij * dz;
-        v[3] += 0.5f * fyij * dy;
-        v[4] += 0.5f * fyij * dz;
-        v[5] += 0.5f * fzij * dz;
-      }
+      if (r2 < rc2 && r2 > 1e-10f)
+        lj_ref_pair(__ldg(&lj[ti * ntypes + __float_as_int(pj.w)]), dx, dy, dz, r2, fx, fy, fz, pe, v);
     }
     force[i] = make_float4(fx, fy, fz, pe);
   }
@@ -349,6 +355,84 @@ __global__ void k_tile_pairs(const float4* tmin, const float4* tmax, int ntiles,
     run += __popc(m);
   }
   if (!WRITE && lane == 0) cnt[a] = run;
+}
+
+// LJ over the tile list, a warp per i-tile (the tile-pair form of the LJ
+// pass over TileList's pairs): one lane per i atom; each partner j-tile's 32
+// positions are staged in the warp's shared-memory slice (the next partner's
+// loaded ahead into a register) and every lane evaluates its atom against
+// all 32.  Masked per tile pair: the atom itself, its excluded partners (the
+// exclusion CSR the Verlet build takes; one bit per j slot, set from the
+// atom's few partners) and slots past natoms.  Each pair is evaluated from
+// both tiles (force on i only, half the energy and virial per side) with
+// k_lj's pair arithmetic, so the forces differ from k_lj's by summation
+// order only.
+constexpr int kTileWarps = 4;
+__global__ void __launch_bounds__(32 * kTileWarps) k_lj_tiles(const float4* __restrict__ pos,
+                                                               float4* __restrict__ force, float* __restrict__ virial,
+                                                               const float2* __restrict__ lj,
+                                                               const int* __restrict__ toff,
+                                                               const int* __restrict__ tnbr,
+                                                               const int* __restrict__ xoff,
+                                                               const int* __restrict__ xlist, int n, int ntiles,
+                                                               int ntypes, float rc2, float L, float inv_L) {
+  __shared__ float4 s_pos[kTileWarps][32];
+  __shared__ float sm[kTileWarps][6];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = blockIdx.x * kTileWarps + w;
+  float fx = 0, fy = 0, fz = 0, pe = 0;
+  float v[6] = {0, 0, 0, 0, 0, 0};
+  if (a < ntiles) {  // warp-uniform
+    const int i = a * 32 + lane;
+    const bool live = i < n;
+    const float4 pi = live ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int ti = __float_as_int(pi.w);
+    const int x0 = live && xoff ? xoff[i] : 0, x1 = live && xoff ? xoff[i + 1] : 0;
+    const int p0 = toff[a], p1 = toff[a + 1];
+    float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (p0 < p1) {
+      const int j = tnbr[p0] * 32 + lane;
+      if (j < n) nxt = pos[j];
+    }
+    for (int p = p0; p < p1; ++p) {
+      const int jb = tnbr[p] * 32;
+      __syncwarp();  // the previous partner's slice is no longer read
+      s_pos[w][lane] = nxt;
+      if (p + 1 < p1) {
+        const int j = tnbr[p + 1] * 32 + lane;
+        nxt = j < n ? pos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      __syncwarp();
+      uint32_t skip = n - jb >= 32 ? 0u : ~0u << (n - jb);
+      if (jb == a * 32) skip |= 1u << lane;
+      for (int e = x0; e < x1; ++e) {
+        const int jx = xlist[e] - jb;
+        if ((unsigned)jx < 32u) skip |= 1u << jx;
+      }
+      if (live) {
+#pragma unroll 4
+        for (int jj = 0; jj < 32; ++jj) {
+          const float4 pj = s_pos[w][jj];
+          const float dx = min_image_f(pi.x - pj.x, L, inv_L);
+          const float dy = min_image_f(pi.y - pj.y, L, inv_L);
+          const float dz = min_image_f(pi.z - pj.z, L, inv_L);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 < rc2 && r2 > 1e-10f && !((skip >> jj) & 1u))
+            lj_ref_pair(__ldg(&lj[ti * ntypes + __float_as_int(pj.w)]), dx, dy, dz, r2, fx, fy, fz, pe, v);
+        }
+      }
+    }
+    if (live) force[i] = make_float4(fx, fy, fz, pe);
+  }
+  for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
+  if (lane == 0)
+    for (int c = 0; c < 6; ++c) sm[w][c] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    float s = 0;
+    for (int k = 0; k < kTileWarps; ++k) s += sm[k][threadIdx.x];
+    atomicAdd(&virial[threadIdx.x], s);
+  }
 }
 
 struct TileScratch {
@@ -573,6 +657,23 @@ FMD_API fmd_status fmd_launch_tile_list(const void* pos, int32_t natoms, float b
       FMD_CUDA(cudaStreamSynchronize(st));
       if (*npairs > capacity) throw Error(FMD_ERR_OVERFLOW, "tile pairs exceed the capacity");
     }
+  });
+}
+
+FMD_API fmd_status fmd_launch_lj_tiles(const void* pos, void* force, float* virial, const void* lj_params,
+                                       const int32_t* tile_offsets, const int32_t* tile_neighbors,
+                                       const int32_t* exclusion_offsets, const int32_t* exclusion_list,
+                                       int32_t natoms, int32_t ntypes, float rc2, float box_L, float inv_L,
+                                       void* stream) {
+  return guarded([&] {
+    if (!pos || !force || !virial || !lj_params || !tile_offsets || !tile_neighbors || natoms <= 0 || ntypes <= 0)
+      throw Error(FMD_ERR_ARG, "bad argument");
+    if (!exclusion_offsets != !exclusion_list) throw Error(FMD_ERR_ARG, "exclusion offsets and list go together");
+    const int T = (natoms + 31) / 32;
+    k_lj_tiles<<<div_up(T, kTileWarps), 32 * kTileWarps, 0, (cudaStream_t)stream>>>(
+        (const float4*)pos, (float4*)force, virial, (const float2*)lj_params, tile_offsets, tile_neighbors,
+        exclusion_offsets, exclusion_list, natoms, T, ntypes, rc2, box_L, inv_L);
+    FMD_CUDA_LAUNCH();
   });
 }
 

@@ -308,7 +308,7 @@ struct StepShape {
   int has_table;        // some replica has tabulated pairs: the table pass follows the forces
 };
 using RebuildShape = StepShape;
-constexpr int kForceVariants = 9;
+constexpr int kForceVariants = 13;
 constexpr int kNbrVariants = 3;
 // One step with direct launches.  The rebuild form is read back from the
 // device after the per-replica commits (one small host read per step).

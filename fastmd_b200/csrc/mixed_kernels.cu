@@ -829,6 +829,18 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// The same copy with L1 bypassed (streamed data), the commit of this
+// thread's copies issued so far as one group, and the wait until at most N
+// of its groups are still in flight.
+__device__ __forceinline__ void cp_async16_stream(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 constexpr int kNbrWarps = kNbrThreads / 32;
 constexpr int kNbrWin = 1024;     // staged candidates per window
@@ -1340,29 +1352,32 @@ __device__ __forceinline__ float3 entry_shift(uint32_t w, const float4* s_shift,
 // The LJ loop over one atom's list in batches of B entries: all list loads,
 // then all position gathers, then the arithmetic.  PF: the next batch's list
 // words are loaded before this batch's gathers (software pipelining, B more
-// registers).  nn is the padded length (a multiple of B).
-template <bool EV, int B, bool PF, int KB, bool ONE, int SH, bool P2>
+// registers).  nn is the padded length (a multiple of B).  LPA lanes per
+// atom: this lane walks the batches starting at entry k0 = (its lane group)
+// * B, every LPA-th batch.
+template <bool EV, int B, bool PF, int KB, bool ONE, int SH, bool P2, int LPA = 1>
 __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float4* pbase, float4 pi,
                                         const float4* s_shift, const float* s_axis, int ti, int nt,
                                         const float* s_eps24, const float* s_sig2, float rc2, KahanF& fx, KahanF& fy,
-                                        KahanF& fz, PairAcc& acc) {
+                                        KahanF& fz, PairAcc& acc, int k0 = 0) {
+  constexpr int STEP = B * LPA;
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
   uint32_t wn[B];
   if (PF) {
 #pragma unroll
-    for (int q = 0; q < B; ++q) wn[q] = nn > 0 ? __ldg(lst + (size_t)q * 32) : 0u;
+    for (int q = 0; q < B; ++q) wn[q] = nn > k0 ? __ldg(lst + (size_t)(k0 + q) * 32) : 0u;
   }
   // plain sums over KB batches (KB * B <= 8 pairs), then one compensated add
   PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
   int kb = 0;
-  for (int k = 0; k < nn; k += B) {
+  for (int k = k0; k < nn; k += STEP) {
     uint32_t w[B];
     if (PF) {
 #pragma unroll
       for (int q = 0; q < B; ++q) w[q] = wn[q];
-      if (k + B < nn) {
+      if (k + STEP < nn) {
 #pragma unroll
-        for (int q = 0; q < B; ++q) wn[q] = __ldg(lst + (size_t)(k + B + q) * 32);
+        for (int q = 0; q < B; ++q) wn[q] = __ldg(lst + (size_t)(k + STEP + q) * 32);
       }
     } else {
 #pragma unroll
@@ -1388,7 +1403,7 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
         lj_pair<EV>(g, pi, entry_shift<SH>(w[q], s_shift, s_axis), pj[q], rc2, e24, sig2);
       }
     }
-    if (++kb == KB || k + B >= nn) {
+    if (++kb == KB || k + STEP >= nn) {
       fx.add(g.fx);
       fy.add(g.fy);
       fz.add(g.fz);
@@ -1396,6 +1411,83 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
       kb = 0;
     }
   }
+  acc.pe = g.pe;
+  acc.v0 = g.v0;
+  acc.v1 = g.v1;
+  acc.v2 = g.v2;
+  acc.v3 = g.v3;
+  acc.v4 = g.v4;
+  acc.v5 = g.v5;
+}
+
+// The LJ loop with the list rows staged through a shared-memory ring of D
+// batches per warp.  A warp's 32 atoms share one 32-slot tile of the
+// transposed list, whose rows (128 bytes: entry k of the 32 atoms) are
+// contiguous, so a batch of 4 rows (512 bytes) is fetched by one 16-byte
+// asynchronous copy per lane (L1 bypassed), D - 1 batches ahead of its use,
+// without registers held for it; each lane then reads its own words from
+// shared memory.  The warp walks its longest list (nmax, warp-uniform): a
+// lane's entries past its own length nn read as its padding entry and its
+// compensated adds stop at nn, so the forces are bitwise those of lj_loop
+// with B = 4 and the same KB, SH and P2.
+template <bool EV, int KB, bool ONE, int SH, bool P2, int D>
+__device__ __forceinline__ void lj_loop_ring(const uint32_t* tile_rows, uint32_t* ring, int lane, int nn, int nmax,
+                                             uint32_t pad, const float4* pbase, float4 pi, const float4* s_shift,
+                                             const float* s_axis, int ti, int nt, const float* s_eps24,
+                                             const float* s_sig2, float rc2, KahanF& fx, KahanF& fy, KahanF& fz,
+                                             PairAcc& acc) {
+  constexpr int B = 4;
+  constexpr int W = B * 32;  // words per batch
+  const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
+  const int nb = nmax / B;
+#pragma unroll
+  for (int b = 0; b < D - 1; ++b) {
+    if (b < nb) cp_async16_stream(ring + (b % D) * W + lane * 4, tile_rows + (size_t)b * W + lane * 4);
+    cp_async_commit();
+  }
+  PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
+  int kb = 0;
+  for (int b = 0; b < nb; ++b) {
+    __syncwarp();  // every lane is done with the slot refilled here
+    const int bn = b + D - 1;
+    if (bn < nb) cp_async16_stream(ring + (bn % D) * W + lane * 4, tile_rows + (size_t)bn * W + lane * 4);
+    cp_async_commit();
+    cp_async_wait_group<D - 1>();  // this lane's part of batch b has landed
+    __syncwarp();                  // and every other lane's
+    const uint32_t* slot = ring + (b % D) * W;
+    const int k = b * B;
+    uint32_t w[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) w[q] = k + q < nn ? slot[q * 32 + lane] : pad;
+    float4 pj[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+    if (P2 && ONE && !EV) {
+#pragma unroll
+      for (int q = 0; q < B; q += 2)
+        lj_pair2(g, pi, entry_shift<SH>(w[q], s_shift, s_axis), pj[q], entry_shift<SH>(w[q + 1], s_shift, s_axis),
+                 pj[q + 1], rc2, e24_0, sig2_0);
+    } else {
+#pragma unroll
+      for (int q = 0; q < B; ++q) {
+        float e24 = e24_0, sig2 = sig2_0;
+        if (!ONE) {
+          const int pidx = ti * nt + w_type(w_bits(pj[q].w));
+          e24 = s_eps24[pidx];
+          sig2 = s_sig2[pidx];
+        }
+        lj_pair<EV>(g, pi, entry_shift<SH>(w[q], s_shift, s_axis), pj[q], rc2, e24, sig2);
+      }
+    }
+    if (k < nn && (++kb == KB || k + B >= nn)) {
+      fx.add(g.fx);
+      fy.add(g.fy);
+      fz.add(g.fz);
+      g.fx = g.fy = g.fz = 0.0f;
+      kb = 0;
+    }
+  }
+  cp_async_wait_group<0>();
   acc.pe = g.pe;
   acc.v0 = g.v0;
   acc.v1 = g.v1;
@@ -1538,8 +1630,75 @@ __device__ __forceinline__ void angle_term(float4 ri, float4 rj, float4 rk, int 
 // LISTED: the work-list launch itself (replicas rebuilt or re-filtered this
 // step), which walks the rc + skin list and, where the replica keeps a
 // pruned list, writes it (the filter) and its displacement reference.
-template <bool EV, int B, bool PF, int KB, bool LISTED, int SH, bool P2>
+// Bonded terms of the atom in slot s, gathered: its bonds and angles
+// first, first + stride, ... (lanes that share an atom split them; one lane
+// per atom takes all with first = 0, stride = 1).
+template <bool EV>
+__device__ __forceinline__ void bonded_terms(const Dev& d, const Rep& R, int s, const float4* pbase, float4 pi, int G,
+                                             float h, float inv_h, float dL, int first, int stride, KahanF& fx,
+                                             KahanF& fy, KahanF& fz, float& pe, float* bv, int& status) {
+  const int tc = d.tcnt[s];
+  const int nbd = tc & 0xFF, nang = tc >> 8;
+  // FENE + WCA (fene.cu:18-73), gathered: this atom's force; the bond's
+  // energy is split half per atom and its virial carried by the first atom.
+  const uint32_t* bl = d.bnd + (size_t)s * kMaxBondsPerAtom;
+  for (int b = first; b < nbd; b += stride) {
+    const uint32_t bw = bl[b];
+    const int bt = (bw >> 26) & 0xF;
+    const float4 pj = pbase[bw & kSlotMask26];
+    const float3 dr = bonded_dr(pi, pj, G, h, inv_h, dL);
+    const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+    const float kf = R.fene[4 * bt], R02 = R.fene[4 * bt + 1], eps = R.fene[4 * bt + 2], sig2 = R.fene[4 * bt + 3];
+    if (r2 >= R02 * 0.9999f) status |= kStatusFeneStretch;
+    const float r2s = fminf(fmaxf(r2, 1e-6f), R02 * 0.9999f);
+    float ff = -kf * R02 * __fdividef(1.0f, R02 - r2s);
+    float wpe = 0.0f;
+    if (r2s < sig2 * 1.2599210498948732f) {
+      const float r2inv = __fdividef(1.0f, r2s);
+      const float sr2 = sig2 * r2inv;
+      const float sr6 = sr2 * sr2 * sr2;
+      ff = fmaf(24.0f * eps * r2inv * sr6, 2.0f * sr6 - 1.0f, ff);
+      if (EV) wpe = 4.0f * eps * sr6 * (sr6 - 1.0f) + eps;
+    }
+    fx.add(__fmul_rn(ff, dr.x));
+    fy.add(__fmul_rn(ff, dr.y));
+    fz.add(__fmul_rn(ff, dr.z));
+    if (EV) {
+      pe += 0.5f * (-0.5f * kf * R02 * log1pf(-r2s / R02) + wpe);
+      if ((bw >> 30) & 1) {
+        bv[0] = fmaf(ff * dr.x, dr.x, bv[0]);
+        bv[1] = fmaf(ff * dr.x, dr.y, bv[1]);
+        bv[2] = fmaf(ff * dr.x, dr.z, bv[2]);
+        bv[3] = fmaf(ff * dr.y, dr.y, bv[3]);
+        bv[4] = fmaf(ff * dr.y, dr.z, bv[4]);
+        bv[5] = fmaf(ff * dr.z, dr.z, bv[5]);
+      }
+    }
+  }
+  // Harmonic angles this atom belongs to, by role.
+  const uint2* al = d.ang + (size_t)s * kMaxAnglesPerAtom;
+  for (int a = first; a < nang; a += stride) {
+    const uint2 aw = al[a];
+    const int role = (aw.x >> 26) & 3, at = (aw.y >> 26) & 0xF;
+    const float4 p1 = pbase[aw.x & kSlotMask26];
+    const float4 p2 = pbase[aw.y & kSlotMask26];
+    const float kt = R.angp[2 * at], th0 = R.angp[2 * at + 1];
+    // members in angle order (i, j = vertex, k); the table holds the other two
+    const float4 ri = role == 0 ? pi : p1;
+    const float4 rj = role == 1 ? pi : (role == 0 ? p1 : p2);
+    const float4 rk = role == 2 ? pi : p2;
+    angle_term<EV>(ri, rj, rk, role, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
+  }
+}
+
+// PF: 0 = list words loaded with the batch, 1 = the next batch's words
+// loaded ahead into registers, D >= 2 = the ring of D batches (per-chunk
+// kernel; the work-list kernel then loads ahead into registers).
+template <bool EV, int B, int PF, int KB, bool LISTED, int SH, bool P2>
 __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_rebuilt) {
+  constexpr bool RING = PF >= 2 && !LISTED;
+  constexpr bool PFR = PF != 0;  // register look-ahead in the loops below
+  static_assert(!RING || B == 4, "the ring stages batches of 4 rows");
   const int4 ci = d.chunk_rep[chunk];
   const int r = ci.x;
   if (r < 0) return;
@@ -1575,12 +1734,35 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
   const float rc2 = (float)(R.rc * R.rc);
   double vals[7] = {0, 0, 0, 0, 0, 0, 0};
   int status = 0;
+  KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
+  PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if constexpr (RING) {
+    // the whole warp walks its tile's lists (lanes past natoms with none)
+    __shared__ __align__(16) uint32_t s_ring[(kChunk / 32) * (RING ? PF : 1) * 4 * 32];
+    const bool valid = local < R.natoms;
+    const float4 pi = valid ? d.pos[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int ti = w_type(w_bits(pi.w));
+    const bool keeps = R.prune_delta > 0.f;
+    const int nn = !valid ? 0
+                   : keeps ? (d.pcnt[s] + kPrunePad - 1) & ~(kPrunePad - 1)
+                           : (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
+    const int nmax = __reduce_max_sync(0xffffffffu, nn);
+    const uint32_t* tile_rows = (keeps ? d.pnbr : d.nbr) + (size_t)R.nbr_base + (size_t)(local >> 5) * R.M * 32;
+    uint32_t* ring = s_ring + (threadIdx.x >> 5) * (PF * 4 * 32);
+    const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
+    if (nt == 1)
+      lj_loop_ring<EV, KB, true, SH, P2, (RING ? PF : 2)>(tile_rows, ring, threadIdx.x & 31, nn, nmax, pad,
+                                                          d.pos + base, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2,
+                                                          rc2, fx, fy, fz, acc);
+    else
+      lj_loop_ring<EV, KB, false, SH, P2, (RING ? PF : 2)>(tile_rows, ring, threadIdx.x & 31, nn, nmax, pad,
+                                                           d.pos + base, pi, s_shift, s_axis, ti, nt, s_eps24,
+                                                           s_sig2, rc2, fx, fy, fz, acc);
+  }
   if (local < R.natoms) {
     const float4 pi = d.pos[s];
     const uint32_t ui = w_bits(pi.w);
     const int ti = w_type(ui);
-    KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
-    PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     static_assert(kListPad % B == 0 && kPrunePad % B == 0, "list padding must cover whole batches");
     // the pruned list when the replica keeps one (same layout and bases)
     const bool keeps = R.prune_delta > 0.f;
@@ -1589,25 +1771,27 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     const int nn = pruned ? (d.pcnt[s] + kPrunePad - 1) & ~(kPrunePad - 1) : (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
     const uint32_t* lst = (pruned ? d.pnbr : d.nbr) + row;
     const float4* pbase = d.pos + base;
-    if (LISTED && keeps) {
+    if (RING) {
+      // the LJ sums are in already
+    } else if (LISTED && keeps) {
       const float rcd = (float)(R.rc + (double)R.prune_delta);
       const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
-      const int pc = nt == 1 ? lj_loop_filter<EV, B, PF, KB, true, SH>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi,
-                                                                        s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2,
-                                                                        fx, fy, fz, acc, pad)
-                             : lj_loop_filter<EV, B, PF, KB, false, SH>(lst, nn, d.pnbr + row, rcd * rcd, pbase, pi,
-                                                                         s_shift, s_axis, ti, nt, s_eps24, s_sig2,
-                                                                         rc2, fx, fy, fz, acc, pad);
+      const int pc = nt == 1 ? lj_loop_filter<EV, B, PFR, KB, true, SH>(lst, nn, d.pnbr + row, rcd * rcd, pbase,
+                                                                         pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2,
+                                                                         rc2, fx, fy, fz, acc, pad)
+                             : lj_loop_filter<EV, B, PFR, KB, false, SH>(lst, nn, d.pnbr + row, rcd * rcd, pbase,
+                                                                          pi, s_shift, s_axis, ti, nt, s_eps24,
+                                                                          s_sig2, rc2, fx, fy, fz, acc, pad);
       d.pcnt[s] = pc;
       const float4 q = d.ref[s];
       d.ref[s] = make_float4(pi.x, pi.y, pi.z, q.w);
     } else if (nt == 1) {
       // one type (the Kremer-Grest melt): the pair parameters are loop constants
-      lj_loop<EV, B, PF, KB, true, SH, P2>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2, fx,
-                                            fy, fz, acc);
-    } else {
-      lj_loop<EV, B, PF, KB, false, SH, P2>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2, fx,
+      lj_loop<EV, B, PFR, KB, true, SH, P2>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2, fx,
                                              fy, fz, acc);
+    } else {
+      lj_loop<EV, B, PFR, KB, false, SH, P2>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2, fx,
+                                              fy, fz, acc);
     }
     float pe = acc.pe;
     // LJ virial: 1/2 f (x) r per half pair (lj.cu:56-61).
@@ -1626,58 +1810,7 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
       fy = {ly, 0.0f};
       fz = {lz, 0.0f};
     }
-    const int tc = d.tcnt[s];
-    const int nbd = tc & 0xFF, nang = tc >> 8;
-    // FENE + WCA (fene.cu:18-73), gathered: this atom's force; the bond's
-    // energy is split half per atom and its virial carried by the first atom.
-    const uint32_t* bl = d.bnd + (size_t)s * kMaxBondsPerAtom;
-    for (int b = 0; b < nbd; ++b) {
-      const uint32_t bw = bl[b];
-      const int bt = (bw >> 26) & 0xF;
-      const float4 pj = pbase[bw & kSlotMask26];
-      const float3 dr = bonded_dr(pi, pj, G, h, inv_h, dL);
-      const float r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
-      const float kf = R.fene[4 * bt], R02 = R.fene[4 * bt + 1], eps = R.fene[4 * bt + 2], sig2 = R.fene[4 * bt + 3];
-      if (r2 >= R02 * 0.9999f) status |= kStatusFeneStretch;
-      const float r2s = fminf(fmaxf(r2, 1e-6f), R02 * 0.9999f);
-      float ff = -kf * R02 * __fdividef(1.0f, R02 - r2s);
-      float wpe = 0.0f;
-      if (r2s < sig2 * 1.2599210498948732f) {
-        const float r2inv = __fdividef(1.0f, r2s);
-        const float sr2 = sig2 * r2inv;
-        const float sr6 = sr2 * sr2 * sr2;
-        ff = fmaf(24.0f * eps * r2inv * sr6, 2.0f * sr6 - 1.0f, ff);
-        if (EV) wpe = 4.0f * eps * sr6 * (sr6 - 1.0f) + eps;
-      }
-      fx.add(__fmul_rn(ff, dr.x));
-      fy.add(__fmul_rn(ff, dr.y));
-      fz.add(__fmul_rn(ff, dr.z));
-      if (EV) {
-        pe += 0.5f * (-0.5f * kf * R02 * log1pf(-r2s / R02) + wpe);
-        if ((bw >> 30) & 1) {
-          bv[0] = fmaf(ff * dr.x, dr.x, bv[0]);
-          bv[1] = fmaf(ff * dr.x, dr.y, bv[1]);
-          bv[2] = fmaf(ff * dr.x, dr.z, bv[2]);
-          bv[3] = fmaf(ff * dr.y, dr.y, bv[3]);
-          bv[4] = fmaf(ff * dr.y, dr.z, bv[4]);
-          bv[5] = fmaf(ff * dr.z, dr.z, bv[5]);
-        }
-      }
-    }
-    // Harmonic angles this atom belongs to, by role.
-    const uint2* al = d.ang + (size_t)s * kMaxAnglesPerAtom;
-    for (int a = 0; a < nang; ++a) {
-      const uint2 aw = al[a];
-      const int role = (aw.x >> 26) & 3, at = (aw.y >> 26) & 0xF;
-      const float4 p1 = pbase[aw.x & kSlotMask26];
-      const float4 p2 = pbase[aw.y & kSlotMask26];
-      const float kt = R.angp[2 * at], th0 = R.angp[2 * at + 1];
-      // members in angle order (i, j = vertex, k); the table holds the other two
-      const float4 ri = role == 0 ? pi : p1;
-      const float4 rj = role == 1 ? pi : (role == 0 ? p1 : p2);
-      const float4 rk = role == 2 ? pi : p2;
-      angle_term<EV>(ri, rj, rk, role, kt, th0, G, h, inv_h, dL, fx, fy, fz, pe, bv);
-    }
+    bonded_terms<EV>(d, R, s, pbase, pi, G, h, inv_h, dL, 0, 1, fx, fy, fz, pe, bv, status);
     const float ox = fx.s - fx.c, oy = fy.s - fy.c, oz = fz.s - fz.c;
     if (!isfinite(ox + oy + oz + pe)) status |= kStatusNonFinite;
     d.force[s] = make_float4(ox, oy, oz, pe);
@@ -1691,17 +1824,199 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
   if (EV) block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
 }
 
+// The list filter alone: the entries of the atom's rc + skin list (nn
+// padded entries) within rc + prune_delta, in list order, padded to whole
+// force batches; returns their count.  The filter test rounds as pair_r2.
+template <int SH>
+__device__ __forceinline__ int filter_list(const uint32_t* lst, int nn, uint32_t* pout, float rcd2,
+                                           const float4* pbase, float4 pi, const float4* s_shift, const float* s_axis,
+                                           uint32_t pad) {
+  int pc = 0;
+  for (int k = 0; k < nn; k += kListPad) {
+    uint32_t w[kListPad];
+    float4 pj[kListPad];
+#pragma unroll
+    for (int q = 0; q < kListPad; ++q) w[q] = __ldg(lst + (size_t)(k + q) * 32);
+#pragma unroll
+    for (int q = 0; q < kListPad; ++q) pj[q] = __ldg(pbase + (w[q] & kIdxMask));
+#pragma unroll
+    for (int q = 0; q < kListPad; ++q) {
+      float dx, dy, dz;
+      if (pair_r2(pi, entry_shift<SH>(w[q], s_shift, s_axis), pj[q], dx, dy, dz) < rcd2)
+        pout[(size_t)(pc++) * 32] = w[q];
+    }
+  }
+  const int padded = (pc + kPrunePad - 1) & ~(kPrunePad - 1);
+  for (int k = pc; k < padded; ++k) pout[(size_t)k * 32] = pad;
+  return pc;
+}
+
+// Compensated sums of the lanes that share an atom (lane group g = lane /
+// APW, APW = 32 / LPA atoms per warp), combined into group 0's lane by a
+// shuffle tree in a fixed order: each step adds the partner's sum and then
+// its compensation.
+template <int LPA>
+__device__ __forceinline__ void lanes_combine(KahanF& k) {
+#pragma unroll
+  for (int off = 16; off >= 32 / LPA; off >>= 1) {
+    const float ps = __shfl_down_sync(0xffffffffu, k.s, off);
+    const float pc = __shfl_down_sync(0xffffffffu, k.c, off);
+    k.add(ps);
+    k.add(-pc);
+  }
+}
+template <int LPA>
+__device__ __forceinline__ void lanes_sum(float& v) {
+#pragma unroll
+  for (int off = 16; off >= 32 / LPA; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+}
+
+// Lanes per atom (LPA = 2 or 4): LPA lanes of a warp share one atom, 32 / LPA
+// atoms per warp with an atom's lanes 32 / LPA apart, and the chunk's atoms
+// are taken in LPA passes of 128 / LPA.  Lane group g walks the list batches
+// g, g + LPA, ... (a load of one batch row reads 32 / LPA neighboring atoms'
+// words: whole 32-byte sectors for LPA <= 4), then its share of the bonded
+// terms; the groups' compensated sums are combined in group 0.  A replica
+// whose pruned list is due (LISTED) first has it filtered, one thread per
+// atom, and the lanes then walk the new pruned list as the per-chunk kernel
+// will at the next steps, so a re-evaluation reproduces the forces.
+template <bool EV, int B, bool PF, int KB, bool LISTED, int SH, bool P2, int LPA>
+__device__ __forceinline__ void force_chunk_lanes(const Dev& d, int chunk, bool skip_rebuilt) {
+  static_assert(LPA == 2 || LPA == 4, "two or four lanes per atom");
+  constexpr int APW = 32 / LPA;
+  const int4 ci = d.chunk_rep[chunk];
+  const int r = ci.x;
+  if (r < 0) return;
+  const Rep& R = d.reps[r];
+  if (!R.adv) return;
+  if (need_ev(R) != EV) return;
+  if (skip_rebuilt && R.rebuild_now) return;
+  __shared__ float4 s_shift[SH == 0 ? kShiftCodes : 1];
+  __shared__ float s_axis[5];
+  __shared__ float s_eps24[kMaxTypes * kMaxTypes], s_sig2[kMaxTypes * kMaxTypes];
+  const int nt = R.ntypes;
+  const int G = R.G;
+  const float h = R.h, inv_h = 1.0f / h;
+  const float dL = (float)(R.L - (double)G * (double)h);
+  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
+    s_eps24[k] = R.lj_eps24[k];
+    s_sig2[k] = R.lj_sig2[k];
+  }
+  if (SH == 0 && threadIdx.x < kShiftCodes) {
+    const int c = threadIdx.x;
+    const int ax = c / 25, ay = (c / 5) % 5, az = c % 5;
+    s_shift[c] = make_float4(shift_term(axis_code_e(ax), axis_code_k(ax), h, dL),
+                             shift_term(axis_code_e(ay), axis_code_k(ay), h, dL),
+                             shift_term(axis_code_e(az), axis_code_k(az), h, dL), 0.0f);
+  }
+  if (SH == 1 && threadIdx.x < 5)
+    s_axis[threadIdx.x] = shift_term(axis_code_e(threadIdx.x), axis_code_k(threadIdx.x), h, dL);
+  __syncthreads();
+  const int base = R.slot_base;
+  const float4* pbase = d.pos + base;
+  const bool keeps = R.prune_delta > 0.f;
+  if (LISTED && keeps) {
+    const int local = ci.w * kChunk + threadIdx.x;
+    if (local < R.natoms) {
+      const int s = ci.y + threadIdx.x;
+      const float4 pi = d.pos[s];
+      const float rcd = (float)(R.rc + (double)R.prune_delta);
+      const size_t row = (size_t)R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+      const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
+      const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
+      d.pcnt[s] = filter_list<SH>(d.nbr + row, nn, d.pnbr + row, rcd * rcd, pbase, pi, s_shift, s_axis, pad);
+      const float4 q = d.ref[s];
+      d.ref[s] = make_float4(pi.x, pi.y, pi.z, q.w);
+    }
+    __syncthreads();  // the block's pruned lists are written
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane / APW;
+  const float rc2 = (float)(R.rc * R.rc);
+  double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+  int status = 0;
+  static_assert(kListPad % B == 0 && kPrunePad % B == 0, "list padding must cover whole batches");
+#pragma unroll 1
+  for (int pass = 0; pass < LPA; ++pass) {
+    const int at = pass * (kChunk / LPA) + warp * APW + lane % APW;
+    const int local = ci.w * kChunk + at;
+    const int s = ci.y + at;
+    const bool valid = local < R.natoms;
+    KahanF fx = {0, 0}, fy = {0, 0}, fz = {0, 0};
+    PairAcc acc = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+      pi = d.pos[s];
+      const int ti = w_type(w_bits(pi.w));
+      const size_t row = (size_t)R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
+      const int nn = keeps ? (d.pcnt[s] + kPrunePad - 1) & ~(kPrunePad - 1)
+                           : (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
+      const uint32_t* lst = (keeps ? d.pnbr : d.nbr) + row;
+      if (nt == 1)
+        lj_loop<EV, B, PF, KB, true, SH, P2, LPA>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2, rc2,
+                                                  fx, fy, fz, acc, g * B);
+      else
+        lj_loop<EV, B, PF, KB, false, SH, P2, LPA>(lst, nn, pbase, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2,
+                                                   rc2, fx, fy, fz, acc, g * B);
+    }
+    if (R.fcap > 0.0) {  // push-off caps the non-bonded force total (replica-uniform branch)
+      lanes_combine<LPA>(fx);
+      lanes_combine<LPA>(fy);
+      lanes_combine<LPA>(fz);
+      float lx = fx.s - fx.c, ly = fy.s - fy.c, lz = fz.s - fz.c;
+      const float m2 = lx * lx + ly * ly + lz * lz;
+      const float cap = (float)R.fcap;
+      if (m2 > cap * cap) {
+        const float sc = cap * rsqrtf(m2);
+        lx *= sc;
+        ly *= sc;
+        lz *= sc;
+      }
+      const bool own = g == 0;
+      fx = {own ? lx : 0.0f, 0.0f};
+      fy = {own ? ly : 0.0f, 0.0f};
+      fz = {own ? lz : 0.0f, 0.0f};
+    }
+    float pe = acc.pe;
+    float bv[6] = {0.5f * acc.v0, 0.5f * acc.v1, 0.5f * acc.v2, 0.5f * acc.v3, 0.5f * acc.v4, 0.5f * acc.v5};
+    if (valid) bonded_terms<EV>(d, R, s, pbase, pi, G, h, inv_h, dL, g, LPA, fx, fy, fz, pe, bv, status);
+    lanes_combine<LPA>(fx);
+    lanes_combine<LPA>(fy);
+    lanes_combine<LPA>(fz);
+    if (EV) {
+      lanes_sum<LPA>(pe);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) lanes_sum<LPA>(bv[c]);
+    }
+    if (valid && g == 0) {
+      const float ox = fx.s - fx.c, oy = fy.s - fy.c, oz = fz.s - fz.c;
+      if (!isfinite(ox + oy + oz + pe)) status |= kStatusNonFinite;
+      d.force[s] = make_float4(ox, oy, oz, pe);
+      if (EV) {
+        vals[0] += pe;
+        for (int c = 0; c < 6; ++c) vals[1 + c] += bv[c];
+      }
+    }
+  }
+  status = __syncthreads_or(status);
+  if (threadIdx.x == 0 && status) atomicOr((int*)&d.reps[r].status, status);
+  if (EV) block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
+}
+
 // One block per chunk of the batch.
-template <bool EV, int B, int MINB, bool PF, int KB, int SH, bool P2>
+template <bool EV, int B, int MINB, int PF, int KB, int SH, bool P2, int LPA>
 __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt) {
   count_launch(d, EV ? kKForceEv : kKForce);
-  force_chunk<EV, B, PF, KB, false, SH, P2>(d, blockIdx.x, skip_rebuilt != 0);
+  if constexpr (LPA == 1)
+    force_chunk<EV, B, PF, KB, false, SH, P2>(d, blockIdx.x, skip_rebuilt != 0);
+  else
+    force_chunk_lanes<EV, B, (PF != 0), KB, false, SH, P2, LPA>(d, blockIdx.x, skip_rebuilt != 0);
 }
 
 // The chunks of the replicas on the rebuild work list (a resident grid
 // striding over them), launched after their rebuild while the other
 // replicas' forces run beside it; it also writes their pruned lists.
-template <bool EV, int B, int MINB, bool PF, int KB, int SH, bool P2>
+template <bool EV, int B, int MINB, int PF, int KB, int SH, bool P2, int LPA>
 __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
   count_launch(d, EV ? kKForceEv : kKForce);
   const int n = rb_count(d);
@@ -1712,7 +2027,10 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force_rb(Dev d) {
     cur.seek(item);
     __syncthreads();  // the previous item's shared tables are no longer read
     const Rep& R = d.reps[rb_rep(d, cur.i)];
-    force_chunk<EV, B, PF, KB, true, SH, P2>(d, R.chunk_base + (item - cur.lo), false);
+    if constexpr (LPA == 1)
+      force_chunk<EV, B, PF, KB, true, SH, P2>(d, R.chunk_base + (item - cur.lo), false);
+    else
+      force_chunk_lanes<EV, B, (PF != 0), KB, true, SH, P2, LPA>(d, R.chunk_base + (item - cur.lo), false);
   }
 }
 
@@ -2375,23 +2693,27 @@ constexpr int kForceCarveoutPct = 16;  // percent of the SM's shared-memory maxi
 // Parameters: list entries per batch, blocks per SM, next batch's list words
 // loaded ahead, batches per compensated add, shift lookup (0: 125-entry 3D
 // table, 1: per-axis 5-value table), pairs evaluated two at a time in packed
-// FP32x2 arithmetic.
+// FP32x2 arithmetic, lanes per atom.
 template <bool EV>
 void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(Dev)) {
   constexpr int E = 5;  // blocks per SM of the energy flavours (more registers)
-#define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2)          \
-  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2>; \
-  *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB, SH, P2>;
+#define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2, LPA)          \
+  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>; \
+  *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>;
   switch (variant) {
-    case 1: FMD_FORCE_VARIANT(4, 8, true, 2, 0, false) break;
-    case 2: FMD_FORCE_VARIANT(4, 8, true, 1, 1, false) break;
-    case 3: FMD_FORCE_VARIANT(4, 8, true, 2, 1, false) break;
-    case 4: FMD_FORCE_VARIANT(4, 8, true, 1, 1, true) break;
-    case 5: FMD_FORCE_VARIANT(4, 8, true, 2, 1, true) break;
-    case 6: FMD_FORCE_VARIANT(4, 7, true, 1, 1, true) break;
-    case 7: FMD_FORCE_VARIANT(4, 9, true, 1, 1, true) break;
-    case 8: FMD_FORCE_VARIANT(4, 6, true, 1, 1, false) break;
-    default: FMD_FORCE_VARIANT(4, 8, true, 1, 0, false) break;
+    case 1: FMD_FORCE_VARIANT(4, 8, true, 2, 0, false, 1) break;
+    case 2: FMD_FORCE_VARIANT(4, 8, true, 1, 1, false, 1) break;
+    case 3: FMD_FORCE_VARIANT(4, 8, true, 2, 1, false, 1) break;
+    case 4: FMD_FORCE_VARIANT(4, 8, true, 1, 1, true, 1) break;
+    case 5: FMD_FORCE_VARIANT(4, 8, true, 2, 1, true, 1) break;
+    case 6: FMD_FORCE_VARIANT(4, 7, true, 1, 1, true, 1) break;
+    case 7: FMD_FORCE_VARIANT(4, 9, true, 1, 1, true, 1) break;
+    case 8: FMD_FORCE_VARIANT(4, 6, true, 1, 1, false, 1) break;
+    case 9: FMD_FORCE_VARIANT(4, 8, true, 1, 1, true, 2) break;
+    case 10: FMD_FORCE_VARIANT(4, 8, true, 1, 1, true, 4) break;
+    case 11: FMD_FORCE_VARIANT(4, 8, 3, 1, 1, true, 1) break;
+    case 12: FMD_FORCE_VARIANT(4, 8, 4, 1, 1, true, 1) break;
+    default: FMD_FORCE_VARIANT(4, 8, true, 1, 0, false, 1) break;
   }
 #undef FMD_FORCE_VARIANT
 }
@@ -2400,9 +2722,13 @@ void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(De
 // smallest shared-memory carve-out, leaving the rest of the SM's unified
 // L1 / shared array to cache the neighbor-position gathers.
 template <typename K>
-void prefer_l1(K kernel) {
-  FMD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, kForceCarveoutPct));
+void prefer_l1(K kernel, int pct = kForceCarveoutPct) {
+  FMD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
 }
+
+// The ring variants hold 6-8 KB of list rows per block: a carve-out that
+// keeps 8 of their blocks resident.
+inline int force_carveout_pct(int variant) { return variant == 11 || variant == 12 ? 40 : kForceCarveoutPct; }
 
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st, bool skip_rebuilt) {
   void (*per_chunk)(Dev, int) = nullptr;
@@ -2412,7 +2738,7 @@ void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t 
   static bool set[2][kForceVariants] = {};
   bool& done = set[ev ? 1 : 0][variant >= 0 && variant < kForceVariants ? variant : 0];
   if (!done) {
-    prefer_l1(per_chunk);
+    prefer_l1(per_chunk, force_carveout_pct(variant));
     prefer_l1(listed);
     done = true;
   }

@@ -508,6 +508,20 @@ FMD_API fmd_status fmd_tile_list_scratch_bytes(int32_t natoms, size_t* bytes);
 FMD_API fmd_status fmd_launch_tile_list(const void* pos, int32_t natoms, float box_L, float rc_skin,
                                         int32_t* offsets, int32_t* neighbors, int32_t capacity, int32_t* npairs,
                                         void* scratch, size_t scratch_bytes, void* stream);
+/* LJ over a tile list (offsets / neighbors as fmd_launch_tile_list writes
+ * them, built at rc or beyond), a warp per 32-atom tile with each partner
+ * tile staged in shared memory: a consumer of TileList's tile pairs
+ * (neighbor/tile_list.cuh:3-23), which the reference defines but none of
+ * its force kernels walks.  The same outputs and pair arithmetic as fmd_launch_lj
+ * (force[i] = (F, pe_i) overwritten, virial[6] accumulated); the pairs are
+ * every (i, j != i) within rc2 (minimum image) of the listed tile pairs,
+ * less the exclusions: exclusion_offsets[natoms + 1] / exclusion_list in the
+ * form fmd_launch_verlet_build_static takes (both NULL: none). */
+FMD_API fmd_status fmd_launch_lj_tiles(const void* pos, void* force, float* virial, const void* lj_params,
+                                       const int32_t* tile_offsets, const int32_t* tile_neighbors,
+                                       const int32_t* exclusion_offsets, const int32_t* exclusion_list,
+                                       int32_t natoms, int32_t ntypes, float rc2, float box_L, float inv_L,
+                                       void* stream);
 /* 30-bit Morton sort of pos and vel, replacing MortonSorter::sort_and_permute
  * (core/morton.cuh:17-18; morton.cu:65-85); the permutation is bit-exact with
  * a stable sort of (key, index).  perm (device, [padded natoms]) receives the

@@ -788,6 +788,13 @@ struct orc_sim {
   double vir[6];
   double L, V0, Q1, Qr, W;
   double xi[10], vxi[10], eps, veps, carry, nh_scale;
+  // Work of the kinetic barostat term the reference's NPT equations leave out
+  // (Martyna-Tuckerman-Klein: d v_eps / dt gains (3 / N_f) 2 KE): with the
+  // particle velocities scaled by exp(-(1 + 3 / N_f) v_eps / W dt / 2) but
+  // no such term in the barostat force, the extended energy changes at
+  // -(3 / N_f) (v_eps / W) 2 KE; this sums that rate over the steps taken,
+  // for diagnostics only (orc_sim_conserved_mtk).
+  double mtk_work = 0.0;
   int64_t step;
   int64_t rebuilds;
   int32_t since;
@@ -965,6 +972,7 @@ struct orc_sim {
       V = V0 * std::exp(3.0 * eps);
       L = std::cbrt(V);
       const double vW = veps / W;
+      mtk_work += 3.0 * Nf_inv * vW * dt * 2.0 * total_KE;
       const double bscale = std::exp(-(1.0 + 3.0 * Nf_inv) * vW * hdt);
       double KE = total_KE * bscale * bscale;
       double sc;
@@ -1106,6 +1114,11 @@ double orc_sim_conserved(const orc_sim* s) {
   }
   return e;
 }
+
+// The NPT extended energy plus the summed work of the missing kinetic
+// barostat term: constant to the integrator's order if that term is the
+// only gap between the equations of motion and the extended energy.
+double orc_sim_conserved_mtk(const orc_sim* s) { return orc_sim_conserved(s) + s->mtk_work; }
 
 void orc_sim_destroy(orc_sim* s) { delete s; }
 

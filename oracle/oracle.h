@@ -124,6 +124,7 @@ void orc_sim_thermo(const orc_sim* s, double* out9);
 double orc_sim_rg(const orc_sim* s);
 /* Extended energy: KE + PE + chain + barostat (+ P V for NPT), per atom. */
 double orc_sim_conserved(const orc_sim* s);
+double orc_sim_conserved_mtk(const orc_sim* s);
 void orc_sim_destroy(orc_sim* s);
 
 #ifdef __cplusplus

@@ -95,6 +95,8 @@ def lib():
         L.orc_sim_rg.restype = C.c_double
         L.orc_sim_rg.argtypes = [C.c_void_p]
         L.orc_sim_conserved.restype = C.c_double
+        L.orc_sim_conserved_mtk.restype = C.c_double
+        L.orc_sim_conserved_mtk.argtypes = [C.c_void_p]
         L.orc_sim_conserved.argtypes = [C.c_void_p]
         L.orc_sim_destroy.argtypes = [C.c_void_p]
         _LIB = L
@@ -331,6 +333,11 @@ class Sim:
 
     def conserved(self):
         return lib().orc_sim_conserved(self._h)
+
+    def conserved_mtk(self):
+        """NPT extended energy plus the summed work of the kinetic barostat
+        term the reference's equations omit (a diagnostic)."""
+        return lib().orc_sim_conserved_mtk(self._h)
 
     def __del__(self):
         try:

@@ -228,3 +228,100 @@ def test_tile_list_launcher_reports_overflow():
     d = fm.generate_melt(30, 100, density=0.85, seed=3)
     st, off, nbr, npairs = tile_list(_pos4(_compact(d.xyz, d.box_L)), d.box_L, 2.8, cap=10)
     assert st == 5 and npairs > 10 and len(nbr) == 10   # FMD_ERR_OVERFLOW, the first 10 written
+
+
+def _compact_order(xyz, L, bits=10):
+    """The permutation _compact applies."""
+    q = np.clip((xyz / L * (1 << bits)).astype(np.int64), 0, (1 << bits) - 1)
+    key = np.zeros(len(xyz), np.int64)
+    for b in range(bits):
+        for d in range(3):
+            key |= ((q[:, d] >> b) & 1) << (3 * b + d)
+    return np.argsort(key, kind="stable")
+
+
+def lj_tiles(p4, L, rc, off, nbr, excl=None):
+    torch = _torch()
+    lib = fm.lib()
+    n = len(p4)
+    pos = torch.from_numpy(np.ascontiguousarray(p4, np.float32)).cuda()
+    toff = torch.from_numpy(np.ascontiguousarray(off, np.int32)).cuda()
+    tnbr = torch.from_numpy(np.ascontiguousarray(nbr, np.int32)).cuda()
+    force = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6, dtype=torch.float32, device="cuda")
+    lj = torch.tensor([1.0, 1.0], dtype=torch.float32, device="cuda")
+    eo = el = None
+    if excl is not None:
+        eo = torch.from_numpy(excl[0]).cuda()
+        el = torch.from_numpy(excl[1]).cuda()
+    lib.fmd_launch_lj_tiles.restype = C.c_int32
+    st = lib.fmd_launch_lj_tiles(C.c_void_p(pos.data_ptr()), C.c_void_p(force.data_ptr()),
+                                 C.c_void_p(vir.data_ptr()), C.c_void_p(lj.data_ptr()), C.c_void_p(toff.data_ptr()),
+                                 C.c_void_p(tnbr.data_ptr()), C.c_void_p(eo.data_ptr() if eo is not None else None),
+                                 C.c_void_p(el.data_ptr() if el is not None else None), C.c_int32(n), C.c_int32(1),
+                                 C.c_float(rc * rc), C.c_float(L), C.c_float(1.0 / L), None)
+    assert st == 0
+    return force.cpu().numpy(), vir.cpu().numpy()
+
+
+def lj_verlet(p4, L, rc, rcs, bonds=None):
+    torch = _torch()
+    lib = fm.lib()
+    n = len(p4)
+    pos, nbr, cnt, flag = verlet(p4[:, :3], L, rcs, bonds=bonds)
+    assert int(flag.item()) == 0
+    force = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    vir = torch.zeros(6, dtype=torch.float32, device="cuda")
+    lj = torch.tensor([1.0, 1.0], dtype=torch.float32, device="cuda")
+    lib.fmd_launch_lj.restype = C.c_int32
+    st = lib.fmd_launch_lj(C.c_void_p(pos.data_ptr()), C.c_void_p(force.data_ptr()), C.c_void_p(vir.data_ptr()),
+                           C.c_void_p(lj.data_ptr()), C.c_void_p(nbr.data_ptr()), C.c_void_p(cnt.data_ptr()),
+                           C.c_int32(n), C.c_int32(1), C.c_float(rc * rc), C.c_float(L), C.c_float(1.0 / L), None)
+    assert st == 0
+    return force.cpu().numpy(), vir.cpu().numpy()
+
+
+@pytest.mark.parametrize("case", ["lj64", "melt3000"])
+def test_lj_tiles_launcher_matches_oracle_and_verlet_lj(case):
+    """The warp-per-tile LJ over the tile list against the FP64 oracle and
+    the Verlet-list LJ launcher on the same positions: the same pairs and
+    pair arithmetic, only the summation order differs."""
+    from oracle import pyoracle as po
+    if case == "lj64":
+        xyz, L, bonds = G["lj64_pos"].astype(np.float64), 8.0, None
+    else:
+        d = fm.generate_melt(30, 100, density=0.85, seed=3)
+        order = _compact_order(d.xyz, d.box_L)
+        rank = np.empty_like(order)
+        rank[order] = np.arange(len(order))
+        xyz, L = d.xyz[order], d.box_L
+        bonds = rank[np.asarray(d.bonds).reshape(-1, 2)]
+    n = len(xyz)
+    p4 = _pos4(xyz)
+    rc = 2.5
+    st, off, nbr, _ = tile_list(p4, L, rc)
+    assert st == 0
+    excl = _excl(n, bonds) if bonds is not None else None
+    ft, vt = lj_tiles(p4, L, rc, off, nbr, excl)
+    fv, vv = lj_verlet(p4, L, rc, 2.8, bonds=bonds)
+    assert rel_rms(ft[:, :3], fv[:, :3]) < 1e-6
+    assert abs(ft[:, 3].sum() - fv[:, 3].sum()) < 1e-5 * abs(fv[:, 3]).sum()
+    assert np.max(np.abs(vt - vv)) < 1e-4 * np.max(np.abs(vv))
+    osys = po.System(xyz=xyz, L=L, type=np.zeros(n, np.int32), mass=np.ones(1), lj=np.ones((1, 1, 2)), skin=0.3,
+                     lj_clamp=1, bonds=bonds if bonds is not None else np.zeros((0, 2), np.int32))
+    fo, peo, vo = po.forces(osys, "lj")
+    assert rel_rms(ft[:, :3], fo) < 1e-5
+    assert abs(ft[:, 3].sum() - peo.sum()) < 1e-5 * abs(peo).sum()
+
+
+def test_lj_tiles_launcher_rejects_half_exclusions():
+    torch = _torch()
+    lib = fm.lib()
+    pos = torch.zeros((32, 4), dtype=torch.float32, device="cuda")
+    off = torch.zeros(2, dtype=torch.int32, device="cuda")
+    lib.fmd_launch_lj_tiles.restype = C.c_int32
+    st = lib.fmd_launch_lj_tiles(C.c_void_p(pos.data_ptr()), C.c_void_p(pos.data_ptr()), C.c_void_p(pos.data_ptr()),
+                                 C.c_void_p(pos.data_ptr()), C.c_void_p(off.data_ptr()), C.c_void_p(off.data_ptr()),
+                                 C.c_void_p(off.data_ptr()), None, C.c_int32(32), C.c_int32(1), C.c_float(6.25),
+                                 C.c_float(8.0), C.c_float(0.125), None)
+    assert st == 1   # FMD_ERR_ARG, nothing launched

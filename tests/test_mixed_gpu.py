@@ -210,17 +210,23 @@ def test_observing_does_not_perturb(ens):
     b.close()
 
 
-def test_observing_every_step_does_not_perturb():
+@pytest.mark.parametrize("fv", [-1, 9, 10, 11])
+def test_observing_every_step_does_not_perturb(fv):
     """Forces read after every step, so also right after the steps whose
     work-list force launch rebuilt or re-filtered the pruned list while
     evaluating the forces: the re-evaluation over the pruned list it wrote
     reproduces those forces bit for bit, and the trajectory stays identical
-    to an unobserved one."""
+    to an unobserved one.  fv: the default force variant, the two
+    lanes-per-atom variants (which filter first, then walk the new list) and
+    a shared-memory ring variant (whose work-list kernel loads ahead into
+    registers instead)."""
     conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 9", nsteps=10_000)
     m = _melt(15, 40, seed=33)
     a = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    a.set_variants(fv, -1)
     sa = a.add(conf, desc=m)
     b = fm.Batch(max_replicas=2, max_atoms=1 << 13)
+    b.set_variants(fv, -1)
     sb = b.add(conf, desc=m)
     for _ in range(150):
         a.run(1)
