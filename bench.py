@@ -816,10 +816,14 @@ def wl_drift(args, fm):
     (two types as C2, npt_nh T = 1 Tdamp = 0.1, P = 0 Pdamp = 1, chain 3) at
     dt, and the plain FP64 form on two NVT replicas for comparison."""
     lj2 = ((0, 0, 1.0, 1.0), (1, 1, 1.0, 1.0), (0, 1, 0.9, 1.0))
+    npt = "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3"
     cases = [("nvt", "nvt_nh 1.0 1.0 0.5 3", 1, ((0, 0, 1.0, 1.0),), 0, 0.001),
              ("nvt", "nvt_nh 1.0 1.0 0.5 3", 1, ((0, 0, 1.0, 1.0),), 0, 0.0005),
-             ("npt", "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3", 2, lj2, 50, 0.001),
-             ("npt", "npt_nh 1.0 1.0 0.1 0.0 0.0 1.0 3", 2, lj2, 50, 0.0005)]
+             ("npt", npt, 2, lj2, 50, 0.001),
+             ("npt", npt, 2, lj2, 50, 0.0005),
+             # the same with the chain's upper accelerations carried between half steps
+             ("nptc", npt + "\nnh_chain_carry 1", 2, lj2, 50, 0.001),
+             ("nptc", npt + "\nnh_chain_carry 1", 2, lj2, 50, 0.0005)]
     wanted = set(args.drift_cases.split(","))
     cases = [c for c in cases if f"{c[0]}{c[5]}" in wanted or c[0] in wanted]
     out = {"workload": "nh_drift_batched", "replicas": args.drift_reps, "beads_per_replica": NCHAINS * CHAIN_LEN,
@@ -843,7 +847,7 @@ def wl_drift(args, fm):
         nrun = int(args.drift_run * 0.001 / dt)
         every = max(1, nrun // 100)
         e = np.zeros((nrun // every, len(slots)))
-        nshift = min(args.drift_shift_check, len(slots)) if name == "npt" else 0
+        nshift = min(args.drift_shift_check, len(slots)) if name.startswith("npt") else 0
         es = np.zeros((nrun // every, nshift))
         vol = np.zeros((nrun // every, len(slots)))
         for k in range(nrun // every):
@@ -855,10 +859,10 @@ def wl_drift(args, fm):
                 es[k, j] = e[k, j] + cutoff_jump_energy(*b.force_frame(slots[j]), lj, tb) / (NCHAINS * CHAIN_LEN)
         t = np.arange(1, nrun // every + 1) * float(every)
         rel = slopes(e, t) * 1e6
-        row = {"ensemble": ens, "dt": dt, "steps": nrun, "relative_per_1e6_steps": float(rel.mean()),
+        row = {"ensemble": ens.replace("\n", "; "), "dt": dt, "steps": nrun, "relative_per_1e6_steps": float(rel.mean()),
                "stderr": float(rel.std(ddof=1) / np.sqrt(len(rel))), "per_replica": rel.tolist(),
                "relative_per_tau": float(rel.mean() / (1e6 * dt))}
-        if name == "npt":
+        if name.startswith("npt"):
             vrel = slopes(vol, t) * 1e6
             row["volume_relative_per_1e6_steps"] = {"mean": float(vrel.mean()),
                                                     "stderr": float(vrel.std(ddof=1) / np.sqrt(len(vrel)))}
@@ -883,7 +887,7 @@ def wl_drift(args, fm):
                     th = ps.thermo()
                     ee.append(th.conserved)
                     vv.append(th.box_L ** 3)
-                    if name == "npt":
+                    if name.startswith("npt"):
                         es_.append(th.conserved + cutoff_jump_energy(ps.state()[0], th.box_L, lj, tb)
                                    / (NCHAINS * CHAIN_LEN))
                 ps.close()
@@ -894,7 +898,7 @@ def wl_drift(args, fm):
             row["plain_fp64"] = {"relative_per_1e6_steps": prel.tolist(), "replicas": len(pl),
                                  "volume_relative_per_1e6_steps": (slopes(np.array(plv).T, t) * 1e6).tolist(),
                                  "note": "from the mixed replicas' relaxed states"}
-            if name == "npt":
+            if name.startswith("npt"):
                 row["plain_fp64"]["with_shifted_lj_energy"] = (slopes(np.array(pls).T, t) * 1e6).tolist()
         b.close()
         out["cases"].append(row)
@@ -1075,7 +1079,8 @@ def main():
     ap.add_argument("--c1-stat-steps", type=int, default=20_000, help="c1: steps of the <T>, <P>, Rg comparison")
     ap.add_argument("--npt-equil", type=int, default=20_000, help="npt_drift: relaxation steps at P = 0")
     ap.add_argument("--drift-reps", type=int, default=16, help="drift: replicas per case")
-    ap.add_argument("--drift-cases", default="nvt,npt", help="drift: nvt, npt, or nvt0.001 / npt0.0005 ...")
+    ap.add_argument("--drift-cases", default="nvt,npt,nptc",
+                    help="drift: nvt, npt, nptc (NPT, chain accelerations carried), or nvt0.001 / npt0.0005 ...")
     ap.add_argument("--drift-plain", type=int, default=2, help="drift: plain FP64 replicas at dt = 0.001")
     ap.add_argument("--drift-shift-check", type=int, default=4,
                     help="drift: NPT replicas whose extended energy is also reported with the LJ shifted at rc")

@@ -284,6 +284,7 @@ static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
   R.ntypes = cfg.ntypes;
   R.ensemble = cfg.ensemble;
   R.chain_M = cfg.chain_length;
+  R.chain_carry = cfg.nh_chain_carry;
   R.max_between = 20;  // main.cu:401
   R.thermo_freq = cfg.thermo_on ? cfg.thermo_freq : 0;
   R.stress_freq = cfg.stress_on ? cfg.stress_freq : 0;
@@ -370,6 +371,7 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   R.nh.L = L;
   R.nh.inv_L = 1.0 / L;
   R.nh.V = L * L * L;
+  R.nh.carry_dd = R.chain_carry;
   R.pending_scale = 1.0;
   R.defer = 0;
   R.force_ev = 0;
@@ -1140,6 +1142,7 @@ void put_nh(StateFile& s, const NHScalars& nh) {
   s.put("nh_vxi", std::vector<double>(nh.vxi, nh.vxi + 10));
   s.put("nh_scalars", {nh.eps, nh.veps, nh.carry, nh.scale, nh.L, nh.inv_L, nh.V, nh.bscale, nh.exp_vW, nh.vWdt,
                        nh.fpos, nh.ke_raw, nh.vir_tr});
+  s.put("nh_dd", std::vector<double>(nh.dd, nh.dd + 10));
 }
 void get_nh(const StateFile& s, NHScalars& nh) {
   const auto& xi = s.get("nh_xi");
@@ -1163,6 +1166,11 @@ void get_nh(const StateFile& s, NHScalars& nh) {
   nh.fpos = c[10];
   nh.ke_raw = c[11];
   nh.vir_tr = c[12];
+  if (s.has("nh_dd")) {
+    const auto& dd = s.get("nh_dd");
+    if (dd.size() != 10) throw Error(FMD_ERR_IO, "bad chain state in sidecar");
+    for (int k = 0; k < 10; ++k) nh.dd[k] = dd[k];
+  }
 }
 }  // namespace
 

@@ -49,6 +49,9 @@ struct RunConfig {
   double T_start = 0, T_stop = 0, Tdamp = 0;
   double P_start = 0, P_stop = 0, Pdamp = 0;
   int32_t chain_length = 3;
+  // nh_chain_carry 1: the chain's upper accelerations carried between half
+  // steps (LAMMPS fix nh); 0, the default, is the reference's scheme.
+  int32_t nh_chain_carry = 0;
   uint64_t seed = 0;  // SimParams is zero-initialized; nvt_langevin defaults it to 42 (config.cpp:11, 79-81)
   std::string data_file, coords_file, forces_dump_file;
   std::vector<double> lj;                   // [ntypes*ntypes*2] (eps, sig)

@@ -139,6 +139,9 @@ RunConfig parse_run_conf(const std::string& text) {
       c.ensemble = FMD_NPT_NH;
       iss >> c.T_start >> c.T_stop >> c.Tdamp >> c.P_start >> c.P_stop >> c.Pdamp;
       if (!(iss >> c.chain_length)) c.chain_length = 3;
+    } else if (key == "nh_chain_carry") {
+      iss >> c.nh_chain_carry;
+      if (c.nh_chain_carry != 0 && c.nh_chain_carry != 1) bad("nh_chain_carry must be 0 or 1");
     } else if (key == "coords_file") iss >> c.coords_file;
     else if (key == "lammps_data_file") iss >> c.data_file;
     else if (key == "lj") {

@@ -104,6 +104,7 @@ struct Rep {
   int32_t ntypes;
   int32_t ensemble;
   int32_t chain_M;
+  int32_t chain_carry;           // run.conf nh_chain_carry: chain accelerations kept between half steps
   int32_t max_between;           // forced rebuild cadence (steps; kNoForcedRebuild: skin trigger only)
   int64_t nsteps;                // run.conf nsteps (ramp denominator)
   uint64_t seed;

@@ -74,7 +74,8 @@ __device__ __noinline__ void compute_step_scalars(const Rep& R, StepScalars& S) 
     S.c2kT = (float)(sqrt(1.0 - c1 * c1) * sqrt(kT));
   } else if (S.ens == FMD_NVT_NH) {
     const double kT = ramp(R, S.step, R.T0, R.T1);
-    const double sc = nhc_half_step(S.nh.xi, S.nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, S.nh.carry, 0.5 * dt);
+    const double sc = nhc_half_step(S.nh.xi, S.nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, S.nh.carry, 0.5 * dt,
+                                    S.nh.carry_dd ? S.nh.dd : nullptr);
     S.nh.scale = sc;
     S.vscale = (float)(R.pending_scale * sc);
   } else {
@@ -2334,7 +2335,8 @@ __global__ void __launch_bounds__(32) k_post_commit(Dev d, int kick) {
       } else if (ens == FMD_NVT_NH) {
         const double kT = ramp(R, R.step, R.T0, R.T1);
         const double ke = 0.5 * ke_raw;
-        const double sc = nhc_half_step(R.nh.xi, R.nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, ke, 0.5 * dt);
+        const double sc = nhc_half_step(R.nh.xi, R.nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, ke, 0.5 * dt,
+                                        R.nh.carry_dd ? R.nh.dd : nullptr);
         R.nh.scale = sc;
         R.nh.carry = ke * sc * sc;
         R.pending_scale = sc;

@@ -26,6 +26,12 @@ struct NHScalars {
   double fpos;       // dt exp(x) sinh(x)/x, x = vWdt/2
   double ke_raw;     // sum m v^2 of the last reduction
   double vir_tr;     // virial trace of the last reduction
+  // Opt-in (run.conf nh_chain_carry 1): the chain's upper accelerations
+  // carried from one half step to the next, as LAMMPS's fix nh keeps its
+  // eta_dotdot; 0 follows the reference, which starts every half step from
+  // zero (nose_hoover.cu:101, :251, :369).
+  int32_t carry_dd;
+  double dd[10];
 };
 
 FMD_HD double nh_exp6(double x) {
@@ -41,13 +47,20 @@ FMD_HD double nh_exp6(double x) {
 }
 
 // One chain half step of length half_dt against total kinetic energy
-// total_KE (= 0.5 sum m v^2); returns the velocity scale.
+// total_KE (= 0.5 sum m v^2); returns the velocity scale.  dd_keep: NULL
+// for the reference's scheme, whose downward sweep drives the upper chain
+// elements with zero accelerations (the array is reset every half step);
+// otherwise the accelerations of the previous half step's upward sweep are
+// read from it and this half step's are stored back (LAMMPS's eta_dotdot).
+// The reset makes the chain update irreversible to first order in dt: with
+// Tdamp = 100 dt the extended energy of a 600-bead melt gains about 1.5 kT
+// per tau in NVT; carried, it stays flat.
 FMD_HD double nhc_half_step(double* xi, double* vxi, int M, double Q1, double Qr, double kT, int natoms,
-                            double total_KE, double half_dt) {
+                            double total_KE, double half_dt, double* dd_keep = nullptr) {
   const double Nf = FMD_DMUL(3.0, (double)natoms);
   const double dt2 = half_dt, dt4 = FMD_DMUL(half_dt, 0.5), dt8 = FMD_DMUL(half_dt, 0.25);
   double dd[10];
-  for (int k = 0; k < 10; ++k) dd[k] = 0.0;
+  for (int k = 0; k < 10; ++k) dd[k] = (dd_keep && k > 0) ? dd_keep[k] : 0.0;
   double T = FMD_DDIV(FMD_DMUL(2.0, total_KE), Nf);
   if (Q1 > 0.0) dd[0] = FMD_DDIV(FMD_DSUB(FMD_DMUL(Nf, T), FMD_DMUL(Nf, kT)), Q1);
   const double ncfac = 1.0;
@@ -76,6 +89,8 @@ FMD_HD double nhc_half_step(double* xi, double* vxi, int M, double Q1, double Qr
     vxi[ich] = FMD_DADD(vxi[ich], FMD_DMUL(FMD_DMUL(dd[ich], ncfac), dt4));
     vxi[ich] = FMD_DMUL(vxi[ich], ef);
   }
+  if (dd_keep)
+    for (int k = 1; k < 10; ++k) dd_keep[k] = dd[k];
   return fe;
 }
 
@@ -116,7 +131,7 @@ FMD_HD void npt_chain_baro(NHScalars& s, bool pre_force, double total_KE_raw, do
   const double hx = 0.5 * s.vWdt;
   const double sinhc = (hx < 1e-6 && hx > -1e-6) ? 1.0 + hx * hx / 6.0 : sh(hx) / hx;
   s.fpos = dt * ex(hx) * sinhc;
-  s.scale = nhc_half_step(s.xi, s.vxi, M, Q1, Qr, kT, natoms, KE, half_dt);
+  s.scale = nhc_half_step(s.xi, s.vxi, M, Q1, Qr, kT, natoms, KE, half_dt, s.carry_dd ? s.dd : nullptr);
   if (!pre_force) s.carry = KE * s.scale * s.scale;
 }
 

@@ -228,7 +228,7 @@ __global__ void k_nvt_chain(NHScalars* st, const double* ke_raw, int pre_force, 
                             double kT, double hdt, int natoms) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double ke = pre_force ? st->carry : (*ke_raw) * 0.5;
-  const double sc = nhc_half_step(st->xi, st->vxi, M, Q1, Qr, kT, natoms, ke, hdt);
+  const double sc = nhc_half_step(st->xi, st->vxi, M, Q1, Qr, kT, natoms, ke, hdt, st->carry_dd ? st->dd : nullptr);
   st->scale = sc;
   if (!pre_force) st->carry = ke * sc * sc;
 }
@@ -694,6 +694,7 @@ class PlainEngine final : public SimEngine {
       s.L = L_;
       s.inv_L = 1.0 / L_;
       s.V = V0_;
+      s.carry_dd = cfg_.nh_chain_carry;
       FMD_CUDA(cudaMemcpy(nh_, &s, sizeof(s), cudaMemcpyHostToDevice));
     }
     setup_forces();
@@ -803,6 +804,7 @@ class PlainEngine final : public SimEngine {
     s.put("nh_vxi", std::vector<double>(nh.vxi, nh.vxi + 10));
     s.put("nh_scalars", {nh.eps, nh.veps, nh.carry, nh.scale, nh.L, nh.inv_L, nh.V, nh.bscale, nh.exp_vW, nh.vWdt,
                          nh.fpos, nh.ke_raw, nh.vir_tr});
+    s.put("nh_dd", std::vector<double>(nh.dd, nh.dd + 10));
     restore(t, s);
   }
 
@@ -837,6 +839,11 @@ class PlainEngine final : public SimEngine {
     nh.fpos = c[10];
     nh.ke_raw = c[11];
     nh.vir_tr = c[12];
+    if (s.has("nh_dd")) {
+      const auto& dd = s.get("nh_dd");
+      if (dd.size() != 10) throw Error(FMD_ERR_IO, "bad chain state in sidecar");
+      for (int k = 0; k < 10; ++k) nh.dd[k] = dd[k];
+    }
     FMD_CUDA(cudaMemcpy(nh_, &nh, sizeof(nh), cudaMemcpyHostToDevice));
   }
 

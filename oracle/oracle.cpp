@@ -479,11 +479,17 @@ double nh_exp6(double x) {
          x6 * (1.0 / 720.0);
 }
 
+// dd_keep: NULL for the reference's scheme (every half step starts its
+// upper-chain accelerations from zero, nose_hoover.cu:101, :251, :369); otherwise
+// they are read from it and stored back, as LAMMPS's fix nh keeps
+// eta_dotdot between calls (the run.conf nh_chain_carry option).
 void nhc_half(double* xi, double* vxi, int M, double Q1, double Qr, double kT, int natoms,
-              double total_KE, double half_dt, double* scale_out) {
+              double total_KE, double half_dt, double* scale_out, double* dd_keep = nullptr) {
   const double Nf = 3.0 * (double)natoms;
   const double dt2 = half_dt, dt4 = half_dt * 0.5, dt8 = half_dt * 0.25;
   double dd[10] = {0};
+  if (dd_keep)
+    for (int k = 1; k < 10; ++k) dd[k] = dd_keep[k];
   double T = (2.0 * total_KE) / Nf;
   if (Q1 > 0.0) dd[0] = (Nf * T - Nf * kT) / Q1;
   const double ncfac = 1.0;
@@ -513,6 +519,8 @@ void nhc_half(double* xi, double* vxi, int M, double Q1, double Qr, double kT, i
     vxi[ich] += dd[ich] * ncfac * dt4;
     vxi[ich] *= ef;
   }
+  if (dd_keep)
+    for (int k = 1; k < 10; ++k) dd_keep[k] = dd[k];
 }
 
 void set_threads(int n) {
@@ -788,6 +796,7 @@ struct orc_sim {
   double vir[6];
   double L, V0, Q1, Qr, W;
   double xi[10], vxi[10], eps, veps, carry, nh_scale;
+  double dd[10] = {0};  // carried chain accelerations (run.chain_carry)
   // Work of the kinetic barostat term the reference's NPT equations leave out
   // (Martyna-Tuckerman-Klein: d v_eps / dt gains (3 / N_f) 2 KE): with the
   // particle velocities scaled by exp(-(1 + 3 / N_f) v_eps / W dt / 2) but
@@ -877,7 +886,7 @@ struct orc_sim {
       // main.cu:452-481 -> nose_hoover.cu:86-178 (carry) and :606-664.
       const double kT = ramp(run.T_start, run.T_stop);
       double sc;
-      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, carry, hdt, &sc);
+      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, carry, hdt, &sc, run.chain_carry ? dd : nullptr);
       nh_scale = sc;
       for (int32_t i = 0; i < n; ++i) {
         const double hm = hdt / mass[type[i]];
@@ -901,7 +910,7 @@ struct orc_sim {
       const double exp_vW = std::exp(vW * dt);
       const double vWdt = vW * dt;
       double sc;
-      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, KE, hdt, &sc);
+      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, KE, hdt, &sc, run.chain_carry ? dd : nullptr);
       nh_scale = sc;
       const double hx = 0.5 * vWdt;
       const double sinhc = (std::fabs(hx) < 1e-6) ? 1.0 + hx * hx / 6.0 : std::sinh(hx) / hx;
@@ -942,7 +951,7 @@ struct orc_sim {
       }
       const double KE = ke_raw() * 0.5;
       double sc;
-      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, KE, hdt, &sc);
+      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, KE, hdt, &sc, run.chain_carry ? dd : nullptr);
       nh_scale = sc;
       carry = KE * sc * sc;
       for (int32_t i = 0; i < 3 * n; ++i) v[i] *= sc;
@@ -976,7 +985,7 @@ struct orc_sim {
       const double bscale = std::exp(-(1.0 + 3.0 * Nf_inv) * vW * hdt);
       double KE = total_KE * bscale * bscale;
       double sc;
-      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, KE, hdt, &sc);
+      nhc_half(xi, vxi, run.chain_length, Q1, Qr, kT, n, KE, hdt, &sc, run.chain_carry ? dd : nullptr);
       nh_scale = sc;
       carry = KE * sc * sc;
       for (int32_t i = 0; i < 3 * n; ++i) v[i] = (v[i] * bscale) * sc;

@@ -59,6 +59,7 @@ typedef struct orc_run {
   int32_t max_steps_between_rebuilds; /* 20 in main.cu:401 */
   double force_cap;         /* > 0: cap |F_i| (push-off); 0: off */
   int32_t nthreads;         /* OpenMP threads (0: default) */
+  int32_t chain_carry;      /* 1: chain accelerations kept between half steps (LAMMPS); 0: the reference */
 } orc_run;
 
 typedef struct orc_sim orc_sim;

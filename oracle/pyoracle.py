@@ -42,7 +42,7 @@ class OrcRun(C.Structure):
         ("P_start", C.c_double), ("P_stop", C.c_double), ("Pdamp", C.c_double),
         ("chain_length", C.c_int32), ("seed", C.c_uint64), ("nsteps", C.c_int64),
         ("max_steps_between_rebuilds", C.c_int32), ("force_cap", C.c_double),
-        ("nthreads", C.c_int32),
+        ("nthreads", C.c_int32), ("chain_carry", C.c_int32),
     ]
 
 
@@ -276,7 +276,7 @@ class Sim:
     """FP64 whole-step simulation mirroring the reference's step loop."""
 
     def __init__(self, sysm: System, ensemble="langevin", dt=0.001, T=(1.0, 1.0, 1.0), P=(0.0, 0.0, 1.0),
-                 chain=3, seed=42, nsteps=1000, force_cap=0.0, nthreads=0, max_between=20):
+                 chain=3, seed=42, nsteps=1000, force_cap=0.0, nthreads=0, max_between=20, chain_carry=0):
         L = lib()
         self._s, self._keep = sysm.c_struct()
         r = OrcRun()
@@ -290,6 +290,7 @@ class Sim:
         r.max_steps_between_rebuilds = max_between
         r.force_cap = force_cap
         r.nthreads = nthreads
+        r.chain_carry = chain_carry
         self._r = r
         self.n = len(sysm.type)
         x = np.ascontiguousarray(sysm.xyz, dtype=np.float64).reshape(-1)

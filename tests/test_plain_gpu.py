@@ -87,3 +87,44 @@ def test_plain_thermo_rg_known_answers():
     d = fm.SystemDesc(xyz=xyz, box_L=10.0, type=np.zeros(3, np.int32), image=img, mol=np.ones(3, np.int32))
     sim = fm.Simulation(run_conf(bond=None, angle=None, rc=2.5), desc=d, form=fm.FMD_FORM_PLAIN_FP64)
     assert abs(sim.rg() - np.sqrt(8.0 / 3.0)) < 1e-12
+
+
+def _nh_kw(ens):
+    name = ens.split()[0]
+    a = [float(t) for t in ens.split()[1:]]
+    if name == "nvt_nh":
+        return dict(ensemble="nvt_nh", T=tuple(a[:3]), chain=int(a[3]))
+    return dict(ensemble="npt_nh", T=tuple(a[:3]), P=tuple(a[3:6]), chain=int(a[6]))
+
+
+@pytest.mark.parametrize("form", ["plain", "mixed"])
+@pytest.mark.parametrize("ens", ["nvt_nh 1.0 1.0 0.1 3", "npt_nh 1.0 1.0 0.1 0.5 0.5 1.0 3"])
+def test_chain_carry_follows_the_oracle(ens, form):
+    """run.conf nh_chain_carry 1 (chain accelerations carried between half
+    steps): after 100 steps at Tdamp = 100 dt the extended energy per atom is
+    the oracle's with the same option (plain form: to FP64 round-off; mixed:
+    much closer than the two schemes are to each other), and the two schemes
+    have parted."""
+    pre = fm.Simulation(run_conf(), gen=dict(nchains=20, chain_length=30, density=0.85, seed=11, pushoff_steps=2000),
+                        form=fm.FMD_FORM_MIXED)
+    d = _melt(20, 30, seed=11)
+    d.xyz, d.vel, d.image = pre.state()
+    pre.close()
+    n = len(d.type)
+    conf = run_conf(ensemble=ens, nsteps=1000, extra="nh_chain_carry 1")
+    sim = fm.Simulation(conf, desc=d, form=fm.FMD_FORM_PLAIN_FP64 if form == "plain" else fm.FMD_FORM_MIXED)
+    x0, v0, i0 = sim.state()
+    kw = _nh_kw(ens)
+    o1 = po.Sim(oracle_system(d, xyz=x0, vel=v0, image=i0), dt=0.001, nsteps=1000, chain_carry=1, **kw)
+    o0 = po.Sim(oracle_system(d, xyz=x0, vel=v0, image=i0), dt=0.001, nsteps=1000, chain_carry=0, **kw)
+    for _ in range(5):
+        sim.step(20)
+        o1.step(20)
+        o0.step(20)
+    e = sim.thermo().conserved
+    e1, e0 = o1.conserved() / n, o0.conserved() / n
+    assert abs(e1 - e0) > 1e-7 * abs(e1)
+    if form == "plain":
+        assert abs(e - e1) < 1e-10 * abs(e1)
+    else:
+        assert abs(e - e1) < 0.2 * abs(e1 - e0)
