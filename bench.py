@@ -307,7 +307,8 @@ GRAPH_CAPTURE_STEPS = 50  # one replay of a batch's default step graph
 # force-kernel variants, in the library's order (fastmd_b200/csrc/mixed_kernels.cu, force_kernels)
 FORCE_VARIANTS = ["m8 k1 t3", "m8 k2 t3", "m8 k1 a5", "m8 k2 a5", "m8 k1 a5 x2", "m8 k2 a5 x2", "m7 k1 a5 x2",
                   "m9 k1 a5 x2", "m6 k1 a5", "m8 k1 a5 x2 l2", "m8 k1 a5 x2 l4",
-                  "m8 k1 a5 x2 r3", "m8 k1 a5 x2 r4"]
+                  "m8 k1 a5 x2 r3", "m8 k1 a5 x2 r4", "m8 k1 a5 x2 r2", "m9 k1 a5 x2 r2",
+                  "m8 k1 a5 x2 sm"]
 
 
 def _dev_run(fm, b, nsteps):
@@ -545,9 +546,13 @@ def wl_tiles(args, fm):
     lib.fmd_tile_list_scratch_bytes(C.c_int32(n), C.byref(sb))
     tscr = torch.empty(sb.value, dtype=torch.uint8, device="cuda")
     toff = torch.zeros(T + 1, dtype=torch.int32, device="cuda")
-    cap = T * 64
-    tnbr = torch.zeros(cap, dtype=torch.int32, device="cuda")
     npairs = C.c_int32()
+    # count first (capacity 0: FMD_ERR_OVERFLOW with the count), then build
+    st = lib.fmd_launch_tile_list(ptr(pos), C.c_int32(n), Lf, C.c_float(rc), ptr(toff), None, C.c_int32(0),
+                                  C.byref(npairs), ptr(tscr), C.c_size_t(sb.value), None)
+    assert st in (0, 5), st
+    cap = max(1, npairs.value)
+    tnbr = torch.zeros(cap, dtype=torch.int32, device="cuda")
     assert lib.fmd_launch_tile_list(ptr(pos), C.c_int32(n), Lf, C.c_float(rc), ptr(toff), ptr(tnbr), C.c_int32(cap),
                                     C.byref(npairs), ptr(tscr), C.c_size_t(sb.value), None) == 0
     # Verlet list at rc + skin
@@ -1086,6 +1091,8 @@ def main():
                     help="drift: NPT replicas whose extended energy is also reported with the LJ shifted at rc")
     ap.add_argument("--drift-relax", type=int, default=20_000, help="drift: relaxation steps (at dt = 0.001)")
     ap.add_argument("--tiles-chains", type=int, default=300, help="tiles: chains of 100 beads in the melt")
+    ap.add_argument("--force-variant", type=int, default=-1,
+                    help="after the autotuner, pin this force-kernel variant (default: its pick)")
     ap.add_argument("--drift-run", type=int, default=200_000, help="drift: measured steps (at dt = 0.001)")
     ap.add_argument("--npt-time", type=float, default=20.0, help="npt_drift: simulated time per run (tau)")
     ap.add_argument("--serve-seconds", type=float, default=30.0, help="c4: arrival window")
@@ -1132,6 +1139,9 @@ def main():
     # warm-up, then the force-kernel autotuner on the live state
     b.run(args.warmup)
     variant, variant_ms = b.autotune(20)
+    if args.force_variant >= 0:  # a pinned variant (profiling one variant)
+        b.set_variants(args.force_variant, -1)
+        variant = args.force_variant
     # The autotuner's choices invalidate the step graph: replay one graph's
     # worth of steps untimed so that its capture (host work while the device
     # idles) is not inside the timed region.  The graph length divides the
@@ -1185,9 +1195,11 @@ def main():
                             "legend": "m = min blocks per SM, k = batches of 4 list entries per compensated add, "
                                       "t3 = shift from the 125-entry 3D table, a5 = per-axis 5-value table, "
                                       "x2 = pairs two at a time in packed FP32x2 arithmetic, l2 / l4 = two / "
-                                      "four lanes per atom (one otherwise), r3 / r4 = list rows staged through a "
-                                      "shared-memory ring 2 / 3 batches ahead by asynchronous copies (otherwise "
-                                      "the next batch's list words are loaded ahead into registers)"}
+                                      "four lanes per atom (one otherwise), r2 / r3 / r4 = list rows staged through "
+                                      "a shared-memory ring 1 / 2 / 3 batches ahead by asynchronous copies (otherwise "
+                                      "the next batch's list words are loaded ahead into registers), sm = a "
+                                      "resident grid taking chunks in SM-affine ranges (one block per chunk "
+                                      "otherwise)"}
         line["launches_by_kernel"] = launched
         line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
                                     "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0),

@@ -527,7 +527,8 @@ class Batch:
         """Pick the fastest force-kernel and neighbor-list variants on the
         current state and lift the forced rebuild cadence of the active
         replicas."""
-        ms = np.zeros(16)
+        nf, nn = self.variants()[2:4]
+        ms = np.zeros(nf + nn + 1)   # force variants, list variants, the chosen list variant
         v = C.c_int32()
         _call("fmd_batch_autotune", self._h, C.c_int32(iters), C.byref(v), _ptr(ms), C.c_int32(len(ms)))
         return v.value, ms

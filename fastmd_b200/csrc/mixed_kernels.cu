@@ -2004,14 +2004,62 @@ __device__ __forceinline__ void force_chunk_lanes(const Dev& d, int chunk, bool 
   if (EV) block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
 }
 
-// One block per chunk of the batch.
-template <bool EV, int B, int MINB, int PF, int KB, int SH, bool P2, int LPA>
+// One block per chunk of the batch (SCHED = 0).  SCHED = 1: a resident grid
+// whose blocks take chunks from a range of consecutive chunks assigned to
+// the SM they run on (%smid modulo the SM count), then help the ranges not
+// yet exhausted; the blocks resident on one SM so work on neighbouring
+// chunks, whose neighbour positions they share in that SM's L1.  Each chunk
+// is claimed once (atomic counters), so the forces are those of SCHED = 0.
+// The last block to finish clears the counters for the next launch.
+template <bool EV, int B, int MINB, int PF, int KB, int SH, bool P2, int LPA, int SCHED>
 __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt) {
   count_launch(d, EV ? kKForceEv : kKForce);
-  if constexpr (LPA == 1)
-    force_chunk<EV, B, PF, KB, false, SH, P2>(d, blockIdx.x, skip_rebuilt != 0);
-  else
-    force_chunk_lanes<EV, B, (PF != 0), KB, false, SH, P2, LPA>(d, blockIdx.x, skip_rebuilt != 0);
+  if constexpr (SCHED == 0) {
+    if constexpr (LPA == 1)
+      force_chunk<EV, B, PF, KB, false, SH, P2>(d, blockIdx.x, skip_rebuilt != 0);
+    else
+      force_chunk_lanes<EV, B, (PF != 0), KB, false, SH, P2, LPA>(d, blockIdx.x, skip_rebuilt != 0);
+  } else {
+    static_assert(LPA == 1, "SM-affine order with one lane per atom");
+    int* const sched = d.sched + (EV ? kSchedWords : 0);  // the flavours may run at once: a set each
+    __shared__ int s_claim;
+    unsigned sm;
+    asm("mov.u32 %0, %%smid;" : "=r"(sm));
+    const int nr = min(max(d.sched_ranges, 1), kSchedRanges);
+    const int n = d.sched_n;
+    const int q = (n + nr - 1) / nr;  // chunks per range
+    const int own = (int)(sm % (unsigned)nr);
+    for (int t = 0; t < nr; ++t) {
+      const int r = own + t < nr ? own + t : own + t - nr;
+      if (t > 0) {  // skip a range seen exhausted (read once, shared: the branch is block-uniform)
+        __syncthreads();
+        if (threadIdx.x == 0) s_claim = (__ldcg(sched + kSchedFlags + (r >> 5)) >> (r & 31)) & 1;
+        __syncthreads();
+        if (s_claim) continue;
+      }
+      for (;;) {
+        __syncthreads();  // the previous chunk's shared tables and s_claim are no longer read
+        if (threadIdx.x == 0) s_claim = atomicAdd(sched + r, 1);
+        __syncthreads();
+        const int chunk = r * q + s_claim;
+        if (s_claim >= q || chunk >= n) {
+          if (threadIdx.x == 0) atomicOr(sched + kSchedFlags + (r >> 5), 1 << (r & 31));
+          break;
+        }
+        force_chunk<EV, B, PF, KB, false, SH, P2>(d, chunk, skip_rebuilt != 0);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(sched + kSchedDone, 1) == (int)gridDim.x - 1) {
+        for (int k = 0; k < nr; ++k) sched[k] = 0;
+        for (int k = 0; k < kSchedRanges / 32; ++k) sched[kSchedFlags + k] = 0;
+        sched[kSchedDone] = 0;
+        __threadfence();
+      }
+    }
+  }
 }
 
 // The chunks of the replicas on the rebuild work list (a resident grid
@@ -2699,9 +2747,10 @@ constexpr int kForceCarveoutPct = 16;  // percent of the SM's shared-memory maxi
 template <bool EV>
 void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(Dev)) {
   constexpr int E = 5;  // blocks per SM of the energy flavours (more registers)
-#define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2, LPA)          \
-  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>; \
+#define FMD_FORCE_VARIANT_S(B, MINB, PF, KB, SH, P2, LPA, SCHED)          \
+  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA, SCHED>; \
   *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>;
+#define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2, LPA) FMD_FORCE_VARIANT_S(B, MINB, PF, KB, SH, P2, LPA, 0)
   switch (variant) {
     case 1: FMD_FORCE_VARIANT(4, 8, true, 2, 0, false, 1) break;
     case 2: FMD_FORCE_VARIANT(4, 8, true, 1, 1, false, 1) break;
@@ -2715,10 +2764,17 @@ void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(De
     case 10: FMD_FORCE_VARIANT(4, 8, true, 1, 1, true, 4) break;
     case 11: FMD_FORCE_VARIANT(4, 8, 3, 1, 1, true, 1) break;
     case 12: FMD_FORCE_VARIANT(4, 8, 4, 1, 1, true, 1) break;
+    case 13: FMD_FORCE_VARIANT(4, 8, 2, 1, 1, true, 1) break;
+    case 14: FMD_FORCE_VARIANT(4, 9, 2, 1, 1, true, 1) break;
+    case 15: FMD_FORCE_VARIANT_S(4, 8, 1, 1, 1, true, 1, 1) break;
     default: FMD_FORCE_VARIANT(4, 8, true, 1, 0, false, 1) break;
   }
 #undef FMD_FORCE_VARIANT
+#undef FMD_FORCE_VARIANT_S
 }
+
+// Variants whose per-chunk kernel is a resident grid in SM-affine order.
+inline bool force_variant_sched(int variant) { return variant == 15; }
 
 // The force kernels use 4 KB of shared memory per block: ask for the
 // smallest shared-memory carve-out, leaving the rest of the SM's unified
@@ -2728,9 +2784,11 @@ void prefer_l1(K kernel, int pct = kForceCarveoutPct) {
   FMD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
 }
 
-// The ring variants hold 6-8 KB of list rows per block: a carve-out that
-// keeps 8 of their blocks resident.
-inline int force_carveout_pct(int variant) { return variant == 11 || variant == 12 ? 40 : kForceCarveoutPct; }
+// The ring variants hold 4-8 KB of list rows per block besides the 2 KB of
+// tables: carve-outs that keep 8 (9) of their blocks resident.
+inline int force_carveout_pct(int variant) {
+  return variant == 11 || variant == 12 ? 40 : variant == 13 || variant == 14 ? 28 : kForceCarveoutPct;
+}
 
 void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t st, bool skip_rebuilt) {
   void (*per_chunk)(Dev, int) = nullptr;
@@ -2738,11 +2796,21 @@ void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t 
   if (ev) force_kernels<true>(variant, &per_chunk, &listed);
   else force_kernels<false>(variant, &per_chunk, &listed);
   static bool set[2][kForceVariants] = {};
-  bool& done = set[ev ? 1 : 0][variant >= 0 && variant < kForceVariants ? variant : 0];
+  static int grid[2][kForceVariants] = {};
+  const int v = variant >= 0 && variant < kForceVariants ? variant : 0;
+  bool& done = set[ev ? 1 : 0][v];
   if (!done) {
     prefer_l1(per_chunk, force_carveout_pct(variant));
     prefer_l1(listed);
+    if (force_variant_sched(v)) grid[ev ? 1 : 0][v] = resident_grid(per_chunk, kChunk);
     done = true;
+  }
+  if (force_variant_sched(v)) {
+    Dev ds = d;
+    ds.sched_n = nchunks;
+    ds.sched_ranges = num_sms();
+    per_chunk<<<std::min(nchunks, grid[ev ? 1 : 0][v]), kChunk, 0, st>>>(ds, skip_rebuilt ? 1 : 0);
+    return;
   }
   per_chunk<<<nchunks, kChunk, 0, st>>>(d, skip_rebuilt ? 1 : 0);
 }

@@ -210,7 +210,7 @@ def test_observing_does_not_perturb(ens):
     b.close()
 
 
-@pytest.mark.parametrize("fv", [-1, 9, 10, 11])
+@pytest.mark.parametrize("fv", [-1, 9, 10, 11, 15])
 def test_observing_every_step_does_not_perturb(fv):
     """Forces read after every step, so also right after the steps whose
     work-list force launch rebuilt or re-filtered the pruned list while
@@ -219,7 +219,7 @@ def test_observing_every_step_does_not_perturb(fv):
     to an unobserved one.  fv: the default force variant, the two
     lanes-per-atom variants (which filter first, then walk the new list) and
     a shared-memory ring variant (whose work-list kernel loads ahead into
-    registers instead)."""
+    registers instead) and the SM-affine resident-grid variant."""
     conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 9", nsteps=10_000)
     m = _melt(15, 40, seed=33)
     a = fm.Batch(max_replicas=2, max_atoms=1 << 13)
@@ -543,3 +543,20 @@ def test_table_replica_over_rebuilds_and_filters(tmp_path):
         assert b.info(s).status_word == 0
     assert b.info(s).rebuilds - r0 >= 1
     b.close()
+
+
+def test_chain_carry_survives_the_pushoff():
+    """A replica added with a push-off starts its run with a fresh chain;
+    run.conf nh_chain_carry 1 still applies to it: over 500 steps at Tdamp =
+    100 dt the extended energy holds where the reference's scheme moves."""
+    out = {}
+    for carry in (0, 1):
+        b = fm.Batch(max_replicas=1, max_atoms=1 << 13)
+        s = b.add(run_conf(ensemble="nvt_nh 1.0 1.0 0.1 3", nsteps=10_000, extra=f"nh_chain_carry {carry}"),
+                  gen=dict(nchains=20, chain_length=30, density=0.85, seed=11, pushoff_steps=2000))
+        b.run(0)
+        e0 = b.thermo(s).conserved
+        b.run(500)
+        out[carry] = b.thermo(s).conserved - e0
+        b.close()
+    assert abs(out[1]) < 0.2 * abs(out[0]), out
