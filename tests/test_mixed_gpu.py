@@ -547,16 +547,22 @@ def test_table_replica_over_rebuilds_and_filters(tmp_path):
 
 def test_chain_carry_survives_the_pushoff():
     """A replica added with a push-off starts its run with a fresh chain;
-    run.conf nh_chain_carry 1 still applies to it: over 500 steps at Tdamp =
-    100 dt the extended energy holds where the reference's scheme moves."""
-    out = {}
+    run.conf nh_chain_carry 1 still applies to it.  At Tdamp = 100 dt, after
+    2,000 steps of settling, the extended energy of the 600-bead melt rises
+    steadily under the reference's scheme (about 0.6 kT per tau for the
+    system in the FP64 oracle) and holds with the accelerations carried:
+    slopes fitted to 16 samples over 16,000 steps."""
+    slope = {}
     for carry in (0, 1):
         b = fm.Batch(max_replicas=1, max_atoms=1 << 13)
-        s = b.add(run_conf(ensemble="nvt_nh 1.0 1.0 0.1 3", nsteps=10_000, extra=f"nh_chain_carry {carry}"),
+        s = b.add(run_conf(ensemble="nvt_nh 1.0 1.0 0.1 3", nsteps=100_000, extra=f"nh_chain_carry {carry}"),
                   gen=dict(nchains=20, chain_length=30, density=0.85, seed=11, pushoff_steps=2000))
-        b.run(0)
-        e0 = b.thermo(s).conserved
-        b.run(500)
-        out[carry] = b.thermo(s).conserved - e0
+        n = b.info(s).natoms
+        b.run(2000)
+        e = []
+        for _ in range(16):
+            b.run(1000)
+            e.append(b.thermo(s).conserved * n)
+        slope[carry] = float(np.polyfit(np.arange(1, 17) * 1.0, e, 1)[0])  # kT per tau, whole melt
         b.close()
-    assert abs(out[1]) < 0.2 * abs(out[0]), out
+    assert slope[0] > 0.15 and abs(slope[1]) < 0.3 * slope[0], slope
