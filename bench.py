@@ -1197,9 +1197,9 @@ def main():
                                       "x2 = pairs two at a time in packed FP32x2 arithmetic, l2 / l4 = two / "
                                       "four lanes per atom (one otherwise), r2 / r3 / r4 = list rows staged through "
                                       "a shared-memory ring 1 / 2 / 3 batches ahead by asynchronous copies (otherwise "
-                                      "the next batch's list words are loaded ahead into registers), sm = a "
-                                      "resident grid taking chunks in SM-affine ranges (one block per chunk "
-                                      "otherwise)"}
+                                      "the next batch's list words are loaded ahead into registers), sm = each "
+                                      "block claims its chunk from a range of neighbouring chunks kept for "
+                                      "its SM (block b takes chunk b otherwise)"}
         line["launches_by_kernel"] = launched
         line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
                                     "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0),

@@ -1425,9 +1425,9 @@ __device__ __forceinline__ void lj_loop(const uint32_t* lst, int nn, const float
 // batches per warp.  A warp's 32 atoms share one 32-slot tile of the
 // transposed list, whose rows (128 bytes: entry k of the 32 atoms) are
 // contiguous, so a batch of 4 rows (512 bytes) is fetched by one 16-byte
-// asynchronous copy per lane (L1 bypassed), D - 1 batches ahead of its use,
-// without registers held for it; each lane then reads its own words from
-// shared memory.  The warp walks its longest list (nmax, warp-uniform): a
+// asynchronous copy per lane (L1 bypassed), D - 1 batches ahead of its use
+// (D - 2 while it is read), without registers held for it; each lane then
+// reads its own words from shared memory.  The warp walks its longest list (nmax, warp-uniform): a
 // lane's entries past its own length nn read as its padding entry and its
 // compensated adds stop at nn, so the forces are bitwise those of lj_loop
 // with B = 4 and the same KB, SH and P2.
@@ -1441,21 +1441,28 @@ __device__ __forceinline__ void lj_loop_ring(const uint32_t* tile_rows, uint32_t
   constexpr int W = B * 32;  // words per batch
   const float e24_0 = s_eps24[0], sig2_0 = s_sig2[0];
   const int nb = nmax / B;
+  // batches 0 .. D - 2 in flight before the loop; batch b + D - 1 is issued
+  // once batch b has landed, into the slot batch b - 1 was read from
+  const uint32_t* src = tile_rows + lane * 4;
+  uint32_t* const dst = ring + lane * 4;
 #pragma unroll
   for (int b = 0; b < D - 1; ++b) {
-    if (b < nb) cp_async16_stream(ring + (b % D) * W + lane * 4, tile_rows + (size_t)b * W + lane * 4);
+    if (b < nb) cp_async16_stream(dst + b * W, src);
     cp_async_commit();
+    src += W;
   }
   PairAcc g = {0, 0, 0, acc.pe, acc.v0, acc.v1, acc.v2, acc.v3, acc.v4, acc.v5};
   int kb = 0;
+  int rd = 0, wr = D - 1;  // ring slots of batch b and of batch b + D - 1
   for (int b = 0; b < nb; ++b) {
-    __syncwarp();  // every lane is done with the slot refilled here
-    const int bn = b + D - 1;
-    if (bn < nb) cp_async16_stream(ring + (bn % D) * W + lane * 4, tile_rows + (size_t)bn * W + lane * 4);
+    cp_async_wait_group<D - 2>();  // this lane's part of batch b has landed
+    __syncwarp();  // every lane's part has, and every lane is done reading slot wr (batch b - 1)
+    if (b + D - 1 < nb) cp_async16_stream(dst + wr * W, src);
     cp_async_commit();
-    cp_async_wait_group<D - 1>();  // this lane's part of batch b has landed
-    __syncwarp();                  // and every other lane's
-    const uint32_t* slot = ring + (b % D) * W;
+    src += W;
+    const uint32_t* slot = ring + rd * W;
+    rd = rd + 1 == D ? 0 : rd + 1;
+    wr = wr + 1 == D ? 0 : wr + 1;
     const int k = b * B;
     uint32_t w[B];
 #pragma unroll
@@ -2004,13 +2011,15 @@ __device__ __forceinline__ void force_chunk_lanes(const Dev& d, int chunk, bool 
   if (EV) block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
 }
 
-// One block per chunk of the batch (SCHED = 0).  SCHED = 1: a resident grid
-// whose blocks take chunks from a range of consecutive chunks assigned to
-// the SM they run on (%smid modulo the SM count), then help the ranges not
-// yet exhausted; the blocks resident on one SM so work on neighbouring
-// chunks, whose neighbour positions they share in that SM's L1.  Each chunk
-// is claimed once (atomic counters), so the forces are those of SCHED = 0.
-// The last block to finish clears the counters for the next launch.
+// One block per chunk of the batch.  SCHED = 0: block b takes chunk b.
+// SCHED = 1: a block takes the next unclaimed chunk of a range of
+// consecutive chunks assigned to the SM it runs on (%smid modulo the SM
+// count; an exhausted range sends it on to the next ones), so the blocks
+// resident on one SM work on neighbouring chunks and share their neighbour
+// positions in that SM's L1.  Every block claims exactly one chunk (atomic
+// counters; as many blocks as chunks), so the forces are those of
+// SCHED = 0.  The last block to finish clears the counters for the next
+// launch.
 template <bool EV, int B, int MINB, int PF, int KB, int SH, bool P2, int LPA, int SCHED>
 __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt) {
   count_launch(d, EV ? kKForceEv : kKForce);
@@ -2022,37 +2031,31 @@ __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt)
   } else {
     static_assert(LPA == 1, "SM-affine order with one lane per atom");
     int* const sched = d.sched + (EV ? kSchedWords : 0);  // the flavours may run at once: a set each
-    __shared__ int s_claim;
-    unsigned sm;
-    asm("mov.u32 %0, %%smid;" : "=r"(sm));
-    const int nr = min(max(d.sched_ranges, 1), kSchedRanges);
-    const int n = d.sched_n;
-    const int q = (n + nr - 1) / nr;  // chunks per range
-    const int own = (int)(sm % (unsigned)nr);
-    for (int t = 0; t < nr; ++t) {
-      const int r = own + t < nr ? own + t : own + t - nr;
-      if (t > 0) {  // skip a range seen exhausted (read once, shared: the branch is block-uniform)
-        __syncthreads();
-        if (threadIdx.x == 0) s_claim = (__ldcg(sched + kSchedFlags + (r >> 5)) >> (r & 31)) & 1;
-        __syncthreads();
-        if (s_claim) continue;
+    __shared__ int s_chunk;
+    if (threadIdx.x == 0) {
+      unsigned sm;
+      asm("mov.u32 %0, %%smid;" : "=r"(sm));
+      const int nr = min(max(d.sched_ranges, 1), kSchedRanges);
+      const int n = d.sched_n;
+      const int q = (n + nr - 1) / nr;  // chunks per range
+      const int own = (int)(sm % (unsigned)nr);
+      int chunk = -1;
+      for (int t = 0; t < nr && chunk < 0; ++t) {
+        const int r = own + t < nr ? own + t : own + t - nr;
+        if (t > 0 && ((__ldcg(sched + kSchedFlags + (r >> 5)) >> (r & 31)) & 1)) continue;  // exhausted
+        const int c = atomicAdd(sched + r, 1);
+        if (c < q && r * q + c < n) chunk = r * q + c;
+        else atomicOr(sched + kSchedFlags + (r >> 5), 1 << (r & 31));
       }
-      for (;;) {
-        __syncthreads();  // the previous chunk's shared tables and s_claim are no longer read
-        if (threadIdx.x == 0) s_claim = atomicAdd(sched + r, 1);
-        __syncthreads();
-        const int chunk = r * q + s_claim;
-        if (s_claim >= q || chunk >= n) {
-          if (threadIdx.x == 0) atomicOr(sched + kSchedFlags + (r >> 5), 1 << (r & 31));
-          break;
-        }
-        force_chunk<EV, B, PF, KB, false, SH, P2>(d, chunk, skip_rebuilt != 0);
-      }
+      s_chunk = chunk;
     }
     __syncthreads();
+    const int chunk = s_chunk;
+    if (chunk >= 0) force_chunk<EV, B, PF, KB, false, SH, P2>(d, chunk, skip_rebuilt != 0);
     if (threadIdx.x == 0) {
       __threadfence();
       if (atomicAdd(sched + kSchedDone, 1) == (int)gridDim.x - 1) {
+        const int nr = min(max(d.sched_ranges, 1), kSchedRanges);
         for (int k = 0; k < nr; ++k) sched[k] = 0;
         for (int k = 0; k < kSchedRanges / 32; ++k) sched[kSchedFlags + k] = 0;
         sched[kSchedDone] = 0;
@@ -2773,7 +2776,7 @@ void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(De
 #undef FMD_FORCE_VARIANT_S
 }
 
-// Variants whose per-chunk kernel is a resident grid in SM-affine order.
+// Variants whose per-chunk kernel claims chunks in SM-affine order.
 inline bool force_variant_sched(int variant) { return variant == 15; }
 
 // The force kernels use 4 KB of shared memory per block: ask for the
@@ -2796,20 +2799,18 @@ void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t 
   if (ev) force_kernels<true>(variant, &per_chunk, &listed);
   else force_kernels<false>(variant, &per_chunk, &listed);
   static bool set[2][kForceVariants] = {};
-  static int grid[2][kForceVariants] = {};
   const int v = variant >= 0 && variant < kForceVariants ? variant : 0;
   bool& done = set[ev ? 1 : 0][v];
   if (!done) {
     prefer_l1(per_chunk, force_carveout_pct(variant));
     prefer_l1(listed);
-    if (force_variant_sched(v)) grid[ev ? 1 : 0][v] = resident_grid(per_chunk, kChunk);
     done = true;
   }
   if (force_variant_sched(v)) {
     Dev ds = d;
     ds.sched_n = nchunks;
     ds.sched_ranges = num_sms();
-    per_chunk<<<std::min(nchunks, grid[ev ? 1 : 0][v]), kChunk, 0, st>>>(ds, skip_rebuilt ? 1 : 0);
+    per_chunk<<<nchunks, kChunk, 0, st>>>(ds, skip_rebuilt ? 1 : 0);
     return;
   }
   per_chunk<<<nchunks, kChunk, 0, st>>>(d, skip_rebuilt ? 1 : 0);
