@@ -307,8 +307,7 @@ GRAPH_CAPTURE_STEPS = 50  # one replay of a batch's default step graph
 # force-kernel variants, in the library's order (fastmd_b200/csrc/mixed_kernels.cu, force_kernels)
 FORCE_VARIANTS = ["m8 k1 t3", "m8 k2 t3", "m8 k1 a5", "m8 k2 a5", "m8 k1 a5 x2", "m8 k2 a5 x2", "m7 k1 a5 x2",
                   "m9 k1 a5 x2", "m6 k1 a5", "m8 k1 a5 x2 l2", "m8 k1 a5 x2 l4",
-                  "m8 k1 a5 x2 r3", "m8 k1 a5 x2 r4", "m8 k1 a5 x2 r2", "m9 k1 a5 x2 r2",
-                  "m8 k1 a5 x2 sm"]
+                  "m8 k1 a5 x2 r3", "m8 k1 a5 x2 r4", "m8 k1 a5 x2 r2", "m9 k1 a5 x2 r2"]
 
 
 def _dev_run(fm, b, nsteps):
@@ -1197,9 +1196,7 @@ def main():
                                       "x2 = pairs two at a time in packed FP32x2 arithmetic, l2 / l4 = two / "
                                       "four lanes per atom (one otherwise), r2 / r3 / r4 = list rows staged through "
                                       "a shared-memory ring 1 / 2 / 3 batches ahead by asynchronous copies (otherwise "
-                                      "the next batch's list words are loaded ahead into registers), sm = each "
-                                      "block claims its chunk from a range of neighbouring chunks kept for "
-                                      "its SM (block b takes chunk b otherwise)"}
+                                      "the next batch's list words are loaded ahead into registers)"}
         line["launches_by_kernel"] = launched
         line["replica_rebuilds"] = {"total": int(rebuilds1 - rebuilds0),
                                     "mean_interval_steps": args.steps * len(slots) / max(1, rebuilds1 - rebuilds0),

@@ -167,7 +167,6 @@ Batch::Batch(const fmd_batch_opts& o, const BatchCaps* exact) {
   kcount_.alloc_zero(kKernelKinds);
   acf_.alloc_zero((size_t)max_reps_ * kAcfWords);
   rb_.alloc_zero(kRbHead + (size_t)max_reps_ + kRbOffArrays * ((size_t)max_reps_ + 1));
-  sched_.alloc_zero(2 * (size_t)kSchedWords);  // one set per force flavour
   cell_cnt_.alloc_zero(c.cells);
   cell_start_.alloc_zero(c.cells);
   cell_fill_.alloc_zero(c.cells);
@@ -232,9 +231,6 @@ Dev Batch::dev() const {
   d.tab = tab_.p;
   d.rb = rb_;
   d.rb_cap = max_reps_;
-  d.sched = sched_;
-  d.sched_n = 0;
-  d.sched_ranges = 1;
   return d;
 }
 

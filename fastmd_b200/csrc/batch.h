@@ -167,7 +167,6 @@ class Batch {
   DevBuf<float2> tab_;  // pair-table points of every replica (appended at add)
   std::vector<float2> tab_host_;
   DevBuf<int> rb_;  // rebuild work list
-  DevBuf<int> sched_;  // SM-affine chunk scheduling counters of the force kernel
   std::vector<int> wl_;  // host staging of a host-written work list (kept alive for the async copy)
   int host_mode_ = 0;  // rebuild form of the current step, read back by direct-launch steps
   DevBuf<int32_t> cell_cnt_, cell_start_, cell_fill_;

@@ -233,17 +233,7 @@ struct Dev {
   // items)
   int* rb;
   int rb_cap;
-  // SM-affine chunk order of the force kernel (SCHED variants): per range
-  // claim counters, the ranges' exhausted flags, a finished-blocks counter;
-  // sched_n: the chunks of the launch (set by the launcher)
-  int* sched;
-  int sched_n;
-  int sched_ranges;  // one range per SM
 };
-constexpr int kSchedRanges = 1024;                    // SM ids covered (ids beyond share ranges)
-constexpr int kSchedFlags = kSchedRanges;             // + kSchedRanges / 32 words of exhausted bits
-constexpr int kSchedDone = kSchedRanges + kSchedRanges / 32;
-constexpr int kSchedWords = kSchedDone + 1;
 
 // Axis part of the shift code for cell shift e and wrap count k; -1 when
 // (e, k) is not one of the five representable cases.
@@ -319,7 +309,7 @@ struct StepShape {
   int has_table;        // some replica has tabulated pairs: the table pass follows the forces
 };
 using RebuildShape = StepShape;
-constexpr int kForceVariants = 16;
+constexpr int kForceVariants = 15;
 constexpr int kNbrVariants = 3;
 // One step with direct launches.  The rebuild form is read back from the
 // device after the per-replica commits (one small host read per step).

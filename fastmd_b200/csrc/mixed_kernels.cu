@@ -2011,58 +2011,14 @@ __device__ __forceinline__ void force_chunk_lanes(const Dev& d, int chunk, bool 
   if (EV) block_partials<kChunk>(vals, 7, d.part + (size_t)chunk * kNumPartials);
 }
 
-// One block per chunk of the batch.  SCHED = 0: block b takes chunk b.
-// SCHED = 1: a block takes the next unclaimed chunk of a range of
-// consecutive chunks assigned to the SM it runs on (%smid modulo the SM
-// count; an exhausted range sends it on to the next ones), so the blocks
-// resident on one SM work on neighbouring chunks and share their neighbour
-// positions in that SM's L1.  Every block claims exactly one chunk (atomic
-// counters; as many blocks as chunks), so the forces are those of
-// SCHED = 0.  The last block to finish clears the counters for the next
-// launch.
-template <bool EV, int B, int MINB, int PF, int KB, int SH, bool P2, int LPA, int SCHED>
+// One block per chunk of the batch.
+template <bool EV, int B, int MINB, int PF, int KB, int SH, bool P2, int LPA>
 __global__ void __launch_bounds__(kChunk, MINB) k_force(Dev d, int skip_rebuilt) {
   count_launch(d, EV ? kKForceEv : kKForce);
-  if constexpr (SCHED == 0) {
-    if constexpr (LPA == 1)
-      force_chunk<EV, B, PF, KB, false, SH, P2>(d, blockIdx.x, skip_rebuilt != 0);
-    else
-      force_chunk_lanes<EV, B, (PF != 0), KB, false, SH, P2, LPA>(d, blockIdx.x, skip_rebuilt != 0);
-  } else {
-    static_assert(LPA == 1, "SM-affine order with one lane per atom");
-    int* const sched = d.sched + (EV ? kSchedWords : 0);  // the flavours may run at once: a set each
-    __shared__ int s_chunk;
-    if (threadIdx.x == 0) {
-      unsigned sm;
-      asm("mov.u32 %0, %%smid;" : "=r"(sm));
-      const int nr = min(max(d.sched_ranges, 1), kSchedRanges);
-      const int n = d.sched_n;
-      const int q = (n + nr - 1) / nr;  // chunks per range
-      const int own = (int)(sm % (unsigned)nr);
-      int chunk = -1;
-      for (int t = 0; t < nr && chunk < 0; ++t) {
-        const int r = own + t < nr ? own + t : own + t - nr;
-        if (t > 0 && ((__ldcg(sched + kSchedFlags + (r >> 5)) >> (r & 31)) & 1)) continue;  // exhausted
-        const int c = atomicAdd(sched + r, 1);
-        if (c < q && r * q + c < n) chunk = r * q + c;
-        else atomicOr(sched + kSchedFlags + (r >> 5), 1 << (r & 31));
-      }
-      s_chunk = chunk;
-    }
-    __syncthreads();
-    const int chunk = s_chunk;
-    if (chunk >= 0) force_chunk<EV, B, PF, KB, false, SH, P2>(d, chunk, skip_rebuilt != 0);
-    if (threadIdx.x == 0) {
-      __threadfence();
-      if (atomicAdd(sched + kSchedDone, 1) == (int)gridDim.x - 1) {
-        const int nr = min(max(d.sched_ranges, 1), kSchedRanges);
-        for (int k = 0; k < nr; ++k) sched[k] = 0;
-        for (int k = 0; k < kSchedRanges / 32; ++k) sched[kSchedFlags + k] = 0;
-        sched[kSchedDone] = 0;
-        __threadfence();
-      }
-    }
-  }
+  if constexpr (LPA == 1)
+    force_chunk<EV, B, PF, KB, false, SH, P2>(d, blockIdx.x, skip_rebuilt != 0);
+  else
+    force_chunk_lanes<EV, B, (PF != 0), KB, false, SH, P2, LPA>(d, blockIdx.x, skip_rebuilt != 0);
 }
 
 // The chunks of the replicas on the rebuild work list (a resident grid
@@ -2750,10 +2706,9 @@ constexpr int kForceCarveoutPct = 16;  // percent of the SM's shared-memory maxi
 template <bool EV>
 void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(Dev)) {
   constexpr int E = 5;  // blocks per SM of the energy flavours (more registers)
-#define FMD_FORCE_VARIANT_S(B, MINB, PF, KB, SH, P2, LPA, SCHED)          \
-  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA, SCHED>; \
+#define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2, LPA)          \
+  *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>; \
   *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>;
-#define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2, LPA) FMD_FORCE_VARIANT_S(B, MINB, PF, KB, SH, P2, LPA, 0)
   switch (variant) {
     case 1: FMD_FORCE_VARIANT(4, 8, true, 2, 0, false, 1) break;
     case 2: FMD_FORCE_VARIANT(4, 8, true, 1, 1, false, 1) break;
@@ -2769,15 +2724,10 @@ void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(De
     case 12: FMD_FORCE_VARIANT(4, 8, 4, 1, 1, true, 1) break;
     case 13: FMD_FORCE_VARIANT(4, 8, 2, 1, 1, true, 1) break;
     case 14: FMD_FORCE_VARIANT(4, 9, 2, 1, 1, true, 1) break;
-    case 15: FMD_FORCE_VARIANT_S(4, 8, 1, 1, 1, true, 1, 1) break;
     default: FMD_FORCE_VARIANT(4, 8, true, 1, 0, false, 1) break;
   }
 #undef FMD_FORCE_VARIANT
-#undef FMD_FORCE_VARIANT_S
 }
-
-// Variants whose per-chunk kernel claims chunks in SM-affine order.
-inline bool force_variant_sched(int variant) { return variant == 15; }
 
 // The force kernels use 4 KB of shared memory per block: ask for the
 // smallest shared-memory carve-out, leaving the rest of the SM's unified
@@ -2805,13 +2755,6 @@ void launch_force(const Dev& d, int nchunks, bool ev, int variant, cudaStream_t 
     prefer_l1(per_chunk, force_carveout_pct(variant));
     prefer_l1(listed);
     done = true;
-  }
-  if (force_variant_sched(v)) {
-    Dev ds = d;
-    ds.sched_n = nchunks;
-    ds.sched_ranges = num_sms();
-    per_chunk<<<nchunks, kChunk, 0, st>>>(ds, skip_rebuilt ? 1 : 0);
-    return;
   }
   per_chunk<<<nchunks, kChunk, 0, st>>>(d, skip_rebuilt ? 1 : 0);
 }

@@ -210,7 +210,7 @@ def test_observing_does_not_perturb(ens):
     b.close()
 
 
-@pytest.mark.parametrize("fv", [-1, 9, 10, 11, 15])
+@pytest.mark.parametrize("fv", [-1, 9, 10, 11])
 def test_observing_every_step_does_not_perturb(fv):
     """Forces read after every step, so also right after the steps whose
     work-list force launch rebuilt or re-filtered the pruned list while
@@ -219,7 +219,7 @@ def test_observing_every_step_does_not_perturb(fv):
     to an unobserved one.  fv: the default force variant, the two
     lanes-per-atom variants (which filter first, then walk the new list) and
     a shared-memory ring variant (whose work-list kernel loads ahead into
-    registers instead) and the SM-affine chunk-claim variant."""
+    registers instead)."""
     conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 9", nsteps=10_000)
     m = _melt(15, 40, seed=33)
     a = fm.Batch(max_replicas=2, max_atoms=1 << 13)
