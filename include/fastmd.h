@@ -351,14 +351,16 @@ FMD_API fmd_status fmd_batch_set_list_prune(fmd_batch* b, int32_t slot, double d
  * it beyond summation order. */
 FMD_API fmd_status fmd_batch_set_list_buffer(fmd_batch* b, int32_t slot, double skin);
 FMD_API fmd_status fmd_batch_get_list_buffer(fmd_batch* b, int32_t slot, double* skin);
-/* Autotuner: time each force-kernel variant (list entries per batch, blocks
- * per SM, pipelined list loads) `iters` times on the current state and each
- * neighbor-list variant on a full rebuild (ballot form with 8 or 6 blocks
- * per SM, row form), keep the
+/* Autotuner: time each force-kernel variant (blocks per SM, batches per
+ * compensated add, shift lookup, packed pair arithmetic, lanes per atom,
+ * list words loaded ahead in registers or staged in a shared-memory ring)
+ * `iters` times on the current state and each neighbor-list variant on a
+ * full rebuild (ballot form with 8 or 6 blocks per SM, row form), keep the
  * fastest for all following steps.  chosen = force variant index;
  * ms_per_variant (cap entries, may be NULL) = device ms per launch of each
- * force variant (7), then ms per full rebuild of each neighbor variant (3),
- * then the chosen neighbor variant.  It also lifts the forced rebuild
+ * force variant (n_force of fmd_batch_get_variants), then ms per full
+ * rebuild of each neighbor variant (n_nbr), then the chosen neighbor
+ * variant.  It also lifts the forced rebuild
  * cadence of the active replicas (rebuilds then follow the skin/2
  * displacement trigger alone; fmd_batch_set_rebuild_cadence restores one)
  * and widens the list buffer of replicas with a pruned list to the cell
