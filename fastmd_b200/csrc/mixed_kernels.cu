@@ -216,22 +216,22 @@ __global__ void __launch_bounds__(kChunk / APT, APT == 1 ? 6 : 12) k_pre(Dev d, 
     d.rb[kRbRebuilds] = 0;
     d.rb[kRbMode] = kRbNone;
   }
-  const int4 ci = d.chunk_rep[blockIdx.x];
-  if (ci.x < 0) return;
-  // The atoms' data depends neither on the replica record nor on the step
-  // scalars: issue their loads first.
+  // The atoms' data depends neither on the chunk's record nor on the replica
+  // record or the step scalars: issue their loads first.  Chunk b holds slots
+  // [b kChunk, (b + 1) kChunk), all allocated; the slots past the replica's
+  // atoms (or of a free chunk) are loaded and left unused.
+  const int base = blockIdx.x * kChunk;
   float4 p[APT], v[APT], f[APT], q[APT];
 #pragma unroll
   for (int k = 0; k < APT; ++k) {
     const int t = threadIdx.x + k * T;
-    p[k] = v[k] = f[k] = q[k] = make_float4(0, 0, 0, 0);
-    if (t < ci.z) {
-      p[k] = d.pos[ci.y + t];
-      v[k] = d.vel[ci.y + t];
-      f[k] = d.force[ci.y + t];
-      q[k] = d.ref[ci.y + t];
-    }
+    p[k] = d.pos[base + t];
+    v[k] = d.vel[base + t];
+    f[k] = d.force[base + t];
+    q[k] = d.ref[base + t];
   }
+  const int4 ci = d.chunk_rep[blockIdx.x];
+  if (ci.x < 0) return;
   Rep& R = d.reps[ci.x];
   __shared__ StepScalars S;
   __shared__ uint32_t wmax[T / 32];
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kChunk / APT, APT == 1 ? 6 : 12) k_pre(Dev d, 
 #pragma unroll
   for (int k = 0; k < APT; ++k) {
     const int t = threadIdx.x + k * T;
-    if (t < ci.z) pre_atom(d, R, S, ci.y + t, deferred, p[k], v[k], f[k], q[k], d2bits, bad);
+    if (t < ci.z) pre_atom(d, R, S, base + t, deferred, p[k], v[k], f[k], q[k], d2bits, bad);
   }
   warp_max_u32(d2bits);
   if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = d2bits;
