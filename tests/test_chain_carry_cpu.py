@@ -63,3 +63,19 @@ def test_run_conf_key():
         assert fm.parse_run_conf(base + f"nh_chain_carry {v}\n")["chain_length"] == 3
     with pytest.raises(fm.FastMDError):
         fm.parse_run_conf(base + "nh_chain_carry 2\n")
+
+
+def test_barostat_kinetic_term_diagnostic():
+    """orc_sim_conserved_mtk adds the summed work of the (3 / N_f) 2 KE term
+    the reference's barostat force leaves out: zero under NVT, nonzero and
+    small (next to the extended energy) under NPT."""
+    system, st, L = _melt_state()
+    for ens, kw in (("nvt_nh", {}), ("npt_nh", dict(P=(0.0, 0.0, 1.0)))):
+        sim = po.Sim(system(st["x"], L, st["v"], st["image"]), ensemble=ens, dt=0.001, T=(1.0, 1.0, 0.5),
+                     chain=3, nsteps=10 ** 8, nthreads=4, **kw)
+        sim.step(500)
+        gap = sim.conserved_mtk() - sim.conserved()
+        if ens == "nvt_nh":
+            assert gap == 0.0
+        else:
+            assert gap != 0.0 and abs(gap) < 1e-3 * abs(sim.conserved())
