@@ -139,6 +139,26 @@ __device__ __forceinline__ void count_launch(const Dev& d, int kind) {
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(d.kcount + kind, 1ull);
 }
 
+// 16-byte asynchronous global -> shared copy (cp.async, L1-cached) and the
+// wait for all of this thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// The same copy with L1 bypassed (streamed data), the commit of this
+// thread's copies issued so far as one group, and the wait until at most N
+// of its groups are still in flight.
+__device__ __forceinline__ void cp_async16_stream(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------- pre-force
 // One atom's pre-force update on its loaded state (p, v, f, q); returns the
 // squared displacement bits since the last rebuild and a non-finite flag.
@@ -262,6 +282,78 @@ __global__ void __launch_bounds__(kChunk / APT, APT == 1 ? 6 : 12) k_pre(Dev d, 
     atomicMax(&R.maxdisp_bits, m);
     if (bad) atomicOr(&R.status, kStatusNonFinite);
   }
+}
+
+// The pre-force update as a resident grid streaming over the chunks: each
+// block walks chunks blockIdx.x, + gridDim.x, ... with the next chunk's
+// four arrays (positions, velocities, forces, displacement references;
+// 8 KB) copied into shared memory by asynchronous 16-byte copies while it
+// updates the current one, so its loads stay in flight behind the
+// arithmetic instead of heading each block's dependent chain; the step
+// scalars are read once per replica met in a row.  The update of each atom
+// is pre_atom's, so the results are those of k_pre.
+constexpr int kPreStreamBlocksPerSM = 8;
+__global__ void __launch_bounds__(kChunk, kPreStreamBlocksPerSM) k_pre_stream(Dev d, StepConds cond, int nchunks) {
+  count_launch(d, kKPre);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    d.rb[kRbCount] = 0;
+    d.rb[kRbRebuilds] = 0;
+    d.rb[kRbMode] = kRbNone;
+  }
+  __shared__ __align__(16) float4 buf[2][4][kChunk];
+  __shared__ StepScalars S;
+  __shared__ uint32_t wmax[kChunk / 32];
+  const int t = threadIdx.x;
+  auto stage = [&](int c, int slot) {
+    const size_t k = (size_t)c * kChunk + t;
+    cp_async16_stream(&buf[slot][0][t], d.pos + k);
+    cp_async16_stream(&buf[slot][1][t], d.vel + k);
+    cp_async16_stream(&buf[slot][2][t], d.force + k);
+    cp_async16_stream(&buf[slot][3][t], d.ref + k);
+  };
+  int cur = 0, loaded = -1;
+  if (blockIdx.x < nchunks) stage(blockIdx.x, 0);
+  cp_async_commit();
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    const int cn = c + gridDim.x;
+    if (cn < nchunks) stage(cn, cur ^ 1);
+    cp_async_commit();
+    cp_async_wait_group<1>();  // chunk c's part of this thread has landed
+    __syncthreads();           // and every thread's
+    const int4 ci = d.chunk_rep[c];
+    Rep& R = d.reps[ci.x < 0 ? 0 : ci.x];
+    if (ci.x >= 0 && R.active && R.step < R.stop_step) {  // block-uniform
+      if (ci.x != loaded) {
+        if (R.next_valid) {
+          constexpr int nw = (int)(sizeof(StepScalars) / sizeof(uint32_t));
+          const uint32_t* src = reinterpret_cast<const uint32_t*>(&R.next);
+          uint32_t* dst = reinterpret_cast<uint32_t*>(&S);
+          for (int k = t; k < nw; k += kChunk) dst[k] = src[k];
+        } else if (t == 0) {
+          compute_step_scalars(R, S);
+        }
+        loaded = ci.x;
+        __syncthreads();
+      }
+      uint32_t d2bits = 0;
+      int bad = 0;
+      if (t < ci.z)
+        pre_atom(d, R, S, ci.y + t, R.defer != 0, buf[cur][0][t], buf[cur][1][t], buf[cur][2][t], buf[cur][3][t],
+                 d2bits, bad);
+      warp_max_u32(d2bits);
+      if ((t & 31) == 0) wmax[t >> 5] = d2bits;
+      bad = __syncthreads_or(bad);
+      if (t == 0) {
+        uint32_t m = 0;
+        for (int w = 0; w < kChunk / 32; ++w) m = max(m, wmax[w]);
+        atomicMax(&R.maxdisp_bits, m);
+        if (bad) atomicOr(&R.status, kStatusNonFinite);
+      }
+    }
+    __syncthreads();  // chunk c's slot and wmax are free for the next round
+    cur ^= 1;
+  }
+  cp_async_wait_group<0>();
 }
 
 constexpr int kPreAPT = 2;  // atoms per thread of the launched pre-force kernel
@@ -823,25 +915,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
 // is deterministic.  Pairs within rc + skin, 1-2 bonded pairs excluded
 // (verlet_list.cu:108-335 semantics), exclusions compared as slots from the
 // per-slot bond table.
-// 16-byte asynchronous global -> shared copy (cp.async, L1-cached) and the
-// wait for all of this thread's copies.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-// The same copy with L1 bypassed (streamed data), the commit of this
-// thread's copies issued so far as one group, and the wait until at most N
-// of its groups are still in flight.
-__device__ __forceinline__ void cp_async16_stream(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait_group() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
+
 
 constexpr int kNbrWarps = kNbrThreads / 32;
 constexpr int kNbrWin = 1024;     // staged candidates per window
@@ -2469,11 +2543,37 @@ int num_sms() {
   if (!cache[dev]) FMD_CUDA(cudaDeviceGetAttribute(&cache[dev], cudaDevAttrMultiProcessorCount, dev));
   return cache[dev];
 }
+
+// Blocks of a persistent (grid-stride) kernel: exactly the number that are
+// resident at once, so no block waits for a second wave.
+template <typename K>
+int resident_grid(K kernel, int threads) {
+  int per_sm = 0;
+  FMD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+  return num_sms() * (per_sm > 0 ? per_sm : 1);
+}
 }  // namespace
+
+// The pre-force update of every chunk: the streaming resident grid (all of
+// the SM's shared memory asked for: its blocks hold two chunks each), or the
+// block-per-chunk kernel (kPreStream false).
+constexpr bool kPreStream = true;
+void launch_pre(const Dev& d, const StepConds& c, int nchunks, cudaStream_t st) {
+  if (!kPreStream) {
+    k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
+    return;
+  }
+  static int grid = 0;
+  if (!grid) {
+    FMD_CUDA(cudaFuncSetAttribute(k_pre_stream, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    grid = resident_grid(k_pre_stream, kChunk);
+  }
+  k_pre_stream<<<std::min(nchunks, grid), kChunk, 0, st>>>(d, c, nchunks);
+}
 
 void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t st) {
   const StepConds none{0, 0, 0, 0, 0, 0, 0};
-  k_pre<kPreAPT><<<g.nchunks, kChunk / kPreAPT, 0, st>>>(d, none);
+  launch_pre(d, none, g.nchunks, st);
   k_commit<<<g.nreps, 32, 0, st>>>(d, none);
   FMD_CUDA(cudaMemcpyAsync(host_mode, d.rb + kRbMode, sizeof(int), cudaMemcpyDeviceToHost, st));
   FMD_CUDA(cudaStreamSynchronize(st));
@@ -2541,7 +2641,7 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.force_ev, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.post, g, 0u, cudaGraphCondAssignDefault));
   FMD_CUDA(cudaGraphConditionalHandleCreate(&c.prune, g, 0u, cudaGraphCondAssignDefault));
-  k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
+  launch_pre(d, c, nchunks, st);
   k_commit<<<nreps, 32, 0, st>>>(d, c);
   // Four parallel branches, each one conditional node: the two rebuild forms
   // (they exclude each other), each followed by the forces of the replicas
@@ -2606,14 +2706,6 @@ void capture_step(const Dev& d, const StepShape& shape, cudaStream_t st, cudaStr
 }
 
 namespace {
-// Blocks of a persistent (grid-stride) kernel: exactly the number that are
-// resident at once, so no block waits for a second wave.
-template <typename K>
-int resident_grid(K kernel, int threads) {
-  int per_sm = 0;
-  FMD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
-  return num_sms() * (per_sm > 0 ? per_sm : 1);
-}
 
 int rebuild_priority() {
   static const int p = [] {
