@@ -284,78 +284,6 @@ __global__ void __launch_bounds__(kChunk / APT, APT == 1 ? 6 : 12) k_pre(Dev d, 
   }
 }
 
-// The pre-force update as a resident grid streaming over the chunks: each
-// block walks chunks blockIdx.x, + gridDim.x, ... with the next chunk's
-// four arrays (positions, velocities, forces, displacement references;
-// 8 KB) copied into shared memory by asynchronous 16-byte copies while it
-// updates the current one, so its loads stay in flight behind the
-// arithmetic instead of heading each block's dependent chain; the step
-// scalars are read once per replica met in a row.  The update of each atom
-// is pre_atom's, so the results are those of k_pre.
-constexpr int kPreStreamBlocksPerSM = 8;
-__global__ void __launch_bounds__(kChunk, kPreStreamBlocksPerSM) k_pre_stream(Dev d, StepConds cond, int nchunks) {
-  count_launch(d, kKPre);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    d.rb[kRbCount] = 0;
-    d.rb[kRbRebuilds] = 0;
-    d.rb[kRbMode] = kRbNone;
-  }
-  __shared__ __align__(16) float4 buf[2][4][kChunk];
-  __shared__ StepScalars S;
-  __shared__ uint32_t wmax[kChunk / 32];
-  const int t = threadIdx.x;
-  auto stage = [&](int c, int slot) {
-    const size_t k = (size_t)c * kChunk + t;
-    cp_async16_stream(&buf[slot][0][t], d.pos + k);
-    cp_async16_stream(&buf[slot][1][t], d.vel + k);
-    cp_async16_stream(&buf[slot][2][t], d.force + k);
-    cp_async16_stream(&buf[slot][3][t], d.ref + k);
-  };
-  int cur = 0, loaded = -1;
-  if (blockIdx.x < nchunks) stage(blockIdx.x, 0);
-  cp_async_commit();
-  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
-    const int cn = c + gridDim.x;
-    if (cn < nchunks) stage(cn, cur ^ 1);
-    cp_async_commit();
-    cp_async_wait_group<1>();  // chunk c's part of this thread has landed
-    __syncthreads();           // and every thread's
-    const int4 ci = d.chunk_rep[c];
-    Rep& R = d.reps[ci.x < 0 ? 0 : ci.x];
-    if (ci.x >= 0 && R.active && R.step < R.stop_step) {  // block-uniform
-      if (ci.x != loaded) {
-        if (R.next_valid) {
-          constexpr int nw = (int)(sizeof(StepScalars) / sizeof(uint32_t));
-          const uint32_t* src = reinterpret_cast<const uint32_t*>(&R.next);
-          uint32_t* dst = reinterpret_cast<uint32_t*>(&S);
-          for (int k = t; k < nw; k += kChunk) dst[k] = src[k];
-        } else if (t == 0) {
-          compute_step_scalars(R, S);
-        }
-        loaded = ci.x;
-        __syncthreads();
-      }
-      uint32_t d2bits = 0;
-      int bad = 0;
-      if (t < ci.z)
-        pre_atom(d, R, S, ci.y + t, R.defer != 0, buf[cur][0][t], buf[cur][1][t], buf[cur][2][t], buf[cur][3][t],
-                 d2bits, bad);
-      warp_max_u32(d2bits);
-      if ((t & 31) == 0) wmax[t >> 5] = d2bits;
-      bad = __syncthreads_or(bad);
-      if (t == 0) {
-        uint32_t m = 0;
-        for (int w = 0; w < kChunk / 32; ++w) m = max(m, wmax[w]);
-        atomicMax(&R.maxdisp_bits, m);
-        if (bad) atomicOr(&R.status, kStatusNonFinite);
-      }
-    }
-    __syncthreads();  // chunk c's slot and wmax are free for the next round
-    cur ^= 1;
-  }
-  cp_async_wait_group<0>();
-}
-
 constexpr int kPreAPT = 2;  // atoms per thread of the launched pre-force kernel
 
 // Per-replica commit of the pre-force update (one thread per replica, after
@@ -2554,21 +2482,12 @@ int resident_grid(K kernel, int threads) {
 }
 }  // namespace
 
-// The pre-force update of every chunk: the streaming resident grid (all of
-// the SM's shared memory asked for: its blocks hold two chunks each), or the
-// block-per-chunk kernel (kPreStream false).
-constexpr bool kPreStream = true;
+// The pre-force update of every chunk, one block per chunk.  (A resident
+// grid streaming the chunks through shared memory by asynchronous copies
+// measured the same, 50.7 against 48.7 us on 64 x 30K: long-scoreboard
+// stalls stayed the limit.)
 void launch_pre(const Dev& d, const StepConds& c, int nchunks, cudaStream_t st) {
-  if (!kPreStream) {
-    k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
-    return;
-  }
-  static int grid = 0;
-  if (!grid) {
-    FMD_CUDA(cudaFuncSetAttribute(k_pre_stream, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    grid = resident_grid(k_pre_stream, kChunk);
-  }
-  k_pre_stream<<<std::min(nchunks, grid), kChunk, 0, st>>>(d, c, nchunks);
+  k_pre<kPreAPT><<<nchunks, kChunk / kPreAPT, 0, st>>>(d, c);
 }
 
 void launch_step(const Dev& d, const StepShape& g, int* host_mode, cudaStream_t st) {
