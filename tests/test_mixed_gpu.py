@@ -566,3 +566,28 @@ def test_chain_carry_survives_the_pushoff():
         slope[carry] = float(np.polyfit(np.arange(1, 17) * 1.0, e, 1)[0])  # kT per tau, whole melt
         b.close()
     assert slope[0] > 0.15 and abs(slope[1]) < 0.3 * slope[0], slope
+
+
+@pytest.mark.parametrize("fv", [9, 10, 11, 13])
+@pytest.mark.parametrize("ens", ["nvt_langevin 1.0 1.0 1.0 5", "npt_nh 1.0 1.0 0.5 0.5 0.5 1.0 3"])
+def test_two_type_forces_lanes_and_ring_variants(ens, fv):
+    """The lanes-per-atom and shared-memory ring force variants on a two-type
+    melt (per-pair parameter lookup), through 60 steps of their own (pruned
+    list with filters under Langevin, the full list under NPT): forces at the
+    force frame against the FP64 oracle."""
+    lj = [(0, 0, 1.0, 1.0), (1, 1, 1.0, 1.0), (0, 1, 0.9, 1.0)]
+    b = fm.Batch(max_replicas=1, max_atoms=1 << 13)
+    b.set_variants(fv, -1)
+    s = b.add(run_conf(ensemble=ens, ntypes=2, lj=lj, nsteps=1000),
+              gen=dict(nchains=20, chain_length=100, density=0.85, seed=3, pushoff_steps=1000, type_block=50))
+    b.run(60)
+    assert b.variants()[0] == fv
+    f, _, _ = b.forces(s)
+    x, L = b.force_frame(s)
+    d = _melt(20, 100, seed=3, type_block=50)
+    tab = np.ones((2, 2, 2))
+    tab[0, 1, 0] = tab[1, 0, 0] = 0.9
+    fo, _, _ = po.forces(oracle_system(d, xyz=x, L=L, lj_table=tab))
+    assert rel_rms(f, fo) < FORCE_RMS_TOL
+    assert b.info(s).status_word == 0
+    b.close()
