@@ -443,8 +443,8 @@ int Batch::add(const RunConfig& cfg, Topology t, const fmd_melt_spec* pushoff) {
       break;
     }
   if (r < 0) throw Error(FMD_ERR_CAPACITY, "no free replica slot");
-  // neighbor-list entries address a replica's slots with 25 bits
-  if ((int64_t)t.natoms + kChunk >= (int64_t)kIdxMask) throw Error(FMD_ERR_CAPACITY, "replica too large (max 33,554,000 atoms)");
+  // neighbor-list entries address a replica's slots with 22 bits
+  if ((int64_t)t.natoms + kChunk >= (int64_t)kIdxMask) throw Error(FMD_ERR_CAPACITY, "replica too large (max 4,194,000 atoms)");
   const ReplicaPlan p = plan_replica(cfg, t.natoms, t.box_L);
   const int64_t need = estimate_bytes(p, t.nbonds(), t.nangles());
   if (bytes_in_use_ + need > budget_bytes_) throw Error(FMD_ERR_CAPACITY, "device-memory budget exhausted");

@@ -13,9 +13,9 @@
 //   force[s] float4 {fx, fy, fz, pe_i}
 //   ref[s]   float4 offsets at the last rebuild (displacement test); .w = atom id
 //   img[s]   int4   {ix, iy, iz, atom id}  image flags + replica-local atom id
-//   nbr      uint32 per (tile, k, lane): replica-local slot of j (25 bits) and
-//            the periodic shift of j relative to i as one of 125 codes in the
-//            top 7 bits (see kCodeShift below)
+//   nbr      uint32 per (tile, k, lane): replica-local slot of j (22 bits) and
+//            the periodic shift of j relative to i as three 3-bit axis codes
+//            above it (see entry_code below)
 //
 // A position is r = (c + 0) * h + o with h = L / G the cell edge; pair
 // displacements are formed as (o_i - o_j) - e * h, so their precision is set by
@@ -36,21 +36,27 @@ constexpr int kMaxTypes = 16;
 constexpr int kMaxTables = 8;  // distinct pair tables per replica
 constexpr int kGhostType = 31;
 constexpr int kMaxG = 512;        // cells per axis (9 bits)
-// Neighbor-list entry: slot (25 bits) | shift code (7 bits).  The shift
-// code names one of 125 periodic shift vectors: per axis a in 0..4 for
-// e*h + k*dL with (e, k) = (-1,-1), (-1,0), (0,0), (1,0), (1,1), code =
-// 25 ax + 5 ay + az.  The vector is the same for every atom of a replica.
-constexpr uint32_t kIdxMask = (1u << 25) - 1;
-constexpr int kCodeShift = 25;
-constexpr int kShiftCodes = 125;
-constexpr uint32_t kZeroShiftCode = 62;  // (0, 0, 0): 2 * 25 + 2 * 5 + 2
+// Neighbor-list entry: slot (22 bits) | ax << 22 | ay << 25 | az << 28.  The
+// three axis codes name one of 125 periodic shift vectors: per axis a in 0..4
+// for e*h + k*dL with (e, k) = (-1,-1), (-1,0), (0,0), (1,0), (1,1).  The
+// vector is the same for every atom of a replica.  Each code sits in a field
+// of its own, so a force loop reads it with one bit-field extract.
+constexpr int kSlotBits = 22;
+constexpr uint32_t kIdxMask = (1u << kSlotBits) - 1;
+constexpr int kShiftCodes = 125;  // 25 ax + 5 ay + az: the index into a table of all 125 vectors
+__host__ __device__ inline uint32_t entry_code(int ax, int ay, int az) {
+  return ((uint32_t)ax << kSlotBits) | ((uint32_t)ay << (kSlotBits + 3)) | ((uint32_t)az << (kSlotBits + 6));
+}
+__host__ __device__ inline int entry_ax(uint32_t w) { return (int)((w >> kSlotBits) & 7u); }
+__host__ __device__ inline int entry_ay(uint32_t w) { return (int)((w >> (kSlotBits + 3)) & 7u); }
+__host__ __device__ inline int entry_az(uint32_t w) { return (int)(w >> (kSlotBits + 6)); }
 // Lists are padded to a multiple of kListPad entries with the atom's own
-// slot and the shift (h + dL) on every axis (code 124: (e, k) = (1, 1)), so
+// slot and the shift (h + dL) on every axis (codes 4, 4, 4: (e, k) = (1, 1)), so
 // the force loop runs whole batches and a padding entry lies sqrt(3) (h + dL)
 // > rc away: the cutoff test alone gives it an exact zero.  (The cell edge h
 // is at least rc + skin at a rebuild; an NPT contraction shrinks it by at
 // most rc / (rc + skin) before the rebuild trigger fires, so h >= rc.)
-constexpr uint32_t kPadCode = 124;
+constexpr uint32_t kPadBits = (4u << kSlotBits) | (4u << (kSlotBits + 3)) | (4u << (kSlotBits + 6));
 constexpr int kListPad = 8;
 constexpr int kPrunePad = 4;  // the pruned list: padded to whole force batches only
 constexpr double kPruneDelta = 0.12;  // pruned-list margin beyond rc (sigma)

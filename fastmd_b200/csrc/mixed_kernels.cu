@@ -817,7 +817,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
                   for (int b = b0; b < b1; ++b) excl |= (d.bent[R.bond_base + b].x == idj);
                   if (excl) continue;
                   if (count < M)
-                    out[(size_t)count * 32] = (uint32_t)j | ((uint32_t)(ax * 25 + ay * 5 + az) << kCodeShift);
+                    out[(size_t)count * 32] = (uint32_t)j | entry_code(ax, ay, az);
                   ++count;
                 }
               }
@@ -827,7 +827,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
         d.ncnt[base + il] = min(count, M);
         if (count > M) overflow |= kStatusOverflow;
         for (int k = count; k < ((count + kListPad - 1) & ~(kListPad - 1)) && k < M; ++k)
-          out[(size_t)k * 32] = (uint32_t)il | (kPadCode << kCodeShift);
+          out[(size_t)k * 32] = (uint32_t)il | kPadBits;
       }
     }
   }
@@ -896,8 +896,7 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
       s_sx[t] = shift_term(dx, kx, h, dL);
       s_sy[t] = shift_term(dy, ky, h, dL);
       s_sz[t] = shift_term(dz, kz, h, dL);
-      s_code[t] = (uint32_t)(axis_shift_code(dx, kx) * 25 + axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz))
-                  << kCodeShift;
+      s_code[t] = entry_code(axis_shift_code(dx, kx), axis_shift_code(dy, ky), axis_shift_code(dz, kz));
     }
     int incl = cnt;
 #pragma unroll
@@ -1007,7 +1006,7 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
           if (count <= M) {
             const int padded = (count + kListPad - 1) & ~(kListPad - 1);
             if (lane < padded - count)
-              __stcg(out + (size_t)(count + lane) * 32, (uint32_t)i | (kPadCode << kCodeShift));
+              __stcg(out + (size_t)(count + lane) * 32, (uint32_t)i | kPadBits);
           }
           if (lane == 0) {
             d.ncnt[base + i] = min(count, M);
@@ -1063,7 +1062,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
   __shared__ int s_ns[kNbrUnion], s_off[kNbrUnion + 1];
   __shared__ float s_sx[kNbrUnion], s_sy[kNbrUnion], s_sz[kNbrUnion];
   __shared__ int s_ax[kNbrUnion];   // wrap count kx of the union column
-  __shared__ int s_ayz[kNbrUnion];  // (axis code y) * 5 + (axis code z)
+  __shared__ uint32_t s_ayz[kNbrUnion];  // the y and z axis codes' fields of the entry
   if (threadIdx.x < nu) {
     const int u = threadIdx.x;
     const int row = u / ux, col = u % ux;
@@ -1082,7 +1081,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
     s_sy[u] = shift_term(dy, ky, h, dL);
     s_sz[u] = shift_term(dz, kz, h, dL);
     s_ax[u] = kx;
-    s_ayz[u] = axis_shift_code(dy, ky) * 5 + axis_shift_code(dz, kz);
+    s_ayz[u] = entry_code(0, axis_shift_code(dy, ky), axis_shift_code(dz, kz));
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1129,8 +1128,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
       for (int row = 0; row < 9; ++row) {
         for (int dx = -1; dx <= 1; ++dx) {
           const int u = row * ux + a + 1 + dx;
-          const uint32_t code =
-              (uint32_t)(axis_shift_code(dx, s_ax[u]) * 25 + s_ayz[u]) << kCodeShift;
+          const uint32_t code = entry_code(axis_shift_code(dx, s_ax[u]), 0, 0) | s_ayz[u];
           const int k0 = s_off[u], k1 = s_off[u + 1];
           const float sx = s_sx[u], sy = s_sy[u], sz = s_sz[u];
           const int ns = s_ns[u];
@@ -1159,7 +1157,7 @@ __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
           overflow |= kStatusOverflow;
         } else {
           for (int k = count; k < ((count + kListPad - 1) & ~(kListPad - 1)); ++k)
-            __stcg(out + (size_t)k * 32, (uint32_t)i | (kPadCode << kCodeShift));
+            __stcg(out + (size_t)k * 32, (uint32_t)i | kPadBits);
         }
       }
     }
@@ -1334,21 +1332,17 @@ __device__ __forceinline__ void lj_pair2(PairAcc& a, float4 pi, float3 sha, floa
 }
 
 // Periodic shift vector of a list entry.  SH = 0: the entry's 3D vector from
-// the 125-entry table (one 16-byte shared load, whose lanes conflict across
-// banks).  SH = 1: the code's three axis codes (code = 25 ax + 5 ay + az)
-// and each axis value from the 5-value table (three 4-byte shared loads that
-// never conflict: the table spans 5 banks).  The same values either way.
+// the 125-entry table (index 25 ax + 5 ay + az; one 16-byte shared load,
+// whose lanes conflict across banks).  SH = 1: each axis value from the
+// 5-value table (three 4-byte shared loads that never conflict: the table
+// spans 5 banks).  The same values either way.
 template <int SH>
 __device__ __forceinline__ float3 entry_shift(uint32_t w, const float4* s_shift, const float* s_axis) {
-  const uint32_t c = w >> kCodeShift;
+  const int ax = entry_ax(w), ay = entry_ay(w), az = entry_az(w);
   if (SH == 0) {
-    const float4 v = s_shift[c];
+    const float4 v = s_shift[25 * ax + 5 * ay + az];
     return make_float3(v.x, v.y, v.z);
   }
-  const uint32_t ax = (c * 41u) >> 10;  // c / 25 for c < 125
-  const uint32_t rem = c - 25u * ax;
-  const uint32_t ay = (rem * 13u) >> 6;  // rem / 5 for rem < 25
-  const uint32_t az = rem - 5u * ay;
   return make_float3(s_axis[ax], s_axis[ay], s_axis[az]);
 }
 
@@ -1759,7 +1753,7 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
     const int nmax = __reduce_max_sync(0xffffffffu, nn);
     const uint32_t* tile_rows = (keeps ? d.pnbr : d.nbr) + (size_t)R.nbr_base + (size_t)(local >> 5) * R.M * 32;
     uint32_t* ring = s_ring + (threadIdx.x >> 5) * (PF * 4 * 32);
-    const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
+    const uint32_t pad = (uint32_t)local | kPadBits;
     if (nt == 1)
       lj_loop_ring<EV, KB, true, SH, P2, (RING ? PF : 2)>(tile_rows, ring, threadIdx.x & 31, nn, nmax, pad,
                                                           d.pos + base, pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2,
@@ -1785,7 +1779,7 @@ __device__ __forceinline__ void force_chunk(const Dev& d, int chunk, bool skip_r
       // the LJ sums are in already
     } else if (LISTED && keeps) {
       const float rcd = (float)(R.rc + (double)R.prune_delta);
-      const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
+      const uint32_t pad = (uint32_t)local | kPadBits;
       const int pc = nt == 1 ? lj_loop_filter<EV, B, PFR, KB, true, SH>(lst, nn, d.pnbr + row, rcd * rcd, pbase,
                                                                          pi, s_shift, s_axis, ti, nt, s_eps24, s_sig2,
                                                                          rc2, fx, fy, fz, acc, pad)
@@ -1933,7 +1927,7 @@ __device__ __forceinline__ void force_chunk_lanes(const Dev& d, int chunk, bool 
       const float rcd = (float)(R.rc + (double)R.prune_delta);
       const size_t row = (size_t)R.nbr_base + ((size_t)(local >> 5) * R.M) * 32 + (local & 31);
       const int nn = (d.ncnt[s] + kListPad - 1) & ~(kListPad - 1);
-      const uint32_t pad = (uint32_t)local | (kPadCode << kCodeShift);
+      const uint32_t pad = (uint32_t)local | kPadBits;
       d.pcnt[s] = filter_list<SH>(d.nbr + row, nn, d.pnbr + row, rcd * rcd, pbase, pi, s_shift, s_axis, pad);
       const float4 q = d.ref[s];
       d.ref[s] = make_float4(pi.x, pi.y, pi.z, q.w);
@@ -2104,7 +2098,7 @@ __global__ void __launch_bounds__(kChunk) k_prune(Dev d) {
       }
     }
     const int padded = (cnt + kPrunePad - 1) & ~(kPrunePad - 1);
-    for (int k = cnt; k < padded; ++k) out[(size_t)k * 32] = (uint32_t)local | (kPadCode << kCodeShift);
+    for (int k = cnt; k < padded; ++k) out[(size_t)k * 32] = (uint32_t)local | kPadBits;
     d.pcnt[s] = cnt;
     const float4 q = d.ref[s];
     d.ref[s] = make_float4(pi.x, pi.y, pi.z, q.w);
