@@ -289,8 +289,8 @@ static void fill_static(Rep& R, const RunConfig& cfg, const Topology& t) {
   R.thermo_freq = cfg.thermo_on ? cfg.thermo_freq : 0;
   R.stress_freq = cfg.stress_on ? cfg.stress_freq : 0;
   // pruned list at rc + kPruneDelta: walked by the force kernels between
-  // filters (not under NPT, nor with a skin no wider than the margin)
-  R.prune_delta = (cfg.ensemble != FMD_NPT_NH && cfg.skin > kPruneDelta) ? (float)kPruneDelta : 0.f;
+  // filters (not with a skin no wider than the margin)
+  R.prune_delta = cfg.skin > kPruneDelta ? (float)kPruneDelta : 0.f;
   R.ntables = (int32_t)cfg.tables.size();
   for (int k = 0; k < kMaxTypes * kMaxTypes; ++k) R.table_of[k] = -1;
   for (size_t k = 0; k < cfg.table_of.size() && k < (size_t)(kMaxTypes * kMaxTypes); ++k)
@@ -358,6 +358,8 @@ static void init_dynamic(Rep& R, double L, int G_alloc, double rcs) {
   R.L = L;
   R.L_list = L;
   R.list_scale = 1.0;
+  R.L_filter = L;
+  R.filter_scale = 1.0;
   R.Lpos = L;
   R.h = (float)(L / G);
   R.maxdisp_bits = 0;
@@ -671,6 +673,8 @@ void Batch::setup(const std::vector<int>& rs) {
     R.since = 0;
     R.L_list = R.L;
     R.list_scale = 1.0;
+    R.L_filter = R.L;
+    R.filter_scale = 1.0;
     R.maxdisp_bits = 0;
     R.disp_acc = 0.f;
     R.force_ev = 1;
@@ -997,17 +1001,19 @@ void Batch::list_stats(int64_t* entries, int32_t* max_per_atom) {
 }
 
 // Turn a replica's pruned list on (margin delta beyond rc) or off (delta <=
-// 0).  Turning it on filters the list at once; under NPT it stays off.
+// 0).  Turning it on filters the list at once.
 void Batch::set_list_prune(int r, double delta) {
   download_reps();
   Rep& R = h_reps_[r];
-  const bool on = delta > 0.0 && R.ensemble != FMD_NPT_NH;
+  const bool on = delta > 0.0;
   R.prune_delta = on ? (float)delta : 0.f;
   if (on) {
     // a filter now: the displacement since the last reference joins the
     // accumulated bound and the current positions become the reference
     R.disp_acc += std::sqrt(uint_as_float_host(R.maxdisp_bits));
     R.maxdisp_bits = 0;
+    R.L_filter = R.L;
+    R.filter_scale = 1.0;
     R.rebuild_now = 2;
     upload_reps();
     write_rebuild_list(std::vector<int>{r}, 0);
@@ -1212,7 +1218,7 @@ void Batch::restore(int r, const Topology& t, const StateFile& s) {
   if (s.has("rebuilds")) R.rebuilds = (int64_t)s.get1("rebuilds");
   if (s.has("list_buffer")) R.skin = s.get1("list_buffer");
   if (s.has("rebuild_cadence")) R.max_between = (int32_t)s.get1("rebuild_cadence");
-  if (s.has("prune_delta")) R.prune_delta = R.ensemble == FMD_NPT_NH ? 0.f : (float)s.get1("prune_delta");
+  if (s.has("prune_delta")) R.prune_delta = (float)s.get1("prune_delta");
   get_nh(s, R.nh);
   // the cell grid of the box, as a fresh replica derives it
   int G = (int)std::floor(R.L / ((R.rc + R.skin) * 1.0001));

@@ -140,6 +140,8 @@ struct Rep {
   double Lpos;   // box the stored positions are wrapped in (last pre-force)
   double L_list; // box the neighbor list was built in (box-shrink term of the rebuild trigger)
   double list_scale;  // product of the NPT position scale factors since the list was built
+  double L_filter;    // box, and product of the position scale factors, since the pruned
+  double filter_scale;  // list was last filtered (its own box-shrink term)
   float h;
   uint32_t maxdisp_bits;
   // Pruned list: the pairs of the rc + skin list within rc + prune_delta,
@@ -148,9 +150,10 @@ struct Rep {
   // then holds the positions of the last filter (or rebuild), and disp_acc
   // the sum of the largest displacements of the filters since the rebuild,
   // so that largest displacement since the last filter + disp_acc bounds
-  // every displacement since the rebuild (the full list's trigger).
-  // prune_delta = 0: no pruned list (also under NPT, whose co-scaled frame
-  // can stretch past displacements).
+  // every displacement since the rebuild (the full list's trigger).  Under
+  // NPT the filter's trigger takes the contraction since the filter into
+  // account as the rebuild's does (L_filter, filter_scale).
+  // prune_delta = 0: no pruned list.
   float prune_delta;
   float disp_acc;
   int32_t status;

@@ -337,24 +337,32 @@ __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& con
   // constant box, the trigger of skin_trigger.cuh:6-33).  Pairs inside the
   // box scale with the positions' factors, pairs across a face with the box:
   // s is the smaller of the two.
-  if (S.ens == FMD_NPT_NH) R.list_scale *= (double)S.ev;
+  if (S.ens == FMD_NPT_NH) {
+    R.list_scale *= (double)S.ev;
+    R.filter_scale *= (double)S.ev;
+  }
   const float maxd2 = __uint_as_float(R.maxdisp_bits);
   const double s = fmin(R.L / R.L_list, R.list_scale);
   const float hs = (float)(s < 1.0 ? 0.5 * (s * (R.rc + R.skin) - R.rc) : 0.5 * R.skin);
   const bool trig = hs <= 0.f || maxd2 > hs * hs;
-  // With a pruned list (pairs within rc + prune_delta, no NPT), maxd2 is the
+  // With a pruned list (pairs within rc + prune_delta), maxd2 is the
   // displacement since the last filter and disp_acc adds those of the earlier
   // filters: the full list's bound is their sum; the pruned list holds while
-  // the displacement since its filter stays below prune_delta / 2.  A
-  // rebuild filters its new list too.
+  // the displacement since its filter stays below (sp (rc + prune_delta) -
+  // rc) / 2, sp the contraction since the filter (prune_delta / 2 at
+  // constant box).  A rebuild filters its new list too.
   bool rtrig = trig;
   const float dmax = sqrtf(maxd2);
   if (R.disp_acc > 0.f) rtrig = hs <= 0.f || dmax + R.disp_acc > hs;
-  const bool ptrig = R.prune_delta > 0.f && dmax > 0.5f * R.prune_delta;
+  const double sp = fmin(R.L / R.L_filter, R.filter_scale);
+  const float hp = (float)(sp < 1.0 ? 0.5 * (sp * (R.rc + (double)R.prune_delta) - R.rc) : 0.5 * R.prune_delta);
+  const bool ptrig = R.prune_delta > 0.f && (hp <= 0.f || dmax > hp);
   if (rtrig || R.since >= R.max_between) {
     R.since = 0;
     R.L_list = R.L;
     R.list_scale = 1.0;
+    R.L_filter = R.L;
+    R.filter_scale = 1.0;
     R.maxdisp_bits = 0u;
     R.disp_acc = 0.f;
     R.rebuilds += 1;
@@ -364,6 +372,8 @@ __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& con
   } else if (ptrig) {
     R.disp_acc += dmax;
     R.maxdisp_bits = 0u;
+    R.L_filter = R.L;
+    R.filter_scale = 1.0;
     R.rebuild_now = 2;
     d.rb[kRbHead + atomicAdd(d.rb + kRbCount, 1)] = r;
   } else {
