@@ -334,12 +334,13 @@ FMD_API fmd_status fmd_batch_kernels_per_step(fmd_batch* b, int32_t* n);
 FMD_API fmd_status fmd_batch_launch_counts(fmd_batch* b, int64_t* counts, int32_t n);
 /* Pruned pair list of a replica: the pairs of the rc + skin Verlet list
  * within rc + delta, re-filtered whenever a displacement since the last
- * filter exceeds delta / 2, are what the force kernels walk (fewer entries
- * than the full list; a rebuild then waits for the displacement since the
- * rebuild, bounded by the filters' displacements, to reach skin / 2).  On by
- * default with delta = 0.12 in the mixed form when the skin is wider, except
- * under NPT; delta <= 0 turns it off.  A refinement of the reference's single list
- * (neighbor/verlet_list.cu), same forces up to summation order. */
+ * filter exceeds delta / 2 (under NPT, (s (rc + delta) - rc) / 2 with s the
+ * contraction since the filter), are what the force kernels walk (fewer
+ * entries than the full list; a rebuild then waits for the displacement
+ * since the rebuild, bounded by the filters' displacements, to reach
+ * skin / 2).  On by default with delta = 0.12 in the mixed form when the
+ * skin is wider; delta <= 0 turns it off.  A refinement of the reference's
+ * single list (neighbor/verlet_list.cu), same forces up to summation order. */
 FMD_API fmd_status fmd_batch_set_list_prune(fmd_batch* b, int32_t slot, double delta);
 /* List buffer of a replica: the Verlet list holds the pairs within rc + skin
  * and is rebuilt after a displacement of skin / 2 (neighbor/verlet_list.cu,
