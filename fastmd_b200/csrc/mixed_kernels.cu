@@ -2720,7 +2720,7 @@ constexpr int kForceCarveoutPct = 16;  // percent of the SM's shared-memory maxi
 // FP32x2 arithmetic, lanes per atom.
 template <bool EV>
 void force_kernels(int variant, void (**per_chunk)(Dev, int), void (**listed)(Dev)) {
-  constexpr int E = 5;  // blocks per SM of the energy flavours (more registers)
+  constexpr int E = 6;  // blocks per SM of the energy flavours (more registers: up to 85)
 #define FMD_FORCE_VARIANT(B, MINB, PF, KB, SH, P2, LPA)          \
   *per_chunk = k_force<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>; \
   *listed = k_force_rb<EV, B, EV ? E : MINB, PF, KB, SH, P2, LPA>;
