@@ -30,7 +30,9 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CLI = os.path.join(ROOT, "fastmd_b200", "bin", "fastmd")
-ENSEMBLES = ["nvt_langevin 1.0 1.2 1.0 9", "nvt_nh 1.0 1.0 0.5 3", "npt_nh 1.0 1.0 0.5 0.5 0.5 1.0 3"]
+ENSEMBLES = ["nvt_langevin 1.0 1.2 1.0 9", "nvt_nh 1.0 1.0 0.5 3", "npt_nh 1.0 1.0 0.5 0.5 0.5 1.0 3",
+             # the carried chain accelerations come back from the sidecar too
+             "npt_nh 1.0 1.0 0.1 0.5 0.5 1.0 3\nnh_chain_carry 1"]
 
 
 def _pushed(nchains=20, length=50, seed=11):
