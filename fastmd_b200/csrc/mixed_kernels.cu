@@ -1270,8 +1270,20 @@ __device__ __forceinline__ float pair_r2(float4 pi, float3 sh, float4 pj, float&
 // included) give an exact zero.  The reference also skips r^2 <= 1e-10
 // (coincident atoms); here such a pair's F/r clamps to +-1000 times a
 // separation below 1e-5, and only its energy is left out.
+// 1 / r^2 of a pair: the approximate reciprocal instruction alone (r^2 is
+// never subnormal: a listed pair's r^2 lies between the overlap clamp and
+// (rc + skin)^2, a padding entry's near 3 (h + dL)^2; r^2 = 0 gives +inf,
+// which the force clamp turns into +-1000 as before).  The force launch at
+// 64 x 30K is 2-4 % faster than with the fast-divide intrinsic, whose range
+// scaling the pair loop never needs.
+__device__ __forceinline__ float recip_r2(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ float lj_fr(float r2, float rc2, float e24, float sig2, float& inv, float& sr6) {
-  inv = __fdividef(1.0f, r2);
+  inv = recip_r2(r2);
   const float sr2 = __fmul_rn(sig2, inv);
   sr6 = __fmul_rn(__fmul_rn(sr2, sr2), sr2);
   const float t = __fmaf_rn(sr6, 2.0f, -1.0f);
@@ -1326,7 +1338,7 @@ __device__ __forceinline__ void lj_pair2(PairAcc& a, float4 pi, float3 sha, floa
   const float dzb = __fsub_rn(__fsub_rn(pi.z, pjb.z), shb.z);
   const float2 ma = __fmul2_rn(dxya, dxya), mb = __fmul2_rn(dxyb, dxyb);
   const float2 r2 = make_float2(__fmaf_rn(dza, dza, __fadd_rn(ma.x, ma.y)), __fmaf_rn(dzb, dzb, __fadd_rn(mb.x, mb.y)));
-  const float2 inv = make_float2(__fdividef(1.0f, r2.x), __fdividef(1.0f, r2.y));
+  const float2 inv = make_float2(recip_r2(r2.x), recip_r2(r2.y));
   const float2 sr2 = __fmul2_rn(make_float2(sig2, sig2), inv);
   const float2 sr6 = __fmul2_rn(__fmul2_rn(sr2, sr2), sr2);
   const float2 t = __ffma2_rn(sr6, make_float2(2.0f, 2.0f), make_float2(-1.0f, -1.0f));
