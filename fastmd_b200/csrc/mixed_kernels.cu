@@ -49,7 +49,11 @@ __device__ __forceinline__ double ramp(const Rep& R, int64_t step, double a, dou
   return a + (b - a) * frac;
 }
 
-__device__ __noinline__ void compute_step_scalars(const Rep& R, StepScalars& S) {
+// Scalars of the step after R.step.  The single-thread commit kernels inline
+// this into a local and store the result once (next_scalars): through a
+// reference that may point into R (R.next), every store would order the
+// later reads of R behind it, one dependent memory round trip per field.
+__device__ __forceinline__ void step_scalars(const Rep& R, StepScalars& S) {
   S.adv = R.active && R.step < R.stop_step;
   S.step = R.step + 1;
   S.ens = (R.mode == kModePushoff) ? FMD_LANGEVIN : R.ensemble;
@@ -95,6 +99,17 @@ __device__ __noinline__ void compute_step_scalars(const Rep& R, StepScalars& S) 
     // up w * (L_new - L_old * ev) per period w it lies outside.
     S.dW = (float)(S.nh.L - R.Lpos * S.nh.exp_vW);
   }
+}
+
+// The pre-force kernel's rare fallback (a stale copy after a host upload):
+// an out-of-line call, so the kernel's hot path keeps its registers.
+__device__ __noinline__ void compute_step_scalars(const Rep& R, StepScalars& S) { step_scalars(R, S); }
+
+// R.next from R, built in a local and stored once.
+__device__ __forceinline__ void next_scalars(Rep& R) {
+  StepScalars nx;
+  step_scalars(R, nx);
+  R.next = nx;
 }
 
 // Three standard normals from the same Philox words as rng_normal3 (seed,
@@ -318,7 +333,7 @@ __global__ void __launch_bounds__(32) k_commit(Dev d, StepConds cond) {
 __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& cond) {
   StepScalars S;
   if (R.next_valid) S = R.next;
-  else compute_step_scalars(R, S);
+  else step_scalars(R, S);
   R.next_valid = 0;
   R.step = S.step;
   R.nh = S.nh;
@@ -394,7 +409,7 @@ __device__ void commit_replica(const Dev& d, Rep& R, int r, const StepConds& con
   if (!post) {
     // a skipped post-force computes no scalars for the next step: do it here
     // (a Langevin post changes none of their inputs)
-    compute_step_scalars(R, R.next);
+    next_scalars(R);
     R.next_valid = 1;
   }
 }
@@ -407,7 +422,7 @@ __global__ void __launch_bounds__(32) k_prepare(Dev d) {
   if (threadIdx.x != 0 || r >= d.rb_cap) return;
   Rep& R = d.reps[r];
   if (!R.active || R.next_valid) return;
-  compute_step_scalars(R, R.next);
+  next_scalars(R);
   R.next_valid = 1;
 }
 
@@ -2351,35 +2366,40 @@ __global__ void __launch_bounds__(32) k_post_commit(Dev d, int kick) {
       const int ens = (R.mode == kModePushoff) ? FMD_LANGEVIN : R.ensemble;
       if (need_ev(R)) R.ev_step = R.step;
       R.force_ev = 0;
+      // the chain / barostat state is updated in a local copy and stored
+      // once: in place, its arrays' stores would order every later read of
+      // the record behind them
+      NHScalars nh = R.nh;
       if (kick == 2) {
         // re-evaluation of the current state: reductions only
       } else if (!kick) {
         // Setup: the chain carry starts at the current KE (main.cu:376-390).
-        R.nh.carry = 0.5 * ke_raw;
+        nh.carry = 0.5 * ke_raw;
         R.pending_scale = 1.0;
       } else if (ens == FMD_NVT_NH) {
         const double kT = ramp(R, R.step, R.T0, R.T1);
         const double ke = 0.5 * ke_raw;
-        const double sc = nhc_half_step(R.nh.xi, R.nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, ke, 0.5 * dt,
-                                        R.nh.carry_dd ? R.nh.dd : nullptr);
-        R.nh.scale = sc;
-        R.nh.carry = ke * sc * sc;
+        const double sc = nhc_half_step(nh.xi, nh.vxi, R.chain_M, R.Q1, R.Qr, kT, R.natoms, ke, 0.5 * dt,
+                                        nh.carry_dd ? nh.dd : nullptr);
+        nh.scale = sc;
+        nh.carry = ke * sc * sc;
         R.pending_scale = sc;
       } else if (ens == FMD_NPT_NH) {
         const double kT = ramp(R, R.step, R.T0, R.T1), Pt = ramp(R, R.step, R.P0, R.P1);
         const double vtr = R.vir[0] + R.vir[3] + R.vir[5];
-        npt_chain_baro(R.nh, false, ke_raw, vtr, R.chain_M, R.Q1, R.Qr, R.W, 0.5 * dt, dt, R.V0, R.natoms, kT, Pt,
+        npt_chain_baro(nh, false, ke_raw, vtr, R.chain_M, R.Q1, R.Qr, R.W, 0.5 * dt, dt, R.V0, R.natoms, kT, Pt,
                        DExp(), DCbrt(), DSinh());
-        R.L = R.nh.L;
-        R.pending_scale = R.nh.bscale * R.nh.scale;
+        R.L = nh.L;
+        R.pending_scale = nh.bscale * nh.scale;
       } else {
         R.pending_scale = 1.0;
       }
+      R.nh = nh;
       R.thermo_step = R.step;
       R.adv = 0;
       R.rebuild_now = 0;
       // scalars of the next pre-force, computed once here for all its blocks
-      compute_step_scalars(R, R.next);
+      next_scalars(R);
       R.next_valid = 1;
     }
     // Stress steps: the thermo row's pressure tensor, (KE tensor (with the
