@@ -115,15 +115,17 @@ __device__ __forceinline__ void next_scalars(Rep& R) {
 // Three standard normals from the same Philox words as rng_normal3 (seed,
 // stream, step, atom id), transformed in FP32: Box-Muller with u1 = (a + 1)
 // 2^-32 and the angle split into quadrant (top two bits of b) and a quarter
-// turn fraction, evaluated with the CUDA math library's logf / sincospif.
-// Agrees with the FP64 transform to FP32 rounding (the mixed form casts the
-// deviates to FP32 in any case).
+// turn fraction, evaluated with the hardware-approximate __logf / __sincosf
+// (absolute errors near 2^-21 on these ranges; the accurate logf / sincospif
+// made the pre-force kernel 5 % slower).  Agrees with the FP64 transform to
+// within those errors; the radius is clamped at zero, since near u1 = 1 the
+// approximate logarithm's absolute error can exceed -ln u1 itself.
 __device__ __forceinline__ void normal_pair_f32(uint32_t a, uint32_t b, float& z0, float& z1) {
   const float u1 = ((float)a + 1.0f) * 0x1.0p-32f;
-  const float r = sqrtf(-2.0f * logf(u1));
   const float f = (float)(b & 0x3FFFFFFFu) * 0x1.0p-30f;
   float s, c;
-  sincospif(0.5f * f, &s, &c);
+  const float r = sqrtf(fmaxf(-2.0f * __logf(u1), 0.0f));
+  __sincosf(1.5707963267948966f * f, &s, &c);
   const uint32_t q = b >> 30;
   const float cs = q == 0 ? c : (q == 1 ? -s : (q == 2 ? -c : s));
   const float sn = q == 0 ? s : (q == 1 ? c : (q == 2 ? -s : -c));
