@@ -480,6 +480,8 @@ def wl_c2(args, fm):
         row = b.thermo(s)
         e.append(row.conserved)
         L.append(row.box_L)
+    if args.timeline:
+        kernel_timeline(b, args.timeline_steps, args.timeline)
     e = np.array(e)
     steps = np.arange(1, len(e) + 1) * 1000.0
     slope = float(np.polyfit(steps, e, 1)[0]) if len(e) > 1 else 0.0

@@ -226,6 +226,7 @@ Dev Batch::dev() const {
   d.bnd = bnd_;
   d.ang = ang_;
   d.part = part_;
+  d.part_stride = caps_.slots / kChunk;
   d.kcount = kcount_;
   d.acf = acf_;
   d.tab = tab_.p;

@@ -233,7 +233,8 @@ struct Dev {
   int32_t* ncnt;
   uint32_t* pnbr;                // pruned list (same layout and bases as nbr)
   int32_t* pcnt;
-  double* part;                  // [chunks][kNumPartials]
+  double* part;                  // [kNumPartials][part_stride]: value q of chunk c at q * part_stride + c
+  int64_t part_stride;           // chunks allocated
   double* acf;                   // [replica][kAcfWords] stress autocorrelator state
   const float2* tab;             // pair-table points (force, energy) of every replica's tables
   unsigned long long* kcount;    // [kKernelKinds] launches executed (block 0 of each launch counts)
