@@ -702,6 +702,7 @@ void Batch::check_status(int r, bool throw_on_fault) {
   if (R.status & kStatusCellCapacity) throw Error(FMD_ERR_OVERFLOW, "cell grid capacity exceeded");
   if (R.status & kStatusNonFinite) throw Error(FMD_ERR_FAULT, "non-finite state");
   if (R.status & kStatusFeneStretch) throw Error(FMD_ERR_FAULT, "FENE bond stretched to R0");
+  if (R.status & kStatusStaleScalars) throw Error(FMD_ERR_FAULT, "pre-force step without its step scalars");
   throw Error(FMD_ERR_FAULT, "replica fault");
 }
 

@@ -25,6 +25,7 @@ enum : int32_t {
   kStatusFeneStretch = 4,  // a FENE bond reached R0 (the reference clamps silently)
   kStatusCellCapacity = 8, // cell grid / cell occupancy capacity exceeded
   kStatusTimeout = 16,     // a bounded device wait expired
+  kStatusStaleScalars = 32,  // a pre-force found no precomputed step scalars
 };
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }

@@ -101,10 +101,6 @@ __device__ __forceinline__ void step_scalars(const Rep& R, StepScalars& S) {
   }
 }
 
-// The pre-force kernel's rare fallback (a stale copy after a host upload):
-// an out-of-line call, so the kernel's hot path keeps its registers.
-__device__ __noinline__ void compute_step_scalars(const Rep& R, StepScalars& S) { step_scalars(R, S); }
-
 // R.next from R, built in a local and stored once.
 __device__ __forceinline__ void next_scalars(Rep& R) {
   StepScalars nx;
@@ -274,13 +270,19 @@ __global__ void __launch_bounds__(kChunk / APT, APT == 1 ? 6 : 12) k_pre(Dev d, 
   __shared__ uint32_t wmax[T / 32];
   if (!(R.active && R.step < R.stop_step)) return;
   const bool deferred = R.defer != 0;
-  if (R.next_valid) {
+  // Every host upload is followed by k_prepare and every commit leaves
+  // R.next valid, so a stale copy here is a fault, raised rather than
+  // computed: an out-of-line call to compute it cost this kernel 18
+  // registers, a stack frame and 4 blocks per SM.
+  if (!R.next_valid) {
+    if (threadIdx.x == 0) atomicOr(&R.status, kStatusStaleScalars);
+    return;
+  }
+  {
     constexpr int nw = (int)(sizeof(StepScalars) / sizeof(uint32_t));
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&R.next);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&S);
     for (int k = threadIdx.x; k < nw; k += T) dst[k] = src[k];
-  } else if (threadIdx.x == 0) {
-    compute_step_scalars(R, S);
   }
   __syncthreads();
   uint32_t d2bits = 0;
