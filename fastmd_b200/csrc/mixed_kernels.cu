@@ -527,7 +527,7 @@ __global__ void __launch_bounds__(kPlanThreads) k_rbplan_home(Dev d, int variant
   const int n = rb_count(d);
   rb_scan(d, n, rb_off(d, 2), [&](int r) {
     const int G = d.reps[r].G;
-    if (d.reps[r].rebuild_now != 1) return 0;
+    if (d.reps[r].rebuild_now != 1 || G < 3) return 0;  // small boxes: k_neighbors_small
     return variant == 1 ? nbr_items(G) : G * G * G;
   });
 }
@@ -941,13 +941,7 @@ constexpr int kNbrGroup = 64;     // home atoms per pass
 __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
   const int G = R.G;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (G < 3) {
-    if (warp == 0) {
-      const int ov = neighbors_small_box(d, R, lc, lane);
-      if (ov) atomicOr(&R.status, ov);
-    }
-    return;
-  }
+  if (G < 3) return;  // boxes under three cells per axis: k_neighbors_small
   const int M = R.M;
   const int base = R.slot_base;
   const int cell_base = R.cell_base;
@@ -1125,13 +1119,7 @@ __device__ void neighbors_cell_ballot(const Dev& d, Rep& R, int lc) {
 __device__ void neighbors_row(const Dev& d, Rep& R, int item) {
   const int G = R.G;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (G < 3) {
-    if (warp == 0) {
-      const int ov = neighbors_small_box(d, R, item, lane);
-      if (ov) atomicOr(&R.status, ov);
-    }
-    return;
-  }
+  if (G < 3) return;  // boxes under three cells per axis: k_neighbors_small
   const int nrow = (G + kNbrRow - 1) / kNbrRow;
   const int bx = item % nrow, hy = (item / nrow) % G, hz = item / (nrow * G);
   const int hx0 = bx * kNbrRow;
@@ -1272,6 +1260,22 @@ __global__ void __launch_bounds__(kNbrThreads, MINB) k_neighbors(Dev d) {
     else
       neighbors_row(d, d.reps[rb_rep(d, cur.i)], item - cur.lo);
   }
+}
+
+// Lists of the rebuilding replicas whose box holds fewer than three cells
+// per axis (L < 3 (rc + skin), a few hundred beads): one warp per work-list
+// replica walks its G^3 home cells with the de-duplicated small-box form.
+// The ballot and row kernels skip those replicas, which keeps the small
+// form's dynamically indexed cell list (a stack frame) out of their
+// registers: 72 instead of 80 at 6 blocks per SM, and no spill at 8.
+__global__ void __launch_bounds__(32) k_neighbors_small(Dev d) {
+  if ((int)blockIdx.x >= rb_count(d)) return;
+  Rep& R = d.reps[rb_rep(d, blockIdx.x)];
+  const int G = R.G;
+  if (R.rebuild_now != 1 || G >= 3) return;
+  int ov = 0;
+  for (int lc = 0; lc < G * G * G; ++lc) ov |= neighbors_small_box(d, R, lc, threadIdx.x);
+  if (ov) atomicOr(&R.status, ov);
 }
 
 // ---------------------------------------------------------------- forces
@@ -2793,6 +2797,7 @@ void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st, b
   launch_hi(k_permute_g, g.nchunks, kChunk, st, d);
   launch_hi(k_topo_g, g.nchunks, kChunk, st, d);
   launch_hi(k_neighbors_g, dim3(g.max_home, nr), kNbrThreads, st, d);
+  launch_hi(k_neighbors_small, nr, 32, st, d);
   if (filter) launch_prune(d, st);
 }
 
@@ -2816,6 +2821,7 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st, b
     launch_hi(k_neighbors<0, 6>, g_nbr2, kNbrThreads, st, d);
   else
     launch_hi(k_neighbors<0, 8>, g_nbr0, kNbrThreads, st, d);
+  launch_hi(k_neighbors_small, nreps, 32, st, d);
   if (filter) launch_prune(d, st);
 }
 
