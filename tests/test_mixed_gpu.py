@@ -151,6 +151,35 @@ def test_trigger_only_rebuilds_keep_list_complete(ens):
     b.close()
 
 
+@pytest.mark.parametrize("nchains,length", [(6, 20), (10, 30)])
+def test_small_box_lists_over_rebuilds(nchains, length):
+    """Boxes under three cells per axis (G = 1 at 120 beads, G = 2 at 300)
+    get their lists from the small-box list kernel: rebuilt on every step
+    (direct launches and graph steps) beside a larger replica that takes the
+    ballot kernel, their forces stay the oracle's."""
+    pre = fm.Simulation(run_conf(), gen=dict(nchains=nchains, chain_length=length, density=0.85, seed=11,
+                                             pushoff_steps=2000), form=fm.FMD_FORM_MIXED)
+    x0, v0, i0 = pre.state()
+    d = _melt(nchains, length, seed=11)
+    d.xyz, d.vel, d.image = x0, v0, i0
+    b = fm.Batch(max_replicas=2, max_atoms=1 << 14)
+    s = b.add(run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 9", nsteps=400), desc=d)
+    b.add(run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 10", nsteps=400),
+          gen=dict(nchains=20, chain_length=50, density=0.85, seed=6, pushoff_steps=300))
+    b.set_rebuild_cadence(s, 1)
+    assert d.box_L < 3 * 2.8
+    r0 = b.info(s).rebuilds
+    for n in (25, 25, 50, 50):  # direct launches, then the step graph
+        b.run(n)
+        f, _, _ = b.forces(s)
+        x, Lf = b.force_frame(s)
+        fo, _, _ = po.forces(oracle_system(d, xyz=x, L=Lf))
+        assert rel_rms(f, fo) < FORCE_RMS_TOL, (nchains, rel_rms(f, fo))
+        assert b.info(s).status_word == 0
+    assert b.info(s).rebuilds - r0 >= 150
+    b.close()
+
+
 def test_pushoff_then_langevin_is_stable():
     conf = run_conf(ensemble="nvt_langevin 1.0 1.0 1.0 42", nsteps=2000)
     sim = fm.Simulation(conf, gen=dict(nchains=30, chain_length=100, density=0.85, seed=42, pushoff_steps=2000),
