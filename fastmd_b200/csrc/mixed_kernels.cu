@@ -835,7 +835,7 @@ __global__ void __launch_bounds__(kChunk) k_topo(Dev d) {
 // skin)): one warp per home cell, the distinct neighbor cells de-duplicated,
 // each pair's periodic shift derived from the two cells and offsets.
 // Candidates are broadcast 32 at a time with shuffles.
-__device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
+__device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane, int first = 0, int stride = 32) {
   const int G = R.G;
   const float h = R.h, inv_h = 1.0f / h;
   const float dL = (float)(R.L - (double)G * (double)h);
@@ -849,7 +849,7 @@ __device__ int neighbors_small_box(const Dev& d, Rep& R, int lc, int lane) {
     const uint32_t hkey = cell_key(hx, hy, hz);
     const int hs = d.cell_start[R.cell_base + hkey];
     const int he = d.cell_fill[R.cell_base + hkey];
-    for (int hb = hs; hb < he; hb += 32) {
+    for (int hb = hs + first; hb < he; hb += stride) {
       const int il = hb + lane;
       const bool act = il < he;
       float4 pi = make_float4(0, 0, 0, 0);
@@ -1266,18 +1266,25 @@ __global__ void __launch_bounds__(kNbrThreads, MINB) k_neighbors(Dev d) {
 }
 
 // Lists of the rebuilding replicas whose box holds fewer than three cells
-// per axis (L < 3 (rc + skin), a few hundred beads): one warp per work-list
-// replica walks its G^3 home cells with the de-duplicated small-box form.
-// The ballot and row kernels skip those replicas, which keeps the small
-// form's dynamically indexed cell list (a stack frame) out of their
-// registers: 72 instead of 80 at 6 blocks per SM, and no spill at 8.
-__global__ void __launch_bounds__(32) k_neighbors_small(Dev d) {
-  if ((int)blockIdx.x >= rb_count(d)) return;
-  Rep& R = d.reps[rb_rep(d, blockIdx.x)];
+// per axis (L < 3 (rc + skin), a few hundred beads): one block per (home
+// cell, work-list replica) -- G <= 2, so at most 8 cells -- its warps taking
+// the cell's home atoms 32 at a time in turn with the de-duplicated small-box
+// form (each list is its lane's own: the split changes no entry).  The ballot
+// and row kernels skip those replicas, which keeps the small form's
+// dynamically indexed cell list (a stack frame) out of their registers: 72
+// instead of 80 at 6 blocks per SM, and no spill at 8.  (One warp walking a
+// replica's 8 cells in turn made a 500-bead replica's rebuild the long pole
+// of the step: 256 uneven replicas fell from 3.0e9 to 1.8e9 atom-steps/s.)
+constexpr int kSmallWarps = 4;
+
+__global__ void __launch_bounds__(32 * kSmallWarps) k_neighbors_small(Dev d) {
+  if ((int)blockIdx.y >= rb_count(d)) return;
+  Rep& R = d.reps[rb_rep(d, blockIdx.y)];
   const int G = R.G;
   if (R.rebuild_now != 1 || G >= 3) return;
-  int ov = 0;
-  for (int lc = 0; lc < G * G * G; ++lc) ov |= neighbors_small_box(d, R, lc, threadIdx.x);
+  const int lc = blockIdx.x;
+  if (lc >= G * G * G) return;
+  const int ov = neighbors_small_box(d, R, lc, threadIdx.x & 31, 32 * (threadIdx.x >> 5), 32 * kSmallWarps);
   if (ov) atomicOr(&R.status, ov);
 }
 
@@ -2800,7 +2807,7 @@ void launch_rebuild_full(const Dev& d, const RebuildShape& g, cudaStream_t st, b
   launch_hi(k_permute_g, g.nchunks, kChunk, st, d);
   launch_hi(k_topo_g, g.nchunks, kChunk, st, d);
   launch_hi(k_neighbors_g, dim3(g.max_home, nr), kNbrThreads, st, d);
-  launch_hi(k_neighbors_small, nr, 32, st, d);
+  launch_hi(k_neighbors_small, dim3(8, nr), 32 * kSmallWarps, st, d);
   if (filter) launch_prune(d, st);
 }
 
@@ -2824,7 +2831,7 @@ void launch_rebuild(const Dev& d, int nreps, int nbr_variant, cudaStream_t st, b
     launch_hi(k_neighbors<0, 6>, g_nbr2, kNbrThreads, st, d);
   else
     launch_hi(k_neighbors<0, 8>, g_nbr0, kNbrThreads, st, d);
-  launch_hi(k_neighbors_small, nreps, 32, st, d);
+  launch_hi(k_neighbors_small, dim3(8, nreps), 32 * kSmallWarps, st, d);
   if (filter) launch_prune(d, st);
 }
 
